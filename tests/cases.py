@@ -1,0 +1,98 @@
+"""
+Test-side description of the golden cases (tests/golden/*.npz): turns a
+fixture's recorded setup name and parameters into an oracle configuration,
+with the physics each reference setup would hand to the solver
+(sailfish/setups/circumbinary_disk.py, binary_bondi.py, simple2d.py).
+"""
+
+import glob
+import json
+import math
+import os
+
+import numpy as np
+
+from oracle import host as oh
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    data = {k: z[k] for k in z.files}
+    data["meta"] = json.loads(str(data["meta"]))
+    return data
+
+
+CBD_DEFAULTS = dict(domain_radius=12.0, mach_number=10.0, eccentricity=0.0, mass_ratio=1.0, sink_rate=10.0,
+                    sink_radius=0.05, softening_length=0.05, buffer_is_enabled=True, sink_model="torque_free",
+                    nu=0.001, initial_sigma=1.0)
+KITP_DEFAULTS = dict(mach_number=10.0, eccentricity=0.0, mass_ratio=1.0, sink_radius=0.05, softening_length=0.05,
+                     nu=0.001, sink_model="acceleration_free", domain_radius=8.0, sink_rate=10.0,
+                     buffer_is_enabled=True)
+BONDI_DEFAULTS = dict(aspect=1, height=1.0, x_bin=0.0, sound_speed=1.0, wind_vel=1.0, bh_sep=0.25, bh_mass=1.0,
+                      sink_radius=0.05, sink_model="acceleration_free", sink_rate=1e2, mass_ratio=1.0,
+                      eccentricity=0.0, softening_length=0.05)
+
+
+def kitp_sigma(r):
+    """KitpCodeComparison.primitive surface density (circumbinary_disk.py:242-263)."""
+    return 1.0 * (1e-5 + (1 - 1e-5) * math.exp(-((2.5 / r) ** 12)))
+
+
+def oracle_config(meta):
+    """Oracle configuration for one golden case."""
+    x0, y0, x1, y1, ni, nj = meta["mesh"]
+    common = dict(x0=x0, x1=x1, y0=y0, y1=y1, ni=int(ni), nj=int(nj), rk_order=meta["rk"],
+                  plm_theta=meta["theta"])
+    setup = meta["setup"]
+    if setup == "circumbinary-disk":
+        p = dict(CBD_DEFAULTS, **meta["params"])
+        return oh.Config(
+            **common, eos_type=2, mach_number=p["mach_number"], nu=p["nu"],
+            buffer_is_enabled=p["buffer_is_enabled"], buffer_driving_rate=100.0, buffer_onset_width=1.0,
+            buffer_surface_density=p["initial_sigma"],
+            masses=oh.binary_masses(1.0, 1.0, p["mass_ratio"], p["eccentricity"], p["softening_length"],
+                                    p["sink_model"], p["sink_rate"], p["sink_radius"]))
+    if setup == "kitp-code-comparison":
+        p = dict(KITP_DEFAULTS, **meta["params"])
+        return oh.Config(
+            **common, eos_type=2, mach_number=p["mach_number"], nu=p["nu"],
+            buffer_is_enabled=p["buffer_is_enabled"], buffer_driving_rate=100.0, buffer_onset_width=1.0,
+            buffer_surface_density=kitp_sigma(math.sqrt((x1 - 1.0) ** 2 + 0.0)),
+            masses=oh.binary_masses(1.0, 1.0, p["mass_ratio"], p["eccentricity"], p["softening_length"],
+                                    p["sink_model"], p["sink_rate"], p["sink_radius"]))
+    if setup == "binary-bondi":
+        p = dict(BONDI_DEFAULTS, **meta["params"])
+        return oh.Config(
+            **common, eos_type=1, sound_speed=p["sound_speed"], nu=0.0, reference_time_scale=1.0,
+            masses=oh.binary_masses(p["bh_sep"], p["bh_mass"] * (1 + p["mass_ratio"]), p["mass_ratio"],
+                                    p["eccentricity"], p["softening_length"], p["sink_model"], p["sink_rate"],
+                                    p["sink_radius"], x_offset=p["x_bin"]))
+    if setup == "cylindrical-explosion":
+        return oh.Config(**common, eos_type=1, sound_speed=1.0, nu=0.0, reference_time_scale=1.0)
+    raise ValueError(setup)
+
+
+def initial_state(data):
+    """The fixture's starting primitive state: setup data plus the seeded noise."""
+    meta = data["meta"]
+    prim = np.array(data["ic"], dtype=np.float64)
+    if meta["seed"] is not None:
+        ni, nj = prim.shape[:2]
+        prim[..., 0] += oh.seeded_noise(ni, nj, meta["seed"])
+    return prim
+
+
+def diagnostics(meta):
+    out = []
+    for d in meta["diagnostics"]:
+        d = dict(d)
+        if d.get("radial_cut") is not None:
+            d["radial_cut"] = tuple(d["radial_cut"])
+        out.append(d)
+    return out
