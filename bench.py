@@ -1,0 +1,349 @@
+"""
+Benchmark: zone-updates/s of the plain cbdiso_2d drop-in on one B200.
+
+Workload (the north-star throughput configuration): circumbinary disk on
+[-8, 8]^2 at 4096^2 zones, FP64, equal-mass circular binary (softening 0.05,
+sink radius 0.05, sink rate 10, torque-free sinks), Mach 10 locally
+isothermal, nu = 1e-3, PLM theta 1.5, RK2, CFL 0.3, Keplerian buffer beyond
+r = 7, with the accretion-rate and torque reductions every step. One "step"
+is one driver iteration: dt from the CFL wavespeed, advance(dt), reductions().
+Synthetic data: the setup's initial disk plus seeded 1e-3 noise on Sigma.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size N]
+
+Each state array is 403 MB at 4096^2, larger than the 126 MB L2, so no L2
+flush is needed between steps. Rank 0 prints one JSON line.
+"""
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_ZONE_UPDATE = 120.0  # RK2 x FP64 x 3 fields: 48 B stage 1 + 72 B stage 2
+DIAGNOSTICS = [dict(quantity="time"), dict(quantity="mdot", which_mass=1, accretion=True),
+               dict(quantity="mdot", which_mass=2, accretion=True),
+               dict(quantity="torque", which_mass="both", gravity=True)]
+SETUP_PARAMS = dict(domain_radius=8.0, mach_number=10.0, mass_ratio=1.0, eccentricity=0.0, sink_rate=10.0,
+                    sink_radius=0.05, softening_length=0.05, nu=0.001)
+THETA = 1.5
+CFL = 0.3
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--size", type=int, default=4096)
+    p.add_argument("--precision", default="exact", choices=["exact", "fma", "fast"])
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def initial_state(n, seed):
+    from sailfish_b200.cbdiso_2d import initial_condition
+    from sailfish_b200.setups import CircumbinaryDisk
+
+    setup = CircumbinaryDisk(**SETUP_PARAMS)
+    mesh = setup.mesh(n)
+    prim = initial_condition(setup, mesh, 0.0)
+    rng = np.random.default_rng(seed)
+    prim[..., 0] += 1e-3 * rng.uniform(-1.0, 1.0, size=(n, n))
+    return setup, mesh, prim
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device_index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+
+
+def stage_kernel_time(solver, repeats=20):
+    """Average device time of one fused stage launch (alternating the two RK2
+    stages on the resident state), measured with CUDA events on the launching
+    stream."""
+    import torch
+
+    dt = solver.mesh.min_spacing() / solver.maximum_wavespeed() * CFL
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(2):
+        solver.advance(dt)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(repeats):
+        solver.advance(dt)
+    stop.record()
+    torch.cuda.synchronize()
+    return start.elapsed_time(stop) * 1e-3 / (2 * repeats)
+
+
+def run_ours(args, rank, world):
+    import torch
+
+    from sailfish_b200 import make_solver
+
+    torch.cuda.set_device(rank % max(torch.cuda.device_count(), 1))
+    n = args.size
+    setup, mesh, prim = initial_state(n, args.seed + rank)
+    physics = setup.physics
+    physics["diagnostics"] = DIAGNOSTICS
+    zones = n * n
+
+    def fresh():
+        return make_solver("cbdiso_2d", physics, dict(rk_order=2, plm_theta=THETA, precision=args.precision),
+                           setup=setup, mesh=mesh, solution=prim)
+
+    solver = fresh()
+
+    def step():
+        dt = mesh.min_spacing() / solver.maximum_wavespeed() * CFL
+        solver.advance(dt)
+        return solver.reductions()
+
+    for _ in range(args.warmup):
+        step()
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+        tdist.barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h2d0, d2h0 = solver.h2d_bytes, solver.d2h_bytes
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        start.record()
+        for _ in range(args.steps):
+            step()
+        stop.record()
+        torch.cuda.synchronize()
+    elapsed = start.elapsed_time(stop) * 1e-3
+    if dist:
+        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        elapsed = float(t.item())
+        tdist.barrier()
+    h2d = (solver.h2d_bytes - h2d0) / args.steps
+    d2h = (solver.d2h_bytes - d2h0) / args.steps
+    value = zones * args.steps * world / elapsed
+
+    # end-to-end through the public API, from host data: upload the initial
+    # state, run the steps, download the final state (amortised per step)
+    e2e_steps = max(1, min(args.steps, 50))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s2 = fresh()
+    for _ in range(e2e_steps):
+        dt = mesh.min_spacing() / s2.maximum_wavespeed() * CFL
+        s2.advance(dt)
+        s2.reductions()
+    final = s2.solution
+    t1 = time.perf_counter()
+    e2e_elapsed = t1 - t0
+    if dist:
+        t = torch.tensor([e2e_elapsed], device="cuda", dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        e2e_elapsed = float(t.item())
+    e2e_value = zones * e2e_steps * world / e2e_elapsed
+    e2e_h2d = (s2.h2d_bytes + prim.nbytes) / e2e_steps
+    e2e_d2h = (s2.d2h_bytes + final.nbytes) / e2e_steps
+    del s2
+
+    kernel_s = stage_kernel_time(solver)
+    peak, peak_kind = measured_peaks()
+    achieved = BYTES_PER_ZONE_UPDATE / 2 * zones / kernel_s / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                "kernel": "stage_kernel (one fused RK stage)", "kernel_ms": round(kernel_s * 1e3, 4),
+                "bytes_per_launch": BYTES_PER_ZONE_UPDATE / 2 * zones}
+
+    line = {
+        "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"cbdiso_2d circumbinary disk {n}x{n} FP64 RK2 theta {THETA} CFL {CFL}, "
+                               "per-step mdot/torque reductions", "zones": zones, "precision": args.precision,
+                   "l2": "state arrays (403 MB each at 4096^2) exceed L2; no flush",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": int(e2e_h2d),
+                "d2h_bytes_per_step": int(e2e_d2h), "steps": e2e_steps,
+                "includes": "initial-state upload, public-API driver loop, final-state download"},
+        "step_io": {"h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": 2 * args.steps,
+        "roofline": roofline,
+        "clocks": clocks.summary(),
+    }
+    return line
+
+
+# ---------------------------------------------------------------------------
+# the reference's CPU kernels (oracle/_ref) and the oracle port
+# ---------------------------------------------------------------------------
+
+
+def cpu_config(n):
+    from oracle import host as oh
+
+    return oh.Config(-8.0, 8.0, -8.0, 8.0, n, n, eos_type=2, mach_number=10.0, nu=1e-3, buffer_is_enabled=True,
+                     buffer_driving_rate=100.0, buffer_onset_width=1.0, buffer_surface_density=1.0,
+                     masses=oh.binary_masses(1.0, 1.0, 1.0, 0.0, 0.05, "torque_free", 10.0, 0.05),
+                     plm_theta=THETA)
+
+
+def cpu_kernels():
+    from oracle import host as oh
+
+    try:
+        return oh.Kernels("ref", THETA, threads="omp"), "reference"
+    except (FileNotFoundError, OSError):
+        return oh.Kernels("oracle", THETA), "port"
+
+
+def time_cpu(n, steps, warmup, seed):
+    """Driver loop of the CPU kernels; returns zone-updates/s and the kind."""
+    from oracle import host as oh
+
+    _, _, prim = initial_state(n, seed)
+    kernels, kind = cpu_kernels()
+    solver = oh.OracleSolver(cpu_config(n), prim, 0.0, kernels)
+    diags = [d for d in DIAGNOSTICS]
+    for _ in range(warmup):
+        solver.advance(oh.driver_dt(solver, CFL))
+        solver.reductions(diags)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        solver.advance(oh.driver_dt(solver, CFL))
+        solver.reductions(diags)
+    el = time.perf_counter() - t0
+    return n * n * steps / el, kind, el
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    n = args.size
+    # each step is a full 4096^2 driver iteration; the count is capped so the
+    # whole run stays within a few minutes
+    per_step = 6.0 * (n / 4096.0) ** 2 * 8 / max(1, os.cpu_count())
+    steps = max(1, min(args.steps, int(120.0 / max(per_step, 1e-3))))
+    warmup = min(args.warmup, 1)
+    value, kind, el = time_cpu(n, steps, warmup, args.seed)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    return {
+        "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": el / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"cbdiso_2d circumbinary disk {n}x{n} FP64 RK2 theta {THETA} CFL {CFL}, "
+                               "per-step mdot/torque reductions", "zones": n * n},
+        "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": cores, "kind": kind,
+                         "sample": f"{steps} full driver steps at {n}^2 (advance + wavespeed + reductions)"},
+        "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        line = run_ours(args, rank, world)
+        if rank == 0 and not args.no_cpu_baseline:
+            n = args.size
+            v, kind, el = time_cpu(n, 2 if n >= 2048 else 5, 1, args.seed)
+            line["cpu_baseline"] = {"value": v, "unit": "zone-updates/s",
+                                    "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())), "kind": kind,
+                                    "sample": f"{2 if n >= 2048 else 5} driver steps at {n}^2"}
+    if world > 1 and args.impl == "ours":
+        import torch.distributed as tdist
+
+        tdist.destroy_process_group()
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

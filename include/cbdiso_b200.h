@@ -1,0 +1,218 @@
+/*
+ * cbdiso_b200: a B200 (sm_100a) implementation of sailfish's 2D isothermal
+ * circumbinary-disk solver, cbdiso_2d, as a C-ABI shared library
+ * (libcbdiso_b200.so).
+ *
+ * Two groups of entry points:
+ *
+ *  1. Drop-in kernels. Same symbol names and the same positional arguments as
+ *     the four public kernels of sailfish/solvers/cbdiso_2d.c, so a binding
+ *     written for the reference's kernel library can call them unchanged. The
+ *     differences: array pointers are DEVICE pointers, launches go to the
+ *     library's current stream (cbdiso_b200_set_stream), the PLM parameter
+ *     theta is a library setting (cbdiso_b200_set_plm_theta, default 1.8 as in
+ *     cbdiso_2d.c:11), and each returns an int status (0 = success) where the
+ *     reference returns void.
+ *
+ *  2. The fused product path used by the Python solver: one kernel per RK
+ *     stage with boundary conditions, the RK average and, on the final stage,
+ *     the next step's CFL wavespeed and the diagnostics reductions fused in;
+ *     plus the batched many-disk form and the tangent / adjoint kernels.
+ *
+ * Arrays use the reference layout: C-contiguous (ni + 4, nj + 4, 3) float64,
+ * two guard zones per side, j fastest, then the field (Sigma, vx, vy) or
+ * (Sigma, Sigma vx, Sigma vy).
+ */
+#ifndef CBDISO_B200_H
+#define CBDISO_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------
+ * status codes
+ * ---------------------------------------------------------------------- */
+enum {
+    CBD_OK = 0,
+    CBD_ERR_ARGUMENT = 1,   /* bad sizes, null pointers, unsupported option */
+    CBD_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+    CBD_ERR_NONFINITE = 3,  /* a non-finite value was found where it must not be */
+    CBD_ERR_TIMEOUT = 4,    /* a bounded device-side wait ran out */
+    CBD_ERR_KEPLER = 5,     /* device Kepler solve did not converge in 10 steps */
+    CBD_ERR_CAPACITY = 6    /* request exceeds a fixed capacity of the library */
+};
+
+/* arithmetic of the fused stencil */
+enum {
+    CBD_PRECISION_EXACT = 0, /* IEEE divide / sqrt, the reference's operation order, no FMA contraction */
+    CBD_PRECISION_FMA = 1,   /* as EXACT but the compiler may contract a*b+c into FMA */
+    CBD_PRECISION_FAST = 2   /* FMA, reciprocal multiplies, rsqrt-based gravity */
+};
+
+/* ------------------------------------------------------------------------
+ * 1. drop-in kernels (sailfish/solvers/cbdiso_2d.c:385-722)
+ * ---------------------------------------------------------------------- */
+
+/* replaces cbdiso_2d_advance_rk, sailfish/solvers/cbdiso_2d.c:385-426 */
+int cbdiso_2d_advance_rk(
+    int ni, int nj,
+    double patch_xl, double patch_xr, double patch_yl, double patch_yr,
+    double *conserved_rk, double *primitive_rd, double *primitive_wr,
+    double buffer_surface_density, double buffer_central_mass, double buffer_driving_rate,
+    double buffer_outer_radius, double buffer_onset_width, int buffer_is_enabled,
+    double x1, double y1, double vx1, double vy1, double mass1, double softening_length1,
+    double sink_rate1, double sink_radius1, int sink_model1,
+    double x2, double y2, double vx2, double vy2, double mass2, double softening_length2,
+    double sink_rate2, double sink_radius2, int sink_model2,
+    double cs2, double mach_squared, int eos_type, double nu, double a, double dt,
+    double velocity_ceiling, double density_floor);
+
+/* replaces cbdiso_2d_primitive_to_conserved, sailfish/solvers/cbdiso_2d.c:606-610 */
+int cbdiso_2d_primitive_to_conserved(int ni, int nj, double *primitive, double *conserved);
+
+/* replaces cbdiso_2d_point_mass_source_term, sailfish/solvers/cbdiso_2d.c:626-643 */
+int cbdiso_2d_point_mass_source_term(
+    int ni, int nj,
+    double patch_xl, double patch_xr, double patch_yl, double patch_yr,
+    double x1, double y1, double vx1, double vy1, double mass1, double softening_length1,
+    double sink_rate1, double sink_radius1, int sink_model1,
+    double *primitive, double *cons_rate);
+
+/* replaces cbdiso_2d_wavespeed, sailfish/solvers/cbdiso_2d.c:666-695 */
+int cbdiso_2d_wavespeed(
+    int ni, int nj,
+    double patch_xl, double patch_xr, double patch_yl, double patch_yr,
+    double soundspeed2, double mach_squared, int eos_type,
+    double x1, double y1, double vx1, double vy1, double mass1, double softening_length1,
+    double sink_rate1, double sink_radius1, int sink_model1,
+    double x2, double y2, double vx2, double vy2, double mass2, double softening_length2,
+    double sink_rate2, double sink_radius2, int sink_model2,
+    double *primitive, double *wavespeed);
+
+/* library settings used by the drop-in kernels (no counterpart in the
+ * reference, whose kernels take no stream and fix theta at compile time) */
+int cbdiso_b200_set_stream(void *cuda_stream);
+int cbdiso_b200_set_plm_theta(double theta);
+int cbdiso_b200_set_precision(int precision);
+const char *cbdiso_b200_status_string(int status);
+int cbdiso_b200_version(void);
+
+/* ------------------------------------------------------------------------
+ * 2. fused product path
+ * ---------------------------------------------------------------------- */
+
+/* One point mass (sailfish/physics/circumbinary.py:41-95). */
+typedef struct cbd_mass {
+    double x, y, vx, vy;
+    double mass;
+    double softening_length;
+    double sink_rate;
+    double sink_radius;
+    int sink_model;  /* 0 inactive, 1 acceleration-free, 2 torque-free, 3 force-free */
+    int _pad0;
+} cbd_mass_t;
+
+/* Mesh, equation of state and solver options: constant over a run. */
+typedef struct cbd_grid {
+    int ni, nj;
+    double xl, xr, yl, yr;  /* patch extent (vertex coordinates); dx = (xr - xl) / ni */
+    double plm_theta;
+    int eos_type;           /* 1 globally isothermal, 2 locally isothermal */
+    int precision;          /* CBD_PRECISION_* */
+    double cs2;             /* sound_speed^2 (eos 1) */
+    double mach2;           /* mach_number^2 (eos 2) */
+    double nu;              /* constant kinematic viscosity, 0 = inviscid */
+    double velocity_ceiling;
+    double density_floor;
+    int buffer_is_enabled;
+    int tile_columns;       /* CTA strip width: 64 or 128; 0 = library default */
+    int tile_rows;          /* rows per CTA segment; 0 = library default */
+    int _pad1;
+    double buffer_surface_density;
+    double buffer_driving_rate;
+    double buffer_outer_radius;
+    double buffer_onset_width;
+} cbd_grid_t;
+
+/* Everything that changes per RK stage. */
+typedef struct cbd_stage {
+    cbd_mass_t mass[2];     /* point masses at the stage's start time */
+    double a;               /* RK weight of u_n: u <- (1 - a) (u + du) + a u_n */
+    double dt;
+    double buffer_central_mass;  /* m1 + m2 */
+} cbd_stage_t;
+
+/* Diagnostics (sailfish/physics/circumbinary.py:24-38, cbdiso_2d.py:383-471) */
+enum {
+    CBD_Q_MDOT = 1, CBD_Q_FX = 2, CBD_Q_FY = 3, CBD_Q_TORQUE = 4, CBD_Q_SIGMA_M1 = 5,
+    CBD_Q_ECCENTRICITY_VECTOR = 6, CBD_Q_ANGULAR_MOMENTUM = 7, CBD_Q_MASS = 8, CBD_Q_POWER = 9
+};
+#define CBD_MAX_DIAG 16
+
+typedef struct cbd_diag {
+    int quantity;           /* CBD_Q_* */
+    int which_mass;         /* 1, 2, or 3 for 'both' */
+    int gravity;            /* include the gravity term */
+    int accretion;          /* include the accretion term */
+    int has_cut;            /* radial cut r0 < r < r1 */
+    int _pad;
+    double r0, r1;
+} cbd_diag_t;
+
+/* Quantities computed on the updated state at the end of a step: the CFL
+ * wavespeed maximum and the diagnostic sums, with point masses at `mass`
+ * (the end-of-step time). Results land in `result`:
+ *   result[0] = max wavespeed, result[1 + 2k], result[2 + 2k] = real and
+ *   imaginary part of sum_cells f_k (not yet multiplied by dx dy). */
+typedef struct cbd_epilogue {
+    cbd_mass_t mass[2];
+    int want_wavespeed;
+    int num_diag;
+    cbd_diag_t diag[CBD_MAX_DIAG];
+} cbd_epilogue_t;
+
+/* sizeof of cbd_mass_t, cbd_grid_t, cbd_stage_t, cbd_epilogue_t, for
+ * bindings to check their struct layouts against. */
+void cbdiso_b200_abi_sizes(size_t out[4]);
+
+/* Bytes of device scratch the fused reductions need for this grid. */
+size_t cbdiso_b200_scratch_bytes(const cbd_grid_t *grid);
+
+/* Fill the two guard zones per side by zero-gradient extrapolation
+ * (equivalent to cbdiso_2d.py:553-586 on one patch). */
+int cbdiso_b200_fill_guards(const cbd_grid_t *grid, double *primitive, void *stream);
+
+/* One fused RK stage: reads primitive_rd (guards valid), writes the interior
+ * and the guard zones of primitive_wr. For a > 0 the stage's u_n is formed
+ * from primitive_n (the state at the start of the step). primitive_wr may
+ * equal primitive_n (in-place final stage). If `epilogue` is non-null its
+ * quantities are reduced into `result` using `scratch`
+ * (cbdiso_b200_scratch_bytes). `stage_dev`, when non-null, is a device-side
+ * stage record written by the library's own device stepping kernels and read
+ * instead of `stage` (used under CUDA graph capture). */
+int cbdiso_b200_advance_stage(
+    const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
+    const double *primitive_rd, const double *primitive_n, double *primitive_wr,
+    const cbd_epilogue_t *epilogue, double *scratch, double *result, void *stream);
+
+/* Size of the device-side stage record, and a host routine that fills one
+ * from a stage (and the end-of-step masses of an epilogue, may be null). A
+ * caller copies records to device memory and passes them as `stage_dev`, so
+ * a step's inputs travel as one explicit host-to-device copy. */
+size_t cbdiso_b200_stage_record_bytes(void);
+int cbdiso_b200_stage_record(const cbd_grid_t *grid, const cbd_stage_t *stage, const cbd_epilogue_t *epilogue,
+                             void *record);
+
+/* The epilogue quantities alone, on a given state (guards not needed). */
+int cbdiso_b200_reduce(
+    const cbd_grid_t *grid, const cbd_epilogue_t *epilogue, const double *primitive,
+    double *scratch, double *result, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CBDISO_B200_H */

@@ -1,0 +1,139 @@
+"""
+ctypes binding of libcbdiso_b200.so (include/cbdiso_b200.h).
+
+The library is loaded from the package directory, where
+`python -m sailfish_b200._build` (or __graft_entry__.build()) puts it. There is
+no fallback: if the library is missing, `lib()` raises.
+"""
+
+import ctypes
+import os
+from ctypes import POINTER, Structure, c_double, c_int, c_size_t, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcbdiso_b200.so")
+
+CBD_OK = 0
+STATUS = {
+    0: "success",
+    1: "invalid argument",
+    2: "CUDA runtime error",
+    3: "non-finite value",
+    4: "device wait timed out",
+    5: "Kepler solve did not converge",
+    6: "request exceeds library capacity",
+}
+PRECISION = {"exact": 0, "fma": 1, "fast": 2}
+MAX_DIAG = 16
+MAX_FUSED = 4
+QUANTITY = dict(mdot=1, fx=2, fy=3, torque=4, sigma_m1=5, eccentricity_vector=6, angular_momentum=7, mass=8,
+                power=9)
+
+
+class CbdError(RuntimeError):
+    """A libcbdiso_b200 entry point returned a non-zero status."""
+
+    def __init__(self, status, where=""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS.get(status, 'unknown status')} (status {status})")
+
+
+class Mass(Structure):
+    _fields_ = [("x", c_double), ("y", c_double), ("vx", c_double), ("vy", c_double), ("mass", c_double),
+                ("softening_length", c_double), ("sink_rate", c_double), ("sink_radius", c_double),
+                ("sink_model", c_int), ("_pad0", c_int)]
+
+
+class Grid(Structure):
+    _fields_ = [("ni", c_int), ("nj", c_int), ("xl", c_double), ("xr", c_double), ("yl", c_double),
+                ("yr", c_double), ("plm_theta", c_double), ("eos_type", c_int), ("precision", c_int),
+                ("cs2", c_double), ("mach2", c_double), ("nu", c_double), ("velocity_ceiling", c_double),
+                ("density_floor", c_double), ("buffer_is_enabled", c_int), ("tile_columns", c_int),
+                ("tile_rows", c_int), ("_pad1", c_int), ("buffer_surface_density", c_double),
+                ("buffer_driving_rate", c_double), ("buffer_outer_radius", c_double),
+                ("buffer_onset_width", c_double)]
+
+
+class Stage(Structure):
+    _fields_ = [("mass", Mass * 2), ("a", c_double), ("dt", c_double), ("buffer_central_mass", c_double)]
+
+
+class Diag(Structure):
+    _fields_ = [("quantity", c_int), ("which_mass", c_int), ("gravity", c_int), ("accretion", c_int),
+                ("has_cut", c_int), ("_pad", c_int), ("r0", c_double), ("r1", c_double)]
+
+
+class Epilogue(Structure):
+    _fields_ = [("mass", Mass * 2), ("want_wavespeed", c_int), ("num_diag", c_int), ("diag", Diag * MAX_DIAG)]
+
+
+_lib = None
+_DP = POINTER(c_double)
+
+
+def _declare(lib):
+    I, D, P, V = c_int, c_double, c_void_p, c_void_p
+    m9 = [D] * 8 + [I]
+    sig = {
+        "cbdiso_2d_advance_rk": [I, I, D, D, D, D, P, P, P, D, D, D, D, D, I] + m9 + m9 + [D, D, I, D, D, D, D, D],
+        "cbdiso_2d_primitive_to_conserved": [I, I, P, P],
+        "cbdiso_2d_point_mass_source_term": [I, I, D, D, D, D] + m9 + [P, P],
+        "cbdiso_2d_wavespeed": [I, I, D, D, D, D, D, D, I] + m9 + m9 + [P, P],
+        "cbdiso_b200_set_stream": [V],
+        "cbdiso_b200_set_plm_theta": [D],
+        "cbdiso_b200_set_precision": [I],
+        "cbdiso_b200_version": [],
+        "cbdiso_b200_fill_guards": [POINTER(Grid), P, V],
+        "cbdiso_b200_advance_stage": [POINTER(Grid), POINTER(Stage), P, P, P, P, POINTER(Epilogue), P, P, V],
+        "cbdiso_b200_reduce": [POINTER(Grid), POINTER(Epilogue), P, P, P, V],
+    }
+    for name, args in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = c_int
+    lib.cbdiso_b200_scratch_bytes.argtypes = [POINTER(Grid)]
+    lib.cbdiso_b200_scratch_bytes.restype = c_size_t
+    lib.cbdiso_b200_stage_record_bytes.argtypes = []
+    lib.cbdiso_b200_stage_record_bytes.restype = c_size_t
+    lib.cbdiso_b200_stage_record.argtypes = [POINTER(Grid), POINTER(Stage), POINTER(Epilogue), c_void_p]
+    lib.cbdiso_b200_stage_record.restype = c_int
+    lib.cbdiso_b200_abi_sizes.argtypes = [POINTER(c_size_t)]
+    lib.cbdiso_b200_abi_sizes.restype = None
+    lib.cbdiso_b200_status_string.argtypes = [c_int]
+    lib.cbdiso_b200_status_string.restype = ctypes.c_char_p
+    return lib
+
+
+def lib():
+    """The loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m sailfish_b200._build` "
+                "(there is no CPU fallback)")
+        _lib = _declare(ctypes.CDLL(LIB_PATH))
+    return _lib
+
+
+def check(status, where=""):
+    if status != CBD_OK:
+        raise CbdError(status, where)
+
+
+def exported_symbols():
+    """Names declared in include/cbdiso_b200.h (for the export test)."""
+    return [
+        "cbdiso_2d_advance_rk", "cbdiso_2d_primitive_to_conserved", "cbdiso_2d_point_mass_source_term",
+        "cbdiso_2d_wavespeed", "cbdiso_b200_set_stream", "cbdiso_b200_set_plm_theta", "cbdiso_b200_set_precision",
+        "cbdiso_b200_status_string", "cbdiso_b200_version", "cbdiso_b200_scratch_bytes", "cbdiso_b200_fill_guards",
+        "cbdiso_b200_advance_stage", "cbdiso_b200_reduce", "cbdiso_b200_abi_sizes",
+        "cbdiso_b200_stage_record_bytes", "cbdiso_b200_stage_record",
+    ]
+
+
+def abi_sizes():
+    """(C sizes, ctypes sizes) of the four public structs."""
+    out = (c_size_t * 4)()
+    lib().cbdiso_b200_abi_sizes(out)
+    return list(out), [ctypes.sizeof(t) for t in (Mass, Grid, Stage, Epilogue)]

@@ -1,0 +1,405 @@
+"""
+Drop-in replacement for sailfish's cbdiso_2d solver adapter
+(sailfish/solvers/cbdiso_2d.py:1-590), running on one B200.
+
+Same constructor (setup, mesh, time, solution, num_patches, mode, physics,
+options), same validation errors, same properties and methods
+(`solution`, `primitive`, `time`, `options`, `physics`, `recommended_cfl`,
+`maximum_cfl`, `maximum_wavespeed()`, `advance(dt)`, `reductions()`).
+
+What differs is how a step executes. The state stays in device memory in the
+reference's (ni + 4, nj + 4, 3) layout; each RK stage is one fused kernel of
+libcbdiso_b200.so that also writes the guard zones, so there is no separate
+boundary-condition pass and no separate primitive-to-conserved pass; and the
+final stage of each step computes the next step's wavespeed maximum and the
+diagnostic sums, so `maximum_wavespeed()` and `reductions()` after `advance()`
+only read a few doubles back. The whole grid is one device patch whatever
+`num_patches` says: the reference's patch split is exact (its guard exchange
+followed by zero-gradient edges equals index clamping on the whole grid), so
+only its reduction summation order depends on it.
+
+Extra solver options beyond the reference's (velocity_ceiling, density_floor,
+rk_order): `plm_theta` (default 1.8, the reference's compile-time
+PLM_THETA), `precision` ("exact" | "fma" | "fast"), `fuse_reductions`, and
+`tile` ((columns, rows) of the stage kernel's CTA tile, or None for the
+library default).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from logging import getLogger
+from typing import NamedTuple, Optional
+
+import numpy as np
+
+from . import _capi
+from .mesh import is_planar_cartesian_2d
+from .physics import Diagnostic, Physics, enum_value
+from .solver_base import SolverBase
+
+logger = getLogger(__name__)
+
+NG = 2
+NQ = 3
+RK_WEIGHTS = {1: (0.0,), 2: (0.0, 0.5), 3: (0.0, 0.75, 1.0 / 3.0)}
+COMPLEX_QUANTITIES = ("sigma_m1", "eccentricity_vector")
+
+
+class Options(NamedTuple):
+    """Solver options (cbdiso_2d.py:23-30, plus this build's extensions)."""
+
+    velocity_ceiling: float = 1e12
+    density_floor: float = 1e-12
+    rk_order: int = 2
+    plm_theta: float = 1.8
+    precision: str = "exact"
+    fuse_reductions: bool = True
+    tile: Optional[tuple] = None
+
+
+def initial_condition(setup, mesh, time):
+    """
+    Primitive data (ni, nj, 3) from a setup (cbdiso_2d.py:33-46). Setups with a
+    vectorised `primitive_array(t, x, y)` are evaluated on the whole grid at
+    once; others zone by zone as the reference does.
+    """
+    ni, nj = mesh.shape
+    if hasattr(setup, "primitive_array"):
+        i = np.arange(ni, dtype=np.float64)[:, None]
+        j = np.arange(nj, dtype=np.float64)[None, :]
+        x = np.broadcast_to(mesh.x0 + (i + 0.5) * mesh.dx, (ni, nj))
+        y = np.broadcast_to(mesh.y0 + (j + 0.5) * mesh.dy, (ni, nj))
+        return np.ascontiguousarray(setup.primitive_array(time, x, y), dtype=np.float64)
+    primitive = np.zeros([ni, nj, 3])
+    for i in range(ni):
+        for j in range(nj):
+            setup.primitive(time, mesh.cell_coordinates(i, j), primitive[i, j])
+    return primitive
+
+
+def _as_diagnostic(d):
+    if isinstance(d, dict):
+        return Diagnostic(**d)
+    if isinstance(d, Diagnostic):
+        return d
+    return Diagnostic(d.quantity, d.gravity, d.accretion, d.which_mass, d.radial_cut)
+
+
+def _mass_struct(m, out):
+    out.x = m.position_x
+    out.y = m.position_y
+    out.vx = m.velocity_x
+    out.vy = m.velocity_y
+    out.mass = m.mass
+    out.softening_length = m.softening_length
+    out.sink_rate = m.sink_rate
+    out.sink_radius = m.sink_radius
+    out.sink_model = enum_value(m.sink_model)
+
+
+def _diag_struct(d: Diagnostic, out):
+    out.quantity = _capi.QUANTITY[d.quantity]
+    wm = d.which_mass
+    out.which_mass = 3 if wm == "both" else (int(wm) if wm in (1, 2) else 1)
+    out.gravity = int(bool(d.gravity))
+    out.accretion = int(bool(d.accretion))
+    if d.radial_cut is not None:
+        out.has_cut = 1
+        out.r0, out.r1 = float(d.radial_cut[0]), float(d.radial_cut[1])
+    else:
+        out.has_cut = 0
+
+
+class Solver(SolverBase):
+    """Adapter driving the fused sm_100a kernels of libcbdiso_b200.so."""
+
+    def __init__(self, setup=None, mesh=None, time=0.0, solution=None, num_patches=1, mode="gpu",
+                 physics=dict(), options=dict()):
+        import torch
+
+        physics = dict(physics)
+        physics["diagnostics"] = [_as_diagnostic(v) for v in physics.get("diagnostics", [])]
+        self._physics = physics = Physics(**physics)
+        self._options = options = Options(**options)
+
+        if not is_planar_cartesian_2d(mesh):
+            raise ValueError("solver only supports 2D cartesian mesh")
+        if setup.boundary_condition != "outflow":
+            raise ValueError("solver only supports outflow boundary condition")
+        if enum_value(physics.viscosity_model) not in (0, 1):
+            raise ValueError("solver only supports constant-nu viscosity")
+        if enum_value(physics.eos_type) not in (1, 2):
+            raise ValueError("solver only supports isothermal equation of states")
+        if physics.cooling_coefficient != 0.0:
+            raise ValueError("solver does not support thermal cooling")
+        if not physics.constant_softening:
+            raise ValueError("solver only supports constant gravitational softening")
+        if options.rk_order not in RK_WEIGHTS:
+            raise ValueError(f"rk_order must be 1, 2 or 3, got {options.rk_order}")
+        if options.precision not in _capi.PRECISION:
+            raise ValueError(f"precision must be one of {sorted(_capi.PRECISION)}, got {options.precision}")
+        for d in physics.diagnostics:
+            if d.quantity != "time" and d.quantity not in _capi.QUANTITY:
+                raise ValueError(f"unknown diagnostic quantity {d.quantity}")
+        if not torch.cuda.is_available():
+            raise RuntimeError("sailfish_b200 needs a CUDA device (there is no CPU fallback)")
+
+        self._lib = _capi.lib()
+        self.mesh = mesh
+        self.setup = setup
+        self.num_guard = NG
+        self.num_cons = NQ
+        self.num_patches = num_patches
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        ni, nj = mesh.shape
+
+        logger.info(f"initiate with time={time:0.4f}")
+        logger.info(f"mesh is {mesh}")
+        logger.info("boundary condition is outflow")
+
+        if solution is None:
+            primitive = initial_condition(setup, mesh, time)
+        else:
+            primitive = np.asarray(solution, dtype=np.float64)
+        if primitive.shape != (ni, nj, NQ):
+            raise ValueError(f"solution has shape {primitive.shape}, expected {(ni, nj, NQ)}")
+
+        if physics.buffer_is_enabled:
+            # The buffer's target density is the setup's data at the onset
+            # radius on the x axis, as in cbdiso_2d.py:325-334.
+            buffer_prim = [0.0] * 3
+            buffer_outer_radius = mesh.x1
+            buffer_onset_radius = buffer_outer_radius - physics.buffer_onset_width
+            setup.primitive(time, [buffer_onset_radius, 0.0], buffer_prim)
+            buffer_surface_density = buffer_prim[0]
+        else:
+            buffer_outer_radius = 0.0
+            buffer_surface_density = 0.0
+
+        g = _capi.Grid()
+        g.ni, g.nj = ni, nj
+        g.xl, g.yl = mesh.vertex_coordinates(0, 0)
+        g.xr, g.yr = mesh.vertex_coordinates(ni, nj)
+        g.plm_theta = options.plm_theta
+        g.eos_type = enum_value(physics.eos_type)
+        g.precision = _capi.PRECISION[options.precision]
+        g.cs2 = physics.sound_speed ** 2
+        g.mach2 = physics.mach_number ** 2
+        g.nu = physics.viscosity_coefficient
+        g.velocity_ceiling = options.velocity_ceiling
+        g.density_floor = options.density_floor
+        g.buffer_is_enabled = int(bool(physics.buffer_is_enabled))
+        g.buffer_surface_density = buffer_surface_density
+        g.buffer_driving_rate = physics.buffer_driving_rate
+        g.buffer_outer_radius = buffer_outer_radius
+        g.buffer_onset_width = physics.buffer_onset_width
+        if options.tile:
+            g.tile_columns, g.tile_rows = int(options.tile[0]), int(options.tile[1])
+        self._grid = g
+
+        f64 = dict(dtype=torch.float64, device=self.device)
+        nbuf = 3 if options.rk_order == 3 else 2
+        self._buf = [torch.empty((ni + 2 * NG, nj + 2 * NG, NQ), **f64) for _ in range(nbuf)]
+        self._buf[0][NG:-NG, NG:-NG] = torch.from_numpy(primitive).to(self.device)
+        self._check(self._lib.cbdiso_b200_fill_guards(ctypes.byref(g), self._ptr(self._buf[0]), self._stream()),
+                    "fill_guards")
+        nscratch = int(self._lib.cbdiso_b200_scratch_bytes(ctypes.byref(g)))
+        self._scratch = torch.zeros(nscratch // 8 + 8, **f64)
+        self._result = torch.zeros(1 + 2 * _capi.MAX_DIAG, **f64)
+        self._result_host = torch.zeros(1 + 2 * _capi.MAX_DIAG, dtype=torch.float64).pin_memory()
+
+        # stage records: a small ring of pinned host slots, one device block
+        self._rec_bytes = int(self._lib.cbdiso_b200_stage_record_bytes())
+        nstage = len(RK_WEIGHTS[options.rk_order])
+        self._ring = [torch.zeros(nstage * self._rec_bytes, dtype=torch.uint8).pin_memory() for _ in range(4)]
+        self._ring_events = [None] * len(self._ring)
+        self._ring_next = 0
+        self._records = torch.zeros(nstage * self._rec_bytes, dtype=torch.uint8, device=self.device)
+
+        self._device_diags = [d for d in physics.diagnostics if d.quantity != "time"]
+        self._fused = options.fuse_reductions and len(self._device_diags) <= _capi.MAX_FUSED
+        self._time = float(time)
+        self._cached = None  # result block valid for the current state, read lazily
+        self._result_valid = False
+        self.h2d_bytes = 0
+        self.d2h_bytes = 0
+
+    # ------------------------------------------------------------------
+    # helpers
+    # ------------------------------------------------------------------
+
+    @staticmethod
+    def _ptr(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    @staticmethod
+    def _stream():
+        import torch
+
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def _check(self, status, where):
+        _capi.check(status, where)
+
+    def _epilogue(self, time, want_ws, diags):
+        ep = _capi.Epilogue()
+        m1, m2 = self._physics.point_masses(time)
+        _mass_struct(m1, ep.mass[0])
+        _mass_struct(m2, ep.mass[1])
+        ep.want_wavespeed = int(want_ws)
+        ep.num_diag = len(diags)
+        for k, d in enumerate(diags):
+            _diag_struct(d, ep.diag[k])
+        return ep
+
+    def _read_result(self):
+        import torch
+
+        if self._cached is None:
+            n = 1 + 2 * len(self._device_diags)
+            self._result_host[:n].copy_(self._result[:n], non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            self.d2h_bytes += 8 * n
+            self._cached = self._result_host[:n].numpy().copy()
+        return self._cached
+
+    def _reduce_now(self, want_ws, diags):
+        ep = self._epilogue(self._time, want_ws, diags)
+        self._check(self._lib.cbdiso_b200_reduce(ctypes.byref(self._grid), ctypes.byref(ep),
+                                                 self._ptr(self._buf[0]), self._ptr(self._scratch),
+                                                 self._ptr(self._result), self._stream()), "reduce")
+        self._cached = None
+        self._result_valid = True
+
+    # ------------------------------------------------------------------
+    # SolverBase
+    # ------------------------------------------------------------------
+
+    @property
+    def solution(self):
+        return self._buf[0][NG:-NG, NG:-NG].cpu().numpy()
+
+    @property
+    def primitive(self):
+        """This solver uses primitive data as the solution array."""
+        return None
+
+    @property
+    def time(self):
+        return self._time
+
+    @property
+    def options(self):
+        return self._options._asdict()
+
+    @property
+    def physics(self):
+        return self._physics._asdict()
+
+    @property
+    def recommended_cfl(self):
+        return 0.3
+
+    @property
+    def maximum_cfl(self):
+        return 0.4
+
+    def maximum_wavespeed(self):
+        """Largest |v +- cs| over the grid, with point masses at the current time."""
+        if not self._result_valid:
+            self._reduce_now(True, self._device_diags if self._fused else [])
+        return float(self._read_result()[0])
+
+    def advance(self, dt):
+        import torch
+
+        dt = float(dt)
+        weights = RK_WEIGHTS[self._options.rk_order]
+        time0 = self._time
+        lib, g = self._lib, self._grid
+        stream = self._stream()
+
+        # stage times follow cbdiso_2d.py:239 exactly
+        times = []
+        t = time0
+        for a in weights:
+            times.append(t)
+            t = time0 * a + (t + dt) * (1.0 - a)
+        time_end = t
+
+        epilogue = self._epilogue(time_end, True, self._device_diags if self._fused else [])
+        slot = self._ring_next
+        self._ring_next = (slot + 1) % len(self._ring)
+        if self._ring_events[slot] is not None:
+            self._ring_events[slot].synchronize()
+        host = self._ring[slot]
+        for s, (a, ts) in enumerate(zip(weights, times)):
+            st = _capi.Stage()
+            m1, m2 = self._physics.point_masses(ts)
+            _mass_struct(m1, st.mass[0])
+            _mass_struct(m2, st.mass[1])
+            st.a = a
+            st.dt = dt
+            st.buffer_central_mass = m1.mass + m2.mass
+            self._check(lib.cbdiso_b200_stage_record(ctypes.byref(g), ctypes.byref(st), ctypes.byref(epilogue),
+                                                     ctypes.c_void_p(host.data_ptr() + s * self._rec_bytes)),
+                        "stage_record")
+        self._records.copy_(host, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        self._ring_events[slot] = ev
+        self.h2d_bytes += host.numel()
+
+        A = self._buf[0]
+        B = self._buf[1]
+        if len(weights) == 1:
+            plan = [(A, None, B, epilogue)]
+        elif len(weights) == 2:
+            plan = [(A, None, B, None), (B, A, A, epilogue)]
+        else:
+            C = self._buf[2]
+            plan = [(A, None, B, None), (B, A, C, None), (C, A, A, epilogue)]
+        dummy = _capi.Stage()
+        for s, (rd, pn, wr, ep) in enumerate(plan):
+            dummy.a = weights[s]
+            rec = ctypes.c_void_p(self._records.data_ptr() + s * self._rec_bytes)
+            status = lib.cbdiso_b200_advance_stage(
+                ctypes.byref(g), ctypes.byref(dummy), rec, self._ptr(rd),
+                self._ptr(pn) if pn is not None else None, self._ptr(wr),
+                ctypes.byref(ep) if ep is not None else None, self._ptr(self._scratch), self._ptr(self._result),
+                stream)
+            self._check(status, "advance_stage")
+        if len(weights) == 1:
+            self._buf[0], self._buf[1] = B, A
+        self._time = time_end
+        self._cached = None
+        self._result_valid = True
+
+    def reductions(self):
+        """
+        Time series row in the order of physics.diagnostics: time in units of
+        the setup's reference time scale, then each sum times dx dy
+        (cbdiso_2d.py:370-503). Real quantities are floats, sigma_m1 and
+        eccentricity_vector complex.
+        """
+        diagnostics = self._physics.diagnostics
+        if self._device_diags:
+            if not (self._fused and self._result_valid):
+                self._reduce_now(True, self._device_diags)
+            res = self._read_result()
+        da = self.mesh.dx * self.mesh.dy
+        out = []
+        k = 0
+        for d in diagnostics:
+            if d.quantity == "time":
+                out.append(self._time / self.setup.reference_time_scale)
+                continue
+            re, im = res[1 + 2 * k], res[2 + 2 * k]
+            k += 1
+            if d.quantity in COMPLEX_QUANTITIES:
+                out.append(complex(re, im) * da)
+            else:
+                out.append(float(re) * da)
+        return out

@@ -1,0 +1,22 @@
+// Internal launch interface shared by the host shim (capi.cu) and the three
+// precision-specific translation units of the stage kernel.
+#pragma once
+
+#include "cbd_stencil.cuh"
+
+namespace cbd {
+
+struct LaunchShape {
+    int bj;        // threads per CTA = columns per strip (64, 128, 256)
+    int rows;      // rows per CTA
+    dim3 grid;
+};
+
+cudaError_t launch_stage_exact(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a,
+                               cudaStream_t stream);
+cudaError_t launch_stage_fma(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a,
+                             cudaStream_t stream);
+cudaError_t launch_stage_fast(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a,
+                              cudaStream_t stream);
+
+}  // namespace cbd

@@ -1,0 +1,12 @@
+// Stage kernel at CBD_PRECISION_FMA.
+#include "stage_launch.cuh"
+
+namespace cbd {
+
+cudaError_t launch_stage_fma(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a,
+                              cudaStream_t stream)
+{
+    return launch_stage<CBD_PRECISION_FMA>(s, k, st, a, stream);
+}
+
+}  // namespace cbd

@@ -1,0 +1,372 @@
+"""
+Circumbinary-disk setups that choose the cbdiso_2d solver, with sailfish's
+setup interface (sailfish/setup_base.py:32-286): typed model parameters,
+`primitive(t, coords, out)`, `mesh(resolution)`, `physics`, `solver`,
+`boundary_condition`, `reference_time_scale`, `point_masses(t)`.
+
+Besides the per-zone `primitive`, each setup here has `primitive_array(t, x,
+y)`, a vectorised form used to build the initial state of large grids; it
+returns the same doubles as the per-zone loop (checked by the tests).
+"""
+
+from math import exp, pi, sqrt
+from typing import Any, NamedTuple
+
+import numpy as np
+
+from .kepler import OrbitalElements
+from .mesh import PlanarCartesian2DMesh
+from .physics import EquationOfState, PointMass, SinkModel, ViscosityModel
+
+
+class SetupError(Exception):
+    """Something went wrong during setup configuration"""
+
+
+class Parameter(NamedTuple):
+    default: Any
+    about: str
+    mutable: bool = False
+
+
+param = Parameter
+
+
+class SetupBase:
+    """Typed model parameters as in setup_base.py:43-61."""
+
+    def __init__(self, **kwargs):
+        for key, val, _ in type(self).default_model_parameters():
+            if key in kwargs:
+                if type(kwargs[key]) != type(val):
+                    raise SetupError(
+                        f"parameter '{key}' has type {type(val).__name__} (got {type(kwargs[key]).__name__})")
+                setattr(self, key, kwargs[key])
+            else:
+                setattr(self, key, val)
+        for key in kwargs:
+            if not hasattr(self, key):
+                raise SetupError(f"'{type(self).__name__}' has no parameter '{key}'")
+        self.validate()
+
+    @classmethod
+    def default_model_parameters(cls):
+        for klass in reversed(cls.__mro__):
+            for key, val in vars(klass).items():
+                if type(val) == Parameter:
+                    yield key, val.default, val.about
+
+    def validate(self):
+        pass
+
+    @property
+    def boundary_condition(self):
+        return "outflow"
+
+    @property
+    def reference_time_scale(self):
+        return 1.0
+
+    def checkpoint_diagnostics(self, time):
+        return dict()
+
+
+def _binary_point_masses(setup, time, x_offset=None):
+    m1, m2 = setup.orbital_elements.orbital_state(time)
+    out = []
+    for m in (m1, m2):
+        x = m.position_x if x_offset is None else m.position_x + x_offset
+        out.append(PointMass(
+            mass=m.mass, position_x=x, position_y=m.position_y, velocity_x=m.velocity_x,
+            velocity_y=m.velocity_y, softening_length=setup.softening_length,
+            sink_model=SinkModel[setup.sink_model.upper()], sink_rate=setup.sink_rate,
+            sink_radius=setup.sink_radius))
+    return tuple(out)
+
+
+class CircumbinaryDisk(SetupBase):
+    """
+    Isothermal circumbinary disk (sailfish/setups/circumbinary_disk.py:17-215):
+    uniform surface density, Keplerian rotation about the origin with a
+    softened radius, a binary on a Kepler orbit, Keplerian buffer beyond
+    domain_radius - 1.
+    """
+
+    eos = param("isothermal", "EOS type (only isothermal uses cbdiso_2d)")
+    domain_radius = param(12.0, "half side length of the square computational domain")
+    mach_number = param(10.0, "orbital Mach number (isothermal)", mutable=True)
+    eccentricity = param(0.0, "orbital eccentricity of the binary", mutable=True)
+    mass_ratio = param(1.0, "component mass ratio m2 / m1 <= 1", mutable=True)
+    sink_rate = param(10.0, "component sink rate", mutable=True)
+    sink_radius = param(0.05, "component sink radius", mutable=True)
+    softening_length = param(0.05, "gravitational softening length", mutable=True)
+    buffer_is_enabled = param(True, "whether the buffer zone is enabled", mutable=True)
+    sink_model = param("torque_free", "sink [acceleration_free|force_free|torque_free]", mutable=True)
+    initial_sigma = param(1.0, "initial disk surface density")
+    nu = param(0.001, "kinematic viscosity parameter (isothermal)")
+    constant_softening = param(True, "whether to use constant softening")
+    which_diagnostics = param("none", "diagnostics set to get from solver [none|mdots]")
+
+    def validate(self):
+        if self.eos != "isothermal":
+            raise SetupError(f"this build supports eos=isothermal only, got {self.eos}")
+        if self.which_diagnostics not in ["none", "mdots"]:
+            raise SetupError(f"which_diagnostics must be none or mdots, got {self.which_diagnostics}")
+
+    def primitive(self, t, coords, primitive):
+        GM = 1.0
+        x, y = coords
+        r = sqrt(x * x + y * y)
+        r_softened = sqrt(x * x + y * y + self.softening_length * self.softening_length)
+        phi_hat_x = -y / max(r, 1e-12)
+        phi_hat_y = +x / max(r, 1e-12)
+        primitive[0] = self.initial_sigma
+        primitive[1] = sqrt(GM / r_softened) * phi_hat_x
+        primitive[2] = sqrt(GM / r_softened) * phi_hat_y
+
+    def primitive_array(self, t, x, y):
+        GM = 1.0
+        r = np.sqrt(x * x + y * y)
+        r_softened = np.sqrt(x * x + y * y + self.softening_length * self.softening_length)
+        out = np.empty(np.broadcast(x, y).shape + (3,))
+        out[..., 0] = self.initial_sigma
+        out[..., 1] = np.sqrt(GM / r_softened) * (-y / np.maximum(r, 1e-12))
+        out[..., 2] = np.sqrt(GM / r_softened) * (+x / np.maximum(r, 1e-12))
+        return out
+
+    def mesh(self, resolution):
+        return PlanarCartesian2DMesh.centered_square(self.domain_radius, resolution)
+
+    @property
+    def default_resolution(self):
+        return 512
+
+    @property
+    def physics(self):
+        return dict(
+            eos_type=EquationOfState.LOCALLY_ISOTHERMAL,
+            mach_number=self.mach_number,
+            point_mass_function=self.point_masses,
+            buffer_is_enabled=self.buffer_is_enabled,
+            buffer_driving_rate=100.0,
+            buffer_onset_width=1.0,
+            cooling_coefficient=0.0,
+            constant_softening=self.constant_softening,
+            viscosity_model=ViscosityModel.CONSTANT_NU if self.nu > 0.0 else ViscosityModel.NONE,
+            viscosity_coefficient=self.nu,
+            alpha=0.0,
+            diagnostics=self.diagnostics,
+        )
+
+    @property
+    def diagnostics(self):
+        if self.which_diagnostics != "none":
+            return [
+                dict(quantity="time"),
+                dict(quantity="mdot", which_mass=1, accretion=True),
+                dict(quantity="mdot", which_mass=2, accretion=True),
+            ]
+        return []
+
+    @property
+    def solver(self):
+        return "cbdiso_2d"
+
+    @property
+    def default_end_time(self):
+        return 1000.0
+
+    @property
+    def reference_time_scale(self):
+        return 2.0 * pi
+
+    @property
+    def orbital_elements(self):
+        return OrbitalElements(semimajor_axis=1.0, total_mass=1.0, mass_ratio=self.mass_ratio,
+                               eccentricity=self.eccentricity)
+
+    def point_masses(self, time):
+        return _binary_point_masses(self, time)
+
+    def checkpoint_diagnostics(self, time):
+        return dict(point_masses=self.point_masses(time))
+
+
+class KitpCodeComparison(SetupBase):
+    """
+    The KITP code-comparison disk (circumbinary_disk.py:218-375): a cavity of
+    radius 2.5, a sub-Keplerian profile and a small radial kick.
+    """
+
+    mach_number = param(10.0, "nominal orbital Mach number", mutable=True)
+    eccentricity = param(0.0, "orbital eccentricity")
+    mass_ratio = param(1.0, "binary mass ratio M2 / M1")
+    sink_radius = param(0.05, "sink radius", mutable=True)
+    softening_length = param(0.05, "softening length", mutable=True)
+    nu = param(0.001, "kinematic viscosity coefficient", mutable=True)
+    single_point_mass = param(False, "put one point mass at the origin (no binary)")
+    sink_model = param("acceleration_free", "sink [acceleration_free|force_free|torque_free]", mutable=True)
+    domain_radius = param(8.0, "half side length of the square computational domain")
+    sink_rate = param(10.0, "component sink rate", mutable=True)
+    buffer_is_enabled = param(True, "whether the buffer zone is enabled", mutable=True)
+    disk_kick = param(1e-4, "kick velocity to seed eccentric cavity growth")
+    which_diagnostics = param("kitp", "output diagnostics option [kitp|forces]")
+
+    def validate(self):
+        if self.which_diagnostics not in ["kitp", "forces"]:
+            raise SetupError("Unknown option for diagnostics.")
+
+    def primitive(self, t, coords, primitive):
+        x, y = coords
+        r = sqrt(x * x + y * y)
+        r_cav = 2.5
+        delta0 = 1e-5
+        sigma0 = 1.0
+        sigma = sigma0 * (delta0 + (1 - delta0) * exp(-((r_cav / r) ** 12)))
+        GM = 1.0
+        a = 1.0
+        n = 4.0
+        omegaB = (GM / a**3) ** 0.5
+        omega0 = (GM / r**3 * (1.0 - 1.0 / self.mach_number**2)) ** 0.5
+        omega = (omega0**-n + omegaB**-n) ** (-1 / n)
+        vr_pert = self.disk_kick * y * exp(-((r / 3.5) ** 6))
+        primitive[0] = sigma
+        primitive[1] = omega * -y + vr_pert * x / r
+        primitive[2] = omega * +x + vr_pert * y / r
+
+    def mesh(self, resolution):
+        return PlanarCartesian2DMesh.centered_square(self.domain_radius, resolution)
+
+    @property
+    def default_resolution(self):
+        return 200
+
+    @property
+    def diagnostics(self):
+        if self.which_diagnostics == "kitp":
+            return [
+                dict(quantity="time"),
+                dict(quantity="mdot", which_mass=1, accretion=True),
+                dict(quantity="mdot", which_mass=2, accretion=True),
+                dict(quantity="torque", which_mass="both", gravity=True),
+                dict(quantity="torque", which_mass="both", gravity=True, radial_cut=(1.0, self.domain_radius)),
+                dict(quantity="sigma_m1"),
+                dict(quantity="eccentricity_vector", radial_cut=(1.0, 6.0)),
+            ]
+        return [
+            dict(quantity="time"),
+            dict(quantity="mdot", which_mass=1, accretion=True),
+            dict(quantity="mdot", which_mass=2, accretion=True),
+            dict(quantity="fx", which_mass=1, gravity=True),
+            dict(quantity="fx", which_mass=1, accretion=True),
+            dict(quantity="fy", which_mass=1, gravity=True),
+            dict(quantity="fy", which_mass=1, accretion=True),
+            dict(quantity="fx", which_mass=2, gravity=True),
+            dict(quantity="fx", which_mass=2, accretion=True),
+            dict(quantity="fy", which_mass=2, gravity=True),
+            dict(quantity="fy", which_mass=2, accretion=True),
+        ]
+
+    @property
+    def physics(self):
+        return dict(
+            eos_type=EquationOfState.LOCALLY_ISOTHERMAL,
+            mach_number=self.mach_number,
+            point_mass_function=self.point_masses,
+            buffer_is_enabled=self.buffer_is_enabled,
+            buffer_driving_rate=100.0,
+            buffer_onset_width=1.0,
+            viscosity_coefficient=self.nu,
+            viscosity_model=ViscosityModel.CONSTANT_NU if self.nu > 0.0 else ViscosityModel.NONE,
+            diagnostics=self.diagnostics,
+        )
+
+    @property
+    def solver(self):
+        return "cbdiso_2d"
+
+    @property
+    def default_end_time(self):
+        return 1.0
+
+    @property
+    def reference_time_scale(self):
+        return 2.0 * pi
+
+    @property
+    def orbital_elements(self):
+        return OrbitalElements(semimajor_axis=1.0, total_mass=1.0, mass_ratio=self.mass_ratio,
+                               eccentricity=self.eccentricity)
+
+    def point_masses(self, time):
+        if self.single_point_mass:
+            return PointMass(softening_length=self.softening_length,
+                             sink_model=SinkModel[self.sink_model.upper()], sink_rate=self.sink_rate,
+                             sink_radius=self.sink_radius, mass=1.0)
+        return _binary_point_masses(self, time)
+
+    def checkpoint_diagnostics(self, time):
+        return dict(point_masses=self.point_masses(time), diagnostics=self.diagnostics)
+
+
+class BinaryBondi(SetupBase):
+    """A binary in a uniform wind, globally isothermal (sailfish/setups/binary_bondi.py:19-102)."""
+
+    aspect = param(1, "aspect ratio of the domain, width / height")
+    height = param(1.0, "domain height in units of the binary separation")
+    x_bin = param(0.0, "horizontal offset of binary COM from domain center")
+    sound_speed = param(1.0, "speed of sound (uniform)")
+    wind_vel = param(1.0, "horizontal speed of the background flow")
+    bh_sep = param(0.25, "black hole semi-major axis")
+    bh_mass = param(1.0, "mass of the primary")
+    sink_radius = param(0.05, "black hole sink radius")
+    sink_model = param("acceleration_free", "sink prescription")
+    sink_rate = param(1e2, "sink rate")
+    mass_ratio = param(1.0, "system mass ratio: [0.0-1.0]")
+    eccentricity = param(0.0, "eccentricity")
+    softening_length = param(0.05, "gravitational softening length", mutable=True)
+
+    def primitive(self, t, coords, primitive):
+        primitive[0] = 1.0
+        primitive[1] = self.wind_vel
+        primitive[2] = 0.0
+
+    def primitive_array(self, t, x, y):
+        out = np.zeros(np.broadcast(x, y).shape + (3,))
+        out[..., 0] = 1.0
+        out[..., 1] = self.wind_vel
+        return out
+
+    def mesh(self, resolution):
+        return PlanarCartesian2DMesh.centered_rectangle(self.height, resolution, int(self.aspect))
+
+    @property
+    def physics(self):
+        return dict(eos_type=EquationOfState.GLOBALLY_ISOTHERMAL, sound_speed=self.sound_speed,
+                    point_mass_function=self.point_masses)
+
+    @property
+    def solver(self):
+        return "cbdiso_2d"
+
+    @property
+    def orbital_elements(self):
+        return OrbitalElements(semimajor_axis=self.bh_sep, total_mass=self.bh_mass * (1 + self.mass_ratio),
+                               mass_ratio=self.mass_ratio, eccentricity=self.eccentricity)
+
+    def point_masses(self, time):
+        return _binary_point_masses(self, time, x_offset=self.x_bin)
+
+
+SETUPS = {
+    "circumbinary-disk": CircumbinaryDisk,
+    "kitp-code-comparison": KitpCodeComparison,
+    "binary-bondi": BinaryBondi,
+}
+
+
+def find_setup_class(name):
+    try:
+        return SETUPS[name]
+    except KeyError:
+        raise SetupError(f"no setup named {name}")

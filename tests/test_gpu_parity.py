@@ -1,0 +1,279 @@
+"""
+Parity of the CUDA path with the CPU oracle and the reference fixtures.
+
+Tolerances (north-star: 1e-12 relative per step, 1e-10 after 1000 steps):
+  * EXACT precision runs the reference's arithmetic operation by operation;
+    it differs from the CPU build only where CUDA's pow / exp round
+    differently from glibc's (about one ulp), so its states agree to 1e-14 of
+    each field's maximum per step.
+  * FMA and FAST precision agree to 1e-12 per step.
+The error norm per field is max|a - b| / max|b| (a pointwise relative error
+is ill-conditioned where a velocity component passes through zero).
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from cases import diagnostics, golden_names, initial_state, load, oracle_config
+from oracle import host as oh
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from sailfish_b200 import _capi, make_solver  # noqa: E402
+from sailfish_b200.cbdiso_2d import Solver  # noqa: E402
+from sailfish_b200.mesh import PlanarCartesian2DMesh  # noqa: E402
+from sailfish_b200.physics import EquationOfState, PointMass, SinkModel  # noqa: E402
+from sailfish_b200.setups import BinaryBondi, CircumbinaryDisk, KitpCodeComparison  # noqa: E402
+
+SETUPS = {"circumbinary-disk": CircumbinaryDisk, "kitp-code-comparison": KitpCodeComparison,
+          "binary-bondi": BinaryBondi}
+
+
+def field_error(a, b):
+    return max(float(np.abs(a[..., q] - b[..., q]).max() / max(np.abs(b[..., q]).max(), 1e-300)) for q in range(3))
+
+
+class _ExplosionSetup:
+    """The reference's CylindricalExplosion (isothermal): no point masses."""
+
+    boundary_condition = "outflow"
+    reference_time_scale = 1.0
+    physics = dict(eos_type=EquationOfState.GLOBALLY_ISOTHERMAL, sound_speed=1.0)
+
+    def primitive(self, t, coords, out):
+        raise AssertionError("not used: the fixture provides the initial state")
+
+
+def product_solver(d, precision="exact", **options):
+    meta = d["meta"]
+    x0, y0, x1, y1, ni, nj = meta["mesh"]
+    mesh = PlanarCartesian2DMesh(x0, y0, x1, y1, ni, nj)
+    if meta["setup"] == "cylindrical-explosion":
+        setup = _ExplosionSetup()
+        physics = dict(setup.physics)
+    else:
+        setup = SETUPS[meta["setup"]](**meta["params"])
+        physics = setup.physics
+    physics["diagnostics"] = diagnostics(meta)
+    prim = initial_state(d)
+    opts = dict(rk_order=meta["rk"], plm_theta=meta["theta"], precision=precision)
+    opts.update(options)
+    return make_solver("cbdiso_2d", physics, opts, setup=setup, mesh=mesh, solution=prim,
+                       num_patches=meta["patches"])
+
+
+SMALL = [n for n in golden_names() if not n.startswith("config0")]
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_solver_matches_reference_fixtures_exact(name):
+    d = load(name)
+    meta = d["meta"]
+    s = product_solver(d, "exact")
+    dts, series, first = [], [], None
+    for n in range(meta["steps"]):
+        dt = s.mesh.min_spacing() / s.maximum_wavespeed() * 0.3
+        s.advance(dt)
+        dts.append(dt)
+        series.append(s.reductions())
+        if n == 0:
+            first = s.solution
+    assert field_error(first, d["first"]) <= 1e-14
+    assert field_error(s.solution, d["last"]) <= 1e-13
+    np.testing.assert_allclose(dts, d["dts"], rtol=1e-13, atol=0)
+    got = np.array(series, dtype=complex)
+    want = d["series"]
+    scale = np.maximum(np.abs(want).max(axis=0), 1e-300)
+    assert (np.abs(got - want).max(axis=0) / scale).max() <= 1e-11
+    assert s.time == pytest.approx(float(d["time"]), rel=1e-14)
+
+
+@pytest.mark.parametrize("precision,tol", [("fma", 1e-12), ("fast", 1e-12)])
+@pytest.mark.parametrize("name", ["cbd_t15_n64", "kitp_t18_n64_rk3_p2", "bondi_t18_64x32"])
+def test_solver_one_step_other_precisions(name, precision, tol):
+    d = load(name)
+    s = product_solver(d, precision)
+    dt = float(d["dts"][0])
+    s.advance(dt)
+    assert field_error(s.solution, d["first"]) <= tol
+
+
+def test_config0_256_theta15_100_steps():
+    """256^2, theta 1.5, RK2, CFL 0.3, 100 steps, per-step reductions."""
+    d = load("config0_t15_n256")
+    meta = d["meta"]
+    setup = CircumbinaryDisk(**meta["params"])
+    mesh = setup.mesh(256)
+    physics = setup.physics
+    physics["diagnostics"] = diagnostics(meta)
+    from sailfish_b200.cbdiso_2d import initial_condition
+
+    prim = initial_condition(setup, mesh, 0.0)
+    assert np.array_equal(prim[::8, ::8], d["ic"])
+    prim[..., 0] += oh.seeded_noise(256, 256, meta["seed"])
+    s = make_solver("cbdiso_2d", physics, dict(rk_order=2, plm_theta=1.5), setup=setup, mesh=mesh, solution=prim)
+    series = []
+    for _ in range(meta["steps"]):
+        s.advance(mesh.min_spacing() / s.maximum_wavespeed() * 0.3)
+        series.append(s.reductions())
+    got = s.solution
+    assert field_error(got[::8, ::8], d["last_sub"]) <= 1e-12
+    np.testing.assert_allclose([got[..., q].sum() for q in range(3)], d["last_sums"], rtol=1e-12)
+    want = d["series"].real
+    got_series = np.array(series)
+    scale = np.abs(want).max(axis=0)
+    assert (np.abs(got_series - want).max(axis=0) / scale).max() <= 1e-10
+
+
+# ---------------------------------------------------------------------------
+# the four drop-in kernels through the C-ABI, on device arrays
+# ---------------------------------------------------------------------------
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _oracle_state(name):
+    d = load(name)
+    cfg = oracle_config(d["meta"])
+    s = oh.OracleSolver(cfg, initial_state(d), 0.0, oh.Kernels("oracle", cfg.plm_theta))
+    oh.run(s, 2)
+    s._set_bc()
+    return cfg, s
+
+
+@pytest.mark.parametrize("name", ["cbd_t15_n64", "kitp_t15_n56_rk1_forcefree", "bondi_t18_64x32",
+                                  "cbd_t18_n48_inactive"])
+@pytest.mark.parametrize("a", [0.0, 0.5])
+def test_dropin_advance_rk_matches_oracle(name, a):
+    cfg, s = _oracle_state(name)
+    lib = _capi.lib()
+    assert lib.cbdiso_b200_set_plm_theta(cfg.plm_theta) == 0
+    assert lib.cbdiso_b200_set_precision(0) == 0
+    lib.cbdiso_b200_set_stream(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    u0 = np.zeros_like(s.p1)
+    s.k.primitive_to_conserved(cfg.ni, cfg.nj, s.p1, u0)
+    want = np.zeros_like(s.p1)
+    m1, m2 = cfg.point_masses(s.time)
+    buf = (cfg.buffer_surface_density, m1.mass + m2.mass, cfg.buffer_driving_rate, s.buffer_outer_radius,
+           cfg.buffer_onset_width, int(cfg.buffer_is_enabled))
+    dt = 0.7 * oh.driver_dt(s, 0.3)
+    s.k.advance_rk(cfg.ni, cfg.nj, s.xl, s.xr, s.yl, s.yr, u0, s.p1, want, buf, m1, m2, cfg.sound_speed ** 2,
+                   cfg.mach_number ** 2, cfg.eos_type, cfg.nu, a, dt, cfg.velocity_ceiling, cfg.density_floor)
+    du0, dp, dw = _dev(u0), _dev(s.p1), torch.zeros(s.p1.shape, dtype=torch.float64, device="cuda")
+    st = lib.cbdiso_2d_advance_rk(cfg.ni, cfg.nj, s.xl, s.xr, s.yl, s.yr, _ptr(du0), _ptr(dp), _ptr(dw), *buf,
+                                  *m1.args(), *m2.args(), cfg.sound_speed ** 2, cfg.mach_number ** 2, cfg.eos_type,
+                                  cfg.nu, a, dt, cfg.velocity_ceiling, cfg.density_floor)
+    assert st == 0
+    got = dw.cpu().numpy()
+    ng = 2
+    assert field_error(got[ng:-ng, ng:-ng], want[ng:-ng, ng:-ng]) <= 1e-14
+    # guard zones untouched, as in the reference
+    assert not got[:ng].any() and not got[:, :ng].any()
+    assert lib.cbdiso_b200_set_plm_theta(1.8) == 0
+
+
+@pytest.mark.parametrize("name", ["cbd_t15_n64", "kitp_t18_n64_rk3_p2"])
+def test_dropin_small_kernels_match_oracle(name):
+    cfg, s = _oracle_state(name)
+    lib = _capi.lib()
+    lib.cbdiso_b200_set_stream(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    dp = _dev(s.p1)
+    # primitive_to_conserved: bit-exact
+    du = torch.zeros_like(dp)
+    assert lib.cbdiso_2d_primitive_to_conserved(cfg.ni, cfg.nj, _ptr(dp), _ptr(du)) == 0
+    u0 = np.zeros_like(s.p1)
+    s.k.primitive_to_conserved(cfg.ni, cfg.nj, s.p1, u0)
+    assert np.array_equal(du.cpu().numpy(), u0)
+    # wavespeed: bit-exact (sqrt and divide only)
+    m1, m2 = cfg.point_masses(s.time)
+    dws = torch.zeros(s.p1.shape[:2], dtype=torch.float64, device="cuda")
+    assert lib.cbdiso_2d_wavespeed(cfg.ni, cfg.nj, s.xl, s.xr, s.yl, s.yr, cfg.sound_speed ** 2,
+                                   cfg.mach_number ** 2, cfg.eos_type, *m1.args(), *m2.args(), _ptr(dp),
+                                   _ptr(dws)) == 0
+    ws = np.zeros(s.p1.shape[:2])
+    s.k.wavespeed(cfg.ni, cfg.nj, s.xl, s.xr, s.yl, s.yr, cfg.sound_speed ** 2, cfg.mach_number ** 2,
+                  cfg.eos_type, m1, m2, s.p1, ws)
+    assert np.array_equal(dws.cpu().numpy(), ws)
+    # point-mass source term, both switch settings
+    for which in (1, 2):
+        for grav, acc in ((1.0, 0.0), (0.0, 1.0)):
+            m = (m1, m2)[which - 1]
+            dr = torch.zeros_like(dp)
+            assert lib.cbdiso_2d_point_mass_source_term(cfg.ni, cfg.nj, s.xl, s.xr, s.yl, s.yr,
+                                                        *m.args(grav, acc), _ptr(dp), _ptr(dr)) == 0
+            r = np.zeros_like(s.p1)
+            s.k.point_mass_source_term(cfg.ni, cfg.nj, s.xl, s.xr, s.yl, s.yr, m.args(grav, acc), s.p1, r)
+            assert field_error(dr.cpu().numpy()[2:-2, 2:-2], r[2:-2, 2:-2]) <= 1e-15
+
+
+# ---------------------------------------------------------------------------
+# properties at larger sizes
+# ---------------------------------------------------------------------------
+
+
+def _cbd_solver(n, precision="exact", seed=11, tile=None, theta=1.5, rk=2):
+    setup = CircumbinaryDisk(domain_radius=8.0, nu=1e-3)
+    mesh = setup.mesh(n)
+    physics = setup.physics
+    physics["diagnostics"] = [dict(quantity="time"), dict(quantity="mdot", which_mass=1, accretion=True),
+                              dict(quantity="mdot", which_mass=2, accretion=True),
+                              dict(quantity="torque", which_mass="both", gravity=True)]
+    from sailfish_b200.cbdiso_2d import initial_condition
+
+    prim = initial_condition(setup, mesh, 0.0)
+    prim[..., 0] += oh.seeded_noise(n, n, seed)
+    s = make_solver("cbdiso_2d", physics, dict(rk_order=rk, plm_theta=theta, precision=precision, tile=tile),
+                    setup=setup, mesh=mesh, solution=prim)
+    return s, prim
+
+
+def test_tile_shape_does_not_change_results():
+    """Every face is computed once from the same operands whatever the tiling,
+    so different CTA tiles give bit-identical states."""
+    out = []
+    for tile in [None, (64, 4), (128, 7), (64, 33)]:
+        s, _ = _cbd_solver(200, tile=tile)
+        for _ in range(3):
+            s.advance(s.mesh.min_spacing() / s.maximum_wavespeed() * 0.3)
+        out.append(s.solution)
+    for o in out[1:]:
+        assert np.array_equal(o, out[0])
+
+
+def test_deterministic_reductions():
+    vals = []
+    for _ in range(2):
+        s, _ = _cbd_solver(300)
+        s.advance(s.mesh.min_spacing() / s.maximum_wavespeed() * 0.3)
+        vals.append((s.maximum_wavespeed(), s.reductions()))
+    assert vals[0] == vals[1]
+
+
+@pytest.mark.parametrize("n", [1024])
+def test_one_step_full_grid_against_oracle(n):
+    s, prim = _cbd_solver(n)
+    cfg = oh.Config(-8.0, 8.0, -8.0, 8.0, n, n, eos_type=2, mach_number=10.0, nu=1e-3, buffer_is_enabled=True,
+                    buffer_driving_rate=100.0, buffer_onset_width=1.0, buffer_surface_density=1.0,
+                    masses=oh.binary_masses(), plm_theta=1.5)
+    ref = oh.OracleSolver(cfg, prim, 0.0, oh.Kernels("oracle", 1.5))
+    dt = oh.driver_dt(ref, 0.3)
+    assert s.maximum_wavespeed() == pytest.approx(ref.maximum_wavespeed(), rel=1e-15)
+    ref.advance(dt)
+    s.advance(dt)
+    assert field_error(s.solution, ref.solution) <= 1e-14
+    diags = [dict(quantity="time"), dict(quantity="mdot", which_mass=1, accretion=True),
+             dict(quantity="mdot", which_mass=2, accretion=True),
+             dict(quantity="torque", which_mass="both", gravity=True)]
+    np.testing.assert_allclose(s.reductions(), ref.reductions(diags), rtol=1e-11)
