@@ -211,6 +211,12 @@ int cbdiso_b200_reduce(
     const cbd_grid_t *grid, const cbd_epilogue_t *epilogue, const double *primitive,
     double *scratch, double *result, void *stream);
 
+/* Test hook (no counterpart in the reference): evaluates the correctly
+ * rounded arithmetic the EXACT stencil is built from, on device arrays of n
+ * elements: out[4i] = a/b, out[4i+1] = a^-1.5, out[4i+2] = a^4,
+ * out[4i+3] = PLM slope of (a, b, a + b) with theta 1.5. */
+int cbdiso_b200_eval_primitives(long n, const double *a, const double *b, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -355,12 +355,13 @@ class OracleSolver:
                                       m.args(float(gravity), float(accretion)), self.p1, rate)
         return rate[NG:-NG, NG:-NG]
 
-    def reductions(self, diagnostics, num_patches=1):
+    def reductions(self, diagnostics, num_patches=1, absolute=False):
         """
         cbdiso_2d.py:370-503 with the same numpy arithmetic. `num_patches`
         reproduces the reference's summation order for a run split into that
         many slabs along i (subdivide.py:35-60): per-slab sums of per-slab
-        fields, then their sum.
+        fields, then their sum. With `absolute`, sums |f| instead of f: the
+        scale against which a cancelling sum's rounding error is judged.
         """
         c = self.cfg
         acc = [self.source_rates(1, accretion=True), self.source_rates(2, accretion=True)]
@@ -434,7 +435,8 @@ class OracleSolver:
                     f = rates[1][a:b, :, q]
                 return cut(f, rc)
 
-            return field(d).sum()
+            f = field(d)
+            return np.abs(f).sum() if absolute else f.sum()
 
         out = []
         for d in diagnostics:

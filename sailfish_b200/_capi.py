@@ -97,6 +97,8 @@ def _declare(lib):
     lib.cbdiso_b200_stage_record_bytes.restype = c_size_t
     lib.cbdiso_b200_stage_record.argtypes = [POINTER(Grid), POINTER(Stage), POINTER(Epilogue), c_void_p]
     lib.cbdiso_b200_stage_record.restype = c_int
+    lib.cbdiso_b200_eval_primitives.argtypes = [ctypes.c_long, c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.cbdiso_b200_eval_primitives.restype = c_int
     lib.cbdiso_b200_abi_sizes.argtypes = [POINTER(c_size_t)]
     lib.cbdiso_b200_abi_sizes.restype = None
     lib.cbdiso_b200_status_string.argtypes = [c_int]
@@ -128,7 +130,7 @@ def exported_symbols():
         "cbdiso_2d_wavespeed", "cbdiso_b200_set_stream", "cbdiso_b200_set_plm_theta", "cbdiso_b200_set_precision",
         "cbdiso_b200_status_string", "cbdiso_b200_version", "cbdiso_b200_scratch_bytes", "cbdiso_b200_fill_guards",
         "cbdiso_b200_advance_stage", "cbdiso_b200_reduce", "cbdiso_b200_abi_sizes",
-        "cbdiso_b200_stage_record_bytes", "cbdiso_b200_stage_record",
+        "cbdiso_b200_stage_record_bytes", "cbdiso_b200_stage_record", "cbdiso_b200_eval_primitives",
     ]
 
 

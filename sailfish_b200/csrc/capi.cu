@@ -28,7 +28,9 @@ MassDev mass_dev(const cbd_mass_t &m)
     d.soft2 = m.softening_length * m.softening_length;
     d.sink_rate = m.sink_rate;
     d.sink_radius = m.sink_radius;
+    d.inv_sink_radius = 1.0 / m.sink_radius;
     d.sink_r4 = 4.0 * m.sink_radius;
+    d.sink_hi2 = d.sink_r4 * d.sink_r4 * (1.0 + 1e-10);
     d.sink_model = m.sink_model;
     d._pad = 0;
     return d;
@@ -64,6 +66,7 @@ Consts consts_from_grid(const cbd_grid_t *g)
     k.eos = g->eos_type;
     k.cs2 = g->cs2;
     k.mach2 = g->mach2;
+    k.inv_mach2 = 1.0 / g->mach2;
     k.neg_inv_mach2 = -1.0 / g->mach2;
     k.nu = g->nu;
     k.half_nu = 0.5 * g->nu;
@@ -72,7 +75,9 @@ Consts consts_from_grid(const cbd_grid_t *g)
     k.buffer_on = g->buffer_is_enabled ? 1 : 0;
     k.buf_sigma = g->buffer_surface_density;
     k.buf_onset = g->buffer_outer_radius - g->buffer_onset_width;  // cbdiso_2d.c:229
-    k.buf_onset2 = k.buf_onset * k.buf_onset;
+    // zones with r^2 <= buf_lo2 are inside the onset radius whatever the
+    // rounding of sqrt(r^2); the square root is taken only beyond it
+    k.buf_lo2 = k.buf_onset > 0.0 ? k.buf_onset * k.buf_onset * (1.0 - 1e-10) : -1.0;
     k.buf_span = g->buffer_outer_radius - k.buf_onset;
     k.inv_buf_span = 1.0 / k.buf_span;
     return k;
@@ -142,11 +147,16 @@ StageDev stage_dev_from(const cbd_grid_t *g, const cbd_stage_t *stage, const cbd
 int set_diagnostics(Consts &k, const cbd_epilogue_t *ep, int first, int count)
 {
     k.num_diag = count;
+    k.need_rates = 0;
     for (int d = 0; d < count; ++d) {
         const cbd_diag_t &src = ep->diag[first + d];
-        if (src.quantity < CBD_Q_MDOT || src.quantity > CBD_Q_POWER)
+        if (src.quantity < CBD_Q_MDOT || src.quantity > CBD_Q_POWER || src.which_mass < 1 || src.which_mass > 3)
             return CBD_ERR_ARGUMENT;
         k.diag[d] = src;
+        const bool rate = src.quantity == CBD_Q_MDOT || src.quantity == CBD_Q_FX || src.quantity == CBD_Q_FY ||
+                          src.quantity == CBD_Q_TORQUE || src.quantity == CBD_Q_POWER;
+        if (rate)
+            k.need_rates |= (src.which_mass & 3) << (src.accretion ? 2 : 0);
     }
     return CBD_OK;
 }
@@ -418,6 +428,15 @@ int cbdiso_b200_reduce(
         first += count;
     } while (first < epilogue->num_diag);
     return CBD_OK;
+}
+
+int cbdiso_b200_eval_primitives(long n, const double *a, const double *b, double *out, void *stream)
+{
+    if (n < 0 || (n > 0 && (!a || !b || !out)))
+        return CBD_ERR_ARGUMENT;
+    if (n == 0)
+        return CBD_OK;
+    return status_of(launch_primitives(n, a, b, out, static_cast<cudaStream_t>(stream)));
 }
 
 }  // extern "C"

@@ -16,9 +16,17 @@
 //    CBD_MAX_FUSED diagnostic sums, reduced deterministically (fixed-order warp
 //    and block trees, then a last-CTA pass over per-CTA partials).
 //
-// PREC selects the arithmetic (CBD_PRECISION_*): EXACT and FMA run identical
-// source (the translation unit for EXACT is compiled with -fmad=false); FAST
-// replaces divides by reciprocal multiplies and pow(s2, -1.5) by rsqrt^3.
+// PREC selects the arithmetic (CBD_PRECISION_*). EXACT and FMA run identical
+// source (the EXACT translation unit is compiled with -fmad=false) and return
+// the reference's values: every divide, square root and power is correctly
+// rounded, as in the reference's CPU build, but computed cheaply --
+//   * a / b as a Markstein-corrected product with y = RN(1/b), hoisted to the
+//     host when b is a constant (dx, dy, mach^2, ...);
+//   * (r^2 + s^2)^-1.5 and q^4 in double-double arithmetic, rounded once;
+//   * sqrt only where a threshold test on the squared radius is undecided.
+// Only the sign of an exact zero may differ from the reference, which no
+// nonzero value depends on. FAST replaces these by uncorrected reciprocal
+// multiplies and rsqrt, staying within about an ulp per operation.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -50,20 +58,24 @@ struct Consts {
     int _pad;
     double xl, yl, dx, dy, inv_dx, inv_dy;
     double theta;
-    double cs2, mach2, neg_inv_mach2;
+    double cs2, mach2, inv_mach2, neg_inv_mach2;
     double nu, half_nu;
     double vmax, rho_min;
-    double buf_sigma, buf_onset, buf_onset2, buf_span, inv_buf_span;
+    double buf_sigma, buf_onset, buf_lo2, buf_span, inv_buf_span;
+    int need_rates;     // epilogue: bit p gravity rates of mass p, bit 2 + p accretion rates
+    int _pad2;
     cbd_diag_t diag[CBD_MAX_DIAG];
 };
 
 struct MassDev {
     double x, y, vx, vy;
     double mass;
-    double soft2;       // softening_length^2
+    double soft2;            // softening_length^2
     double sink_rate;
     double sink_radius;
-    double sink_r4;     // 4 * sink_radius
+    double inv_sink_radius;  // RN(1 / sink_radius)
+    double sink_r4;          // 4 * sink_radius
+    double sink_hi2;         // (4 sink_radius)^2 (1 + 1e-10): beyond it a zone is outside the sink
     int sink_model;
     int _pad;
 };
@@ -81,6 +93,60 @@ struct StageDev {
 
 __device__ __forceinline__ double lesser(double a, double b) { return a < b ? a : b; }
 __device__ __forceinline__ double greater(double a, double b) { return a > b ? a : b; }
+
+// a / b rounded to nearest, given y = RN(1/b): the remainder a - q b of
+// q = RN(a y) is exact under FMA, and one correction q + (a - q b) y rounds
+// to RN(a / b) for operands in the normal range (Markstein's theorem).
+template <bool FAST>
+__device__ __forceinline__ double div_by(double a, double b, double y)
+{
+    const double q = a * y;
+    if (FAST)
+        return q;
+    return fma(fma(-q, b, a), y, q);
+}
+
+template <bool FAST>
+__device__ __forceinline__ double div_rn(double a, double b)
+{
+    return div_by<FAST>(a, b, __drcp_rn(b));
+}
+
+// RN(x^-1.5) for positive normal x. 1/x and then its square root are carried
+// as double-double pairs (error-free products via FMA, one Newton correction
+// of the square root), and their product is rounded once; the result equals
+// the correctly rounded power except within ~2^-100 of a rounding midpoint.
+__device__ __forceinline__ double pow_m15_rn(double x)
+{
+    const double u = __drcp_rn(x);
+    const double u_lo = u * fma(-u, x, 1.0);
+    const double w = sqrt(u);
+    const double w_lo = (fma(-w, w, u) + u_lo) * (0.5 * w * x);
+    const double h = u * w;
+    const double h_lo = fma(u, w, -h) + (u * w_lo + u_lo * w);
+    return h + h_lo;
+}
+
+// RN(q^4): q^2 as an exact double-double pair, squared, rounded once.
+__device__ __forceinline__ double pow4_rn(double q)
+{
+    const double h = q * q;
+    const double h_lo = fma(q, q, -h);
+    const double r = h * h;
+    const double r_lo = fma(h, h, -r) + 2.0 * h * h_lo;
+    return r + r_lo;
+}
+
+// s^-1.5 for the gravity term
+template <bool FAST>
+__device__ __forceinline__ double inv_pow15(double s2)
+{
+    if (FAST) {
+        const double rs = rsqrt(s2);
+        return rs * rs * rs;
+    }
+    return (s2 > 0.0 && s2 < 1e300) ? pow_m15_rn(s2) : pow(s2, -1.5);
+}
 
 // Generalised minmod, cbdiso_2d.c:23-29. Returns exactly the value of
 // 0.25 |sgn a + sgn b| (sgn a + sgn c) min(|a|, |b|, |c|), signed zeros
@@ -114,7 +180,7 @@ __device__ __forceinline__ double potential(const MassDev *m, double x, double y
             if (FAST)
                 phi -= m[p].mass * rsqrt(s2);
             else
-                phi -= m[p].mass / sqrt(s2);
+                phi -= div_rn<false>(m[p].mass, sqrt(s2));
         }
     }
     return phi;
@@ -127,7 +193,8 @@ __device__ __forceinline__ double sound_speed2(const Consts &k, const MassDev *m
     if (k.eos == 1)
         return k.cs2;
     if (k.eos == 2)
-        return FAST ? potential<FAST>(m, x, y) * k.neg_inv_mach2 : -potential<FAST>(m, x, y) / k.mach2;
+        return FAST ? potential<FAST>(m, x, y) * k.neg_inv_mach2
+                    : div_by<false>(-potential<FAST>(m, x, y), k.mach2, k.inv_mach2);
     return 1.0;
 }
 
@@ -141,31 +208,27 @@ __device__ __forceinline__ void hlle(const double *pl, const double *pr, double 
     const double vr = DIR == 0 ? pr[1] : pr[2];
     const double gl = pl[0] * cs2;
     const double gr = pr[0] * cs2;
-    double fl0 = vl * ul0, fr0 = vr * ur0, fl1, fl2, fr1, fr2;
-    if (FAST) {
-        fl1 = DIR == 0 ? vl * ul1 + gl : vl * ul1;
-        fl2 = DIR == 1 ? vl * ul2 + gl : vl * ul2;
-        fr1 = DIR == 0 ? vr * ur1 + gr : vr * ur1;
-        fr2 = DIR == 1 ? vr * ur2 + gr : vr * ur2;
-    } else {
-        fl1 = vl * ul1 + gl * (DIR == 0 ? 1.0 : 0.0);
-        fl2 = vl * ul2 + gl * (DIR == 1 ? 1.0 : 0.0);
-        fr1 = vr * ur1 + gr * (DIR == 0 ? 1.0 : 0.0);
-        fr2 = vr * ur2 + gr * (DIR == 1 ? 1.0 : 0.0);
-    }
+    // the pressure enters only the normal-momentum flux (adding the
+    // reference's `pressure * 0` to the other components changes no value)
+    const double fl0 = vl * ul0, fr0 = vr * ur0;
+    const double fl1 = DIR == 0 ? vl * ul1 + gl : vl * ul1;
+    const double fl2 = DIR == 1 ? vl * ul2 + gl : vl * ul2;
+    const double fr1 = DIR == 0 ? vr * ur1 + gr : vr * ur1;
+    const double fr2 = DIR == 1 ? vr * ur2 + gr : vr * ur2;
     const double cs = sqrt(cs2);
     const double am = lesser(0.0, lesser(vl - cs, vr - cs));
     const double ap = greater(0.0, greater(vl + cs, vr + cs));
+    const double den = ap - am;
+    const double y = FAST ? 1.0 / den : __drcp_rn(den);
     if (FAST) {
-        const double inv = 1.0 / (ap - am);
         const double apam = ap * am;
-        f[0] = (fl0 * ap - fr0 * am - (ul0 - ur0) * apam) * inv;
-        f[1] = (fl1 * ap - fr1 * am - (ul1 - ur1) * apam) * inv;
-        f[2] = (fl2 * ap - fr2 * am - (ul2 - ur2) * apam) * inv;
+        f[0] = (fl0 * ap - fr0 * am - (ul0 - ur0) * apam) * y;
+        f[1] = (fl1 * ap - fr1 * am - (ul1 - ur1) * apam) * y;
+        f[2] = (fl2 * ap - fr2 * am - (ul2 - ur2) * apam) * y;
     } else {
-        f[0] = (fl0 * ap - fr0 * am - (ul0 - ur0) * ap * am) / (ap - am);
-        f[1] = (fl1 * ap - fr1 * am - (ul1 - ur1) * ap * am) / (ap - am);
-        f[2] = (fl2 * ap - fr2 * am - (ul2 - ur2) * ap * am) / (ap - am);
+        f[0] = div_by<false>(fl0 * ap - fr0 * am - (ul0 - ur0) * ap * am, den, y);
+        f[1] = div_by<false>(fl1 * ap - fr1 * am - (ul1 - ur1) * ap * am, den, y);
+        f[2] = div_by<false>(fl2 * ap - fr2 * am - (ul2 - ur2) * ap * am, den, y);
     }
 }
 
@@ -182,16 +245,31 @@ __device__ __forceinline__ void rho_strain(double rho, const double *gx, const d
         syy = (4.0 / 3.0) * by - (2.0 / 3.0) * ax;
         sxy = gx[2] * k.inv_dx + gy[1] * k.inv_dy;
     } else {
-        sxx = 4.0 / 3.0 * gx[1] / k.dx - 2.0 / 3.0 * gy[2] / k.dy;
-        syy = -2.0 / 3.0 * gx[1] / k.dx + 4.0 / 3.0 * gy[2] / k.dy;
-        sxy = 1.0 / 1.0 * gx[2] / k.dx + 1.0 / 1.0 * gy[1] / k.dy;
+        // 4.0 / 3.0 * gx[1] / dx - 2.0 / 3.0 * gy[2] / dy, and so on, with
+        // each quotient correctly rounded from the hoisted 1 / dx, 1 / dy
+        const double ix = k.inv_dx, iy = k.inv_dy;
+        sxx = div_by<false>(4.0 / 3.0 * gx[1], k.dx, ix) - div_by<false>(2.0 / 3.0 * gy[2], k.dy, iy);
+        syy = div_by<false>(-2.0 / 3.0 * gx[1], k.dx, ix) + div_by<false>(4.0 / 3.0 * gy[2], k.dy, iy);
+        sxy = div_by<false>(gx[2], k.dx, ix) + div_by<false>(gy[1], k.dy, iy);
     }
     rs[0] = rho * sxx;
     rs[1] = rho * sxy;
     rs[2] = rho * syy;
 }
 
+template <bool FAST>
+__device__ __forceinline__ double fourth_power(double q)
+{
+    if (FAST) {
+        const double h = q * q;
+        return h * h;
+    }
+    return pow4_rn(q);
+}
+
 // Gravity and sink terms of one mass, added into du (cbdiso_2d.c:97-175).
+// Terms that are exactly zero (no mass, or a zone outside 4 sink radii) are
+// skipped: adding them changes no value.
 template <bool FAST>
 __device__ __forceinline__ void mass_source(const MassDev &m, double x, double y, double dt, const double *p,
                                             double *du)
@@ -200,35 +278,26 @@ __device__ __forceinline__ void mass_source(const MassDev &m, double x, double y
     const double dx = x - m.x;
     const double dy = y - m.y;
     const double r2 = dx * dx + dy * dy;
-    double fx, fy, dr = 0.0, s = 0.0;
-    if (FAST) {
-        const double rs = rsqrt(r2 + m.soft2);
-        const double fnum = sigma * m.mass * (rs * rs * rs);
-        fx = -fnum * dx;
-        fy = -fnum * dy;
-        if (r2 < m.sink_r4 * m.sink_r4) {
-            dr = sqrt(r2);
-            if (dr < m.sink_r4)
-                s = m.sink_rate * exp(-pow(dr / m.sink_radius, 4.0));
-        }
-    } else {
-        dr = sqrt(r2);
-        const double fnum = sigma * m.mass * pow(r2 + m.soft2, -1.5);
-        fx = -fnum * dx;
-        fy = -fnum * dy;
-        s = (dr < m.sink_r4) ? m.sink_rate * exp(-pow(dr / m.sink_radius, 4.0)) : 0.0;
+    if (m.mass != 0.0) {
+        const double fnum = sigma * m.mass * inv_pow15<FAST>(r2 + m.soft2);
+        const double fx = -fnum * dx;
+        const double fy = -fnum * dy;
+        du[1] += fx * dt;
+        du[2] += fy * dt;
     }
+    if (m.sink_rate == 0.0 || m.sink_model < 1 || m.sink_model > 3 || !(r2 < m.sink_hi2))
+        return;
+    const double dr = sqrt(r2);
+    if (!(dr < m.sink_r4))
+        return;
+    const double s = m.sink_rate * exp(-fourth_power<FAST>(div_by<FAST>(dr, m.sink_radius, m.inv_sink_radius)));
     double mdot = 0.0;
     if (s > 0.0)
         mdot = -s * sigma;
     else if (s < 0.0)
         mdot = -s;
-
-    if (!FAST)
-        du[0] += 0.0;
-    du[1] += fx * dt;
-    du[2] += fy * dt;
-
+    if (mdot == 0.0)
+        return;
     switch (m.sink_model) {
     case 1:
         du[0] += dt * mdot;
@@ -236,39 +305,20 @@ __device__ __forceinline__ void mass_source(const MassDev &m, double x, double y
         du[2] += dt * mdot * p[2];
         break;
     case 2: {
-        // With mdot == 0 every term below adds a signed zero; that changes du
-        // only where a component is itself zero, so the divisions are skipped
-        // otherwise (FAST skips them always).
-        const bool full = FAST ? (mdot != 0.0) : (mdot != 0.0 || du[1] == 0.0 || du[2] == 0.0);
-        if (full) {
-            if (FAST && dr == 0.0 && r2 != 0.0)
-                dr = sqrt(r2);
-            const double ex = dx / (dr + 1e-12);
-            const double ey = dy / (dr + 1e-12);
-            const double dvr = (p[1] - m.vx) * ex + (p[2] - m.vy) * ey;
-            const double vxs = dvr * ex + m.vx;
-            const double vys = dvr * ey + m.vy;
-            du[0] += dt * mdot;
-            du[1] += dt * mdot * vxs;
-            du[2] += dt * mdot * vys;
-        } else {
-            du[0] += dt * mdot;
-        }
+        const double d = dr + 1e-12;
+        const double yd = FAST ? 1.0 / d : __drcp_rn(d);
+        const double ex = div_by<FAST>(dx, d, yd);
+        const double ey = div_by<FAST>(dy, d, yd);
+        const double dvr = (p[1] - m.vx) * ex + (p[2] - m.vy) * ey;
+        const double vxs = dvr * ex + m.vx;
+        const double vys = dvr * ey + m.vy;
+        du[0] += dt * mdot;
+        du[1] += dt * mdot * vxs;
+        du[2] += dt * mdot * vys;
         break;
     }
-    case 3:
-        du[0] += dt * mdot;
-        if (!FAST) {
-            du[1] += 0.0;
-            du[2] += 0.0;
-        }
-        break;
     default:
-        if (!FAST) {
-            du[0] += 0.0;
-            du[1] += 0.0;
-            du[2] += 0.0;
-        }
+        du[0] += dt * mdot;
         break;
     }
 }
@@ -280,33 +330,20 @@ __device__ __forceinline__ void buffer_source(const Consts &k, const StageDev &s
 {
     if (!k.buffer_on)
         return;
-    if (FAST) {
-        const double r2 = x * x + y * y;
-        if (r2 > k.buf_onset2) {
-            const double rc = sqrt(r2);
-            if (rc > k.buf_onset) {
-                const double irc = 1.0 / rc;
-                const double vk = sqrt(st.buffer_mass * irc);
-                const double t1 = k.buf_sigma * (-y * irc) * vk;
-                const double t2 = k.buf_sigma * (x * irc) * vk;
-                const double rate = st.buffer_k * (rc - k.buf_onset) * k.inv_buf_span * dt;
-                du[0] -= (u[0] - k.buf_sigma) * rate;
-                du[1] -= (u[1] - t1) * rate;
-                du[2] -= (u[2] - t2) * rate;
-            }
-        }
-    } else {
-        const double rc = sqrt(x * x + y * y);
-        if (rc > k.buf_onset) {
-            const double vk = sqrt(st.buffer_mass / rc);
-            const double t1 = k.buf_sigma * (-y / rc) * vk;
-            const double t2 = k.buf_sigma * (+x / rc) * vk;
-            const double rate = st.buffer_k * (rc - k.buf_onset) / k.buf_span;
-            du[0] -= (u[0] - k.buf_sigma) * rate * dt;
-            du[1] -= (u[1] - t1) * rate * dt;
-            du[2] -= (u[2] - t2) * rate * dt;
-        }
-    }
+    const double r2 = x * x + y * y;
+    if (!(r2 > k.buf_lo2))
+        return;
+    const double rc = sqrt(r2);
+    if (!(rc > k.buf_onset))
+        return;
+    const double yr = FAST ? 1.0 / rc : __drcp_rn(rc);
+    const double vk = sqrt(div_by<FAST>(st.buffer_mass, rc, yr));
+    const double t1 = k.buf_sigma * div_by<FAST>(-y, rc, yr) * vk;
+    const double t2 = k.buf_sigma * div_by<FAST>(+x, rc, yr) * vk;
+    const double rate = div_by<FAST>(st.buffer_k * (rc - k.buf_onset), k.buf_span, k.inv_buf_span);
+    du[0] -= (u[0] - k.buf_sigma) * rate * dt;
+    du[1] -= (u[1] - t1) * rate * dt;
+    du[2] -= (u[2] - t2) * rate * dt;
 }
 
 // cbdiso_2d.c:268-283
@@ -315,14 +352,9 @@ __device__ __forceinline__ void cons_to_prim(const double *u, double *p, const C
 {
     const double rho = greater(u[0], k.rho_min);
     p[0] = rho;
-    if (FAST) {
-        const double ir = 1.0 / rho;
-        p[1] = copysign(lesser(fabs(u[1] * ir), k.vmax), u[1]);
-        p[2] = copysign(lesser(fabs(u[2] * ir), k.vmax), u[2]);
-    } else {
-        p[1] = copysign(lesser(fabs(u[1] / rho), k.vmax), u[1]);
-        p[2] = copysign(lesser(fabs(u[2] / rho), k.vmax), u[2]);
-    }
+    const double y = FAST ? 1.0 / rho : __drcp_rn(rho);
+    p[1] = copysign(lesser(fabs(div_by<FAST>(u[1], rho, y)), k.vmax), u[1]);
+    p[2] = copysign(lesser(fabs(div_by<FAST>(u[2], rho, y)), k.vmax), u[2]);
 }
 
 // max |v +- cs| over both directions, cbdiso_2d.c:340-350
@@ -334,26 +366,44 @@ __device__ __forceinline__ double max_wavespeed(const double *p, double cs2)
     return greater(ax, ay);
 }
 
-// Source rates of one mass with dt = 1 and the reference's on/off switches
-// (cbdiso_2d.py:105-137, cbdiso_2d.c:626-664): r = (mdot, fx, fy).
+// Source rates of both masses at the end-of-step time with dt = 1 and the
+// reference's on/off switches (cbdiso_2d.py:105-137, cbdiso_2d.c:626-664):
+// rg[p] with gravity only, ra[p] with accretion only, each (mdot, fx, fy).
+// `need` selects which are evaluated (bit p: rg[p], bit 2 + p: ra[p]).
 template <bool FAST>
-__device__ __forceinline__ void mass_rates(const MassDev &m, bool gravity, bool accretion, double x, double y,
-                                           const double *p, double *r)
+__device__ __forceinline__ void end_rates(const MassDev *e, int need, double x, double y, const double *p,
+                                          double (&rg)[2][3], double (&ra)[2][3])
 {
-    MassDev mm = m;
-    mm.mass = m.mass * (gravity ? 1.0 : 0.0);
-    mm.sink_rate = m.sink_rate * (accretion ? 1.0 : 0.0);
-    r[0] = r[1] = r[2] = 0.0;
-    mass_source<false>(mm, x, y, 1.0, p, r);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        rg[q][0] = rg[q][1] = rg[q][2] = 0.0;
+        ra[q][0] = ra[q][1] = ra[q][2] = 0.0;
+        if (need & (1 << q)) {
+            MassDev m = e[q];
+            m.sink_rate = 0.0;
+            mass_source<FAST>(m, x, y, 1.0, p, rg[q]);
+        }
+        if (need & (4 << q)) {
+            MassDev m = e[q];
+            m.mass = 0.0;
+            mass_source<FAST>(m, x, y, 1.0, p, ra[q]);
+        }
+    }
 }
 
 // Per-zone value of one diagnostic (cbdiso_2d.py:383-471): out = (re, im).
 template <bool FAST>
-__device__ __forceinline__ void diag_value(const cbd_diag_t &d, const MassDev *m, double x, double y,
-                                           const double *p, double *out)
+__device__ __forceinline__ void diag_value(const cbd_diag_t &d, const MassDev *e, double x, double y,
+                                           const double *p, const double (&rg)[2][3], const double (&ra)[2][3],
+                                           double *out)
 {
-    const double r = sqrt(x * x + y * y);
-    const double w = d.has_cut ? ((d.r0 < r) & (r < d.r1) ? 1.0 : 0.0) : 1.0;
+    double w = 1.0, r = 0.0;
+    const bool polar = d.quantity == CBD_Q_SIGMA_M1 || d.quantity == CBD_Q_ECCENTRICITY_VECTOR;
+    if (d.has_cut || polar) {
+        r = sqrt(x * x + y * y);
+        if (d.has_cut)
+            w = ((d.r0 < r) & (r < d.r1)) ? 1.0 : 0.0;
+    }
     out[0] = 0.0;
     out[1] = 0.0;
     switch (d.quantity) {
@@ -362,24 +412,18 @@ __device__ __forceinline__ void diag_value(const cbd_diag_t &d, const MassDev *m
     case CBD_Q_FY:
     case CBD_Q_TORQUE:
     case CBD_Q_POWER: {
-        // the reference picks the accretion rates when both flags are set
-        // (cbdiso_2d.py:457-462)
-        double f[3] = {0.0, 0.0, 0.0};
-        const bool a = d.accretion != 0, g = d.gravity != 0 && !a;
-        if (d.which_mass & 1) {
-            double t[3];
-            mass_rates<FAST>(m[0], g, a, x, y, p, t);
-            f[0] = t[0]; f[1] = t[1]; f[2] = t[2];
+        // the reference takes the accretion rates when both flags are set
+        const bool acc = d.accretion != 0;
+        double r1[3], r2[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            r1[c] = acc ? ra[0][c] : rg[0][c];
+            r2[c] = acc ? ra[1][c] : rg[1][c];
         }
-        if (d.which_mass & 2) {
-            double t[3];
-            mass_rates<FAST>(m[1], g, a, x, y, p, t);
-            if (d.which_mass & 1) {
-                f[0] += t[0]; f[1] += t[1]; f[2] += t[2];
-            } else {
-                f[0] = t[0]; f[1] = t[1]; f[2] = t[2];
-            }
-        }
+        double f[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            f[c] = d.which_mass == 3 ? r1[c] + r2[c] : (d.which_mass == 2 ? r2[c] : r1[c]);
         if (d.quantity == CBD_Q_MDOT)
             out[0] = f[0] * w;
         else if (d.quantity == CBD_Q_FX)
@@ -389,7 +433,7 @@ __device__ __forceinline__ void diag_value(const cbd_diag_t &d, const MassDev *m
         else if (d.quantity == CBD_Q_TORQUE)
             out[0] = x * (f[2] * w) - y * (f[1] * w);
         else {
-            const MassDev &mv = m[d.which_mass == 2 ? 1 : 0];
+            const MassDev &mv = e[d.which_mass == 2 ? 1 : 0];
             out[0] = mv.vx * (f[1] * w) + mv.vy * (f[2] * w);
         }
         break;
@@ -416,6 +460,29 @@ __device__ __forceinline__ void diag_value(const cbd_diag_t &d, const MassDev *m
         break;
     default:
         break;
+    }
+}
+
+// The end-of-step quantities of one zone, accumulated into acc: slot 0 the
+// CFL wavespeed maximum, slots 1 + 2d, 2 + 2d the diagnostics.
+template <bool FAST>
+__device__ __forceinline__ void accumulate_zone(const Consts &k, const MassDev *e, double x, double y,
+                                                const double *p, double (&acc)[PARTIAL_STRIDE])
+{
+    if (k.want_ws)
+        acc[0] = greater(acc[0], max_wavespeed(p, sound_speed2<FAST>(k, e, x, y)));
+    if (k.num_diag > 0) {
+        double rg[2][3], ra[2][3];
+        end_rates<FAST>(e, k.need_rates, x, y, p, rg, ra);
+#pragma unroll
+        for (int d = 0; d < MAX_FUSED; ++d) {
+            if (d < k.num_diag) {
+                double v[2];
+                diag_value<FAST>(k.diag[d], e, x, y, p, rg, ra, v);
+                acc[1 + 2 * d] += v[0];
+                acc[2 + 2 * d] += v[1];
+            }
+        }
     }
 }
 
@@ -705,10 +772,7 @@ __global__ void __launch_bounds__(BJ) stage_kernel(const Consts k, const StageDe
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
                 const double gn = sg[q][t + 1], gs = sg[q][t];
-                if (FAST)
-                    du[q] -= ((f1[q] - f0[q]) * k.inv_dx + (gn - gs) * k.inv_dy) * dt;
-                else
-                    du[q] -= ((f1[q] - f0[q]) / k.dx + (gn - gs) / k.dy) * dt;
+                du[q] -= (div_by<FAST>(f1[q] - f0[q], k.dx, k.inv_dx) + div_by<FAST>(gn - gs, k.dy, k.inv_dy)) * dt;
             }
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
@@ -732,19 +796,7 @@ __global__ void __launch_bounds__(BJ) stage_kernel(const Consts k, const StageDe
                 }
             }
 
-            if (k.want_ws) {
-                const double c2 = sound_speed2<FAST>(k, st.e, xc, yc);
-                acc[0] = greater(acc[0], max_wavespeed(pn, c2));
-            }
-#pragma unroll
-            for (int d = 0; d < MAX_FUSED; ++d) {
-                if (d < k.num_diag) {
-                    double v[2];
-                    diag_value<FAST>(k.diag[d], st.e, xc, yc, pn, v);
-                    acc[1 + 2 * d] += v[0];
-                    acc[2 + 2 * d] += v[1];
-                }
-            }
+            accumulate_zone<FAST>(k, st.e, xc, yc, pn, acc);
         }
 
 #pragma unroll

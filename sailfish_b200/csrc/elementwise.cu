@@ -90,21 +90,25 @@ __global__ void __launch_bounds__(BJ) reduce_kernel(const Consts k, const StageD
         const double pz[3] = {pc[0], pc[1], pc[2]};
         const double xc = k.xl + (i + 0.5) * k.dx;
         const double yc = k.yl + (j + 0.5) * k.dy;
-        if (k.want_ws)
-            acc[0] = greater(acc[0], max_wavespeed(pz, sound_speed2<false>(k, st.e, xc, yc)));
-#pragma unroll
-        for (int d = 0; d < MAX_FUSED; ++d) {
-            if (d < k.num_diag) {
-                double v[2];
-                diag_value<false>(k.diag[d], st.e, xc, yc, pz, v);
-                acc[1 + 2 * d] += v[0];
-                acc[2 + 2 * d] += v[1];
-            }
-        }
+        accumulate_zone<false>(k, st.e, xc, yc, pz, acc);
     }
     double red[PARTIAL_STRIDE];
     block_reduce<BJ>(acc, sred, red);
     grid_finish<BJ>(red, 1 + 2 * k.num_diag, scratch, out0, out_rest, sred);
+}
+
+// Evaluates the stencil's correctly rounded arithmetic on arrays, so tests
+// can compare it with IEEE division and high-precision powers:
+// out[4i] = a / b, out[4i+1] = a^-1.5, out[4i+2] = a^4, out[4i+3] = the
+// limited slope of (a, b, a + b) with theta = 1.5.
+__global__ void primitives_kernel(long n, const double *a, const double *b, double *out)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        out[4 * i] = div_rn<false>(a[i], b[i]);
+        out[4 * i + 1] = pow_m15_rn(a[i]);
+        out[4 * i + 2] = pow4_rn(a[i]);
+        out[4 * i + 3] = limited_slope(a[i], b[i], a[i] + b[i], 1.5);
+    }
 }
 
 inline int blocks_for(long n, int bs, int cap)
@@ -141,6 +145,12 @@ cudaError_t launch_fill_guards(int ni, int nj, double *p, cudaStream_t s)
 {
     const long n = (long)(ni + 2 * NG) * (nj + 2 * NG);
     fill_guards_kernel<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(ni, nj, p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_primitives(long n, const double *a, const double *b, double *out, cudaStream_t s)
+{
+    primitives_kernel<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, a, b, out);
     return cudaGetLastError();
 }
 

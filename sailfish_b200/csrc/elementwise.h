@@ -12,6 +12,7 @@ cudaError_t launch_wavespeed(const Consts &k, const MassDev &m0, const MassDev &
                              cudaStream_t s);
 cudaError_t launch_fill_guards(int ni, int nj, double *p, cudaStream_t s);
 int reduce_ctas(int ni, int nj);
+cudaError_t launch_primitives(long n, const double *a, const double *b, double *out, cudaStream_t s);
 cudaError_t launch_reduce(const Consts &k, const StageDev &st, const double *p, double *scratch, double *out0,
                           double *out_rest, cudaStream_t s);
 

@@ -89,8 +89,12 @@ def test_solver_matches_reference_fixtures_exact(name):
     np.testing.assert_allclose(dts, d["dts"], rtol=1e-13, atol=0)
     got = np.array(series, dtype=complex)
     want = d["series"]
-    scale = np.maximum(np.abs(want).max(axis=0), 1e-300)
-    assert (np.abs(got - want).max(axis=0) / scale).max() <= 1e-11
+    # sums such as torque and sigma_m1 cancel: judge them against sum |f| dA
+    cfg = oracle_config(meta)
+    o = oh.OracleSolver(cfg, d["last"], float(d["time"]), oh.Kernels("oracle", cfg.plm_theta))
+    scale = np.abs(np.array(o.reductions(diagnostics(meta), absolute=True), dtype=complex))
+    scale = np.maximum(scale, np.abs(want).max(axis=0))
+    assert (np.abs(got - want).max(axis=0) / np.maximum(scale, 1e-300)).max() <= 1e-12
     assert s.time == pytest.approx(float(d["time"]), rel=1e-14)
 
 
@@ -124,10 +128,15 @@ def test_config0_256_theta15_100_steps():
         series.append(s.reductions())
     got = s.solution
     assert field_error(got[::8, ::8], d["last_sub"]) <= 1e-12
-    np.testing.assert_allclose([got[..., q].sum() for q in range(3)], d["last_sums"], rtol=1e-12)
+    # the velocity sums cancel: compare them against the sum of magnitudes
+    for q in range(3):
+        assert abs(got[..., q].sum() - d["last_sums"][q]) <= 1e-12 * np.abs(got[..., q]).sum()
     want = d["series"].real
     got_series = np.array(series)
-    scale = np.abs(want).max(axis=0)
+    cfg = oracle_config(meta)
+    full = got.copy()
+    o = oh.OracleSolver(cfg, full, s.time, oh.Kernels("oracle", 1.5))
+    scale = np.maximum(np.array(o.reductions(diagnostics(meta), absolute=True)), np.abs(want).max(axis=0))
     assert (np.abs(got_series - want).max(axis=0) / scale).max() <= 1e-10
 
 
@@ -276,4 +285,5 @@ def test_one_step_full_grid_against_oracle(n):
     diags = [dict(quantity="time"), dict(quantity="mdot", which_mass=1, accretion=True),
              dict(quantity="mdot", which_mass=2, accretion=True),
              dict(quantity="torque", which_mass="both", gravity=True)]
-    np.testing.assert_allclose(s.reductions(), ref.reductions(diags), rtol=1e-11)
+    scale = np.array(ref.reductions(diags, absolute=True))
+    assert np.all(np.abs(np.array(s.reductions()) - np.array(ref.reductions(diags))) <= 1e-12 * scale)
