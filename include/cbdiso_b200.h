@@ -130,7 +130,7 @@ typedef struct cbd_grid {
     int buffer_is_enabled;
     int tile_columns;       /* CTA strip width: 64 or 128; 0 = library default */
     int tile_rows;          /* rows per CTA segment; 0 = library default */
-    int _pad1;
+    int tile_occupancy;     /* resident CTAs per SM the kernel is built for: 0 default, 5 or 6 (128 wide), 10 or 12 (64 wide) */
     double buffer_surface_density;
     double buffer_driving_rate;
     double buffer_outer_radius;

@@ -49,7 +49,7 @@ class Grid(Structure):
                 ("yr", c_double), ("plm_theta", c_double), ("eos_type", c_int), ("precision", c_int),
                 ("cs2", c_double), ("mach2", c_double), ("nu", c_double), ("velocity_ceiling", c_double),
                 ("density_floor", c_double), ("buffer_is_enabled", c_int), ("tile_columns", c_int),
-                ("tile_rows", c_int), ("_pad1", c_int), ("buffer_surface_density", c_double),
+                ("tile_rows", c_int), ("tile_occupancy", c_int), ("buffer_surface_density", c_double),
                 ("buffer_driving_rate", c_double), ("buffer_outer_radius", c_double),
                 ("buffer_onset_width", c_double)]
 

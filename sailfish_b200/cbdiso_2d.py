@@ -21,8 +21,8 @@ only its reduction summation order depends on it.
 Extra solver options beyond the reference's (velocity_ceiling, density_floor,
 rk_order): `plm_theta` (default 1.8, the reference's compile-time
 PLM_THETA), `precision` ("exact" | "fma" | "fast"), `fuse_reductions`, and
-`tile` ((columns, rows) of the stage kernel's CTA tile, or None for the
-library default).
+`tile` ((columns, rows[, occupancy]) of the stage kernel's CTA tile, or
+None for the library default).
 """
 
 from __future__ import annotations
@@ -197,6 +197,8 @@ class Solver(SolverBase):
         g.buffer_onset_width = physics.buffer_onset_width
         if options.tile:
             g.tile_columns, g.tile_rows = int(options.tile[0]), int(options.tile[1])
+            if len(options.tile) > 2:
+                g.tile_occupancy = int(options.tile[2])
         self._grid = g
 
         f64 = dict(dtype=torch.float64, device=self.device)

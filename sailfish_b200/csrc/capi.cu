@@ -90,9 +90,14 @@ double buffer_k(double driving_rate, double central_mass, double onset)
     return driving_rate * std::sqrt(central_mass * std::pow(onset, -3.0));
 }
 
-LaunchShape stage_shape(int ni, int nj, int bj, int rows)
+LaunchShape stage_shape(int ni, int nj, int bj, int rows, int occupancy = 0)
 {
     LaunchShape s;
+    s.minb = 1;
+    if (bj == 128 && (occupancy == 5 || occupancy == 6))
+        s.minb = occupancy;
+    if (bj == 64 && (occupancy == 10 || occupancy == 12))
+        s.minb = occupancy;
     if (bj != 64 && bj != 128)
         bj = nj > 96 ? 128 : 64;
     const int strips = (nj + bj - 1) / bj;
@@ -391,7 +396,7 @@ int cbdiso_b200_advance_stage(
         if (rc != CBD_OK)
             return rc;
     }
-    const LaunchShape s = stage_shape(grid->ni, grid->nj, grid->tile_columns, grid->tile_rows);
+    const LaunchShape s = stage_shape(grid->ni, grid->nj, grid->tile_columns, grid->tile_rows, grid->tile_occupancy);
     k.rows_per_cta = s.rows;
     StageArgs args = {primitive_rd, primitive_n, primitive_wr, static_cast<const StageDev *>(stage_dev), scratch,
                       result};

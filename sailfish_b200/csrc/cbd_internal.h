@@ -7,8 +7,9 @@
 namespace cbd {
 
 struct LaunchShape {
-    int bj;        // threads per CTA = columns per strip (64, 128, 256)
+    int bj;        // threads per CTA = columns per strip (64, 128)
     int rows;      // rows per CTA
+    int minb;      // occupancy target (resident CTAs per SM) the kernel is compiled for; 1 = none
     dim3 grid;
 };
 

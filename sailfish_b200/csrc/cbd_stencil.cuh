@@ -587,8 +587,8 @@ struct StageArgs {
     double *result;      // reductions result (epilogue only)
 };
 
-template <int BJ, int PREC>
-__global__ void __launch_bounds__(BJ) stage_kernel(const Consts k, const StageDev st_param, StageArgs args)
+template <int BJ, int MINB, int PREC>
+__global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const StageDev st_param, StageArgs args)
 {
     constexpr bool FAST = PREC == CBD_PRECISION_FAST;
     constexpr int W4 = BJ + 4;
