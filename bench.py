@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--precision", default="exact", choices=["exact", "fma", "fast"])
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--tile", default=None, help="columns,rows,occupancy of the stage kernel (default: library)")
     return p.parse_args()
 
 
@@ -165,7 +166,9 @@ def run_ours(args, rank, world):
     zones = n * n
 
     def fresh():
-        return make_solver("cbdiso_2d", physics, dict(rk_order=2, plm_theta=THETA, precision=args.precision),
+        tile = tuple(int(v) for v in args.tile.split(",")) if args.tile else None
+        return make_solver("cbdiso_2d", physics,
+                           dict(rk_order=2, plm_theta=THETA, precision=args.precision, tile=tile),
                            setup=setup, mesh=mesh, solution=prim)
 
     solver = fresh()

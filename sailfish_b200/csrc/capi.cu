@@ -90,22 +90,28 @@ double buffer_k(double driving_rate, double central_mass, double onset)
     return driving_rate * std::sqrt(central_mass * std::pow(onset, -3.0));
 }
 
+// Launch shape of the stage kernel. Defaults: 128-column strips compiled for
+// 6 resident CTAs per SM (64-column strips and 12 CTAs for narrow grids), and
+// the largest row count <= 32 that still gives at least two full waves.
 LaunchShape stage_shape(int ni, int nj, int bj, int rows, int occupancy = 0)
 {
     LaunchShape s;
+    if (bj != 64 && bj != 128) {
+        bj = nj > 96 ? 128 : 64;
+        if (occupancy == 0)
+            occupancy = bj == 128 ? 6 : 12;
+    }
     s.minb = 1;
     if (bj == 128 && (occupancy == 5 || occupancy == 6))
         s.minb = occupancy;
     if (bj == 64 && (occupancy == 10 || occupancy == 12))
         s.minb = occupancy;
-    if (bj != 64 && bj != 128)
-        bj = nj > 96 ? 128 : 64;
     const int strips = (nj + bj - 1) / bj;
     if (rows <= 0) {
-        const int target = 4 * 148;
-        const int segs = (target + strips - 1) / strips;
-        rows = (ni + segs - 1) / segs;
-        rows = rows < 4 ? 4 : (rows > 64 ? 64 : rows);
+        const int slots = 148 * (s.minb > 1 ? s.minb : 4);
+        rows = 32;
+        while (rows > 8 && (long)strips * ((ni + rows - 1) / rows) < 2L * slots)
+            rows /= 2;
     }
     if (rows < 4)
         rows = 4;
@@ -324,6 +330,8 @@ int cbdiso_2d_wavespeed(
     k.eos = eos_type;
     k.cs2 = soundspeed2;
     k.mach2 = mach_squared;
+    k.inv_mach2 = 1.0 / mach_squared;
+    k.neg_inv_mach2 = -1.0 / mach_squared;
     const MassDev m0 = mass_dev(x1, y1, vx1, vy1, mass1, softening_length1, sink_rate1, sink_radius1, sink_model1);
     const MassDev m1 = mass_dev(x2, y2, vx2, vy2, mass2, softening_length2, sink_rate2, sink_radius2, sink_model2);
     return status_of(launch_wavespeed(k, m0, m1, primitive, wavespeed, g_stream));
