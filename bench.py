@@ -29,6 +29,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_ZONE_UPDATE = 120.0  # RK2 x FP64 x 3 fields: 48 B stage 1 + 72 B stage 2
+# DRAM bytes per zone and stage launch measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum, mean of an RK2 stage 1 and stage 2 launch at 2048^2,
+# profiles/stage_kernel_2048_exact_full.md); scaled by the zone count.
+NCU_TRAFFIC_PER_ZONE_LAUNCH = (108.9e6 + 74.2e6 + 213.7e6 + 69.8e6) / 2 / 2048 ** 2
 DIAGNOSTICS = [dict(quantity="time"), dict(quantity="mdot", which_mass=1, accretion=True),
                dict(quantity="mdot", which_mass=2, accretion=True),
                dict(quantity="torque", which_mass="both", gravity=True)]
@@ -229,7 +233,8 @@ def run_ours(args, rank, world):
     peak, peak_kind = measured_peaks()
     achieved = BYTES_PER_ZONE_UPDATE / 2 * zones / kernel_s / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                "frac": round(achieved / peak, 4), "traffic": round(NCU_TRAFFIC_PER_ZONE_LAUNCH * zones),
+                "traffic_source": "ncu at 2048^2 scaled by zones", "peak_source": peak_kind,
                 "kernel": "stage_kernel (one fused RK stage)", "kernel_ms": round(kernel_s * 1e3, 4),
                 "bytes_per_launch": BYTES_PER_ZONE_UPDATE / 2 * zones}
 
