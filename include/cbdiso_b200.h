@@ -206,6 +206,30 @@ size_t cbdiso_b200_stage_record_bytes(void);
 int cbdiso_b200_stage_record(const cbd_grid_t *grid, const cbd_stage_t *stage, const cbd_epilogue_t *epilogue,
                              void *record);
 
+/* cbdiso_b200_advance_stage without a scratch argument (no counterpart in the
+ * reference, whose kernels take only the solver's own arrays).
+ *
+ * Some callers cannot allocate device memory: a binding written against the
+ * reference's kernel interface passes only the arrays its solver already owns
+ * and has no buffer to offer as scratch, and host applications that account
+ * for all device memory through their own pool do not let a library call
+ * cudaMalloc behind their back. This entry point allocates nothing. The
+ * epilogue's reductions scratch is a fixed 5 MiB array inside the library's
+ * device memory (each GPU that loads the library holds it until the process
+ * exits); the caller still passes the state arrays and `result`.
+ *
+ * Limit: grids whose cbdiso_b200_scratch_bytes() exceeds 5 MiB are rejected
+ * with CBD_ERR_CAPACITY before anything is launched; 4096 x 4096 fits.
+ * The first call with an epilogue on a device looks up the array's device
+ * address for that device, so make that first call before any stream
+ * capture. All calls on a device share the array, which keeps the last
+ * call's contents (each call clears the counter it needs zeroed): calls that
+ * overlap on the GPU, from different streams or threads, race on it. */
+int cbdiso_b200_advance_stage_noalloc(
+    const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
+    const double *primitive_rd, const double *primitive_n, double *primitive_wr,
+    const cbd_epilogue_t *epilogue, double *result, void *stream);
+
 /* The epilogue quantities alone, on a given state (guards not needed). */
 int cbdiso_b200_reduce(
     const cbd_grid_t *grid, const cbd_epilogue_t *epilogue, const double *primitive,

@@ -85,6 +85,7 @@ def _declare(lib):
         "cbdiso_b200_version": [],
         "cbdiso_b200_fill_guards": [POINTER(Grid), P, V],
         "cbdiso_b200_advance_stage": [POINTER(Grid), POINTER(Stage), P, P, P, P, POINTER(Epilogue), P, P, V],
+        "cbdiso_b200_advance_stage_noalloc": [POINTER(Grid), POINTER(Stage), P, P, P, P, POINTER(Epilogue), P, V],
         "cbdiso_b200_reduce": [POINTER(Grid), POINTER(Epilogue), P, P, P, V],
     }
     for name, args in sig.items():
@@ -131,6 +132,7 @@ def exported_symbols():
         "cbdiso_b200_status_string", "cbdiso_b200_version", "cbdiso_b200_scratch_bytes", "cbdiso_b200_fill_guards",
         "cbdiso_b200_advance_stage", "cbdiso_b200_reduce", "cbdiso_b200_abi_sizes",
         "cbdiso_b200_stage_record_bytes", "cbdiso_b200_stage_record", "cbdiso_b200_eval_primitives",
+        "cbdiso_b200_advance_stage_noalloc",
     ]
 
 
