@@ -575,6 +575,21 @@ __device__ void grid_finish(const double (&mine)[PARTIAL_STRIDE], int n, double 
 }
 
 // ---------------------------------------------------------------------------
+// asynchronous global -> shared copies (cp.async), used to fetch the next row
+// of the march one iteration ahead of its use
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void async_copy8(void *smem, const void *gmem)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+__device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// ---------------------------------------------------------------------------
 // the fused stage kernel
 // ---------------------------------------------------------------------------
 
@@ -596,6 +611,7 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
     __shared__ double sgy[2][NQ][BJ + 2];  // y-slopes ring, columns c0-1 .. c0+BJ
     __shared__ double srs[2][NQ][BJ + 2];  // rho * strain ring, same columns
     __shared__ double sg[NQ][BJ + 1];      // y-face fluxes of the current row
+    __shared__ double sun[2][NQ][BJ];      // u_n source zones, fetched one row ahead
     __shared__ StageDev st;
     __shared__ double sred[PARTIAL_STRIDE * (BJ / 32)];
 
@@ -616,14 +632,32 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
     auto zone = [&](const double *base, int i, int jj) -> const double * {
         return base + (size_t)(i + NG) * row_stride + (size_t)(jj + NG) * NQ;
     };
-    auto load_row = [&](int slot, int i) {
+    // Row i (zones c0-2 .. c0+W+1) into ring slot `slot`, as asynchronous
+    // copies: coalesced over the row's contiguous AoS bytes, scattered into
+    // the field-major shared layout.
+    auto fetch_row = [&](int slot, int i) {
         const double *src = args.prd + (size_t)(i + NG) * row_stride + (size_t)c0 * NQ;
         const int n = NQ * (W + 4);
         for (int d = t; d < n; d += BJ) {
             const int kk = d / 3;
-            sp[slot][d - 3 * kk][kk] = __ldg(src + d);
+            async_copy8(&sp[slot][d - 3 * kk][kk], src + d);
         }
     };
+    // The zone (i, j) of the u_n source array, for this thread's own update.
+    // In the in-place final stage this array is also written, by the same
+    // thread and only after the zone has been consumed.
+    auto fetch_un = [&](int i) {
+        if (k.un_kind != 0 && active) {
+            const double *z = zone(args.un, i, j);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+                async_copy8(&sun[i & 1][q][t], z + q);
+        }
+    };
+    // Lanes that do the strip's extra work, spread over different warps: the
+    // slopes of the two halo columns, and the last y-face of the row.
+    constexpr int HALO_LANE = BJ >= 64 ? 32 : 0;
+    constexpr int FACE_LANE = BJ >= 128 ? 64 : (BJ >= 64 ? 0 : 2);
 
     // per-thread epilogue accumulators
     double acc[PARTIAL_STRIDE];
@@ -634,21 +668,31 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
     // own-column carried state: x-slope and rho*strain of row r, x-face flux F(r - 1/2)
     double gx0[NQ] = {0.0, 0.0, 0.0}, rs0[NQ] = {0.0, 0.0, 0.0}, f0[NQ] = {0.0, 0.0, 0.0};
 
-    load_row((r0 - 2) & 3, r0 - 2);
-    load_row((r0 - 1) & 3, r0 - 1);
+    fetch_row((r0 - 2) & 3, r0 - 2);
+    fetch_row((r0 - 1) & 3, r0 - 1);
+    fetch_row(r0 & 3, r0);
+    async_commit();
 
     for (int r = r0 - 2; r < r1; ++r) {
-        load_row((r + 2) & 3, r + 2);
+        // rows r .. r + 2 (and the u_n zone of row r) were fetched one
+        // iteration ago; after the barrier the slot of row r - 1 is free
+        async_wait_all();
         __syncthreads();
+        if (r + 3 <= r1 + 1)
+            fetch_row((r + 3) & 3, r + 3);
+        if (r + 1 >= r0 && r + 1 < r1)
+            fetch_un(r + 1);
+        async_commit();
 
         const int s0 = r & 3, s1 = (r + 1) & 3, s2 = (r + 2) & 3;
         const int g1 = (r + 1) & 1, g0 = r & 1;
 
         // (1) slopes and rho * strain at row r + 1: own column, plus the two
-        //     halo columns (c0 - 1 and c0 + W) handled by lanes 0 and 1.
+        //     halo columns (c0 - 1 and c0 + W) handled by two lanes of one warp.
         double gx1[NQ] = {0.0, 0.0, 0.0}, rs1[NQ] = {0.0, 0.0, 0.0};
         {
-            const int passes = (t < 2) ? 2 : 1;
+            const bool halo = t == HALO_LANE || t == HALO_LANE + 1;
+            const int passes = halo ? 2 : 1;
             for (int pass = 0; pass < passes; ++pass) {
                 int kk;  // sp column index
                 if (pass == 0) {
@@ -656,7 +700,7 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
                         continue;
                     kk = t + 2;
                 } else {
-                    kk = (t == 0) ? 1 : W + 2;
+                    kk = (t == HALO_LANE) ? 1 : W + 2;
                 }
                 double gx[NQ], gy[NQ], rs[NQ] = {0.0, 0.0, 0.0};
 #pragma unroll
@@ -701,9 +745,9 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
             }
         }
 
-        // (3) y-face fluxes of row r: face c0 + f - 1/2 for f = t, plus f = W by lane 2
+        // (3) y-face fluxes of row r: face c0 + f - 1/2 for f = t, plus f = W
         if (r >= r0) {
-            const int passes = (t == 2) ? 2 : 1;
+            const int passes = (t == FACE_LANE) ? 2 : 1;
             for (int pass = 0; pass < passes; ++pass) {
                 int fidx;
                 if (pass == 0) {
@@ -752,9 +796,7 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
                 un[1] = u[1];
                 un[2] = u[2];
             } else {
-                // plain loads: in the in-place final stage this array is also written
-                const double *z = zone(args.un, r, j);
-                const double z0 = z[0], z1 = z[1], z2 = z[2];
+                const double z0 = sun[r & 1][0][t], z1 = sun[r & 1][1][t], z2 = sun[r & 1][2][t];
                 if (k.un_kind == 1) {
                     un[0] = z0;
                     un[1] = z1 * z0;
