@@ -230,6 +230,40 @@ int cbdiso_b200_advance_stage_noalloc(
     const double *primitive_rd, const double *primitive_n, double *primitive_wr,
     const cbd_epilogue_t *epilogue, double *result, void *stream);
 
+/* ------------------------------------------------------------------------
+ * device-resident stepping (no counterpart in the reference, whose driver
+ * computes dt and the point masses on the host every step)
+ * ---------------------------------------------------------------------- */
+
+/* A binary on a Kepler orbit with identical sink / softening settings for
+ * both components, as the circumbinary setups build it
+ * (sailfish/setups/circumbinary_disk.py:185-212, binary_bondi.py:79-102). */
+typedef struct cbd_orbit {
+    double semimajor_axis, total_mass, mass_ratio, eccentricity;
+    double softening_length, sink_rate, sink_radius;
+    int sink_model;
+    int has_x_offset;       /* shift both x positions by x_offset */
+    double x_offset;
+} cbd_orbit_t;
+
+/* Size of the stepper's device record, and its initial contents (written to
+ * host memory; the caller copies it to device memory). The stepper keeps the
+ * time, the last dt and a status word; min_spacing is the mesh's
+ * min(dx, dy) as the driver uses it; fixed_dt > 0 freezes dt. */
+size_t cbdiso_b200_stepper_bytes(void);
+int cbdiso_b200_stepper_init(const cbd_grid_t *grid, const cbd_orbit_t *orbit, int rk_order, double time,
+                             double cfl, double min_spacing, double fixed_dt, int series_capacity, void *stepper);
+
+/* One step's prologue (a single-thread kernel): records the previous step's
+ * time-series row [time, dt, max wavespeed, num_values reduction values] from
+ * `result` into `series` (if non-null), then, unless `finalize`, takes
+ * dt = min_spacing / max wavespeed * cfl, solves the Kepler orbit at every
+ * stage time and at the end of the step, and writes the stage records that
+ * cbdiso_b200_advance_stage reads as `stage_dev`. A Kepler solve that does
+ * not converge sets the stepper's status to CBD_ERR_KEPLER and stops it. */
+int cbdiso_b200_step_prologue(void *stepper_dev, const double *result, void *records_dev, double *series,
+                              int num_values, int finalize, void *stream);
+
 /* The epilogue quantities alone, on a given state (guards not needed). */
 int cbdiso_b200_reduce(
     const cbd_grid_t *grid, const cbd_epilogue_t *epilogue, const double *primitive,

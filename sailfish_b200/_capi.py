@@ -63,6 +63,12 @@ class Diag(Structure):
                 ("has_cut", c_int), ("_pad", c_int), ("r0", c_double), ("r1", c_double)]
 
 
+class Orbit(Structure):
+    _fields_ = [("semimajor_axis", c_double), ("total_mass", c_double), ("mass_ratio", c_double),
+                ("eccentricity", c_double), ("softening_length", c_double), ("sink_rate", c_double),
+                ("sink_radius", c_double), ("sink_model", c_int), ("has_x_offset", c_int), ("x_offset", c_double)]
+
+
 class Epilogue(Structure):
     _fields_ = [("mass", Mass * 2), ("want_wavespeed", c_int), ("num_diag", c_int), ("diag", Diag * MAX_DIAG)]
 
@@ -100,6 +106,13 @@ def _declare(lib):
     lib.cbdiso_b200_stage_record.restype = c_int
     lib.cbdiso_b200_eval_primitives.argtypes = [ctypes.c_long, c_void_p, c_void_p, c_void_p, c_void_p]
     lib.cbdiso_b200_eval_primitives.restype = c_int
+    lib.cbdiso_b200_stepper_bytes.argtypes = []
+    lib.cbdiso_b200_stepper_bytes.restype = c_size_t
+    lib.cbdiso_b200_stepper_init.argtypes = [POINTER(Grid), POINTER(Orbit), c_int, c_double, c_double, c_double,
+                                             c_double, c_int, c_void_p]
+    lib.cbdiso_b200_stepper_init.restype = c_int
+    lib.cbdiso_b200_step_prologue.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]
+    lib.cbdiso_b200_step_prologue.restype = c_int
     lib.cbdiso_b200_abi_sizes.argtypes = [POINTER(c_size_t)]
     lib.cbdiso_b200_abi_sizes.restype = None
     lib.cbdiso_b200_status_string.argtypes = [c_int]
@@ -132,7 +145,8 @@ def exported_symbols():
         "cbdiso_b200_status_string", "cbdiso_b200_version", "cbdiso_b200_scratch_bytes", "cbdiso_b200_fill_guards",
         "cbdiso_b200_advance_stage", "cbdiso_b200_reduce", "cbdiso_b200_abi_sizes",
         "cbdiso_b200_stage_record_bytes", "cbdiso_b200_stage_record", "cbdiso_b200_eval_primitives",
-        "cbdiso_b200_advance_stage_noalloc",
+        "cbdiso_b200_advance_stage_noalloc", "cbdiso_b200_stepper_bytes", "cbdiso_b200_stepper_init",
+        "cbdiso_b200_step_prologue",
     ]
 
 

@@ -354,6 +354,170 @@ class Solver(SolverBase):
         self._ring_events[slot] = ev
         self.h2d_bytes += host.numel()
 
+        self._launch_stages(weights, epilogue, stream)
+        self._time = time_end
+        self._cached = None
+        self._result_valid = True
+
+    # ------------------------------------------------------------------
+    # device-resident stepping
+    # ------------------------------------------------------------------
+
+    def _device_orbit(self):
+        """
+        The binary's Kepler orbit as the device stepper needs it, taken from a
+        setup with `orbital_elements` and uniform sink / softening parameters
+        (the circumbinary setups). Checked against the physics callback.
+        """
+        setup = self.setup
+        need = ("orbital_elements", "softening_length", "sink_model", "sink_rate", "sink_radius")
+        if not all(hasattr(setup, a) for a in need):
+            raise ValueError("device stepping needs a setup with a Kepler binary (orbital_elements)")
+        el = setup.orbital_elements
+        o = _capi.Orbit()
+        o.semimajor_axis, o.total_mass = float(el.semimajor_axis), float(el.total_mass)
+        o.mass_ratio, o.eccentricity = float(el.mass_ratio), float(el.eccentricity)
+        o.softening_length, o.sink_rate = float(setup.softening_length), float(setup.sink_rate)
+        o.sink_radius = float(setup.sink_radius)
+        model = setup.sink_model
+        o.sink_model = enum_value(model) if not isinstance(model, str) else (
+            dict(inactive=0, acceleration_free=1, torque_free=2, force_free=3)[model.lower()])
+        x_off = getattr(setup, "x_bin", None)
+        if x_off is not None:
+            o.has_x_offset, o.x_offset = 1, float(x_off)
+        from .kepler import OrbitalElements
+
+        orb = OrbitalElements(o.semimajor_axis, o.total_mass, o.mass_ratio, o.eccentricity)
+        for t in (self._time, self._time + 1.2345):
+            got = self._physics.point_masses(t)
+            want = orb.orbital_state(t)
+            for g_, w_ in zip(got, want):
+                wx = w_.position_x + (o.x_offset if o.has_x_offset else 0.0)
+                if (g_.mass, g_.position_x, g_.position_y, g_.velocity_x, g_.velocity_y) != (
+                        w_.mass, wx, w_.position_y, w_.velocity_x, w_.velocity_y) or \
+                        g_.softening_length != o.softening_length or g_.sink_rate != o.sink_rate or \
+                        g_.sink_radius != o.sink_radius or enum_value(g_.sink_model) != o.sink_model:
+                    raise ValueError("the physics point masses are not the setup's Kepler binary")
+        return o
+
+    def run(self, steps, cfl=None, fixed_dt=None, graph=True, steps_per_graph=16):
+        """
+        Advance `steps` iterations entirely on the device: each step's dt is
+        min(dx, dy) / max wavespeed * cfl (driver.py:508-510) from the previous
+        step's fused wavespeed (or `fixed_dt`), and the point masses come from
+        the binary's Kepler orbit solved on the device. With `graph`, a group
+        of `steps_per_graph` steps is captured once in a CUDA graph (cached
+        on the solver) and replayed. Returns the time series: one row per
+        step, the `reductions()` row followed by dt.
+        """
+        import torch
+
+        steps = int(steps)
+        if steps <= 0:
+            return []
+        cfl = self.recommended_cfl if cfl is None else float(cfl)
+        lib, g = self._lib, self._grid
+        orbit = self._device_orbit()
+        if not self._result_valid:
+            self._reduce_now(True, self._device_diags if self._fused else [])
+        nvals = 2 * len(self._device_diags) if self._fused else 0
+        if self._options.rk_order == 1 and steps_per_graph % 2:
+            steps_per_graph += 1  # RK1 swaps the two buffers each step: capture whole pairs
+        nbytes = int(lib.cbdiso_b200_stepper_bytes())
+        if getattr(self, "_stepper_dev", None) is None:
+            self._stepper_dev = torch.zeros(nbytes, dtype=torch.uint8, device=self.device)
+            self._graphs = {}
+        if getattr(self, "_series_dev", None) is None or self._series_dev.shape[0] < steps or \
+                self._series_dev.shape[1] != 3 + nvals:
+            self._series_dev = torch.zeros((max(steps, 64), 3 + nvals), dtype=torch.float64, device=self.device)
+            self._graphs = {}
+        stepper, series = self._stepper_dev, self._series_dev
+        host = torch.zeros(nbytes, dtype=torch.uint8).pin_memory()
+        self._check(lib.cbdiso_b200_stepper_init(ctypes.byref(g), ctypes.byref(orbit), self._options.rk_order,
+                                                 self._time, cfl, float(self.mesh.min_spacing()),
+                                                 float(fixed_dt or 0.0), series.shape[0],
+                                                 ctypes.c_void_p(host.data_ptr())), "stepper_init")
+        stepper.copy_(host, non_blocking=True)
+        self.h2d_bytes += nbytes
+        epilogue = self._epilogue(self._time, True, self._device_diags if self._fused else [])
+        weights = RK_WEIGHTS[self._options.rk_order]
+
+        def one_step():
+            stream = self._stream()
+            self._check(lib.cbdiso_b200_step_prologue(self._ptr(stepper), self._ptr(self._result),
+                                                      self._ptr(self._records), self._ptr(series), nvals, 0,
+                                                      stream), "step_prologue")
+            self._launch_stages(weights, epilogue, stream)
+
+        remaining = steps
+        if graph and steps >= steps_per_graph:
+            # the graph bakes in buffer addresses: RK1 alternates two assignments
+            key = (steps_per_graph, nvals, self._buf[0].data_ptr())
+            cuda_graph = self._graphs.get(key)
+            if cuda_graph is None:
+                side = torch.cuda.Stream()
+                side.wait_stream(torch.cuda.current_stream())
+                cuda_graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(cuda_graph, stream=side):
+                    for _ in range(steps_per_graph):
+                        one_step()
+                torch.cuda.current_stream().wait_stream(side)
+                self._graphs[key] = cuda_graph
+            while remaining >= steps_per_graph:
+                cuda_graph.replay()
+                remaining -= steps_per_graph
+        for _ in range(remaining):
+            one_step()
+        self._check(lib.cbdiso_b200_step_prologue(self._ptr(stepper), self._ptr(self._result),
+                                                  self._ptr(self._records), self._ptr(series), nvals, 1,
+                                                  self._stream()), "step_prologue")
+        state = stepper.cpu()
+        time, status = self._stepper_fields(state)
+        if status != 0:
+            raise _capi.CbdError(status, "device stepping")
+        self._time = time
+        self._cached = None
+        self._result_valid = True
+        rows = series[:steps].cpu().numpy()
+        self.d2h_bytes += rows.nbytes + state.numel()
+        return self._series_rows(rows)
+
+    def _stepper_fields(self, state):
+        raw = state.numpy().tobytes()
+        time = np.frombuffer(raw[0:8], dtype=np.float64)[0]
+        # status follows the orbit record; its offset is fixed by the struct layout
+        status = int(np.frombuffer(raw[self._status_offset():self._status_offset() + 4], dtype=np.int32)[0])
+        return float(time), status
+
+    @staticmethod
+    def _status_offset():
+        # StepperDev: 6 doubles, weights[3], cbd_orbit_t (80 bytes), num_stages, step, status
+        return 8 * 6 + 8 * 3 + ctypes.sizeof(_capi.Orbit) + 8
+
+    def _series_rows(self, rows):
+        """Device time-series rows -> reductions()-shaped rows plus dt."""
+        out = []
+        da = self.mesh.dx * self.mesh.dy
+        for row in rows:
+            t, dt = float(row[0]), float(row[1])
+            vals = []
+            k = 0
+            for d in self._physics.diagnostics:
+                if d.quantity == "time":
+                    vals.append(t / self.setup.reference_time_scale)
+                    continue
+                re, im = row[3 + 2 * k], row[4 + 2 * k]
+                k += 1
+                vals.append(complex(re, im) * da if d.quantity in COMPLEX_QUANTITIES else float(re) * da)
+            out.append(vals + [dt])
+        return out
+
+    def _launch_stages(self, weights, epilogue, stream):
+        """The RK stages of one step, reading the stage records in
+        self._records; the last stage carries the epilogue. Buffers: RK1
+        A -> B (then swapped), RK2 A -> B, B (+A) -> A, RK3 A -> B,
+        B (+A) -> C, C (+A) -> A."""
+        lib, g = self._lib, self._grid
         A = self._buf[0]
         B = self._buf[1]
         if len(weights) == 1:
@@ -375,9 +539,6 @@ class Solver(SolverBase):
             self._check(status, "advance_stage")
         if len(weights) == 1:
             self._buf[0], self._buf[1] = B, A
-        self._time = time_end
-        self._cached = None
-        self._result_valid = True
 
     def reductions(self):
         """

@@ -1,0 +1,197 @@
+// Device-resident time stepping: the driver's CFL time step
+// (sailfish/driver.py:508-510), the RK stage times (cbdiso_2d.py:239) and the
+// binary's Kepler orbit (sailfish/physics/kepler.py:329-366, 414-421) computed
+// on the device, so that a run of steps needs no host round trip and can be
+// captured in a CUDA graph. One single-thread prologue kernel per step writes
+// the stage records that the stage kernels read.
+#include <cmath>
+#include <cstring>
+
+#include "cbd_internal.h"
+#include "stepper.h"
+
+namespace cbd {
+
+namespace {
+
+// Newton iteration of kepler.py:414-421 on E - e sin E = M: stop when
+// |f| <= 1e-15, fail after more than 10 updates.
+__device__ bool eccentric_anomaly(double mean_anomaly, double e, double *out)
+{
+    double k = mean_anomaly;
+    int n = 0;
+    double f = k - e * sin(k) - mean_anomaly;
+    while (fabs(f) > 1e-15) {
+        k -= f / (1.0 - e * cos(k));
+        n += 1;
+        if (n > 10)
+            return false;
+        f = k - e * sin(k) - mean_anomaly;
+    }
+    *out = k;
+    return true;
+}
+
+__device__ MassDev mass_record(double mass, double x, double y, double vx, double vy, const cbd_orbit_t &o)
+{
+    MassDev m;
+    m.x = x;
+    m.y = y;
+    m.vx = vx;
+    m.vy = vy;
+    m.mass = mass;
+    m.soft2 = o.softening_length * o.softening_length;
+    m.sink_rate = o.sink_rate;
+    m.sink_radius = o.sink_radius;
+    m.inv_sink_radius = 1.0 / o.sink_radius;
+    m.sink_r4 = 4.0 * o.sink_radius;
+    m.sink_hi2 = m.sink_r4 * m.sink_r4 * (1.0 + 1e-10);
+    m.sink_model = o.sink_model;
+    m._pad = 0;
+    return m;
+}
+
+// Positions and velocities of the two components at time t
+// (kepler.py:300-373), in the reference's operation order.
+__device__ bool orbit_masses(const cbd_orbit_t &o, double t, MassDev *out)
+{
+    const double a = o.semimajor_axis, m = o.total_mass, q = o.mass_ratio, e = o.eccentricity;
+    const double w = sqrt(1.0 * m / a / a / a);
+    const double period = 2.0 * 3.141592653589793 / w;
+    const double tt = t - period * floor(t / period);
+    double E;
+    if (!eccentric_anomaly(w * tt, e, &E))
+        return false;
+    const double m1 = m / (1.0 + q);
+    const double m2 = m - m1;
+    const double ck = cos(E);
+    const double sk = sin(E);
+    const double x1 = -a * q / (1.0 + q) * (e - ck);
+    const double y1 = +a * q / (1.0 + q) * (sk) * sqrt(1.0 - e * e);
+    const double x2 = -x1 / q;
+    const double y2 = -y1 / q;
+    const double vx1 = -a * q / (1.0 + q) * w / (1.0 - e * ck) * sk;
+    const double vy1 = +a * q / (1.0 + q) * w / (1.0 - e * ck) * ck * sqrt(1.0 - e * e);
+    const double vx2 = -vx1 / q;
+    const double vy2 = -vy1 / q;
+    const double dx = o.has_x_offset ? o.x_offset : 0.0;
+    out[0] = mass_record(m1, o.has_x_offset ? x1 + dx : x1, y1, vx1, vy1, o);
+    out[1] = mass_record(m2, o.has_x_offset ? x2 + dx : x2, y2, vx2, vy2, o);
+    return true;
+}
+
+// One step's prologue. With `finalize`, only records the previous step's
+// time-series row. Otherwise: record the previous row (if any), choose dt,
+// write the stage records of this step, advance the clock.
+__global__ void step_prologue_kernel(StepperDev *s, const double *result, StageDev *records, double *series,
+                                     int num_values, int finalize)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    if (s->status != CBD_OK)
+        return;
+    if (s->step > 0 && series && s->step - 1 < s->series_capacity) {
+        double *row = series + (size_t)(s->step - 1) * (3 + num_values);
+        row[0] = s->time;
+        row[1] = s->dt;
+        row[2] = result[0];
+        for (int v = 0; v < num_values; ++v)
+            row[3 + v] = result[1 + v];
+    }
+    if (finalize)
+        return;
+    const double dt = s->fixed_dt > 0.0 ? s->fixed_dt : s->min_spacing / result[0] * s->cfl;
+    const double time0 = s->time;
+    double t = time0;
+    double times[3];
+    for (int k = 0; k < s->num_stages; ++k) {
+        times[k] = t;
+        t = time0 * s->weights[k] + (t + dt) * (1.0 - s->weights[k]);
+    }
+    MassDev end[2];
+    if (!orbit_masses(s->orbit, t, end)) {
+        s->status = CBD_ERR_KEPLER;
+        return;
+    }
+    for (int k = 0; k < s->num_stages; ++k) {
+        StageDev &r = records[k];
+        if (!orbit_masses(s->orbit, times[k], r.m)) {
+            s->status = CBD_ERR_KEPLER;
+            return;
+        }
+        r.e[0] = end[0];
+        r.e[1] = end[1];
+        r.a = s->weights[k];
+        r.one_minus_a = 1.0 - s->weights[k];
+        r.dt = dt;
+        r.buffer_mass = r.m[0].mass + r.m[1].mass;
+        r.buffer_k = s->buffer_k;
+    }
+    s->dt = dt;
+    s->time = t;
+    s->step += 1;
+}
+
+}  // namespace
+
+cudaError_t launch_step_prologue(StepperDev *s, const double *result, StageDev *records, double *series,
+                                 int num_values, int finalize, cudaStream_t stream)
+{
+    step_prologue_kernel<<<1, 32, 0, stream>>>(s, result, records, series, num_values, finalize);
+    return cudaGetLastError();
+}
+
+}  // namespace cbd
+
+using namespace cbd;
+
+extern "C" {
+
+size_t cbdiso_b200_stepper_bytes(void) { return sizeof(StepperDev); }
+
+int cbdiso_b200_stepper_init(const cbd_grid_t *grid, const cbd_orbit_t *orbit, int rk_order, double time,
+                             double cfl, double min_spacing, double fixed_dt, int series_capacity, void *stepper)
+{
+    if (!grid || !orbit || !stepper || rk_order < 1 || rk_order > 3 || !(cfl > 0.0) || !(min_spacing > 0.0) ||
+        series_capacity < 0)
+        return CBD_ERR_ARGUMENT;
+    if (!(orbit->semimajor_axis > 0.0) || !(orbit->total_mass > 0.0) || !(orbit->mass_ratio > 0.0) ||
+        !(orbit->eccentricity >= 0.0 && orbit->eccentricity < 1.0))
+        return CBD_ERR_ARGUMENT;
+    StepperDev s;
+    std::memset(&s, 0, sizeof(s));
+    s.time = time;
+    s.cfl = cfl;
+    s.fixed_dt = fixed_dt;
+    s.min_spacing = min_spacing;
+    static const double w1[] = {0.0}, w2[] = {0.0, 0.5}, w3[] = {0.0, 0.75, 1.0 / 3.0};
+    const double *w = rk_order == 1 ? w1 : (rk_order == 2 ? w2 : w3);
+    s.num_stages = rk_order;
+    for (int k = 0; k < rk_order; ++k)
+        s.weights[k] = w[k];
+    s.orbit = *orbit;
+    const double m1 = orbit->total_mass / (1.0 + orbit->mass_ratio);
+    const double central = m1 + (orbit->total_mass - m1);
+    const double onset = grid->buffer_outer_radius - grid->buffer_onset_width;
+    s.buffer_k = grid->buffer_is_enabled
+                     ? grid->buffer_driving_rate * std::sqrt(central * std::pow(onset, -3.0))
+                     : 0.0;
+    s.series_capacity = series_capacity;
+    s.status = CBD_OK;
+    std::memcpy(stepper, &s, sizeof(s));
+    return CBD_OK;
+}
+
+int cbdiso_b200_step_prologue(void *stepper_dev, const double *result, void *records_dev, double *series,
+                              int num_values, int finalize, void *stream)
+{
+    if (!stepper_dev || !result || !records_dev || num_values < 0 || num_values > 2 * CBD_MAX_DIAG)
+        return CBD_ERR_ARGUMENT;
+    return launch_step_prologue(static_cast<StepperDev *>(stepper_dev), result,
+                                static_cast<StageDev *>(records_dev), series, num_values, finalize,
+                                static_cast<cudaStream_t>(stream)) == cudaSuccess
+               ? CBD_OK
+               : CBD_ERR_CUDA;
+}
+
+}  // extern "C"

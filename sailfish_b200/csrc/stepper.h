@@ -1,0 +1,26 @@
+// Device-side state of the device-resident time stepper (stepper.cu).
+#pragma once
+
+#include "cbd_stencil.cuh"
+
+namespace cbd {
+
+struct StepperDev {
+    double time;         // simulation time after the last step
+    double dt;           // the last step's dt
+    double min_spacing;  // min(dx, dy) of the mesh, as the driver uses it
+    double cfl;
+    double fixed_dt;     // > 0: use this dt every step instead of the CFL rule
+    double buffer_k;     // buffer driving_rate * sqrt(M onset^-3), from the host libm
+    double weights[3];   // RK weights of u_n per stage
+    cbd_orbit_t orbit;
+    int num_stages;
+    int step;            // steps taken
+    int status;          // CBD_OK, or CBD_ERR_KEPLER once a solve failed (then no further steps)
+    int series_capacity; // rows available in the time-series buffer
+};
+
+cudaError_t launch_step_prologue(StepperDev *s, const double *result, StageDev *records, double *series,
+                                 int num_values, int finalize, cudaStream_t stream);
+
+}  // namespace cbd
