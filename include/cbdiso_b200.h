@@ -264,6 +264,42 @@ int cbdiso_b200_stepper_init(const cbd_grid_t *grid, const cbd_orbit_t *orbit, i
 int cbdiso_b200_step_prologue(void *stepper_dev, const double *result, void *records_dev, double *series,
                               int num_values, int finalize, void *stream);
 
+/* ------------------------------------------------------------------------
+ * batched: many disks of different sizes and physics per launch (no
+ * counterpart in the reference, which advances one grid at a time)
+ * ---------------------------------------------------------------------- */
+
+/* Size of a disk record, and a host routine filling one: the disk's kernel
+ * constants from `grid`, its fused diagnostics (up to four; null: wavespeed
+ * only), its tile shape (strip_width in 32..128 columns, rows per tile), the
+ * offset in doubles of its (ni + 4, nj + 4, 3) state in the batch buffers and
+ * the index of its first tile in the batch; *units receives its tile count.
+ * Records are copied to a device array ordered by unit_begin. */
+size_t cbdiso_b200_batch_disk_bytes(void);
+int cbdiso_b200_batch_disk_record(const cbd_grid_t *grid, const cbd_epilogue_t *diagnostics, int strip_width,
+                                  int rows, long long offset, int unit_begin, int *units, void *record);
+
+/* One RK stage of every disk in one persistent launch: CTAs take tiles from
+ * counters[0] until all total_units are done (both counters return to zero).
+ * Stage records are read from records[disk * num_stages + stage]; with
+ * `epilogue`, each tile's wavespeed / diagnostic partial goes to
+ * partials[tile * 9 ...]. primitive_n (null for the a = 0 stage) gives u_n. */
+int cbdiso_b200_batched_stage(const void *disks, int num_disks, int total_units, const double *primitive_rd,
+                              const double *primitive_n, double *primitive_wr, const void *records, int num_stages,
+                              int stage, int epilogue, double *partials, unsigned int *counters, int precision,
+                              void *stream);
+
+/* Per-disk reduction of the tile partials, in tile order: results[d * stride]
+ * = max wavespeed, then the diagnostic sums. */
+int cbdiso_b200_batched_finalize(const void *disks, int num_disks, const double *partials, double *results,
+                                 int result_stride, void *stream);
+
+/* Per-disk step prologue (see cbdiso_b200_step_prologue), one stepper record
+ * per disk in `steppers`; each disk's series block holds its
+ * series_capacity rows. */
+int cbdiso_b200_batched_prologue(void *steppers, int num_disks, const double *results, int result_stride,
+                                 void *records, double *series, int num_values, int finalize, void *stream);
+
 /* The epilogue quantities alone, on a given state (guards not needed). */
 int cbdiso_b200_reduce(
     const cbd_grid_t *grid, const cbd_epilogue_t *epilogue, const double *primitive,

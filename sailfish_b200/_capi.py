@@ -113,6 +113,19 @@ def _declare(lib):
     lib.cbdiso_b200_stepper_init.restype = c_int
     lib.cbdiso_b200_step_prologue.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]
     lib.cbdiso_b200_step_prologue.restype = c_int
+    lib.cbdiso_b200_batch_disk_bytes.argtypes = []
+    lib.cbdiso_b200_batch_disk_bytes.restype = c_size_t
+    lib.cbdiso_b200_batch_disk_record.argtypes = [POINTER(Grid), POINTER(Epilogue), c_int, c_int,
+                                                  ctypes.c_longlong, c_int, POINTER(c_int), c_void_p]
+    lib.cbdiso_b200_batch_disk_record.restype = c_int
+    lib.cbdiso_b200_batched_stage.argtypes = [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                              c_int, c_int, c_int, c_void_p, c_void_p, c_int, c_void_p]
+    lib.cbdiso_b200_batched_stage.restype = c_int
+    lib.cbdiso_b200_batched_finalize.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p]
+    lib.cbdiso_b200_batched_finalize.restype = c_int
+    lib.cbdiso_b200_batched_prologue.argtypes = [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int,
+                                                 c_int, c_void_p]
+    lib.cbdiso_b200_batched_prologue.restype = c_int
     lib.cbdiso_b200_abi_sizes.argtypes = [POINTER(c_size_t)]
     lib.cbdiso_b200_abi_sizes.restype = None
     lib.cbdiso_b200_status_string.argtypes = [c_int]
@@ -146,7 +159,8 @@ def exported_symbols():
         "cbdiso_b200_advance_stage", "cbdiso_b200_reduce", "cbdiso_b200_abi_sizes",
         "cbdiso_b200_stage_record_bytes", "cbdiso_b200_stage_record", "cbdiso_b200_eval_primitives",
         "cbdiso_b200_advance_stage_noalloc", "cbdiso_b200_stepper_bytes", "cbdiso_b200_stepper_init",
-        "cbdiso_b200_step_prologue",
+        "cbdiso_b200_step_prologue", "cbdiso_b200_batch_disk_bytes", "cbdiso_b200_batch_disk_record",
+        "cbdiso_b200_batched_stage", "cbdiso_b200_batched_finalize", "cbdiso_b200_batched_prologue",
     ]
 
 

@@ -495,9 +495,14 @@ class Solver(SolverBase):
         return 8 * 6 + 8 * 3 + ctypes.sizeof(_capi.Orbit) + 8
 
     def _series_rows(self, rows):
-        """Device time-series rows -> reductions()-shaped rows plus dt."""
+        """
+        Device time-series rows -> reductions()-shaped rows plus dt. Without
+        fused diagnostics (more than four, or fuse_reductions off) the
+        per-step sums are not recorded and appear as None.
+        """
         out = []
         da = self.mesh.dx * self.mesh.dy
+        have = rows.shape[1] > 3
         for row in rows:
             t, dt = float(row[0]), float(row[1])
             vals = []
@@ -505,6 +510,9 @@ class Solver(SolverBase):
             for d in self._physics.diagnostics:
                 if d.quantity == "time":
                     vals.append(t / self.setup.reference_time_scale)
+                    continue
+                if not have:
+                    vals.append(None)
                     continue
                 re, im = row[3 + 2 * k], row[4 + 2 * k]
                 k += 1

@@ -1,0 +1,131 @@
+// Many grids ("disks") of different sizes and physics advanced by one
+// persistent launch per RK stage. The work is the list of all tiles
+// (disk, strip, segment), largest disks first; each CTA takes the next tile
+// from an atomic counter, loads that disk's constants and stage record into
+// shared memory and marches the tile with the same code as the single-grid
+// kernel. Per-tile epilogue partials are reduced per disk afterwards, in tile
+// order, by one CTA per disk.
+#pragma once
+
+#include "cbd_stencil.cuh"
+
+namespace cbd {
+
+struct DiskDev {
+    Consts k;            // the disk's kernel constants (k.rows_per_cta = tile rows)
+    long long offset;    // offset of the disk's state, in doubles, in the batch buffers
+    int strip_width;     // tile columns (<= the kernel's thread count)
+    int strips;
+    int segments;
+    int unit_begin;      // index of the disk's first tile in the batch's tile list
+};
+
+struct BatchArgs {
+    const DiskDev *disks;
+    int num_disks;
+    int total_units;
+    const double *prd;
+    const double *un;    // u_n source (primitive_n), or null for a = 0 stages
+    double *pwr;
+    const StageDev *records;  // records[disk * num_stages + stage]
+    int num_stages;
+    int stage;
+    int epilogue;        // 1 on the step's last stage
+    int _pad;
+    double *partials;    // [total_units][PARTIAL_STRIDE]
+    unsigned int *counters;  // [0] next tile, [1] CTAs finished; both return to zero at the end
+};
+
+template <int BJ, int MINB, int PREC>
+__global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs a)
+{
+    constexpr bool FAST = PREC == CBD_PRECISION_FAST;
+    __shared__ Consts k;
+    __shared__ StageDev st;
+    __shared__ double sred[PARTIAL_STRIDE * (BJ / 32)];
+    __shared__ int s_unit, s_disk;
+    const int t = threadIdx.x;
+
+    for (;;) {
+        if (t == 0) {
+            const int u = (int)atomicAdd(&a.counters[0], 1u);
+            s_unit = u;
+            if (u < a.total_units) {
+                int lo = 0, hi = a.num_disks - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) / 2;
+                    if (a.disks[mid].unit_begin <= u)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                s_disk = lo;
+            }
+        }
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= a.total_units)
+            break;
+        const DiskDev &D = a.disks[s_disk];
+        {
+            const double *src = reinterpret_cast<const double *>(&D.k);
+            double *dst = reinterpret_cast<double *>(&k);
+            for (int w = t; w < (int)(sizeof(Consts) / sizeof(double)); w += BJ)
+                dst[w] = src[w];
+            const double *rs = reinterpret_cast<const double *>(&a.records[(size_t)s_disk * a.num_stages + a.stage]);
+            double *rd = reinterpret_cast<double *>(&st);
+            for (int w = t; w < (int)(sizeof(StageDev) / sizeof(double)); w += BJ)
+                rd[w] = rs[w];
+        }
+        __syncthreads();
+        if (t == 0) {
+            k.un_kind = a.un ? 1 : 0;
+            k.write_guards = 1;
+            if (!a.epilogue) {
+                k.want_ws = 0;
+                k.num_diag = 0;
+            }
+        }
+        __syncthreads();
+        const int local = u - D.unit_begin;
+        const int strip = local % D.strips;
+        const int seg = local / D.strips;
+        StageArgs sa;
+        sa.prd = a.prd + D.offset;
+        sa.un = a.un ? a.un + D.offset : nullptr;
+        sa.pwr = a.pwr + D.offset;
+        sa.stage_dev = nullptr;
+        sa.scratch = nullptr;
+        sa.result = nullptr;
+        double acc[PARTIAL_STRIDE];
+#pragma unroll
+        for (int v = 0; v < PARTIAL_STRIDE; ++v)
+            acc[v] = 0.0;
+        march_tile<BJ, FAST>(k, st, sa, strip * D.strip_width, D.strip_width, seg * k.rows_per_cta, acc);
+        if (a.epilogue) {
+            double red[PARTIAL_STRIDE];
+            block_reduce<BJ>(acc, sred, red);
+            if (t == 0) {
+#pragma unroll
+                for (int v = 0; v < PARTIAL_STRIDE; ++v)
+                    a.partials[(size_t)u * PARTIAL_STRIDE + v] = red[v];
+            }
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        __threadfence();
+        const unsigned int done = atomicAdd(&a.counters[1], 1u);
+        if (done == gridDim.x - 1) {
+            a.counters[0] = 0u;
+            a.counters[1] = 0u;
+            __threadfence();
+        }
+    }
+}
+
+cudaError_t launch_batched_exact(const BatchArgs &a, int ctas, cudaStream_t s);
+cudaError_t launch_batched_fma(const BatchArgs &a, int ctas, cudaStream_t s);
+cudaError_t launch_batched_fast(const BatchArgs &a, int ctas, cudaStream_t s);
+
+}  // namespace cbd

@@ -50,7 +50,9 @@ bool valid_grid(const cbd_grid_t *g)
            (g->eos_type == 1 || g->eos_type == 2);
 }
 
-Consts consts_from_grid(const cbd_grid_t *g)
+}  // namespace
+
+Consts cbd::consts_from_grid(const cbd_grid_t *g)
 {
     Consts k;
     std::memset(&k, 0, sizeof(k));
@@ -82,6 +84,8 @@ Consts consts_from_grid(const cbd_grid_t *g)
     k.inv_buf_span = 1.0 / k.buf_span;
     return k;
 }
+
+namespace {
 
 // driving_rate * omega_outer with omega_outer = sqrt(M onset^-3), evaluated
 // with the host libm as the reference's CPU build does (cbdiso_2d.c:237-238).
@@ -155,7 +159,9 @@ StageDev stage_dev_from(const cbd_grid_t *g, const cbd_stage_t *stage, const cbd
     return st;
 }
 
-int set_diagnostics(Consts &k, const cbd_epilogue_t *ep, int first, int count)
+}  // namespace
+
+int cbd::set_diagnostics(Consts &k, const cbd_epilogue_t *ep, int first, int count)
 {
     k.num_diag = count;
     k.need_rates = 0;
@@ -172,7 +178,6 @@ int set_diagnostics(Consts &k, const cbd_epilogue_t *ep, int first, int count)
     return CBD_OK;
 }
 
-}  // namespace
 
 extern "C" {
 

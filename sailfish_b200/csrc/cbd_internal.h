@@ -20,4 +20,10 @@ cudaError_t launch_stage_fma(const LaunchShape &s, const Consts &k, const StageD
 cudaError_t launch_stage_fast(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a,
                               cudaStream_t stream);
 
+// Kernel constants of a grid (mesh, EOS, options, buffer), with host-side
+// reciprocals of the constant divisors; and the diagnostics of an epilogue
+// (entries first .. first + count - 1) copied into them.
+Consts consts_from_grid(const cbd_grid_t *g);
+int set_diagnostics(Consts &k, const cbd_epilogue_t *ep, int first, int count);
+
 }  // namespace cbd

@@ -602,27 +602,24 @@ struct StageArgs {
     double *result;      // reductions result (epilogue only)
 };
 
-template <int BJ, int MINB, int PREC>
-__global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const StageDev st_param, StageArgs args)
+// One tile of the march: columns c0 .. c0 + width - 1 (width <= BJ) and rows
+// r0 .. r0 + k.rows_per_cta - 1 of one grid. `st` must live in shared memory
+// and be visible after the first barrier; epilogue values of the updated
+// zones are accumulated into `acc`. All threads of the block must call it.
+template <int BJ, bool FAST>
+__device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, const StageArgs &args, int c0,
+                                           int width, int r0, double (&acc)[PARTIAL_STRIDE])
 {
-    constexpr bool FAST = PREC == CBD_PRECISION_FAST;
     constexpr int W4 = BJ + 4;
     __shared__ double sp[4][NQ][W4];       // primitive rows ring, columns c0-2 .. c0+BJ+1
     __shared__ double sgy[2][NQ][BJ + 2];  // y-slopes ring, columns c0-1 .. c0+BJ
     __shared__ double srs[2][NQ][BJ + 2];  // rho * strain ring, same columns
     __shared__ double sg[NQ][BJ + 1];      // y-face fluxes of the current row
     __shared__ double sun[2][NQ][BJ];      // u_n source zones, fetched one row ahead
-    __shared__ StageDev st;
-    __shared__ double sred[PARTIAL_STRIDE * (BJ / 32)];
 
     const int t = threadIdx.x;
-    if (t == 0)
-        st = args.stage_dev ? *args.stage_dev : st_param;
-
     const int ni = k.ni, nj = k.nj;
-    const int c0 = blockIdx.x * BJ;
-    const int W = min(BJ, nj - c0);
-    const int r0 = blockIdx.y * k.rows_per_cta;
+    const int W = min(width, nj - c0);
     const int r1 = min(r0 + k.rows_per_cta, ni);
     const bool active = t < W;
     const int j = c0 + t;
@@ -658,12 +655,6 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
     // slopes of the two halo columns, and the last y-face of the row.
     constexpr int HALO_LANE = BJ >= 64 ? 32 : 0;
     constexpr int FACE_LANE = BJ >= 128 ? 64 : (BJ >= 64 ? 0 : 2);
-
-    // per-thread epilogue accumulators
-    double acc[PARTIAL_STRIDE];
-#pragma unroll
-    for (int v = 0; v < PARTIAL_STRIDE; ++v)
-        acc[v] = 0.0;
 
     // own-column carried state: x-slope and rho*strain of row r, x-face flux F(r - 1/2)
     double gx0[NQ] = {0.0, 0.0, 0.0}, rs0[NQ] = {0.0, 0.0, 0.0}, f0[NQ] = {0.0, 0.0, 0.0};
@@ -849,6 +840,24 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
         }
     }
 
+    // leave the shared buffers free for the block's next tile
+    __syncthreads();
+}
+
+// One RK stage on one grid: CTA (x, y) marches strip x, segment y.
+template <int BJ, int MINB, int PREC>
+__global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const StageDev st_param, StageArgs args)
+{
+    constexpr bool FAST = PREC == CBD_PRECISION_FAST;
+    __shared__ StageDev st;
+    __shared__ double sred[PARTIAL_STRIDE * (BJ / 32)];
+    if (threadIdx.x == 0)
+        st = args.stage_dev ? *args.stage_dev : st_param;
+    double acc[PARTIAL_STRIDE];
+#pragma unroll
+    for (int v = 0; v < PARTIAL_STRIDE; ++v)
+        acc[v] = 0.0;
+    march_tile<BJ, FAST>(k, st, args, blockIdx.x * BJ, BJ, blockIdx.y * k.rows_per_cta, acc);
     if (k.want_ws || k.num_diag > 0) {
         double red[PARTIAL_STRIDE];
         block_reduce<BJ>(acc, sred, red);

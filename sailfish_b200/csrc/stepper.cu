@@ -9,89 +9,28 @@
 
 #include "cbd_internal.h"
 #include "stepper.h"
+#include "orbit.cuh"
 
 namespace cbd {
 
 namespace {
 
-// Newton iteration of kepler.py:414-421 on E - e sin E = M: stop when
-// |f| <= 1e-15, fail after more than 10 updates.
-__device__ bool eccentric_anomaly(double mean_anomaly, double e, double *out)
+// One step's prologue for n independent grids (thread d: grid d). With
+// `finalize`, only records the previous step's time-series row. Otherwise:
+// record the previous row (if any), choose dt, write the stage records of
+// this step, advance the clock.
+__global__ void step_prologue_kernel(StepperDev *steppers, int n, const double *results, int result_stride,
+                                     StageDev *records, double *series, int num_values, int finalize)
 {
-    double k = mean_anomaly;
-    int n = 0;
-    double f = k - e * sin(k) - mean_anomaly;
-    while (fabs(f) > 1e-15) {
-        k -= f / (1.0 - e * cos(k));
-        n += 1;
-        if (n > 10)
-            return false;
-        f = k - e * sin(k) - mean_anomaly;
-    }
-    *out = k;
-    return true;
-}
-
-__device__ MassDev mass_record(double mass, double x, double y, double vx, double vy, const cbd_orbit_t &o)
-{
-    MassDev m;
-    m.x = x;
-    m.y = y;
-    m.vx = vx;
-    m.vy = vy;
-    m.mass = mass;
-    m.soft2 = o.softening_length * o.softening_length;
-    m.sink_rate = o.sink_rate;
-    m.sink_radius = o.sink_radius;
-    m.inv_sink_radius = 1.0 / o.sink_radius;
-    m.sink_r4 = 4.0 * o.sink_radius;
-    m.sink_hi2 = m.sink_r4 * m.sink_r4 * (1.0 + 1e-10);
-    m.sink_model = o.sink_model;
-    m._pad = 0;
-    return m;
-}
-
-// Positions and velocities of the two components at time t
-// (kepler.py:300-373), in the reference's operation order.
-__device__ bool orbit_masses(const cbd_orbit_t &o, double t, MassDev *out)
-{
-    const double a = o.semimajor_axis, m = o.total_mass, q = o.mass_ratio, e = o.eccentricity;
-    const double w = sqrt(1.0 * m / a / a / a);
-    const double period = 2.0 * 3.141592653589793 / w;
-    const double tt = t - period * floor(t / period);
-    double E;
-    if (!eccentric_anomaly(w * tt, e, &E))
-        return false;
-    const double m1 = m / (1.0 + q);
-    const double m2 = m - m1;
-    const double ck = cos(E);
-    const double sk = sin(E);
-    const double x1 = -a * q / (1.0 + q) * (e - ck);
-    const double y1 = +a * q / (1.0 + q) * (sk) * sqrt(1.0 - e * e);
-    const double x2 = -x1 / q;
-    const double y2 = -y1 / q;
-    const double vx1 = -a * q / (1.0 + q) * w / (1.0 - e * ck) * sk;
-    const double vy1 = +a * q / (1.0 + q) * w / (1.0 - e * ck) * ck * sqrt(1.0 - e * e);
-    const double vx2 = -vx1 / q;
-    const double vy2 = -vy1 / q;
-    const double dx = o.has_x_offset ? o.x_offset : 0.0;
-    out[0] = mass_record(m1, o.has_x_offset ? x1 + dx : x1, y1, vx1, vy1, o);
-    out[1] = mass_record(m2, o.has_x_offset ? x2 + dx : x2, y2, vx2, vy2, o);
-    return true;
-}
-
-// One step's prologue. With `finalize`, only records the previous step's
-// time-series row. Otherwise: record the previous row (if any), choose dt,
-// write the stage records of this step, advance the clock.
-__global__ void step_prologue_kernel(StepperDev *s, const double *result, StageDev *records, double *series,
-                                     int num_values, int finalize)
-{
-    if (threadIdx.x != 0 || blockIdx.x != 0)
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n)
         return;
+    StepperDev *s = steppers + d;
+    const double *result = results + (size_t)d * result_stride;
     if (s->status != CBD_OK)
         return;
     if (s->step > 0 && series && s->step - 1 < s->series_capacity) {
-        double *row = series + (size_t)(s->step - 1) * (3 + num_values);
+        double *row = series + ((size_t)d * s->series_capacity + (s->step - 1)) * (3 + num_values);
         row[0] = s->time;
         row[1] = s->dt;
         row[2] = result[0];
@@ -113,8 +52,9 @@ __global__ void step_prologue_kernel(StepperDev *s, const double *result, StageD
         s->status = CBD_ERR_KEPLER;
         return;
     }
+    StageDev *rec = records + (size_t)d * s->num_stages;
     for (int k = 0; k < s->num_stages; ++k) {
-        StageDev &r = records[k];
+        StageDev &r = rec[k];
         if (!orbit_masses(s->orbit, times[k], r.m)) {
             s->status = CBD_ERR_KEPLER;
             return;
@@ -134,10 +74,12 @@ __global__ void step_prologue_kernel(StepperDev *s, const double *result, StageD
 
 }  // namespace
 
-cudaError_t launch_step_prologue(StepperDev *s, const double *result, StageDev *records, double *series,
-                                 int num_values, int finalize, cudaStream_t stream)
+cudaError_t launch_step_prologue(StepperDev *s, int n, const double *results, int result_stride,
+                                 StageDev *records, double *series, int num_values, int finalize,
+                                 cudaStream_t stream)
 {
-    step_prologue_kernel<<<1, 32, 0, stream>>>(s, result, records, series, num_values, finalize);
+    step_prologue_kernel<<<(n + 63) / 64, 64, 0, stream>>>(s, n, results, result_stride, records, series,
+                                                           num_values, finalize);
     return cudaGetLastError();
 }
 
@@ -187,7 +129,7 @@ int cbdiso_b200_step_prologue(void *stepper_dev, const double *result, void *rec
 {
     if (!stepper_dev || !result || !records_dev || num_values < 0 || num_values > 2 * CBD_MAX_DIAG)
         return CBD_ERR_ARGUMENT;
-    return launch_step_prologue(static_cast<StepperDev *>(stepper_dev), result,
+    return launch_step_prologue(static_cast<StepperDev *>(stepper_dev), 1, result, 0,
                                 static_cast<StageDev *>(records_dev), series, num_values, finalize,
                                 static_cast<cudaStream_t>(stream)) == cudaSuccess
                ? CBD_OK

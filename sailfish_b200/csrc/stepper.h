@@ -20,7 +20,10 @@ struct StepperDev {
     int series_capacity; // rows available in the time-series buffer
 };
 
-cudaError_t launch_step_prologue(StepperDev *s, const double *result, StageDev *records, double *series,
-                                 int num_values, int finalize, cudaStream_t stream);
+// Prologue of n grids' steps; grid d reads results + d * result_stride and
+// writes records + d * num_stages and its series block (series_capacity rows).
+cudaError_t launch_step_prologue(StepperDev *s, int n, const double *results, int result_stride,
+                                 StageDev *records, double *series, int num_values, int finalize,
+                                 cudaStream_t stream);
 
 }  // namespace cbd
