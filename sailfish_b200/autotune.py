@@ -80,16 +80,22 @@ def _time(fn, repeats):
     return a.elapsed_time(b) / repeats
 
 
-def tune_batched(ni, nj, precision="exact", candidates=BATCHED_CANDIDATES, steps=4):
-    """Fastest (strip_width, rows) of the batched kernel for an ni x nj disk."""
+def tune_batched(ni, nj, precision="exact", candidates=BATCHED_CANDIDATES, steps=4, fill_zones=1 << 23):
+    """
+    Fastest (strip_width, rows) of the batched kernel for ni x nj disks, timed
+    in a batch of copies holding about `fill_zones` zones, so the GPU is as
+    full as in a real batch and the tile's own cost decides.
+    """
     from .batched import BatchedSolver, Disk
 
     setup, mesh, prim = _disk(ni, nj)
+    disk = Disk(setup, mesh, prim)
+    copies = max(1, fill_zones // (ni * nj))
     best, best_ms = None, float("inf")
     for width, rows in candidates:
         if width > 64 and nj <= 64:
             continue
-        b = BatchedSolver([Disk(setup, mesh, prim)], precision=precision, tiles={(ni, nj): (width, rows)})
+        b = BatchedSolver([disk] * copies, precision=precision, tiles={(ni, nj): (width, rows)})
         ms = _time(lambda: b.run(steps, graph=False), 2)
         del b
         if ms < best_ms:

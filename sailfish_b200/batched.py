@@ -79,13 +79,19 @@ class BatchedSolver:
         # One single-disk Solver per disk builds the grid record, the initial
         # state with its guard zones, and validates the physics exactly as the
         # drop-in does; its device buffers are dropped after the copy.
+        # (the same Disk object listed several times shares one constructed
+        # Solver: its state is copied into each slot)
         self.disks = list(disks)
         self.solvers: List[Solver] = []
+        built = {}
         for d in self.disks:
-            physics = d.setup.physics
-            physics["diagnostics"] = list(self.diagnostics)
-            s = Solver(setup=d.setup, mesh=d.mesh, solution=d.solution, physics=physics, options=opts)
-            s._device_orbit()  # every disk must be a Kepler binary
+            s = built.get(id(d))
+            if s is None:
+                physics = d.setup.physics
+                physics["diagnostics"] = list(self.diagnostics)
+                s = Solver(setup=d.setup, mesh=d.mesh, solution=d.solution, physics=physics, options=opts)
+                s._device_orbit()  # every disk must be a Kepler binary
+                built[id(d)] = s
             self.solvers.append(s)
         n = len(self.solvers)
         sizes = [s.mesh.shape for s in self.solvers]
@@ -138,10 +144,13 @@ class BatchedSolver:
         self._graphs = {}
         self.times = [s.time for s in self.solvers]
         # initial wavespeeds (and sums) per disk, from the standalone reduction
+        done = {}
         for slot, i in enumerate(self.order):
             s = self.solvers[i]
-            s._reduce_now(True, self._device_diags)
-            self._results[slot * RESULT_STRIDE:(slot + 1) * RESULT_STRIDE].copy_(s._result[:RESULT_STRIDE])
+            if id(s) not in done:
+                s._reduce_now(True, self._device_diags)
+                done[id(s)] = s._result[:RESULT_STRIDE].clone()
+            self._results[slot * RESULT_STRIDE:(slot + 1) * RESULT_STRIDE].copy_(done[id(s)])
         for s in self.solvers:  # free the single-disk buffers
             s._buf = None
             s._scratch = None
