@@ -300,6 +300,53 @@ int cbdiso_b200_batched_finalize(const void *disks, int num_disks, const double 
 int cbdiso_b200_batched_prologue(void *steppers, int num_disks, const double *results, int result_stride,
                                  void *records, double *series, int num_values, int finalize, void *stream);
 
+/* ------------------------------------------------------------------------
+ * differentiation: tangent and discrete adjoint of a stage and of the
+ * objective (no counterpart in the reference)
+ *
+ * Parameter vectors have 12 entries: mass 1 (x, y, vx, vy, mass), mass 2
+ * (x, y, vx, vy, mass), nu, sink rate. Stage records are device records as
+ * written by cbdiso_b200_step_prologue / cbdiso_b200_stage_record.
+ * ---------------------------------------------------------------------- */
+
+/* Device workspace bytes for cbdiso_b200_stage_adjoint / objective_adjoint. */
+size_t cbdiso_b200_adjoint_workspace_bytes(const cbd_grid_t *grid);
+
+/* Records the branches the stage took (limiter choices, HLLE wave choices,
+ * floor and ceiling) as one 32-bit word per zone of the padded layout, from
+ * the stage's input and output states, for the adjoint to replay. */
+int cbdiso_b200_stage_record_branches(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
+                                      const double *primitive_out, unsigned int *words, void *stream);
+
+/* Forward-mode tangent of a stage: primitive_out and its derivative along
+ * (dprimitive_rd, dprimitive_n, dmass[10], dnu, drate); guards of both
+ * outputs are filled. primitive_n null means the a = 0 stage. */
+int cbdiso_b200_stage_tangent(const cbd_grid_t *grid, const void *stage_dev, const double *dmass, double dnu,
+                              double drate, const double *primitive_rd, const double *dprimitive_rd,
+                              const double *primitive_n, const double *dprimitive_n, double *primitive_out,
+                              double *dprimitive_out, void *stream);
+
+/* Adjoint of a stage: given lam_out (adjoint of primitive_out, zero guards),
+ * ADDS the adjoint of primitive_rd into lam_rd and of primitive_n into lam_n
+ * (interior zones; guard contributions folded), and ADDS the 12 parameter
+ * derivatives into params_out. */
+int cbdiso_b200_stage_adjoint(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
+                              const double *primitive_n, const double *primitive_out, const unsigned int *words,
+                              const double *lam_out, double *lam_rd, double *lam_n, double *params_out,
+                              void *workspace, void *stream);
+
+/* Objective F = sum over zones of w_mdot * (-(mdot_1 + mdot_2)) + w_torque *
+ * torque, with the stage record's end-of-step masses (cbdiso_2d.py:383-471
+ * rates). Tangent: per-block partial sums of dF into `partials`. Adjoint:
+ * ADDS dF/dprimitive into lam and the 12 parameter derivatives into
+ * params_out. */
+int cbdiso_b200_objective_tangent(const cbd_grid_t *grid, const void *stage_dev, const double *dmass,
+                                  double drate, const double *primitive, const double *dprimitive, double w_mdot,
+                                  double w_torque, double *partials, int num_partials, void *stream);
+int cbdiso_b200_objective_adjoint(const cbd_grid_t *grid, const void *stage_dev, const double *primitive,
+                                  double w_mdot, double w_torque, double *lam, double *params_out, void *workspace,
+                                  void *stream);
+
 /* The epilogue quantities alone, on a given state (guards not needed). */
 int cbdiso_b200_reduce(
     const cbd_grid_t *grid, const cbd_epilogue_t *epilogue, const double *primitive,

@@ -126,6 +126,20 @@ def _declare(lib):
     lib.cbdiso_b200_batched_prologue.argtypes = [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int,
                                                  c_int, c_void_p]
     lib.cbdiso_b200_batched_prologue.restype = c_int
+    lib.cbdiso_b200_adjoint_workspace_bytes.argtypes = [POINTER(Grid)]
+    lib.cbdiso_b200_adjoint_workspace_bytes.restype = c_size_t
+    V = c_void_p
+    D = c_double
+    for name, args in {
+        "cbdiso_b200_stage_record_branches": [POINTER(Grid), V, V, V, V, V],
+        "cbdiso_b200_stage_tangent": [POINTER(Grid), V, V, D, D, V, V, V, V, V, V, V],
+        "cbdiso_b200_stage_adjoint": [POINTER(Grid), V, V, V, V, V, V, V, V, V, V, V],
+        "cbdiso_b200_objective_tangent": [POINTER(Grid), V, V, D, V, V, D, D, V, c_int, V],
+        "cbdiso_b200_objective_adjoint": [POINTER(Grid), V, V, D, D, V, V, V, V],
+    }.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = c_int
     lib.cbdiso_b200_abi_sizes.argtypes = [POINTER(c_size_t)]
     lib.cbdiso_b200_abi_sizes.restype = None
     lib.cbdiso_b200_status_string.argtypes = [c_int]
@@ -161,6 +175,8 @@ def exported_symbols():
         "cbdiso_b200_advance_stage_noalloc", "cbdiso_b200_stepper_bytes", "cbdiso_b200_stepper_init",
         "cbdiso_b200_step_prologue", "cbdiso_b200_batch_disk_bytes", "cbdiso_b200_batch_disk_record",
         "cbdiso_b200_batched_stage", "cbdiso_b200_batched_finalize", "cbdiso_b200_batched_prologue",
+        "cbdiso_b200_adjoint_workspace_bytes", "cbdiso_b200_stage_record_branches", "cbdiso_b200_stage_tangent",
+        "cbdiso_b200_stage_adjoint", "cbdiso_b200_objective_tangent", "cbdiso_b200_objective_adjoint",
     ]
 
 

@@ -1,0 +1,355 @@
+"""
+Gradients of time-averaged sink accretion rate and gravitational torque of a
+circumbinary-disk run, by a hand-written discrete adjoint of the RK2 stage.
+
+Objective (dt sequence frozen at the forward run's values):
+
+    J = ( w_mdot * sum_n dt_n (-(mdot_1 + mdot_2))_n + w_torque * sum_n dt_n torque_n ) / sum_n dt_n
+
+with mdot and torque the reductions of cbdiso_2d.Solver.reductions()
+(cbdiso_2d.py:370-503) of the state after step n, with the end-of-step point
+masses. Gradients are with respect to the initial primitive state (its
+density component is dJ / dSigma_0) and to the parameters
+(q, e, nu, sink_rate) of a CircumbinaryDisk.
+
+Reverse sweep: the forward run keeps a checkpoint every `checkpoint_every`
+steps; each segment is recomputed forward from its checkpoint, recording for
+every stage the branches it took (limiter, HLLE waves, floors) with
+cbdiso_b200_stage_record_branches, and the adjoint kernels then replay those
+branches backward through the segment. Point-mass parameter derivatives of
+every stage are chained through the Kepler orbit on the host with
+complex-step derivatives (exact to rounding: the orbit is analytic in q, e).
+
+The forward-mode tangent of the same run (cbdiso_b200_stage_tangent) gives
+the directional derivative for the dot-product test.
+"""
+
+from __future__ import annotations
+
+import cmath
+import ctypes
+import math
+from typing import NamedTuple, Optional
+
+import numpy as np
+
+from . import _capi
+from .cbdiso_2d import NG, NQ, Solver, initial_condition
+from .kepler import OrbitalElements
+from .setups import CircumbinaryDisk
+
+NPAR = 12
+PARAM_NAMES = ("mass_ratio", "eccentricity", "nu", "sink_rate")
+
+
+class Params(NamedTuple):
+    mass_ratio: float = 0.5
+    eccentricity: float = 0.1
+    nu: float = 1e-3
+    sink_rate: float = 10.0
+
+
+def _kepler_complex(t, a, m, q, e):
+    """kepler.py:329-366 evaluated with complex q and e (complex-step)."""
+    w = math.sqrt(1.0 * m / a / a / a)
+    p = 2.0 * math.pi / w
+    tt = t - p * math.floor(t / p)
+    n = w * tt
+    k = complex(n)
+    it = 0
+    while abs(k - e * cmath.sin(k) - n) > 1e-15:
+        k -= (k - e * cmath.sin(k) - n) / (1.0 - e * cmath.cos(k))
+        it += 1
+        if it > 10:
+            raise ValueError("solve_newton_rapheson: no solution")
+    m1 = m / (1.0 + q)
+    m2 = m - m1
+    ck, sk = cmath.cos(k), cmath.sin(k)
+    x1 = -a * q / (1.0 + q) * (e - ck)
+    y1 = +a * q / (1.0 + q) * sk * cmath.sqrt(1.0 - e * e)
+    vx1 = -a * q / (1.0 + q) * w / (1.0 - e * ck) * sk
+    vy1 = +a * q / (1.0 + q) * w / (1.0 - e * ck) * ck * cmath.sqrt(1.0 - e * e)
+    return [x1, y1, vx1, vy1, m1, -x1 / q, -y1 / q, -vx1 / q, -vy1 / q, m2]
+
+
+def mass_jacobian(t, q, e, a=1.0, m=1.0, h=1e-30):
+    """d(x, y, vx, vy, mass of both masses)/d(q, e) at time t: 10 x 2."""
+    jq = [v.imag / h for v in _kepler_complex(t, a, m, complex(q, h), complex(e, 0.0))]
+    je = [v.imag / h for v in _kepler_complex(t, a, m, complex(q, 0.0), complex(e, h))]
+    return np.array([jq, je]).T
+
+
+class AdjointRun:
+    """
+    A differentiable circumbinary-disk run on one GPU: config-0 physics on
+    [-8, 8]^2 with the given (q, e, nu, sink_rate), RK2, `steps` steps at CFL
+    `cfl` (dt frozen after the first forward run), EXACT precision.
+    """
+
+    def __init__(self, resolution=512, steps=400, checkpoint_every=20, cfl=0.3, plm_theta=1.5, mach=10.0,
+                 domain_radius=8.0):
+        self.n = resolution
+        self.steps = steps
+        self.checkpoint_every = checkpoint_every
+        self.cfl = cfl
+        self.plm_theta = plm_theta
+        self.mach = mach
+        self.domain_radius = domain_radius
+        self.dts: Optional[np.ndarray] = None
+        self._lib = _capi.lib()
+
+    # ------------------------------------------------------------------
+    def setup(self, params: Params):
+        return CircumbinaryDisk(domain_radius=self.domain_radius, mach_number=self.mach,
+                                mass_ratio=float(params.mass_ratio), eccentricity=float(params.eccentricity),
+                                nu=float(params.nu), sink_rate=float(params.sink_rate))
+
+    def initial_state(self, seed=0):
+        setup = self.setup(Params())
+        mesh = setup.mesh(self.n)
+        prim = initial_condition(setup, mesh, 0.0)
+        prim[..., 0] += 1e-3 * np.random.default_rng(seed).uniform(-1.0, 1.0, size=(self.n, self.n))
+        return prim
+
+    def _solver(self, params, prim0):
+        setup = self.setup(params)
+        mesh = setup.mesh(self.n)
+        physics = setup.physics
+        physics["diagnostics"] = [dict(quantity="mdot", which_mass=1, accretion=True),
+                                  dict(quantity="mdot", which_mass=2, accretion=True),
+                                  dict(quantity="torque", which_mass="both", gravity=True)]
+        return make_solver_exact(setup, mesh, physics, prim0, self.plm_theta)
+
+    # ------------------------------------------------------------------
+    def forward(self, prim0, params: Params, freeze=False, keep=False):
+        """
+        Run the steps; returns J = (mean accretion rate, mean torque). The
+        first call (or freeze=True) fixes the dt sequence from the CFL rule;
+        later calls reuse it. With keep, checkpoints are kept for gradient().
+        """
+        s = self._solver(params, prim0)
+        if self.dts is None or freeze:
+            dts = []
+        else:
+            dts = list(self.dts)
+        ts, mdot, torque, cps = [], [], [], {}
+        for n in range(self.steps):
+            if keep and n % self.checkpoint_every == 0:
+                cps[n] = s._buf[0].clone()
+            if len(dts) <= n:
+                dts.append(s.mesh.min_spacing() / s.maximum_wavespeed() * self.cfl)
+            ts.append(s.time)
+            s.advance(dts[n])
+            m1, m2, tq = s.reductions()
+            mdot.append(-(m1 + m2))
+            torque.append(tq)
+        self.dts = np.array(dts)
+        w = self.dts / self.dts.sum()
+        J = np.array([np.dot(w, mdot), np.dot(w, torque)])
+        if keep:
+            self._fwd = dict(solver=s, times=ts, checkpoints=cps, params=params)
+        return J
+
+    # ------------------------------------------------------------------
+    def _records(self, s, t0, dt):
+        """Device stage records of one RK2 step starting at t0."""
+        import torch
+
+        lib = self._lib
+        t1 = t0 * 0.0 + (t0 + dt) * 1.0
+        t_end = t0 * 0.5 + (t1 + dt) * 0.5
+        ep = s._epilogue(t_end, True, [])
+        nb = int(lib.cbdiso_b200_stage_record_bytes())
+        host = bytearray(2 * nb)
+        for k, (a, ts) in enumerate(((0.0, t0), (0.5, t1))):
+            st = _capi.Stage()
+            m1, m2 = s._physics.point_masses(ts)
+            from .cbdiso_2d import _mass_struct
+
+            _mass_struct(m1, st.mass[0])
+            _mass_struct(m2, st.mass[1])
+            st.a, st.dt, st.buffer_central_mass = a, dt, m1.mass + m2.mass
+            buf = (ctypes.c_char * nb)()
+            _capi.check(lib.cbdiso_b200_stage_record(ctypes.byref(s._grid), ctypes.byref(st), ctypes.byref(ep),
+                                                     buf), "stage_record")
+            host[k * nb:(k + 1) * nb] = bytes(buf)
+        dev = torch.frombuffer(host, dtype=torch.uint8).to(s.device)
+        return dev, nb, (t0, t1, t_end)
+
+    def gradient(self, weights=(1.0, 0.0)):
+        """
+        dJ/dprim0 (ni, nj, 3) and dJ/d(q, e, nu, sink_rate) for
+        J = weights[0] * mean accretion + weights[1] * mean torque, at the
+        last forward(keep=True) run.
+        """
+        import torch
+
+        lib = self._lib
+        f = self._fwd
+        s: Solver = f["solver"]
+        params: Params = f["params"]
+        g = ctypes.byref(s._grid)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        P = lambda t: ctypes.c_void_p(t.data_ptr())
+        shape = s._buf[0].shape
+        f64 = dict(dtype=torch.float64, device=s.device)
+        ws = torch.zeros(int(lib.cbdiso_b200_adjoint_workspace_bytes(g)) // 8 + 8, **f64)
+        words = [torch.zeros(shape[:2], dtype=torch.int32, device=s.device) for _ in range(2)]
+        total = self.dts.sum()
+        da = s.mesh.dx * s.mesh.dy
+        lam = torch.zeros(shape, **f64)
+        n_evals = 3 * self.steps
+        pars = torch.zeros((n_evals, NPAR), **f64)
+        eval_times = [0.0] * n_evals
+        steps = self.steps
+        K = self.checkpoint_every
+        work = torch.empty(shape, **f64)
+        for start in reversed(range(0, steps, K)):
+            stop = min(start + K, steps)
+            # recompute the segment, keeping every state and stage output
+            p = [f["checkpoints"][start].clone()]
+            stars, recs = [], []
+            for n in range(start, stop):
+                dev, nb, times = self._records(s, f["times"][n], float(self.dts[n]))
+                pn = p[-1]
+                star = torch.empty(shape, **f64)
+                out = torch.empty(shape, **f64)
+                _capi.check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(_capi.Stage()), P(dev), P(pn), None,
+                                                          P(star), None, P(s._scratch), P(s._result), stream),
+                            "advance_stage")
+                a2 = _capi.Stage()
+                a2.a = 0.5
+                # the in-place final stage is replayed out of place: inputs star, pn -> out
+                _capi.check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(a2), ctypes.c_void_p(dev.data_ptr() + nb),
+                                                          P(star), P(pn), P(out), None, P(s._scratch),
+                                                          P(s._result), stream), "advance_stage")
+                stars.append(star)
+                recs.append((dev, nb, times))
+                p.append(out)
+            # backward through the segment
+            for n in reversed(range(start, stop)):
+                idx = n - start
+                dev, nb, (t0, t1, t_end) = recs[idx]
+                pn, star, out = p[idx], stars[idx], p[idx + 1]
+                rec1, rec2 = P(dev), ctypes.c_void_p(dev.data_ptr() + nb)
+                c = float(self.dts[n]) / total * da
+                row = 3 * n
+                # objective term of step n (state after the step, end masses)
+                _capi.check(lib.cbdiso_b200_objective_adjoint(g, rec2, P(out), weights[0] * c, weights[1] * c,
+                                                              P(lam), P(pars[row + 2]), P(ws), stream),
+                            "objective_adjoint")
+                eval_times[row + 2] = t_end
+                # stage 2: inputs star (read), pn (u_n)
+                _capi.check(lib.cbdiso_b200_stage_record_branches(g, rec2, P(star), P(out), P(words[1]), stream),
+                            "record")
+                lam_star = torch.zeros(shape, **f64)
+                lam_n = torch.zeros(shape, **f64)
+                _capi.check(lib.cbdiso_b200_stage_adjoint(g, rec2, P(star), P(pn), P(out), P(words[1]), P(lam),
+                                                          P(lam_star), P(lam_n), P(pars[row + 1]), P(ws), stream),
+                            "stage_adjoint")
+                eval_times[row + 1] = t1
+                # stage 1: input pn
+                _capi.check(lib.cbdiso_b200_stage_record_branches(g, rec1, P(pn), P(star), P(words[0]), stream),
+                            "record")
+                _capi.check(lib.cbdiso_b200_stage_adjoint(g, rec1, P(pn), None, P(star), P(words[0]), P(lam_star),
+                                                          P(lam_n), None, P(pars[row]), P(ws), stream),
+                            "stage_adjoint")
+                eval_times[row] = t0
+                lam = lam_n
+        grad_state = lam[NG:-NG, NG:-NG].cpu().numpy()
+        pp = pars.cpu().numpy()
+        dq = de = 0.0
+        for r in range(n_evals):
+            jac = mass_jacobian(eval_times[r], params.mass_ratio, params.eccentricity)
+            dq += float(pp[r, :10] @ jac[:, 0])
+            de += float(pp[r, :10] @ jac[:, 1])
+        dnu = float(pp[:, 10].sum())
+        drate = float(pp[:, 11].sum())
+        return grad_state, np.array([dq, de, dnu, drate])
+
+    # ------------------------------------------------------------------
+    def tangent(self, prim0, params: Params, dprim0, dparams, weights=(1.0, 0.0)):
+        """
+        Directional derivative of J along (dprim0, dparams) by the
+        forward-mode tangent kernels, with the frozen dt sequence.
+        """
+        import torch
+
+        lib = self._lib
+        s = self._solver(params, prim0)
+        g = ctypes.byref(s._grid)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        P = lambda t: ctypes.c_void_p(t.data_ptr())
+        shape = s._buf[0].shape
+        f64 = dict(dtype=torch.float64, device=s.device)
+        p = s._buf[0].clone()
+        dp = torch.zeros(shape, **f64)
+        dp[NG:-NG, NG:-NG] = torch.from_numpy(np.ascontiguousarray(dprim0)).to(s.device)
+        _capi.check(lib.cbdiso_b200_fill_guards(g, P(dp), stream), "fill_guards")
+        q, e = params.mass_ratio, params.eccentricity
+        dq, de, dnu, drate = (float(v) for v in dparams)
+        total = self.dts.sum()
+        da = s.mesh.dx * s.mesh.dy
+        parts = torch.zeros(256, **f64)
+        acc = 0.0
+        t = s.time
+        for n in range(self.steps):
+            dt = float(self.dts[n])
+            dev, nb, (t0, t1, t_end) = self._records(s, t, dt)
+            dm0 = mass_jacobian(t0, q, e) @ np.array([dq, de])
+            dm1 = mass_jacobian(t1, q, e) @ np.array([dq, de])
+            dme = mass_jacobian(t_end, q, e) @ np.array([dq, de])
+            star, dstar = torch.empty(shape, **f64), torch.empty(shape, **f64)
+            out, dout = torch.empty(shape, **f64), torch.empty(shape, **f64)
+            d0 = (ctypes.c_double * 10)(*dm0)
+            d1 = (ctypes.c_double * 10)(*dm1)
+            de_ = (ctypes.c_double * 10)(*dme)
+            _capi.check(lib.cbdiso_b200_stage_tangent(g, P(dev), d0, dnu, drate, P(p), P(dp), None, None, P(star),
+                                                      P(dstar), stream), "stage_tangent")
+            _capi.check(lib.cbdiso_b200_stage_tangent(g, ctypes.c_void_p(dev.data_ptr() + nb), d1, dnu, drate,
+                                                      P(star), P(dstar), P(p), P(dp), P(out), P(dout), stream),
+                        "stage_tangent")
+            c = dt / total * da
+            _capi.check(lib.cbdiso_b200_objective_tangent(g, ctypes.c_void_p(dev.data_ptr() + nb), de_, drate,
+                                                          P(out), P(dout), weights[0] * c, weights[1] * c,
+                                                          P(parts), 256, stream), "objective_tangent")
+            acc += float(parts.sum().item())
+            p, dp = out, dout
+            t = t_end
+        return acc
+
+
+def make_solver_exact(setup, mesh, physics, prim0, plm_theta):
+    return Solver(setup=setup, mesh=mesh, solution=prim0, physics=physics,
+                  options=dict(rk_order=2, plm_theta=plm_theta, precision="exact"))
+
+
+# ---------------------------------------------------------------------------
+# torch.autograd interface
+# ---------------------------------------------------------------------------
+
+
+def objective_function(run: AdjointRun, weights=(1.0, 0.0)):
+    """
+    A torch.autograd.Function computing J(sigma0, params) for `run`:
+    sigma0 is the initial surface density (ni, nj) (velocities from the
+    setup), params the tensor (q, e, nu, sink_rate); J is a 0-d tensor.
+    """
+    import torch
+
+    class CircumbinaryObjective(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, sigma0, params):
+            prim = run.initial_state(seed=0)
+            prim[..., 0] = sigma0.detach().cpu().numpy()
+            p = Params(*[float(v) for v in params.detach().cpu().tolist()])
+            J = run.forward(prim, p, keep=True)
+            return torch.tensor(float(weights[0] * J[0] + weights[1] * J[1]), dtype=torch.float64)
+
+        @staticmethod
+        def backward(ctx, gJ):
+            grad_state, grad_params = run.gradient(weights)
+            g = float(gJ)
+            return (torch.from_numpy(grad_state[..., 0] * g), torch.from_numpy(grad_params * g))
+
+    return CircumbinaryObjective

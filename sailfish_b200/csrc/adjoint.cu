@@ -1,0 +1,944 @@
+// Tangent (forward-mode) and discrete adjoint (reverse-mode) of one RK stage
+// and of the end-of-step objective, plus the branch record the adjoint
+// replays. Built with -fmad=false.
+//
+// Adjoint of a stage, as passes over zones and faces (all arrays in the
+// padded (ni + 4, nj + 4) layout; guard entries of adjoints are folded into
+// the zones they copy at the end):
+//   A  zone:  lambda of the output primitives -> lambda of the RK sum
+//             (conserved-to-primitive with the recorded floor / ceiling
+//             flags, the RK weights); u_n part to lambda_un.
+//   B  face:  lambda of each face flux from the two adjacent zones; HLLE and
+//             viscous-term products with the recorded am / ap choices;
+//             face sound-speed terms to the point-mass parameters.
+//   C  zone:  gather the four faces: direct and slope contributions,
+//             rho * strain products, point-mass and buffer sources.
+//   D  zone:  slope products to the three zones of each slope (recorded
+//             limiter choices).
+//   E  zone:  fold guard-zone adjoints into the zones they copy.
+// Parameter derivatives (per mass x, y, vx, vy, mass; nu; sink rate) are
+// summed per block and then per stage, in a fixed order.
+#include <cstring>
+
+#include "adjoint_zone.cuh"
+#include "cbd_internal.h"
+
+namespace cbd {
+
+constexpr int NPAR = 12;  // m1 (x, y, vx, vy, mass), m2 (...), nu, sink rate
+
+namespace {
+
+__device__ __forceinline__ size_t zi(int i, int j, int nj) { return (size_t)(i + NG) * (nj + 2 * NG) + (j + NG); }
+
+struct TangentParams {
+    double dm[2][5];  // d(x, y, vx, vy, mass) of both masses
+    double dnu, drate;
+};
+
+template <class T>
+__device__ __forceinline__ void masses_t(const StageDev &st, const TangentParams *tp, MassT<T> *m);
+
+template <>
+__device__ __forceinline__ void masses_t<Dual>(const StageDev &st, const TangentParams *tp, MassT<Dual> *m)
+{
+    for (int p = 0; p < 2; ++p) {
+        const MassDev &b = st.m[p];
+        m[p].x = dual(b.x, tp->dm[p][0]);
+        m[p].y = dual(b.y, tp->dm[p][1]);
+        m[p].vx = dual(b.vx, tp->dm[p][2]);
+        m[p].vy = dual(b.vy, tp->dm[p][3]);
+        m[p].mass = dual(b.mass, tp->dm[p][4]);
+        m[p].sink_rate = dual(b.sink_rate, tp->drate);
+        m[p].base = &st.m[p];
+    }
+}
+
+template <>
+__device__ __forceinline__ void masses_t<double>(const StageDev &st, const TangentParams *, MassT<double> *m)
+{
+    for (int p = 0; p < 2; ++p) {
+        const MassDev &b = st.m[p];
+        m[p] = MassT<double>{b.x, b.y, b.vx, b.vy, b.mass, b.sink_rate, &st.m[p]};
+    }
+}
+
+// ---------------------------------------------------------------------------
+// tangent of a stage: thread per interior zone
+// ---------------------------------------------------------------------------
+
+__global__ void stage_tangent_kernel(Consts k, const StageDev *stp, TangentParams tp, const double *p,
+                                     const double *dp, const double *pun, const double *dpun, double *out,
+                                     double *dout)
+{
+    __shared__ StageDev st;
+    if (threadIdx.x == 0)
+        st = *stp;
+    __syncthreads();
+    const long n = (long)k.ni * k.nj;
+    const long z = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (z >= n)
+        return;
+    const int i = (int)(z / k.nj), j = (int)(z - (long)i * k.nj);
+    const int nj = k.nj;
+    MassT<Dual> m[2];
+    masses_t<Dual>(st, &tp, m);
+    auto P = [&](int di, int dj, int q) {
+        const size_t o = zi(i + di, j + dj, nj) * 3 + q;
+        return dual(p[o], dp[o]);
+    };
+    Dual un[3];
+    const size_t oc = zi(i, j, nj) * 3;
+    if (pun) {
+        const Dual r = dual(pun[oc], dpun[oc]);
+        un[0] = r;
+        un[1] = dual(pun[oc + 1], dpun[oc + 1]) * r;
+        un[2] = dual(pun[oc + 2], dpun[oc + 2]) * r;
+    } else {
+        const Dual r = P(0, 0, 0);
+        un[0] = r;
+        un[1] = P(0, 0, 1) * r;
+        un[2] = P(0, 0, 2) * r;
+    }
+    Dual o[3];
+    zone_update_generic<Dual>(k, st, m, dual(k.nu, tp.dnu), i, j, P, un, o);
+    for (int q = 0; q < 3; ++q) {
+        out[oc + q] = o[q].v;
+        dout[oc + q] = o[q].d;
+    }
+}
+
+// zero-gradient guard images of a tangent (same rule as the state's guards)
+__global__ void guards_kernel(int ni, int nj, double *a)
+{
+    const long wi = ni + 2 * NG, wj = nj + 2 * NG;
+    for (long z = blockIdx.x * (long)blockDim.x + threadIdx.x; z < wi * wj; z += (long)gridDim.x * blockDim.x) {
+        const int ii = (int)(z / wj) - NG, jj = (int)(z % wj) - NG;
+        if (ii >= 0 && ii < ni && jj >= 0 && jj < nj)
+            continue;
+        const int ci = ii < 0 ? 0 : (ii >= ni ? ni - 1 : ii);
+        const int cj = jj < 0 ? 0 : (jj >= nj ? nj - 1 : jj);
+        for (int q = 0; q < 3; ++q)
+            a[zi(ii, jj, nj) * 3 + q] = a[zi(ci, cj, nj) * 3 + q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// branch record: thread per zone of [-1, ni] x [-1, nj]
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void slopes_at(const Consts &k, const double *p, int i, int j, double *gx, double *gy,
+                                          unsigned *bits)
+{
+    const int nj = k.nj;
+    unsigned b = 0;
+    for (int q = 0; q < 3; ++q) {
+        const double xm = p[zi(i - 1, j, nj) * 3 + q], x0 = p[zi(i, j, nj) * 3 + q], xp = p[zi(i + 1, j, nj) * 3 + q];
+        const double ym = p[zi(i, j - 1, nj) * 3 + q], yp = p[zi(i, j + 1, nj) * 3 + q];
+        const unsigned sx = slope_select(xm, x0, xp, k.theta);
+        const unsigned sy = slope_select(ym, x0, yp, k.theta);
+        gx[q] = slope_generic(xm, x0, xp, k.theta);
+        gy[q] = slope_generic(ym, x0, yp, k.theta);
+        b |= sx << (2 * q);
+        b |= sy << (6 + 2 * q);
+    }
+    if (bits)
+        *bits = b;
+}
+
+__global__ void record_kernel(Consts k, const StageDev *stp, const double *p, const double *pout,
+                              unsigned *words)
+{
+    __shared__ StageDev st;
+    if (threadIdx.x == 0)
+        st = *stp;
+    __syncthreads();
+    const int ni = k.ni, nj = k.nj;
+    const long wi = ni + 2, wj = nj + 2;
+    const long z = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (z >= wi * wj)
+        return;
+    const int i = (int)(z / wj) - 1, j = (int)(z % wj) - 1;
+    MassT<double> m[2];
+    masses_t<double>(st, nullptr, m);
+    double gx[3], gy[3];
+    unsigned w = 0;
+    slopes_at(k, p, i, j, gx, gy, &w);
+    if (i <= ni - 1 && j >= 0 && j < nj) {  // east x-face (i + 1/2)
+        double gx1[3], gy1[3];
+        slopes_at(k, p, i + 1, j, gx1, gy1, nullptr);
+        double pl[3], pr[3], f[3];
+        for (int q = 0; q < 3; ++q) {
+            pl[q] = p[zi(i, j, nj) * 3 + q] + 0.5 * gx[q];
+            pr[q] = p[zi(i + 1, j, nj) * 3 + q] - 0.5 * gx1[q];
+        }
+        unsigned sel;
+        hlle_generic<double, 0>(pl, pr, cs2_generic(k, m, k.xl + (i + 1.0) * k.dx, k.yl + (j + 0.5) * k.dy),
+                                f, &sel);
+        w |= sel << BW_XFACE;
+    }
+    if (i >= 0 && i < ni && j <= nj) {  // south y-face (j - 1/2)
+        double gx0[3], gy0[3];
+        slopes_at(k, p, i, j - 1, gx0, gy0, nullptr);
+        double pl[3], pr[3], f[3];
+        for (int q = 0; q < 3; ++q) {
+            pl[q] = p[zi(i, j - 1, nj) * 3 + q] + 0.5 * gy0[q];
+            pr[q] = p[zi(i, j, nj) * 3 + q] - 0.5 * gy[q];
+        }
+        unsigned sel;
+        hlle_generic<double, 1>(pl, pr, cs2_generic(k, m, k.xl + (i + 0.5) * k.dx, k.yl + (j + 0.0) * k.dy),
+                                f, &sel);
+        w |= sel << BW_YFACE;
+    }
+    if (i >= 0 && i < ni && j >= 0 && j < nj) {
+        const double *o = pout + zi(i, j, nj) * 3;
+        if (!(o[0] > k.rho_min))
+            w |= BW_FLOOR;
+        if (!(fabs(o[1]) < k.vmax))
+            w |= BW_CEIL_X;
+        if (!(fabs(o[2]) < k.vmax))
+            w |= BW_CEIL_Y;
+    }
+    words[zi(i, j, nj)] = w;
+}
+
+// ---------------------------------------------------------------------------
+// adjoint building blocks
+// ---------------------------------------------------------------------------
+
+// d(cs^2)/d(mass parameters) at (x, y), times lam, into par[0..9]
+__device__ __forceinline__ void cs2_param_vjp(const Consts &k, const StageDev &st, double x, double y, double lam,
+                                              double *par)
+{
+    if (k.eos != 2 || lam == 0.0)
+        return;
+    for (int p = 0; p < 2; ++p) {
+        const MassDev &m = st.m[p];
+        if (!(m.mass > 0.0))
+            continue;
+        const double dx = x - m.x, dy = y - m.y;
+        const double S = dx * dx + dy * dy + m.soft2;
+        const double s12 = 1.0 / sqrt(S);
+        const double s32 = s12 / S;
+        par[5 * p + 0] += lam * m.mass * dx * s32 / k.mach2;
+        par[5 * p + 1] += lam * m.mass * dy * s32 / k.mach2;
+        par[5 * p + 4] += lam * s12 / k.mach2;
+    }
+}
+
+// HLLE vector-Jacobian product for the recorded am / ap choice `sel`.
+template <int DIR>
+__device__ __forceinline__ void hlle_vjp(const double *pl, const double *pr, double cs2, unsigned sel,
+                                         const double *lf, double *lpl, double *lpr, double *lcs2)
+{
+    const double ul[3] = {pl[0], pl[1] * pl[0], pl[2] * pl[0]};
+    const double ur[3] = {pr[0], pr[1] * pr[0], pr[2] * pr[0]};
+    const double vl = DIR == 0 ? pl[1] : pl[2];
+    const double vr = DIR == 0 ? pr[1] : pr[2];
+    double fl[3] = {vl * ul[0], vl * ul[1], vl * ul[2]};
+    double fr[3] = {vr * ur[0], vr * ur[1], vr * ur[2]};
+    fl[1 + DIR] += pl[0] * cs2;
+    fr[1 + DIR] += pr[0] * cs2;
+    const double cs = sqrt(cs2);
+    const unsigned s_am = sel & 3u, s_ap = (sel >> 2) & 3u;
+    const double am = s_am == 0 ? 0.0 : (s_am == 1 ? vl - cs : vr - cs);
+    const double ap = s_ap == 0 ? 0.0 : (s_ap == 1 ? vl + cs : vr + cs);
+    const double D = ap - am;
+    double lfl[3], lfr[3], lul[3], lur[3], lap = 0.0, lam = 0.0;
+    for (int q = 0; q < 3; ++q) {
+        const double F = (fl[q] * ap - fr[q] * am - (ul[q] - ur[q]) * ap * am) / D;
+        const double w = lf[q] / D;
+        lfl[q] = w * ap;
+        lfr[q] = -w * am;
+        lul[q] = -w * ap * am;
+        lur[q] = w * ap * am;
+        lap += w * (fl[q] - (ul[q] - ur[q]) * am - F);
+        lam += w * (F - fr[q] - (ul[q] - ur[q]) * ap);
+    }
+    double lvl = 0.0, lvr = 0.0, lcs = 0.0;
+    if (s_am == 1) {
+        lvl += lam;
+        lcs -= lam;
+    } else if (s_am == 2) {
+        lvr += lam;
+        lcs -= lam;
+    }
+    if (s_ap == 1) {
+        lvl += lap;
+        lcs += lap;
+    } else if (s_ap == 2) {
+        lvr += lap;
+        lcs += lap;
+    }
+    if (cs > 0.0)
+        *lcs2 += lcs / (2.0 * cs);
+    // fluxes: f0 = v u0, f1 = v u1 (+ rho cs2 if DIR == 0), f2 = v u2 (+ rho cs2 if DIR == 1)
+    lvl += lfl[0] * ul[0] + lfl[1] * ul[1] + lfl[2] * ul[2];
+    lvr += lfr[0] * ur[0] + lfr[1] * ur[1] + lfr[2] * ur[2];
+    double lrl = lfl[1 + DIR] * cs2, lrr = lfr[1 + DIR] * cs2;
+    *lcs2 += lfl[1 + DIR] * pl[0] + lfr[1 + DIR] * pr[0];
+    for (int q = 0; q < 3; ++q) {
+        lul[q] += lfl[q] * vl;
+        lur[q] += lfr[q] * vr;
+    }
+    // conserved states u = (rho, vx rho, vy rho)
+    lrl += lul[0] + lul[1] * pl[1] + lul[2] * pl[2];
+    lrr += lur[0] + lur[1] * pr[1] + lur[2] * pr[2];
+    double lvxl = lul[1] * pl[0], lvyl = lul[2] * pl[0];
+    double lvxr = lur[1] * pr[0], lvyr = lur[2] * pr[0];
+    if (DIR == 0) {
+        lvxl += lvl;
+        lvxr += lvr;
+    } else {
+        lvyl += lvl;
+        lvyr += lvr;
+    }
+    lpl[0] += lrl;
+    lpl[1] += lvxl;
+    lpl[2] += lvyl;
+    lpr[0] += lrr;
+    lpr[1] += lvxr;
+    lpr[2] += lvyr;
+}
+
+// Gravity of one mass: d(du)/d(sigma) and d(du)/d(mass parameters).
+__device__ __forceinline__ void gravity_vjp(const MassDev &m, double x, double y, double dt, const double *pc,
+                                            const double *ld, double *lp, double *par5)
+{
+    if (m.mass == 0.0)
+        return;
+    const double dx = x - m.x, dy = y - m.y;
+    const double S = dx * dx + dy * dy + m.soft2;
+    const double g = inv_pow15<false>(S);
+    const double h = g / S;
+    const double sig = pc[0];
+    const double a = ld[1] * dx + ld[2] * dy;
+    lp[0] += -m.mass * g * a * dt;
+    par5[4] += -sig * g * a * dt;
+    par5[0] += -sig * m.mass * dt * (ld[1] * (3.0 * dx * dx * h - g) + ld[2] * (3.0 * dx * dy * h));
+    par5[1] += -sig * m.mass * dt * (ld[1] * (3.0 * dx * dy * h) + ld[2] * (3.0 * dy * dy * h - g));
+}
+
+// Sink of one mass, direction by direction through the dual-number sink:
+// inputs (sigma, vx, vy, xp, yp, vxp, vyp, rate).
+__device__ void sink_vjp(const MassDev &m, double x, double y, double dt, const double *pc, const double *ld,
+                         double *lp, double *par5, double *lrate)
+{
+    if (m.sink_rate == 0.0 || m.sink_model < 1 || m.sink_model > 3)
+        return;
+    const double dx = x - m.x, dy = y - m.y;
+    if (!(dx * dx + dy * dy < m.sink_hi2))
+        return;
+    double seed[8];
+    for (int dir = 0; dir < 8; ++dir) {
+        for (int s = 0; s < 8; ++s)
+            seed[s] = s == dir ? 1.0 : 0.0;
+        Dual du[3] = {dual(0.0), dual(0.0), dual(0.0)};
+        sink_generic<Dual>(m, dual(m.x, seed[3]), dual(m.y, seed[4]), dual(m.vx, seed[5]), dual(m.vy, seed[6]),
+                           dual(m.sink_rate, seed[7]), x, y, dt, dual(pc[0], seed[0]), dual(pc[1], seed[1]),
+                           dual(pc[2], seed[2]), du);
+        const double v = ld[0] * du[0].d + ld[1] * du[1].d + ld[2] * du[2].d;
+        if (dir < 3)
+            lp[dir] += v;
+        else if (dir < 7)
+            par5[dir - 3] += v;
+        else
+            *lrate += v;
+    }
+}
+
+template <int BJ>
+__device__ __forceinline__ void block_sum_params(double (&par)[NPAR], double *out)
+{
+    __shared__ double sm[NPAR * (BJ / 32)];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int v = 0; v < NPAR; ++v) {
+        double x = par[v];
+        for (int o = 16; o > 0; o >>= 1)
+            x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0)
+            sm[v * (BJ / 32) + warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < NPAR) {
+        double x = 0.0;
+        for (int w = 0; w < BJ / 32; ++w)
+            x += sm[threadIdx.x * (BJ / 32) + w];
+        out[(size_t)blockIdx.x * NPAR + threadIdx.x] = x;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// adjoint passes
+// ---------------------------------------------------------------------------
+
+// A: zone (interior). lam_d = (1 - a) lambda_u'; lambda_un += p2c^T (a lambda_u').
+__global__ void adj_pass_a(Consts k, const StageDev *stp, const double *pout, const unsigned *words,
+                           const double *lam_out, const double *pun, double *lam_d, double *lam_un)
+{
+    const long n = (long)k.ni * k.nj;
+    const long z = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (z >= n)
+        return;
+    const int i = (int)(z / k.nj), j = (int)(z - (long)i * k.nj);
+    const size_t c = zi(i, j, k.nj);
+    const unsigned w = words[c];
+    const double *o = pout + c * 3;
+    const double *l = lam_out + c * 3;
+    const double rho = o[0];
+    const double lvx = (w & BW_CEIL_X) ? 0.0 : l[1];
+    const double lvy = (w & BW_CEIL_Y) ? 0.0 : l[2];
+    double lu[3];
+    lu[1] = lvx / rho;
+    lu[2] = lvy / rho;
+    lu[0] = (w & BW_FLOOR) ? 0.0 : l[0] - (o[1] * lvx + o[2] * lvy) / rho;
+    const double a = stp->a, b = stp->one_minus_a;
+    for (int q = 0; q < 3; ++q)
+        lam_d[c * 3 + q] = b * lu[q];
+    if (pun && a != 0.0) {
+        const double *pn = pun + c * 3;
+        const double l0 = a * lu[0], l1 = a * lu[1], l2 = a * lu[2];
+        lam_un[c * 3 + 0] += l0 + l1 * pn[1] + l2 * pn[2];
+        lam_un[c * 3 + 1] += l1 * pn[0];
+        lam_un[c * 3 + 2] += l2 * pn[0];
+    }
+}
+
+// slopes and rho * strain of a zone
+__device__ __forceinline__ void zone_slopes(const Consts &k, const double *p, int i, int j, double *gx, double *gy,
+                                            double *rs)
+{
+    slopes_at(k, p, i, j, gx, gy, nullptr);
+    if (k.nu > 0.0)
+        rho_strain_generic(p[zi(i, j, k.nj) * 3], gx, gy, k, rs);
+    else
+        rs[0] = rs[1] = rs[2] = 0.0;
+}
+
+// B: faces. FX[c] holds the x-face i + 1/2 of zone c = (i, j); FY[c] the
+// y-face j - 1/2. Layout per face: lambda of the minus-side face state (3),
+// of the plus-side face state (3), of the two rho*strain components used on
+// the minus side (2) and on the plus side (2).
+template <int BJ>
+__global__ void __launch_bounds__(BJ) adj_pass_b(Consts k, const StageDev *stp, const double *p,
+                                                 const unsigned *words, const double *lam_d, double *fx, double *fy,
+                                                 double *par_out)
+{
+    __shared__ StageDev st;
+    if (threadIdx.x == 0)
+        st = *stp;
+    __syncthreads();
+    const int ni = k.ni, nj = k.nj;
+    const long wi = ni + 2, wj = nj + 2;
+    const long z = blockIdx.x * (long)BJ + threadIdx.x;
+    double par[NPAR];
+    for (int v = 0; v < NPAR; ++v)
+        par[v] = 0.0;
+    MassT<double> m[2];
+    masses_t<double>(st, nullptr, m);
+    const double dt = st.dt, hn = 0.5 * k.nu;
+    if (z < wi * wj) {
+        const int i = (int)(z / wj) - 1, j = (int)(z % wj) - 1;
+        const size_t c = zi(i, j, nj);
+        const unsigned w = words[c];
+        if (i <= ni - 1 && j >= 0 && j < nj) {  // x-face i + 1/2: L = (i, j), R = (i + 1, j)
+            double gxl[3], gyl[3], rsl[3], gxr[3], gyr[3], rsr[3];
+            zone_slopes(k, p, i, j, gxl, gyl, rsl);
+            zone_slopes(k, p, i + 1, j, gxr, gyr, rsr);
+            const size_t cr = zi(i + 1, j, nj);
+            double pl[3], pr[3], lf[3];
+            const bool lin = i >= 0, rin = i + 1 < ni;
+            for (int q = 0; q < 3; ++q) {
+                pl[q] = p[c * 3 + q] + 0.5 * gxl[q];
+                pr[q] = p[cr * 3 + q] - 0.5 * gxr[q];
+                const double ldl = lin ? lam_d[c * 3 + q] : 0.0, ldr = rin ? lam_d[cr * 3 + q] : 0.0;
+                lf[q] = (ldr - ldl) * dt / k.dx;
+            }
+            const double xf = k.xl + (i + 1.0) * k.dx, yc = k.yl + (j + 0.5) * k.dy;
+            const double cs2 = cs2_generic(k, m, xf, yc);
+            double lpl[3] = {0, 0, 0}, lpr[3] = {0, 0, 0}, lcs2 = 0.0;
+            hlle_vjp<0>(pl, pr, cs2, (w >> BW_XFACE) & 15u, lf, lpl, lpr, &lcs2);
+            cs2_param_vjp(k, st, xf, yc, lcs2, par);
+            double *o = fx + c * 10;
+            for (int q = 0; q < 3; ++q) {
+                o[q] = lpl[q];
+                o[3 + q] = lpr[q];
+            }
+            if (k.nu > 0.0) {
+                // f1 -= hn (rsL_xx + rsR_xx), f2 -= hn (rsL_xy + rsR_xy)
+                o[6] = -hn * lf[1];
+                o[7] = -hn * lf[2];
+                o[8] = -hn * lf[1];
+                o[9] = -hn * lf[2];
+                par[10] += -0.5 * (rsl[0] + rsr[0]) * lf[1] - 0.5 * (rsl[1] + rsr[1]) * lf[2];
+            } else {
+                o[6] = o[7] = o[8] = o[9] = 0.0;
+            }
+        }
+        if (i >= 0 && i < ni && j <= nj && j >= 0) {  // y-face j - 1/2: L = (i, j - 1), R = (i, j)
+            const size_t cl = zi(i, j - 1, nj);
+            double gxl[3], gyl[3], rsl[3], gxr[3], gyr[3], rsr[3];
+            zone_slopes(k, p, i, j - 1, gxl, gyl, rsl);
+            zone_slopes(k, p, i, j, gxr, gyr, rsr);
+            double pl[3], pr[3], lf[3];
+            const bool lin = j - 1 >= 0, rin = j < nj;
+            for (int q = 0; q < 3; ++q) {
+                pl[q] = p[cl * 3 + q] + 0.5 * gyl[q];
+                pr[q] = p[c * 3 + q] - 0.5 * gyr[q];
+                const double ldl = lin ? lam_d[cl * 3 + q] : 0.0, ldr = rin ? lam_d[c * 3 + q] : 0.0;
+                lf[q] = (ldr - ldl) * dt / k.dy;
+            }
+            const double xc = k.xl + (i + 0.5) * k.dx, yf = k.yl + (j + 0.0) * k.dy;
+            const double cs2 = cs2_generic(k, m, xc, yf);
+            double lpl[3] = {0, 0, 0}, lpr[3] = {0, 0, 0}, lcs2 = 0.0;
+            hlle_vjp<1>(pl, pr, cs2, (w >> BW_YFACE) & 15u, lf, lpl, lpr, &lcs2);
+            cs2_param_vjp(k, st, xc, yf, lcs2, par);
+            double *o = fy + c * 10;
+            for (int q = 0; q < 3; ++q) {
+                o[q] = lpl[q];
+                o[3 + q] = lpr[q];
+            }
+            if (k.nu > 0.0) {
+                // g1 -= hn (rsL_xy + rsR_xy), g2 -= hn (rsL_yy + rsR_yy)
+                o[6] = -hn * lf[1];
+                o[7] = -hn * lf[2];
+                o[8] = -hn * lf[1];
+                o[9] = -hn * lf[2];
+                par[10] += -0.5 * (rsl[1] + rsr[1]) * lf[1] - 0.5 * (rsl[2] + rsr[2]) * lf[2];
+            } else {
+                o[6] = o[7] = o[8] = o[9] = 0.0;
+            }
+        }
+    }
+    block_sum_params<BJ>(par, par_out);
+}
+
+// C: zones of [-1, ni] x [-1, nj]: face gathers, rho * strain, sources.
+template <int BJ>
+__global__ void __launch_bounds__(BJ) adj_pass_c(Consts k, const StageDev *stp, const double *p,
+                                                 const double *lam_d, const double *fx, const double *fy,
+                                                 double *lam_g, double *lam_p, double *par_out)
+{
+    __shared__ StageDev st;
+    if (threadIdx.x == 0)
+        st = *stp;
+    __syncthreads();
+    const int ni = k.ni, nj = k.nj;
+    const long wi = ni + 2, wj = nj + 2;
+    const long z = blockIdx.x * (long)BJ + threadIdx.x;
+    double par[NPAR];
+    for (int v = 0; v < NPAR; ++v)
+        par[v] = 0.0;
+    if (z < wi * wj) {
+        const int i = (int)(z / wj) - 1, j = (int)(z % wj) - 1;
+        const size_t c = zi(i, j, nj);
+        const double *xe = fx + c * 10;                 // x-face i + 1/2 (zone is its minus side)
+        const double *xw = fx + zi(i - 1, j, nj) * 10;  // x-face i - 1/2 (plus side)
+        const double *ys = fy + c * 10;                 // y-face j - 1/2 (plus side)
+        const double *yn = fy + zi(i, j + 1, nj) * 10;  // y-face j + 1/2 (minus side)
+        double lp[3], lgx[3], lgy[3];
+        for (int q = 0; q < 3; ++q) {
+            lp[q] = xe[q] + xw[3 + q] + yn[q] + ys[3 + q];
+            lgx[q] = 0.5 * xe[q] - 0.5 * xw[3 + q];
+            lgy[q] = 0.5 * yn[q] - 0.5 * ys[3 + q];
+        }
+        if (k.nu > 0.0) {
+            const double lxx = xe[6] + xw[8];
+            const double lxy = xe[7] + xw[9] + yn[6] + ys[8];
+            const double lyy = yn[7] + ys[9];
+            double gx[3], gy[3], rs[3];
+            slopes_at(k, p, i, j, gx, gy, nullptr);
+            const double rho = p[c * 3];
+            rho_strain_generic(1.0, gx, gy, k, rs);  // strain itself
+            lp[0] += rs[0] * lxx + rs[1] * lxy + rs[2] * lyy;
+            lgx[1] += rho * (4.0 / 3.0 * lxx - 2.0 / 3.0 * lyy) / k.dx;
+            lgy[2] += rho * (-2.0 / 3.0 * lxx + 4.0 / 3.0 * lyy) / k.dy;
+            lgx[2] += rho * lxy / k.dx;
+            lgy[1] += rho * lxy / k.dy;
+        }
+        if (i >= 0 && i < ni && j >= 0 && j < nj) {
+            const double *pc = p + c * 3;
+            const double *ld = lam_d + c * 3;
+            const double xc = k.xl + (i + 0.5) * k.dx, yc = k.yl + (j + 0.5) * k.dy;
+            const double dt = st.dt;
+            // u' = (1 - a)(u + du): the direct u term and the buffer's -(u - u0) rate dt
+            const double rate = buffer_rate(k, st, xc, yc);
+            double lu[3];
+            for (int q = 0; q < 3; ++q)
+                lu[q] = ld[q] * (1.0 - rate * dt);
+            for (int q = 0; q < 2; ++q) {
+                gravity_vjp(st.m[q], xc, yc, dt, pc, ld, lp, par + 5 * q);
+                sink_vjp(st.m[q], xc, yc, dt, pc, ld, lp, par + 5 * q, par + 11);
+            }
+            // u = (rho, vx rho, vy rho)
+            lp[0] += lu[0] + lu[1] * pc[1] + lu[2] * pc[2];
+            lp[1] += lu[1] * pc[0];
+            lp[2] += lu[2] * pc[0];
+        }
+        for (int q = 0; q < 3; ++q) {
+            lam_g[c * 6 + q] = lgx[q];
+            lam_g[c * 6 + 3 + q] = lgy[q];
+            lam_p[c * 3 + q] = lp[q];
+        }
+    }
+    block_sum_params<BJ>(par, par_out);
+}
+
+__device__ __forceinline__ void slope_weights(unsigned sel, double theta, double *w)
+{
+    // d g / d(y_minus, y_0, y_plus)
+    w[0] = w[1] = w[2] = 0.0;
+    if (sel == 1) {
+        w[0] = -theta;
+        w[1] = theta;
+    } else if (sel == 2) {
+        w[0] = -0.5;
+        w[2] = 0.5;
+    } else if (sel == 3) {
+        w[1] = -theta;
+        w[2] = theta;
+    }
+}
+
+// D: zones of [-2, ni + 1] x [-2, nj + 1]: slope products to their three zones.
+__global__ void adj_pass_d(Consts k, const unsigned *words, const double *lam_g, double *lam_p)
+{
+    const int ni = k.ni, nj = k.nj;
+    const long wi = ni + 4, wj = nj + 4;
+    const long z = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (z >= wi * wj)
+        return;
+    const int i = (int)(z / wj) - 2, j = (int)(z % wj) - 2;
+    const size_t c = zi(i, j, nj);
+    double acc[3] = {0.0, 0.0, 0.0};
+    // x-slopes of zones i - 1, i, i + 1 (defined on [-1, ni] x [-1, nj])
+    for (int d = -1; d <= 1; ++d) {
+        const int ii = i + d;
+        if (ii < -1 || ii > ni || j < -1 || j > nj)
+            continue;
+        const size_t o = zi(ii, j, nj);
+        const unsigned w = words[o];
+        for (int q = 0; q < 3; ++q) {
+            double wt[3];
+            slope_weights((w >> (2 * q)) & 3u, k.theta, wt);
+            acc[q] += wt[1 - d] * lam_g[o * 6 + q];  // zone i sits at position (i - ii) + 1 of the slope ii
+        }
+    }
+    for (int d = -1; d <= 1; ++d) {
+        const int jj = j + d;
+        if (jj < -1 || jj > nj || i < -1 || i > ni)
+            continue;
+        const size_t o = zi(i, jj, nj);
+        const unsigned w = words[o];
+        for (int q = 0; q < 3; ++q) {
+            double wt[3];
+            slope_weights((w >> (6 + 2 * q)) & 3u, k.theta, wt);
+            acc[q] += wt[1 - d] * lam_g[o * 6 + 3 + q];
+        }
+    }
+    for (int q = 0; q < 3; ++q)
+        lam_p[c * 3 + q] += acc[q];
+}
+
+// E: interior zones gather the adjoints of their guard images.
+__global__ void adj_fold_guards(int ni, int nj, const double *lam_p, double *lam_rd)
+{
+    const long n = (long)ni * nj;
+    const long z = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (z >= n)
+        return;
+    const int i = (int)(z / nj), j = (int)(z - (long)i * nj);
+    const int ilo = i == 0 ? -2 : i, ihi = i == ni - 1 ? ni + 1 : i;
+    const int jlo = j == 0 ? -2 : j, jhi = j == nj - 1 ? nj + 1 : j;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int ii = ilo; ii <= ihi; ++ii)
+        for (int jj = jlo; jj <= jhi; ++jj)
+            for (int q = 0; q < 3; ++q)
+                acc[q] += lam_p[zi(ii, jj, nj) * 3 + q];
+    for (int q = 0; q < 3; ++q)
+        lam_rd[zi(i, j, nj) * 3 + q] += acc[q];
+}
+
+// fixed-order sum of block partials into one parameter row
+__global__ void sum_params(const double *blocks, int nblocks, double *out)
+{
+    if (threadIdx.x >= NPAR)
+        return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b)
+        s += blocks[(size_t)b * NPAR + threadIdx.x];
+    out[threadIdx.x] += s;
+}
+
+// ---------------------------------------------------------------------------
+// objective: F = w_mdot * (-(mdot_1 + mdot_2)) + w_torque * torque, per zone,
+// with the end-of-step masses; dA and the time weight are folded into the
+// weights by the caller
+// ---------------------------------------------------------------------------
+
+template <class T>
+__device__ __forceinline__ T objective_zone(const StageDev &st, const MassT<T> *m, double x, double y, const T *p,
+                                            double wm, double wt)
+{
+    T mdot = T{} * 0.0, tq = T{} * 0.0;
+    for (int q = 0; q < 2; ++q) {
+        // accretion rates: mass off, sink on (cbdiso_2d.py:129-131)
+        T du[3] = {T{} * 0.0, T{} * 0.0, T{} * 0.0};
+        sink_generic(*m[q].base, m[q].x, m[q].y, m[q].vx, m[q].vy, m[q].sink_rate, x, y, 1.0, p[0], p[1], p[2], du);
+        mdot = mdot + du[0];
+        // gravity rates: torque = x fy - y fx
+        if (val(m[q].mass) != 0.0) {
+            const T dx = x - m[q].x, dy = y - m[q].y;
+            const T fnum = p[0] * m[q].mass * g_pow15(dx * dx + dy * dy + m[q].base->soft2);
+            tq = tq + x * (-fnum * dy) - y * (-fnum * dx);
+        }
+    }
+    return -mdot * wm + tq * wt;
+}
+
+__global__ void objective_tangent_kernel(Consts k, const StageDev *stp, TangentParams tp, const double *p,
+                                         const double *dp, double wm, double wt, double *partial)
+{
+    __shared__ StageDev st;
+    __shared__ double sm[8];
+    if (threadIdx.x == 0)
+        st = *stp;
+    __syncthreads();
+    // objective masses are the end-of-step ones
+    MassT<Dual> m[2];
+    for (int q = 0; q < 2; ++q) {
+        const MassDev &b = st.e[q];
+        m[q].x = dual(b.x, tp.dm[q][0]);
+        m[q].y = dual(b.y, tp.dm[q][1]);
+        m[q].vx = dual(b.vx, tp.dm[q][2]);
+        m[q].vy = dual(b.vy, tp.dm[q][3]);
+        m[q].mass = dual(b.mass, tp.dm[q][4]);
+        m[q].sink_rate = dual(b.sink_rate, tp.drate);
+        m[q].base = &st.e[q];
+    }
+    const long n = (long)k.ni * k.nj;
+    double acc = 0.0;
+    for (long z = blockIdx.x * (long)blockDim.x + threadIdx.x; z < n; z += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(z / k.nj), j = (int)(z - (long)i * k.nj);
+        const size_t c = zi(i, j, k.nj) * 3;
+        const Dual pz[3] = {dual(p[c], dp[c]), dual(p[c + 1], dp[c + 1]), dual(p[c + 2], dp[c + 2])};
+        acc += objective_zone<Dual>(st, m, k.xl + (i + 0.5) * k.dx, k.yl + (j + 0.5) * k.dy, pz, wm, wt).d;
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0)
+        sm[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x / 32); ++w)
+            s += sm[w];
+        partial[blockIdx.x] = s;
+    }
+}
+
+// lambda_p += dF/dp per zone; parameter derivatives to blocks
+template <int BJ>
+__global__ void __launch_bounds__(BJ) objective_adjoint_kernel(Consts k, const StageDev *stp, const double *p,
+                                                               double wm, double wt, double *lam,
+                                                               double *par_out)
+{
+    __shared__ StageDev st;
+    if (threadIdx.x == 0)
+        st = *stp;
+    __syncthreads();
+    double par[NPAR];
+    for (int v = 0; v < NPAR; ++v)
+        par[v] = 0.0;
+    const long n = (long)k.ni * k.nj;
+    const long z = blockIdx.x * (long)BJ + threadIdx.x;
+    if (z < n) {
+        const int i = (int)(z / k.nj), j = (int)(z - (long)i * k.nj);
+        const size_t c = zi(i, j, k.nj) * 3;
+        const double x = k.xl + (i + 0.5) * k.dx, y = k.yl + (j + 0.5) * k.dy;
+        const double sig = p[c];
+        for (int q = 0; q < 2; ++q) {
+            const MassDev &b = st.e[q];
+            // torque part: T = -sigma m g (x dy - y dx)
+            if (b.mass != 0.0) {
+                const double dx = x - b.x, dy = y - b.y;
+                const double S = dx * dx + dy * dy + b.soft2;
+                const double g = inv_pow15<false>(S), h = g / S;
+                const double cr = x * dy - y * dx;
+                lam[c] += wt * (-b.mass * g * cr);
+                par[5 * q + 4] += wt * (-sig * g * cr);
+                par[5 * q + 0] += wt * (-sig * b.mass) * (3.0 * dx * h * cr + g * y);
+                par[5 * q + 1] += wt * (-sig * b.mass) * (3.0 * dy * h * cr - g * x);
+            }
+            // accretion part: -mdot, through the dual sink (rare zones)
+            const double dx = x - b.x, dy = y - b.y;
+            if (b.sink_rate != 0.0 && dx * dx + dy * dy < b.sink_hi2) {
+                for (int dir = 0; dir < 8; ++dir) {
+                    double s[8];
+                    for (int t = 0; t < 8; ++t)
+                        s[t] = t == dir ? 1.0 : 0.0;
+                    Dual du[3] = {dual(0.0), dual(0.0), dual(0.0)};
+                    sink_generic<Dual>(b, dual(b.x, s[3]), dual(b.y, s[4]), dual(b.vx, s[5]), dual(b.vy, s[6]),
+                                       dual(b.sink_rate, s[7]), x, y, 1.0, dual(p[c], s[0]), dual(p[c + 1], s[1]),
+                                       dual(p[c + 2], s[2]), du);
+                    const double v = -wm * du[0].d;
+                    if (dir < 3)
+                        lam[c + dir] += v;
+                    else if (dir < 7)
+                        par[5 * q + dir - 3] += v;
+                    else
+                        par[11] += v;
+                }
+            }
+        }
+    }
+    block_sum_params<BJ>(par, par_out);
+}
+
+inline int nblocks(long n, int bs) { return (int)((n + bs - 1) / bs); }
+
+}  // namespace
+
+}  // namespace cbd
+
+using namespace cbd;
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+
+namespace {
+
+bool grid_ok(const cbd_grid_t *g)
+{
+    return g && g->ni > 0 && g->nj > 0 && g->xr > g->xl && g->yr > g->yl && (g->eos_type == 1 || g->eos_type == 2);
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t cbdiso_b200_adjoint_workspace_bytes(const cbd_grid_t *grid)
+{
+    if (!grid_ok(grid))
+        return 0;
+    const size_t zones = (size_t)(grid->ni + 4) * (grid->nj + 4);
+    const size_t blocks = (size_t)nblocks((long)(grid->ni + 2) * (grid->nj + 2), 128) + 1;
+    // lam_d (3) + fx (10) + fy (10) + lam_g (6) + lam_p (3) doubles per zone, 3 x blocks x NPAR partials
+    return zones * (3 + 10 + 10 + 6 + 3) * sizeof(double) + 3 * blocks * NPAR * sizeof(double) + 256;
+}
+
+int cbdiso_b200_stage_record_branches(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
+                                      const double *primitive_out, unsigned int *words, void *stream)
+{
+    if (!grid_ok(grid) || !stage_dev || !primitive_rd || !primitive_out || !words)
+        return CBD_ERR_ARGUMENT;
+    const Consts k = consts_from_grid(grid);
+    const long n = (long)(grid->ni + 2) * (grid->nj + 2);
+    record_kernel<<<nblocks(n, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        k, static_cast<const StageDev *>(stage_dev), primitive_rd, primitive_out, words);
+    return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
+}
+
+int cbdiso_b200_stage_tangent(const cbd_grid_t *grid, const void *stage_dev, const double *dmass, double dnu,
+                              double drate, const double *primitive_rd, const double *dprimitive_rd,
+                              const double *primitive_n, const double *dprimitive_n, double *primitive_out,
+                              double *dprimitive_out, void *stream)
+{
+    if (!grid_ok(grid) || !stage_dev || !primitive_rd || !dprimitive_rd || !primitive_out || !dprimitive_out ||
+        (primitive_n && !dprimitive_n))
+        return CBD_ERR_ARGUMENT;
+    const Consts k = consts_from_grid(grid);
+    TangentParams tp;
+    std::memset(&tp, 0, sizeof(tp));
+    if (dmass)
+        for (int p = 0; p < 2; ++p)
+            for (int v = 0; v < 5; ++v)
+                tp.dm[p][v] = dmass[5 * p + v];
+    tp.dnu = dnu;
+    tp.drate = drate;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const long n = (long)grid->ni * grid->nj;
+    stage_tangent_kernel<<<nblocks(n, 128), 128, 0, s>>>(k, static_cast<const StageDev *>(stage_dev), tp,
+                                                         primitive_rd, dprimitive_rd, primitive_n, dprimitive_n,
+                                                         primitive_out, dprimitive_out);
+    const long ng = (long)(grid->ni + 4) * (grid->nj + 4);
+    guards_kernel<<<nblocks(ng, 256) < 2048 ? nblocks(ng, 256) : 2048, 256, 0, s>>>(grid->ni, grid->nj,
+                                                                                     primitive_out);
+    guards_kernel<<<nblocks(ng, 256) < 2048 ? nblocks(ng, 256) : 2048, 256, 0, s>>>(grid->ni, grid->nj,
+                                                                                     dprimitive_out);
+    return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
+}
+
+int cbdiso_b200_stage_adjoint(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
+                              const double *primitive_n, const double *primitive_out, const unsigned int *words,
+                              const double *lam_out, double *lam_rd, double *lam_n, double *params_out,
+                              void *workspace, void *stream)
+{
+    if (!grid_ok(grid) || !stage_dev || !primitive_rd || !primitive_out || !words || !lam_out || !lam_rd ||
+        !params_out || !workspace || (primitive_n && !lam_n))
+        return CBD_ERR_ARGUMENT;
+    const Consts k = consts_from_grid(grid);
+    const StageDev *st = static_cast<const StageDev *>(stage_dev);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int ni = grid->ni, nj = grid->nj;
+    const size_t zones = (size_t)(ni + 4) * (nj + 4);
+    double *ws = static_cast<double *>(workspace);
+    double *lam_d = ws;
+    double *fx = lam_d + zones * 3;
+    double *fy = fx + zones * 10;
+    double *lam_g = fy + zones * 10;
+    double *lam_p = lam_g + zones * 6;
+    double *parts = lam_p + zones * 3;
+    const long nwide = (long)(ni + 2) * (nj + 2);
+    const int nb = nblocks(nwide, 128);
+    if (cudaMemsetAsync(ws, 0, zones * (3 + 10 + 10 + 6 + 3) * sizeof(double), s) != cudaSuccess)
+        return CBD_ERR_CUDA;
+    adj_pass_a<<<nblocks((long)ni * nj, 128), 128, 0, s>>>(k, st, primitive_out, words, lam_out, primitive_n,
+                                                           lam_d, lam_n);
+    adj_pass_b<128><<<nb, 128, 0, s>>>(k, st, primitive_rd, words, lam_d, fx, fy, parts);
+    sum_params<<<1, 32, 0, s>>>(parts, nb, params_out);
+    adj_pass_c<128><<<nb, 128, 0, s>>>(k, st, primitive_rd, lam_d, fx, fy, lam_g, lam_p, parts);
+    sum_params<<<1, 32, 0, s>>>(parts, nb, params_out);
+    adj_pass_d<<<nblocks((long)zones, 128), 128, 0, s>>>(k, words, lam_g, lam_p);
+    adj_fold_guards<<<nblocks((long)ni * nj, 128), 128, 0, s>>>(ni, nj, lam_p, lam_rd);
+    return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
+}
+
+int cbdiso_b200_objective_tangent(const cbd_grid_t *grid, const void *stage_dev, const double *dmass,
+                                  double drate, const double *primitive, const double *dprimitive, double w_mdot,
+                                  double w_torque, double *partials, int num_partials, void *stream)
+{
+    if (!grid_ok(grid) || !stage_dev || !primitive || !dprimitive || !partials || num_partials < 1)
+        return CBD_ERR_ARGUMENT;
+    const Consts k = consts_from_grid(grid);
+    TangentParams tp;
+    std::memset(&tp, 0, sizeof(tp));
+    if (dmass)
+        for (int p = 0; p < 2; ++p)
+            for (int v = 0; v < 5; ++v)
+                tp.dm[p][v] = dmass[5 * p + v];
+    tp.drate = drate;
+    objective_tangent_kernel<<<num_partials, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        k, static_cast<const StageDev *>(stage_dev), tp, primitive, dprimitive, w_mdot, w_torque, partials);
+    return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
+}
+
+int cbdiso_b200_objective_adjoint(const cbd_grid_t *grid, const void *stage_dev, const double *primitive,
+                                  double w_mdot, double w_torque, double *lam, double *params_out, void *workspace,
+                                  void *stream)
+{
+    if (!grid_ok(grid) || !stage_dev || !primitive || !lam || !params_out || !workspace)
+        return CBD_ERR_ARGUMENT;
+    const Consts k = consts_from_grid(grid);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t zones = (size_t)(grid->ni + 4) * (grid->nj + 4);
+    double *parts = static_cast<double *>(workspace) + zones * (3 + 10 + 10 + 6 + 3);
+    const int nb = nblocks((long)grid->ni * grid->nj, 128);
+    objective_adjoint_kernel<128><<<nb, 128, 0, s>>>(k, static_cast<const StageDev *>(stage_dev), primitive, w_mdot,
+                                                     w_torque, lam, parts);
+    sum_params<<<1, 32, 0, s>>>(parts, nb, params_out);
+    return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,249 @@
+"""
+Tangent and discrete adjoint of the RK2 circumbinary-disk step.
+
+  * the generic per-zone formulation behind the tangent reproduces the fused
+    stage kernel bit for bit;
+  * stage tangent versus central finite differences of the stage kernel;
+  * dot-product tests <lambda, T delta> = <A lambda, delta> for a stage
+    (state and the 12 point-mass / nu / sink-rate parameters) and for the
+    objective;
+  * the whole reverse sweep with checkpointing versus the forward-mode
+    tangent of the run, and versus central finite differences of J.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from sailfish_b200 import _capi  # noqa: E402
+from sailfish_b200.adjoint import AdjointRun, Params, mass_jacobian, objective_function  # noqa: E402
+
+P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _state(run, params, steps=3):
+    """A developed state (a few steps from the seeded disk) and its solver."""
+    prim = run.initial_state(seed=3)
+    s = run._solver(params, prim)
+    for _ in range(steps):
+        s.advance(s.mesh.min_spacing() / s.maximum_wavespeed() * 0.3)
+    return s
+
+
+def _rand_like(t, seed, scale=1.0):
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    return (torch.rand(t.shape, generator=g, dtype=torch.float64) * 2 - 1).to(t.device) * scale
+
+
+@pytest.fixture(scope="module")
+def stage_case():
+    run = AdjointRun(resolution=48, steps=1)
+    params = Params(0.5, 0.1, 1e-3, 10.0)
+    s = _state(run, params)
+    dt = 0.8 * s.mesh.min_spacing() / s.maximum_wavespeed() * 0.3
+    dev, nb, times = run._records(s, s.time, dt)
+    return run, params, s, dev, nb, times
+
+
+def _stage(s, dev, off, a, p, pn):
+    out = torch.empty_like(p)
+    st = _capi.Stage()
+    st.a = a
+    _capi.check(s._lib.cbdiso_b200_advance_stage(ctypes.byref(s._grid), ctypes.byref(st),
+                                                 ctypes.c_void_p(dev.data_ptr() + off), P(p),
+                                                 P(pn) if pn is not None else None, P(out), None, P(s._scratch),
+                                                 P(s._result), _stream()), "stage")
+    return out
+
+
+def _tangent(s, dev, off, p, dp, pn, dpn, dmass, dnu=0.0, drate=0.0):
+    out, dout = torch.empty_like(p), torch.empty_like(p)
+    d = (ctypes.c_double * 10)(*dmass)
+    _capi.check(s._lib.cbdiso_b200_stage_tangent(ctypes.byref(s._grid), ctypes.c_void_p(dev.data_ptr() + off), d,
+                                                 dnu, drate, P(p), P(dp), P(pn) if pn is not None else None,
+                                                 P(dpn) if dpn is not None else None, P(out), P(dout), _stream()),
+                "tangent")
+    return out, dout
+
+
+def _guarded(s, t):
+    _capi.check(s._lib.cbdiso_b200_fill_guards(ctypes.byref(s._grid), P(t), _stream()), "guards")
+    return t
+
+
+@pytest.mark.parametrize("stage", [0, 1])
+def test_generic_zone_update_matches_the_stage_kernel(stage_case, stage):
+    run, params, s, dev, nb, _ = stage_case
+    p = s._buf[0]
+    pn = p if stage == 1 else None
+    want = _stage(s, dev, stage * nb, 0.5 * stage, p, pn)
+    got, _ = _tangent(s, dev, stage * nb, p, torch.zeros_like(p), pn, torch.zeros_like(p) if pn is not None else None,
+                      [0.0] * 10)
+    assert torch.equal(got[2:-2, 2:-2], want[2:-2, 2:-2])
+
+
+@pytest.mark.parametrize("stage", [0, 1])
+def test_stage_tangent_matches_finite_differences(stage_case, stage):
+    run, params, s, dev, nb, _ = stage_case
+    p = s._buf[0]
+    dp = _guarded(s, _rand_like(p, 1) * p.abs().amax(dim=(0, 1)))
+    pn = p.clone() if stage == 1 else None
+    dpn = _guarded(s, _rand_like(p, 2) * p.abs().amax(dim=(0, 1))) if stage == 1 else None
+    _, dout = _tangent(s, dev, stage * nb, p, dp, pn, dpn, [0.0] * 10)
+    h = 1e-7
+    plus = _stage(s, dev, stage * nb, 0.5 * stage, p + h * dp, pn + h * dpn if pn is not None else None)
+    minus = _stage(s, dev, stage * nb, 0.5 * stage, p - h * dp, pn - h * dpn if pn is not None else None)
+    fd = ((plus - minus) / (2 * h))[2:-2, 2:-2]
+    tan = dout[2:-2, 2:-2]
+    for q in range(3):
+        err = (fd[..., q] - tan[..., q]).abs().max() / tan[..., q].abs().max()
+        assert err < 1e-5, (q, float(err))
+
+
+@pytest.mark.parametrize("stage", [0, 1])
+def test_stage_adjoint_dot_product(stage_case, stage):
+    run, params, s, dev, nb, _ = stage_case
+    lib = s._lib
+    g = ctypes.byref(s._grid)
+    p = s._buf[0]
+    pn = p.clone() if stage == 1 else None
+    out = _stage(s, dev, stage * nb, 0.5 * stage, p, pn)
+    words = torch.zeros(p.shape[:2], dtype=torch.int32, device=p.device)
+    rec = ctypes.c_void_p(dev.data_ptr() + stage * nb)
+    _capi.check(lib.cbdiso_b200_stage_record_branches(g, rec, P(p), P(out), P(words), _stream()), "record")
+    scale = p.abs().amax(dim=(0, 1))
+    dp = _guarded(s, _rand_like(p, 11) * scale)
+    dpn = _guarded(s, _rand_like(p, 12) * scale) if stage == 1 else None
+    rng = np.random.default_rng(13)
+    dmass = rng.uniform(-1, 1, 10) * 1e-2
+    dnu, drate = 1e-4, 0.5
+    _, dout = _tangent(s, dev, stage * nb, p, dp, pn, dpn, dmass, dnu, drate)
+    lam = torch.zeros_like(p)
+    lam[2:-2, 2:-2] = _rand_like(lam[2:-2, 2:-2], 14)
+    lam_rd, lam_n = torch.zeros_like(p), torch.zeros_like(p)
+    pars = torch.zeros(12, dtype=torch.float64, device=p.device)
+    ws = torch.zeros(int(lib.cbdiso_b200_adjoint_workspace_bytes(g)) // 8 + 8, dtype=torch.float64, device=p.device)
+    _capi.check(lib.cbdiso_b200_stage_adjoint(g, rec, P(p), P(pn) if pn is not None else None, P(out), P(words),
+                                              P(lam), P(lam_rd), P(lam_n) if pn is not None else None, P(pars),
+                                              P(ws), _stream()), "adjoint")
+    I = (slice(2, -2), slice(2, -2))
+    lhs = float((lam[I] * dout[I]).sum())
+    rhs = float((lam_rd[I] * dp[I]).sum())
+    if stage == 1:
+        rhs += float((lam_n[I] * dpn[I]).sum())
+    pv = pars.cpu().numpy()
+    rhs += float(pv[:10] @ dmass) + pv[10] * dnu + pv[11] * drate
+    assert abs(lhs - rhs) <= 1e-11 * max(abs(lhs), 1e-300), (lhs, rhs)
+
+
+def test_objective_adjoint_dot_product(stage_case):
+    run, params, s, dev, nb, _ = stage_case
+    lib = s._lib
+    g = ctypes.byref(s._grid)
+    p = s._buf[0]
+    rec = ctypes.c_void_p(dev.data_ptr() + nb)
+    dp = _guarded(s, _rand_like(p, 21) * p.abs().amax(dim=(0, 1)))
+    dmass = np.random.default_rng(22).uniform(-1, 1, 10) * 1e-2
+    drate = 0.3
+    parts = torch.zeros(64, dtype=torch.float64, device=p.device)
+    d = (ctypes.c_double * 10)(*dmass)
+    _capi.check(lib.cbdiso_b200_objective_tangent(g, rec, d, drate, P(p), P(dp), 0.7, 1.3, P(parts), 64, _stream()),
+                "objective tangent")
+    lhs = float(parts.sum())
+    lam = torch.zeros_like(p)
+    pars = torch.zeros(12, dtype=torch.float64, device=p.device)
+    ws = torch.zeros(int(lib.cbdiso_b200_adjoint_workspace_bytes(g)) // 8 + 8, dtype=torch.float64, device=p.device)
+    _capi.check(lib.cbdiso_b200_objective_adjoint(g, rec, P(p), 0.7, 1.3, P(lam), P(pars), P(ws), _stream()),
+                "objective adjoint")
+    I = (slice(2, -2), slice(2, -2))
+    pv = pars.cpu().numpy()
+    rhs = float((lam[I] * dp[I]).sum()) + float(pv[:10] @ dmass) + pv[11] * drate
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), 1e-300), (lhs, rhs)
+
+
+def test_kepler_jacobian_matches_finite_differences():
+    from sailfish_b200.kepler import OrbitalElements
+
+    def state(q, e, t):
+        a, b = OrbitalElements(1.0, 1.0, q, e).orbital_state(t)
+        return np.array([a.position_x, a.position_y, a.velocity_x, a.velocity_y, a.mass,
+                         b.position_x, b.position_y, b.velocity_x, b.velocity_y, b.mass])
+
+    for t in (0.0, 0.7, 5.3):
+        j = mass_jacobian(t, 0.5, 0.1)
+        h = 1e-6
+        fq = (state(0.5 + h, 0.1, t) - state(0.5 - h, 0.1, t)) / (2 * h)
+        fe = (state(0.5, 0.1 + h, t) - state(0.5, 0.1 - h, t)) / (2 * h)
+        np.testing.assert_allclose(j[:, 0], fq, rtol=1e-6, atol=1e-9)
+        np.testing.assert_allclose(j[:, 1], fe, rtol=1e-6, atol=1e-9)
+
+
+@pytest.fixture(scope="module")
+def run_case():
+    run = AdjointRun(resolution=48, steps=24, checkpoint_every=5)
+    params = Params(0.5, 0.1, 1e-3, 10.0)
+    prim = run.initial_state(seed=4)
+    run.forward(prim, params, freeze=True, keep=True)
+    return run, params, prim
+
+
+@pytest.mark.parametrize("weights", [(1.0, 0.0), (0.0, 1.0)])
+def test_run_gradient_matches_tangent(run_case, weights):
+    run, params, prim = run_case
+    run.forward(prim, params, keep=True)
+    gs, gp = run.gradient(weights)
+    rng = np.random.default_rng(31)
+    for k in range(2):
+        dprim = np.zeros_like(prim)
+        dprim[..., 0] = rng.uniform(-1, 1, prim.shape[:2]) * 1e-2
+        dpar = rng.uniform(-1, 1, 4) * np.array([0.1, 0.05, 1e-4, 1.0])
+        tan = run.tangent(prim, params, dprim, dpar, weights)
+        adj = float((gs * dprim).sum()) + float(gp @ dpar)
+        assert abs(tan - adj) <= 1e-9 * max(abs(tan), 1e-300), (k, tan, adj)
+
+
+def test_run_gradient_matches_central_differences(run_case):
+    run, params, prim = run_case
+    run.forward(prim, params, keep=True)
+    gs, gp = run.gradient((1.0, 0.0))
+    rng = np.random.default_rng(41)
+    for k in range(3):
+        dprim = np.zeros_like(prim)
+        dprim[..., 0] = rng.uniform(-1, 1, prim.shape[:2])
+        adj = float((gs * dprim).sum())
+        h = 1e-6
+        jp = run.forward(prim + h * dprim, params)[0]
+        jm = run.forward(prim - h * dprim, params)[0]
+        fd = (jp - jm) / (2 * h)
+        assert abs(fd - adj) <= 1e-5 * abs(adj), (k, fd, adj)
+    for i, scale in enumerate([1.0, 1.0, 1e-3, 10.0]):
+        h = 1e-6 * scale
+        dp = np.zeros(4)
+        dp[i] = h
+        jp = run.forward(prim, Params(*(np.array(params) + dp)))[0]
+        jm = run.forward(prim, Params(*(np.array(params) - dp)))[0]
+        fd = (jp - jm) / (2 * h)
+        assert abs(fd - gp[i]) <= 1e-4 * max(abs(gp[i]), 1e-12), (i, fd, gp[i])
+
+
+def test_torch_autograd_function():
+    run = AdjointRun(resolution=32, steps=6, checkpoint_every=4)
+    prim = run.initial_state(seed=5)
+    run.forward(prim, Params(), freeze=True)
+    F = objective_function(run, (1.0, 0.5))
+    sigma0 = torch.from_numpy(prim[..., 0].copy()).requires_grad_(True)
+    params = torch.tensor([0.5, 0.1, 1e-3, 10.0], dtype=torch.float64, requires_grad=True)
+    J = F.apply(sigma0, params)
+    J.backward()
+    assert sigma0.grad.shape == sigma0.shape and params.grad.shape == (4,)
+    assert torch.isfinite(sigma0.grad).all() and torch.isfinite(params.grad).all()
