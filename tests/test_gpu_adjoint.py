@@ -100,14 +100,17 @@ def test_stage_tangent_matches_finite_differences(stage_case, stage):
     pn = p.clone() if stage == 1 else None
     dpn = _guarded(s, _rand_like(p, 2) * p.abs().amax(dim=(0, 1))) if stage == 1 else None
     _, dout = _tangent(s, dev, stage * nb, p, dp, pn, dpn, [0.0] * 10)
-    h = 1e-7
+    # The stage is piecewise smooth (limiter and HLLE branches): h is small
+    # enough that the +-h states take the same branches in all but a zone or
+    # so of this seeded state (larger h straddles near-ties of the limiter).
+    h = 1e-8
     plus = _stage(s, dev, stage * nb, 0.5 * stage, p + h * dp, pn + h * dpn if pn is not None else None)
     minus = _stage(s, dev, stage * nb, 0.5 * stage, p - h * dp, pn - h * dpn if pn is not None else None)
     fd = ((plus - minus) / (2 * h))[2:-2, 2:-2]
     tan = dout[2:-2, 2:-2]
     for q in range(3):
         err = (fd[..., q] - tan[..., q]).abs().max() / tan[..., q].abs().max()
-        assert err < 1e-5, (q, float(err))
+        assert err < 1e-6, (q, float(err))
 
 
 @pytest.mark.parametrize("stage", [0, 1])
@@ -212,6 +215,14 @@ def test_run_gradient_matches_tangent(run_case, weights):
         assert abs(tan - adj) <= 1e-9 * max(abs(tan), 1e-300), (k, tan, adj)
 
 
+def _bump(run, rng):
+    """A smooth surface-density perturbation: a Gaussian of width ~1 at a
+    seeded position (smooth directions keep +-h runs on the same branches)."""
+    x = -8.0 + (np.arange(run.n) + 0.5) * 16.0 / run.n
+    cx, cy = rng.uniform(-1.0, 1.0, 2)  # near the binary, where the accretion rate is sensitive
+    return np.exp(-((x[:, None] - cx) ** 2 + (x[None, :] - cy) ** 2) / 2.0)
+
+
 def test_run_gradient_matches_central_differences(run_case):
     run, params, prim = run_case
     run.forward(prim, params, keep=True)
@@ -219,13 +230,13 @@ def test_run_gradient_matches_central_differences(run_case):
     rng = np.random.default_rng(41)
     for k in range(3):
         dprim = np.zeros_like(prim)
-        dprim[..., 0] = rng.uniform(-1, 1, prim.shape[:2])
+        dprim[..., 0] = _bump(run, rng)
         adj = float((gs * dprim).sum())
         h = 1e-6
         jp = run.forward(prim + h * dprim, params)[0]
         jm = run.forward(prim - h * dprim, params)[0]
         fd = (jp - jm) / (2 * h)
-        assert abs(fd - adj) <= 1e-5 * abs(adj), (k, fd, adj)
+        assert abs(fd - adj) <= 1e-5 * abs(adj) + 1e-10 * abs(jp), (k, fd, adj)
     for i, scale in enumerate([1.0, 1.0, 1e-3, 10.0]):
         h = 1e-6 * scale
         dp = np.zeros(4)
