@@ -254,6 +254,13 @@ size_t cbdiso_b200_stepper_bytes(void);
 int cbdiso_b200_stepper_init(const cbd_grid_t *grid, const cbd_orbit_t *orbit, int rk_order, double time,
                              double cfl, double min_spacing, double fixed_dt, int series_capacity, void *stepper);
 
+/* Attach to a host copy of a stepper record (before copying it to the
+ * device): a device array of dt_count time steps to use instead of the CFL
+ * rule (a frozen dt sequence), and/or a device array of history_capacity *
+ * rk_order stage records that receives every step's stage records. */
+int cbdiso_b200_stepper_attach(void *stepper, const double *dt_sequence, int dt_count, void *history,
+                               int history_capacity);
+
 /* One step's prologue (a single-thread kernel): records the previous step's
  * time-series row [time, dt, max wavespeed, num_values reduction values] from
  * `result` into `series` (if non-null), then, unless `finalize`, takes
@@ -346,6 +353,25 @@ int cbdiso_b200_objective_tangent(const cbd_grid_t *grid, const void *stage_dev,
 int cbdiso_b200_objective_adjoint(const cbd_grid_t *grid, const void *stage_dev, const double *primitive,
                                   double w_mdot, double w_torque, double *lam, double *params_out, void *workspace,
                                   void *stream);
+
+/* Chained forms for a whole reverse sweep: instead of 12 parameter
+ * derivatives per call, the mass-parameter part is contracted on the device
+ * with `jacobian` (device memory, 10 x 2 row-major: d(x, y, vx, vy, mass of
+ * mass 1, then of mass 2) / d(q, e) at this stage's time) and ADDED per
+ * block into `chain_acc` (device, cbdiso_b200_adjoint_chain_blocks(grid) x 4
+ * doubles: d/dq, d/de, d/dnu, d/d(sink rate)), which the caller zeroes once
+ * before the sweep. cbdiso_b200_adjoint_chain_finish ADDS the block sums, in
+ * a fixed order, into out4 (device, 4 doubles). */
+int cbdiso_b200_stage_adjoint_chained(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
+                                      const double *primitive_n, const double *primitive_out,
+                                      const unsigned int *words, const double *lam_out, double *lam_rd,
+                                      double *lam_n, const double *jacobian, double *chain_acc, void *workspace,
+                                      void *stream);
+int cbdiso_b200_objective_adjoint_chained(const cbd_grid_t *grid, const void *stage_dev, const double *primitive,
+                                          double w_mdot, double w_torque, double *lam, const double *jacobian,
+                                          double *chain_acc, void *workspace, void *stream);
+size_t cbdiso_b200_adjoint_chain_blocks(const cbd_grid_t *grid);
+int cbdiso_b200_adjoint_chain_finish(const double *chain_acc, int num_blocks, double *out4, void *stream);
 
 /* The epilogue quantities alone, on a given state (guards not needed). */
 int cbdiso_b200_reduce(

@@ -111,6 +111,8 @@ def _declare(lib):
     lib.cbdiso_b200_stepper_init.argtypes = [POINTER(Grid), POINTER(Orbit), c_int, c_double, c_double, c_double,
                                              c_double, c_int, c_void_p]
     lib.cbdiso_b200_stepper_init.restype = c_int
+    lib.cbdiso_b200_stepper_attach.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_int]
+    lib.cbdiso_b200_stepper_attach.restype = c_int
     lib.cbdiso_b200_step_prologue.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]
     lib.cbdiso_b200_step_prologue.restype = c_int
     lib.cbdiso_b200_batch_disk_bytes.argtypes = []
@@ -128,6 +130,8 @@ def _declare(lib):
     lib.cbdiso_b200_batched_prologue.restype = c_int
     lib.cbdiso_b200_adjoint_workspace_bytes.argtypes = [POINTER(Grid)]
     lib.cbdiso_b200_adjoint_workspace_bytes.restype = c_size_t
+    lib.cbdiso_b200_adjoint_chain_blocks.argtypes = [POINTER(Grid)]
+    lib.cbdiso_b200_adjoint_chain_blocks.restype = c_size_t
     V = c_void_p
     D = c_double
     for name, args in {
@@ -136,6 +140,9 @@ def _declare(lib):
         "cbdiso_b200_stage_adjoint": [POINTER(Grid), V, V, V, V, V, V, V, V, V, V, V],
         "cbdiso_b200_objective_tangent": [POINTER(Grid), V, V, D, V, V, D, D, V, c_int, V],
         "cbdiso_b200_objective_adjoint": [POINTER(Grid), V, V, D, D, V, V, V, V],
+        "cbdiso_b200_stage_adjoint_chained": [POINTER(Grid), V, V, V, V, V, V, V, V, V, V, V, V],
+        "cbdiso_b200_objective_adjoint_chained": [POINTER(Grid), V, V, D, D, V, V, V, V, V],
+        "cbdiso_b200_adjoint_chain_finish": [V, c_int, V, V],
     }.items():
         f = getattr(lib, name)
         f.argtypes = args
@@ -177,6 +184,8 @@ def exported_symbols():
         "cbdiso_b200_batched_stage", "cbdiso_b200_batched_finalize", "cbdiso_b200_batched_prologue",
         "cbdiso_b200_adjoint_workspace_bytes", "cbdiso_b200_stage_record_branches", "cbdiso_b200_stage_tangent",
         "cbdiso_b200_stage_adjoint", "cbdiso_b200_objective_tangent", "cbdiso_b200_objective_adjoint",
+        "cbdiso_b200_stepper_attach", "cbdiso_b200_stage_adjoint_chained", "cbdiso_b200_objective_adjoint_chained",
+        "cbdiso_b200_adjoint_chain_finish", "cbdiso_b200_adjoint_chain_blocks",
     ]
 
 

@@ -12,13 +12,19 @@ masses. Gradients are with respect to the initial primitive state (its
 density component is dJ / dSigma_0) and to the parameters
 (q, e, nu, sink_rate) of a CircumbinaryDisk.
 
-Reverse sweep: the forward run keeps a checkpoint every `checkpoint_every`
-steps; each segment is recomputed forward from its checkpoint, recording for
-every stage the branches it took (limiter, HLLE waves, floors) with
-cbdiso_b200_stage_record_branches, and the adjoint kernels then replay those
-branches backward through the segment. Point-mass parameter derivatives of
-every stage are chained through the Kepler orbit on the host with
-complex-step derivatives (exact to rounding: the orbit is analytic in q, e).
+Forward: the device stepper (Solver.run) advances the run in segments of
+`checkpoint_every` steps with the frozen dt sequence, keeps a copy of the
+state at each segment start and writes every stage record (point masses, dt,
+RK weight) into a history array.
+
+Reverse sweep: each segment is recomputed forward from its checkpoint with the
+recorded stage records, keeping every state; the branches each stage took
+(limiter, HLLE waves, floors) are recorded with
+cbdiso_b200_stage_record_branches, and the chained adjoint kernels replay
+them backward through the segment. Point-mass parameter derivatives are
+contracted on the device with d(mass parameters)/d(q, e) of each stage's time
+(complex-step derivatives of the Kepler orbit, exact to rounding: the orbit is
+analytic in q and e) and accumulated per block across the whole sweep.
 
 The forward-mode tangent of the same run (cbdiso_b200_stage_tangent) gives
 the directional derivative for the dot-product test.
@@ -79,6 +85,40 @@ def mass_jacobian(t, q, e, a=1.0, m=1.0, h=1e-30):
     return np.array([jq, je]).T
 
 
+def _kepler_complex_many(t, a, m, q, e):
+    """_kepler_complex over an array of times (the same Newton iteration and
+    stopping rule, per element): 10 x len(t) complex."""
+    w = math.sqrt(1.0 * m / a / a / a)
+    p = 2.0 * math.pi / w
+    t = np.asarray(t, dtype=np.float64)
+    n = w * (t - p * np.floor(t / p))
+    k = n.astype(np.complex128)
+    for it in range(11):
+        f = k - e * np.sin(k) - n
+        todo = np.abs(f) > 1e-15
+        if not todo.any():
+            break
+        if it == 10:
+            raise ValueError("solve_newton_rapheson: no solution")
+        k = np.where(todo, k - f / (1.0 - e * np.cos(k)), k)
+    m1 = m / (1.0 + q)
+    m2 = m - m1
+    ck, sk = np.cos(k), np.sin(k)
+    x1 = -a * q / (1.0 + q) * (e - ck)
+    y1 = +a * q / (1.0 + q) * sk * np.sqrt(1.0 - e * e)
+    vx1 = -a * q / (1.0 + q) * w / (1.0 - e * ck) * sk
+    vy1 = +a * q / (1.0 + q) * w / (1.0 - e * ck) * ck * np.sqrt(1.0 - e * e)
+    ones = np.ones_like(n)
+    return np.stack([x1, y1, vx1, vy1, m1 * ones, -x1 / q, -y1 / q, -vx1 / q, -vy1 / q, m2 * ones])
+
+
+def mass_jacobians(times, q, e, a=1.0, m=1.0, h=1e-30):
+    """mass_jacobian at every time of `times`: len(times) x 10 x 2."""
+    jq = _kepler_complex_many(times, a, m, complex(q, h), complex(e, 0.0)).imag / h
+    je = _kepler_complex_many(times, a, m, complex(q, 0.0), complex(e, h)).imag / h
+    return np.stack([jq.T, je.T], axis=-1)
+
+
 class AdjointRun:
     """
     A differentiable circumbinary-disk run on one GPU: config-0 physics on
@@ -125,30 +165,50 @@ class AdjointRun:
         """
         Run the steps; returns J = (mean accretion rate, mean torque). The
         first call (or freeze=True) fixes the dt sequence from the CFL rule;
-        later calls reuse it. With keep, checkpoints are kept for gradient().
+        later calls reuse it. With keep, checkpoints and the stage-record
+        history are kept for gradient().
         """
+        import torch
+
         s = self._solver(params, prim0)
-        if self.dts is None or freeze:
-            dts = []
-        else:
-            dts = list(self.dts)
-        ts, mdot, torque, cps = [], [], [], {}
-        for n in range(self.steps):
-            if keep and n % self.checkpoint_every == 0:
-                cps[n] = s._buf[0].clone()
-            if len(dts) <= n:
-                dts.append(s.mesh.min_spacing() / s.maximum_wavespeed() * self.cfl)
-            ts.append(s.time)
-            s.advance(dts[n])
-            m1, m2, tq = s.reductions()
-            mdot.append(-(m1 + m2))
-            torque.append(tq)
-        self.dts = np.array(dts)
+        steps, K = self.steps, self.checkpoint_every
+        fresh = self.dts is None or freeze
+        dts_dev = None if fresh else torch.from_numpy(np.ascontiguousarray(self.dts)).to(s.device)
+        nb = int(self._lib.cbdiso_b200_stage_record_bytes())
+        history = torch.empty(steps * 2 * nb, dtype=torch.uint8, device=s.device) if keep else None
+        t_start = s.time
+        rows, cps = [], {}
+        for start in range(0, steps, K):
+            stop = min(start + K, steps)
+            if keep:
+                cps[start] = s._buf[0].clone()
+            rows += s.run(stop - start, cfl=self.cfl, steps_per_graph=K,
+                          dt_sequence=None if fresh else dts_dev[start:stop],
+                          history=history[start * 2 * nb:stop * 2 * nb] if keep else None)
+        dts = np.array([r[-1] for r in rows])
+        if fresh:
+            self.dts = dts
+        mdot = np.array([-(r[0] + r[1]) for r in rows])
+        torque = np.array([r[2] for r in rows])
         w = self.dts / self.dts.sum()
         J = np.array([np.dot(w, mdot), np.dot(w, torque)])
         if keep:
-            self._fwd = dict(solver=s, times=ts, checkpoints=cps, params=params)
+            self._fwd = dict(solver=s, t_start=t_start, checkpoints=cps, params=params, history=history,
+                             record_bytes=nb)
         return J
+
+    def stage_times(self, t_start):
+        """(t0, t1, t_end) of every step, from the frozen dt sequence with the
+        solver's stage-time rule (cbdiso_2d.py:239): steps x 3."""
+        out = np.empty((self.steps, 3))
+        t = t_start
+        for n, dt in enumerate(self.dts):
+            dt = float(dt)
+            t1 = t * 0.0 + (t + dt) * 1.0
+            t_end = t * 0.5 + (t1 + dt) * 0.5
+            out[n] = (t, t1, t_end)
+            t = t_end
+        return out
 
     # ------------------------------------------------------------------
     def _records(self, s, t0, dt):
@@ -193,79 +253,70 @@ class AdjointRun:
         P = lambda t: ctypes.c_void_p(t.data_ptr())
         shape = s._buf[0].shape
         f64 = dict(dtype=torch.float64, device=s.device)
-        ws = torch.zeros(int(lib.cbdiso_b200_adjoint_workspace_bytes(g)) // 8 + 8, **f64)
-        words = [torch.zeros(shape[:2], dtype=torch.int32, device=s.device) for _ in range(2)]
+        steps, K = self.steps, self.checkpoint_every
+        history, nb = f["history"], f["record_bytes"]
+        rec = lambda n, k: ctypes.c_void_p(history.data_ptr() + (2 * n + k) * nb)
+
+        times = self.stage_times(f["t_start"])
+        jac = torch.from_numpy(mass_jacobians(times.reshape(-1), params.mass_ratio,
+                                              params.eccentricity).reshape(steps, 3, 20)).to(s.device)
+        row = jac.stride(0) * 8
+        jp = lambda n, k: ctypes.c_void_p(jac.data_ptr() + n * row + k * 20 * 8)
+
+        ws = torch.empty(int(lib.cbdiso_b200_adjoint_workspace_bytes(g)) // 8 + 8, **f64)
+        nblk = int(lib.cbdiso_b200_adjoint_chain_blocks(g))
+        chain = torch.zeros(nblk * 4, **f64)
+        words = [torch.empty(shape[:2], dtype=torch.int32, device=s.device) for _ in range(2)]
         total = self.dts.sum()
         da = s.mesh.dx * s.mesh.dy
         lam = torch.zeros(shape, **f64)
-        n_evals = 3 * self.steps
-        pars = torch.zeros((n_evals, NPAR), **f64)
-        eval_times = [0.0] * n_evals
-        steps = self.steps
-        K = self.checkpoint_every
-        work = torch.empty(shape, **f64)
+        lam_n = torch.zeros(shape, **f64)
+        lam_star = torch.empty(shape, **f64)
+        seg = min(K, steps)
+        p = [torch.empty(shape, **f64) for _ in range(seg + 1)]
+        stars = [torch.empty(shape, **f64) for _ in range(seg)]
+        s1, s2 = _capi.Stage(), _capi.Stage()
+        s2.a = 0.5
+        scratch, result = P(s._scratch), P(s._result)
+        check = _capi.check
         for start in reversed(range(0, steps, K)):
             stop = min(start + K, steps)
-            # recompute the segment, keeping every state and stage output
-            p = [f["checkpoints"][start].clone()]
-            stars, recs = [], []
-            for n in range(start, stop):
-                dev, nb, times = self._records(s, f["times"][n], float(self.dts[n]))
-                pn = p[-1]
-                star = torch.empty(shape, **f64)
-                out = torch.empty(shape, **f64)
-                _capi.check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(_capi.Stage()), P(dev), P(pn), None,
-                                                          P(star), None, P(s._scratch), P(s._result), stream),
-                            "advance_stage")
-                a2 = _capi.Stage()
-                a2.a = 0.5
-                # the in-place final stage is replayed out of place: inputs star, pn -> out
-                _capi.check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(a2), ctypes.c_void_p(dev.data_ptr() + nb),
-                                                          P(star), P(pn), P(out), None, P(s._scratch),
-                                                          P(s._result), stream), "advance_stage")
-                stars.append(star)
-                recs.append((dev, nb, times))
-                p.append(out)
-            # backward through the segment
+            # recompute the segment from its checkpoint with the recorded stage
+            # records, keeping every state (the in-place final stage is
+            # replayed out of place: inputs star, p[idx] -> p[idx + 1])
+            p[0].copy_(f["checkpoints"][start])
+            for idx, n in enumerate(range(start, stop)):
+                check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s1), rec(n, 0), P(p[idx]), None,
+                                                    P(stars[idx]), None, scratch, result, stream), "advance_stage")
+                check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s2), rec(n, 1), P(stars[idx]), P(p[idx]),
+                                                    P(p[idx + 1]), None, scratch, result, stream), "advance_stage")
             for n in reversed(range(start, stop)):
                 idx = n - start
-                dev, nb, (t0, t1, t_end) = recs[idx]
                 pn, star, out = p[idx], stars[idx], p[idx + 1]
-                rec1, rec2 = P(dev), ctypes.c_void_p(dev.data_ptr() + nb)
                 c = float(self.dts[n]) / total * da
-                row = 3 * n
                 # objective term of step n (state after the step, end masses)
-                _capi.check(lib.cbdiso_b200_objective_adjoint(g, rec2, P(out), weights[0] * c, weights[1] * c,
-                                                              P(lam), P(pars[row + 2]), P(ws), stream),
-                            "objective_adjoint")
-                eval_times[row + 2] = t_end
+                check(lib.cbdiso_b200_objective_adjoint_chained(g, rec(n, 1), P(out), weights[0] * c,
+                                                                weights[1] * c, P(lam), jp(n, 2), P(chain),
+                                                                P(ws), stream), "objective_adjoint")
                 # stage 2: inputs star (read), pn (u_n)
-                _capi.check(lib.cbdiso_b200_stage_record_branches(g, rec2, P(star), P(out), P(words[1]), stream),
-                            "record")
-                lam_star = torch.zeros(shape, **f64)
-                lam_n = torch.zeros(shape, **f64)
-                _capi.check(lib.cbdiso_b200_stage_adjoint(g, rec2, P(star), P(pn), P(out), P(words[1]), P(lam),
-                                                          P(lam_star), P(lam_n), P(pars[row + 1]), P(ws), stream),
-                            "stage_adjoint")
-                eval_times[row + 1] = t1
+                check(lib.cbdiso_b200_stage_record_branches(g, rec(n, 1), P(star), P(out), P(words[1]), stream),
+                      "record")
+                lam_star.zero_()
+                check(lib.cbdiso_b200_stage_adjoint_chained(g, rec(n, 1), P(star), P(pn), P(out), P(words[1]),
+                                                            P(lam), P(lam_star), P(lam_n), jp(n, 1), P(chain),
+                                                            P(ws), stream), "stage_adjoint")
                 # stage 1: input pn
-                _capi.check(lib.cbdiso_b200_stage_record_branches(g, rec1, P(pn), P(star), P(words[0]), stream),
-                            "record")
-                _capi.check(lib.cbdiso_b200_stage_adjoint(g, rec1, P(pn), None, P(star), P(words[0]), P(lam_star),
-                                                          P(lam_n), None, P(pars[row]), P(ws), stream),
-                            "stage_adjoint")
-                eval_times[row] = t0
-                lam = lam_n
+                check(lib.cbdiso_b200_stage_record_branches(g, rec(n, 0), P(pn), P(star), P(words[0]), stream),
+                      "record")
+                check(lib.cbdiso_b200_stage_adjoint_chained(g, rec(n, 0), P(pn), None, P(star), P(words[0]),
+                                                            P(lam_star), P(lam_n), None, jp(n, 0), P(chain),
+                                                            P(ws), stream), "stage_adjoint")
+                lam, lam_n = lam_n, lam
+                lam_n.zero_()
+        out4 = torch.zeros(4, **f64)
+        check(lib.cbdiso_b200_adjoint_chain_finish(P(chain), nblk, P(out4), stream), "chain_finish")
         grad_state = lam[NG:-NG, NG:-NG].cpu().numpy()
-        pp = pars.cpu().numpy()
-        dq = de = 0.0
-        for r in range(n_evals):
-            jac = mass_jacobian(eval_times[r], params.mass_ratio, params.eccentricity)
-            dq += float(pp[r, :10] @ jac[:, 0])
-            de += float(pp[r, :10] @ jac[:, 1])
-        dnu = float(pp[:, 10].sum())
-        drate = float(pp[:, 11].sum())
-        return grad_state, np.array([dq, de, dnu, drate])
+        return grad_state, out4.cpu().numpy()
 
     # ------------------------------------------------------------------
     def tangent(self, prim0, params: Params, dprim0, dparams, weights=(1.0, 0.0)):

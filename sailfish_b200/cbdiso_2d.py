@@ -400,15 +400,19 @@ class Solver(SolverBase):
                     raise ValueError("the physics point masses are not the setup's Kepler binary")
         return o
 
-    def run(self, steps, cfl=None, fixed_dt=None, graph=True, steps_per_graph=16):
+    def run(self, steps, cfl=None, fixed_dt=None, graph=True, steps_per_graph=16, dt_sequence=None,
+            history=None):
         """
         Advance `steps` iterations entirely on the device: each step's dt is
         min(dx, dy) / max wavespeed * cfl (driver.py:508-510) from the previous
-        step's fused wavespeed (or `fixed_dt`), and the point masses come from
-        the binary's Kepler orbit solved on the device. With `graph`, a group
-        of `steps_per_graph` steps is captured once in a CUDA graph (cached
-        on the solver) and replayed. Returns the time series: one row per
-        step, the `reductions()` row followed by dt.
+        step's fused wavespeed (or `fixed_dt`, or the device array
+        `dt_sequence` of per-step values), and the point masses come from the
+        binary's Kepler orbit solved on the device. With `graph`, a group of
+        `steps_per_graph` steps is captured once in a CUDA graph (cached on
+        the solver) and replayed. `history` (a device uint8 tensor of
+        steps * rk_order stage records) receives every step's stage records.
+        Returns the time series: one row per step, the `reductions()` row
+        followed by dt.
         """
         import torch
 
@@ -437,6 +441,16 @@ class Solver(SolverBase):
                                                  self._time, cfl, float(self.mesh.min_spacing()),
                                                  float(fixed_dt or 0.0), series.shape[0],
                                                  ctypes.c_void_p(host.data_ptr())), "stepper_init")
+        if dt_sequence is not None or history is not None:
+            if dt_sequence is not None and dt_sequence.numel() < steps:
+                raise ValueError("dt_sequence is shorter than steps")
+            self._check(lib.cbdiso_b200_stepper_attach(
+                ctypes.c_void_p(host.data_ptr()),
+                self._ptr(dt_sequence) if dt_sequence is not None else None,
+                int(dt_sequence.numel()) if dt_sequence is not None else 0,
+                self._ptr(history) if history is not None else None,
+                int(history.numel() // (self._rec_bytes * self._options.rk_order)) if history is not None else 0),
+                "stepper_attach")
         stepper.copy_(host, non_blocking=True)
         self.h2d_bytes += nbytes
         epilogue = self._epilogue(self._time, True, self._device_diags if self._fused else [])
@@ -491,7 +505,7 @@ class Solver(SolverBase):
 
     @staticmethod
     def _status_offset():
-        # StepperDev: 6 doubles, weights[3], cbd_orbit_t (80 bytes), num_stages, step, status
+        # StepperDev: 6 doubles, weights[3], cbd_orbit_t, then num_stages, step, status
         return 8 * 6 + 8 * 3 + ctypes.sizeof(_capi.Orbit) + 8
 
     def _series_rows(self, rows):

@@ -3,21 +3,23 @@
 // replays. Built with -fmad=false.
 //
 // Adjoint of a stage, as passes over zones and faces (all arrays in the
-// padded (ni + 4, nj + 4) layout; guard entries of adjoints are folded into
-// the zones they copy at the end):
-//   A  zone:  lambda of the output primitives -> lambda of the RK sum
-//             (conserved-to-primitive with the recorded floor / ceiling
-//             flags, the RK weights); u_n part to lambda_un.
-//   B  face:  lambda of each face flux from the two adjacent zones; HLLE and
-//             viscous-term products with the recorded am / ap choices;
-//             face sound-speed terms to the point-mass parameters.
+// padded (ni + 4, nj + 4) layout):
+//   S  zone:  slopes and rho * strain of the input, once per zone.
+//   B  face:  lambda of each face flux from the two adjacent zones (the
+//             conserved-to-primitive adjoint with the recorded floor / ceiling
+//             flags, inline); HLLE and viscous-term products with the
+//             recorded am / ap choices; face sound-speed terms to the
+//             point-mass parameters.
 //   C  zone:  gather the four faces: direct and slope contributions,
-//             rho * strain products, point-mass and buffer sources.
-//   D  zone:  slope products to the three zones of each slope (recorded
-//             limiter choices).
-//   E  zone:  fold guard-zone adjoints into the zones they copy.
+//             rho * strain products, point-mass and buffer sources, the u_n
+//             adjoint.
+//   D  zone:  per interior zone, the slope products of every zone it feeds
+//             (recorded limiter choices), its guard images folded in
+//             (zero-gradient boundary).
 // Parameter derivatives (per mass x, y, vx, vy, mass; nu; sink rate) are
-// summed per block and then per stage, in a fixed order.
+// summed per block in a fixed order, then either reduced per stage (12
+// values) or chained through the stage's d(mass parameters)/d(q, e) and
+// accumulated per block over the whole reverse sweep (4 values per block).
 #include <cstring>
 
 #include "adjoint_zone.cuh"
@@ -347,8 +349,48 @@ __device__ void sink_vjp(const MassDev &m, double x, double y, double dt, const 
     }
 }
 
-template <int BJ>
-__device__ __forceinline__ void block_sum_params(double (&par)[NPAR], double *out)
+// ---------------------------------------------------------------------------
+// adjoint passes
+// ---------------------------------------------------------------------------
+
+struct AdjArgs {
+    const StageDev *st;
+    const double *p;        // stage input (read by the stencil)
+    const double *pn;       // u_n source (null for a = 0)
+    const double *pout;     // stage output
+    const unsigned *words;  // recorded branches
+    const double *lam_out;  // adjoint of the output (interior)
+    double *lam_rd;         // += adjoint of the input (interior, guards folded)
+    double *lam_n;          // += adjoint of the u_n source (interior)
+    double *sl;             // per zone: gx (3), gy (3), rho * strain (3)
+    double *fx, *fy;        // per face: see adj_faces
+    double *lg, *lp;        // per zone: slope adjoints (6), direct adjoints (3)
+    double *par;            // per block: 12 parameter partials, or 4 chained sums (accumulated)
+    const double *jac;      // d(mass parameters)/d(q, e) of this stage, 10 x 2 (chained form)
+};
+
+// lambda of the RK sum u' of zone (i, j): conserved-to-primitive with the
+// recorded floor / ceiling flags; ld = (1 - a) lambda_u'.
+__device__ __forceinline__ bool lam_rk(const Consts &k, const AdjArgs &a, int i, int j, double *lu)
+{
+    if (i < 0 || i >= k.ni || j < 0 || j >= k.nj) {
+        lu[0] = lu[1] = lu[2] = 0.0;
+        return false;
+    }
+    const size_t c = zi(i, j, k.nj);
+    const unsigned w = a.words[c];
+    const double *o = a.pout + c * 3;
+    const double *l = a.lam_out + c * 3;
+    const double lvx = (w & BW_CEIL_X) ? 0.0 : l[1];
+    const double lvy = (w & BW_CEIL_Y) ? 0.0 : l[2];
+    lu[1] = lvx / o[0];
+    lu[2] = lvy / o[0];
+    lu[0] = (w & BW_FLOOR) ? 0.0 : l[0] - (o[1] * lvx + o[2] * lvy) / o[0];
+    return true;
+}
+
+template <int BJ, bool CHAIN>
+__device__ __forceinline__ void store_params(const AdjArgs &a, double (&par)[NPAR])
 {
     __shared__ double sm[NPAR * (BJ / 32)];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -360,73 +402,58 @@ __device__ __forceinline__ void block_sum_params(double (&par)[NPAR], double *ou
             sm[v * (BJ / 32) + warp] = x;
     }
     __syncthreads();
-    if (threadIdx.x < NPAR) {
-        double x = 0.0;
-        for (int w = 0; w < BJ / 32; ++w)
-            x += sm[threadIdx.x * (BJ / 32) + w];
-        out[(size_t)blockIdx.x * NPAR + threadIdx.x] = x;
+    if (threadIdx.x == 0) {
+        double tot[NPAR];
+        for (int v = 0; v < NPAR; ++v) {
+            double x = 0.0;
+            for (int w = 0; w < BJ / 32; ++w)
+                x += sm[v * (BJ / 32) + w];
+            tot[v] = x;
+        }
+        if (CHAIN) {
+            double q = 0.0, e = 0.0;
+            for (int v = 0; v < 10; ++v) {
+                q += tot[v] * a.jac[2 * v];
+                e += tot[v] * a.jac[2 * v + 1];
+            }
+            double *out = a.par + (size_t)blockIdx.x * 4;
+            out[0] += q;
+            out[1] += e;
+            out[2] += tot[10];
+            out[3] += tot[11];
+        } else {
+            for (int v = 0; v < NPAR; ++v)
+                a.par[(size_t)blockIdx.x * NPAR + v] = tot[v];
+        }
     }
 }
 
-// ---------------------------------------------------------------------------
-// adjoint passes
-// ---------------------------------------------------------------------------
-
-// A: zone (interior). lam_d = (1 - a) lambda_u'; lambda_un += p2c^T (a lambda_u').
-__global__ void adj_pass_a(Consts k, const StageDev *stp, const double *pout, const unsigned *words,
-                           const double *lam_out, const double *pun, double *lam_d, double *lam_un)
+// S: slopes and rho * strain of the zones of [-1, ni] x [-1, nj]
+__global__ void adj_slopes(Consts k, AdjArgs a)
 {
-    const long n = (long)k.ni * k.nj;
+    const long wi = k.ni + 2, wj = k.nj + 2;
     const long z = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (z >= n)
+    if (z >= wi * wj)
         return;
-    const int i = (int)(z / k.nj), j = (int)(z - (long)i * k.nj);
-    const size_t c = zi(i, j, k.nj);
-    const unsigned w = words[c];
-    const double *o = pout + c * 3;
-    const double *l = lam_out + c * 3;
-    const double rho = o[0];
-    const double lvx = (w & BW_CEIL_X) ? 0.0 : l[1];
-    const double lvy = (w & BW_CEIL_Y) ? 0.0 : l[2];
-    double lu[3];
-    lu[1] = lvx / rho;
-    lu[2] = lvy / rho;
-    lu[0] = (w & BW_FLOOR) ? 0.0 : l[0] - (o[1] * lvx + o[2] * lvy) / rho;
-    const double a = stp->a, b = stp->one_minus_a;
-    for (int q = 0; q < 3; ++q)
-        lam_d[c * 3 + q] = b * lu[q];
-    if (pun && a != 0.0) {
-        const double *pn = pun + c * 3;
-        const double l0 = a * lu[0], l1 = a * lu[1], l2 = a * lu[2];
-        lam_un[c * 3 + 0] += l0 + l1 * pn[1] + l2 * pn[2];
-        lam_un[c * 3 + 1] += l1 * pn[0];
-        lam_un[c * 3 + 2] += l2 * pn[0];
-    }
-}
-
-// slopes and rho * strain of a zone
-__device__ __forceinline__ void zone_slopes(const Consts &k, const double *p, int i, int j, double *gx, double *gy,
-                                            double *rs)
-{
-    slopes_at(k, p, i, j, gx, gy, nullptr);
+    const int i = (int)(z / wj) - 1, j = (int)(z % wj) - 1;
+    double *o = a.sl + zi(i, j, k.nj) * 9;
+    slopes_at(k, a.p, i, j, o, o + 3, nullptr);
     if (k.nu > 0.0)
-        rho_strain_generic(p[zi(i, j, k.nj) * 3], gx, gy, k, rs);
+        rho_strain_generic(a.p[zi(i, j, k.nj) * 3], o, o + 3, k, o + 6);
     else
-        rs[0] = rs[1] = rs[2] = 0.0;
+        o[6] = o[7] = o[8] = 0.0;
 }
 
-// B: faces. FX[c] holds the x-face i + 1/2 of zone c = (i, j); FY[c] the
-// y-face j - 1/2. Layout per face: lambda of the minus-side face state (3),
-// of the plus-side face state (3), of the two rho*strain components used on
-// the minus side (2) and on the plus side (2).
-template <int BJ>
-__global__ void __launch_bounds__(BJ) adj_pass_b(Consts k, const StageDev *stp, const double *p,
-                                                 const unsigned *words, const double *lam_d, double *fx, double *fy,
-                                                 double *par_out)
+// B: faces. fx[c] is the x-face i + 1/2 of zone c = (i, j), fy[c] the y-face
+// j - 1/2. Per face: lambda of the minus-side state (3), of the plus-side
+// state (3), of the two rho*strain components of the minus side (2) and of
+// the plus side (2).
+template <int BJ, bool CHAIN>
+__global__ void __launch_bounds__(BJ) adj_faces(Consts k, AdjArgs a)
 {
     __shared__ StageDev st;
     if (threadIdx.x == 0)
-        st = *stp;
+        st = *a.st;
     __syncthreads();
     const int ni = k.ni, nj = k.nj;
     const long wi = ni + 2, wj = nj + 2;
@@ -436,92 +463,79 @@ __global__ void __launch_bounds__(BJ) adj_pass_b(Consts k, const StageDev *stp, 
         par[v] = 0.0;
     MassT<double> m[2];
     masses_t<double>(st, nullptr, m);
-    const double dt = st.dt, hn = 0.5 * k.nu;
+    const double dt = st.dt, hn = 0.5 * k.nu, b = st.one_minus_a;
     if (z < wi * wj) {
         const int i = (int)(z / wj) - 1, j = (int)(z % wj) - 1;
         const size_t c = zi(i, j, nj);
-        const unsigned w = words[c];
+        const unsigned w = a.words[c];
+        double luc[3];
+        lam_rk(k, a, i, j, luc);
         if (i <= ni - 1 && j >= 0 && j < nj) {  // x-face i + 1/2: L = (i, j), R = (i + 1, j)
-            double gxl[3], gyl[3], rsl[3], gxr[3], gyr[3], rsr[3];
-            zone_slopes(k, p, i, j, gxl, gyl, rsl);
-            zone_slopes(k, p, i + 1, j, gxr, gyr, rsr);
             const size_t cr = zi(i + 1, j, nj);
+            const double *sl = a.sl + c * 9, *sr = a.sl + cr * 9;
+            double lur[3];
+            lam_rk(k, a, i + 1, j, lur);
             double pl[3], pr[3], lf[3];
-            const bool lin = i >= 0, rin = i + 1 < ni;
             for (int q = 0; q < 3; ++q) {
-                pl[q] = p[c * 3 + q] + 0.5 * gxl[q];
-                pr[q] = p[cr * 3 + q] - 0.5 * gxr[q];
-                const double ldl = lin ? lam_d[c * 3 + q] : 0.0, ldr = rin ? lam_d[cr * 3 + q] : 0.0;
-                lf[q] = (ldr - ldl) * dt / k.dx;
+                pl[q] = a.p[c * 3 + q] + 0.5 * sl[q];
+                pr[q] = a.p[cr * 3 + q] - 0.5 * sr[q];
+                lf[q] = (b * lur[q] - b * luc[q]) * dt / k.dx;
             }
             const double xf = k.xl + (i + 1.0) * k.dx, yc = k.yl + (j + 0.5) * k.dy;
-            const double cs2 = cs2_generic(k, m, xf, yc);
             double lpl[3] = {0, 0, 0}, lpr[3] = {0, 0, 0}, lcs2 = 0.0;
-            hlle_vjp<0>(pl, pr, cs2, (w >> BW_XFACE) & 15u, lf, lpl, lpr, &lcs2);
+            hlle_vjp<0>(pl, pr, cs2_generic(k, m, xf, yc), (w >> BW_XFACE) & 15u, lf, lpl, lpr, &lcs2);
             cs2_param_vjp(k, st, xf, yc, lcs2, par);
-            double *o = fx + c * 10;
+            double *o = a.fx + c * 10;
             for (int q = 0; q < 3; ++q) {
                 o[q] = lpl[q];
                 o[3 + q] = lpr[q];
             }
             if (k.nu > 0.0) {
-                // f1 -= hn (rsL_xx + rsR_xx), f2 -= hn (rsL_xy + rsR_xy)
-                o[6] = -hn * lf[1];
-                o[7] = -hn * lf[2];
-                o[8] = -hn * lf[1];
-                o[9] = -hn * lf[2];
-                par[10] += -0.5 * (rsl[0] + rsr[0]) * lf[1] - 0.5 * (rsl[1] + rsr[1]) * lf[2];
-            } else {
-                o[6] = o[7] = o[8] = o[9] = 0.0;
+                o[6] = o[8] = -hn * lf[1];
+                o[7] = o[9] = -hn * lf[2];
+                par[10] += -0.5 * (sl[6] + sr[6]) * lf[1] - 0.5 * (sl[7] + sr[7]) * lf[2];
             }
         }
-        if (i >= 0 && i < ni && j <= nj && j >= 0) {  // y-face j - 1/2: L = (i, j - 1), R = (i, j)
+        if (i >= 0 && i < ni && j >= 0 && j <= nj) {  // y-face j - 1/2: L = (i, j - 1), R = (i, j)
             const size_t cl = zi(i, j - 1, nj);
-            double gxl[3], gyl[3], rsl[3], gxr[3], gyr[3], rsr[3];
-            zone_slopes(k, p, i, j - 1, gxl, gyl, rsl);
-            zone_slopes(k, p, i, j, gxr, gyr, rsr);
+            const double *sl = a.sl + cl * 9, *sr = a.sl + c * 9;
+            double lul[3];
+            lam_rk(k, a, i, j - 1, lul);
             double pl[3], pr[3], lf[3];
-            const bool lin = j - 1 >= 0, rin = j < nj;
             for (int q = 0; q < 3; ++q) {
-                pl[q] = p[cl * 3 + q] + 0.5 * gyl[q];
-                pr[q] = p[c * 3 + q] - 0.5 * gyr[q];
-                const double ldl = lin ? lam_d[cl * 3 + q] : 0.0, ldr = rin ? lam_d[c * 3 + q] : 0.0;
-                lf[q] = (ldr - ldl) * dt / k.dy;
+                pl[q] = a.p[cl * 3 + q] + 0.5 * sl[3 + q];
+                pr[q] = a.p[c * 3 + q] - 0.5 * sr[3 + q];
+                lf[q] = (b * luc[q] - b * lul[q]) * dt / k.dy;
             }
             const double xc = k.xl + (i + 0.5) * k.dx, yf = k.yl + (j + 0.0) * k.dy;
-            const double cs2 = cs2_generic(k, m, xc, yf);
             double lpl[3] = {0, 0, 0}, lpr[3] = {0, 0, 0}, lcs2 = 0.0;
-            hlle_vjp<1>(pl, pr, cs2, (w >> BW_YFACE) & 15u, lf, lpl, lpr, &lcs2);
+            hlle_vjp<1>(pl, pr, cs2_generic(k, m, xc, yf), (w >> BW_YFACE) & 15u, lf, lpl, lpr, &lcs2);
             cs2_param_vjp(k, st, xc, yf, lcs2, par);
-            double *o = fy + c * 10;
+            double *o = a.fy + c * 10;
             for (int q = 0; q < 3; ++q) {
                 o[q] = lpl[q];
                 o[3 + q] = lpr[q];
             }
             if (k.nu > 0.0) {
-                // g1 -= hn (rsL_xy + rsR_xy), g2 -= hn (rsL_yy + rsR_yy)
-                o[6] = -hn * lf[1];
-                o[7] = -hn * lf[2];
-                o[8] = -hn * lf[1];
-                o[9] = -hn * lf[2];
-                par[10] += -0.5 * (rsl[1] + rsr[1]) * lf[1] - 0.5 * (rsl[2] + rsr[2]) * lf[2];
-            } else {
-                o[6] = o[7] = o[8] = o[9] = 0.0;
+                o[6] = o[8] = -hn * lf[1];
+                o[7] = o[9] = -hn * lf[2];
+                par[10] += -0.5 * (sl[7] + sr[7]) * lf[1] - 0.5 * (sl[8] + sr[8]) * lf[2];
             }
         }
     }
-    block_sum_params<BJ>(par, par_out);
+    store_params<BJ, CHAIN>(a, par);
 }
 
-// C: zones of [-1, ni] x [-1, nj]: face gathers, rho * strain, sources.
-template <int BJ>
-__global__ void __launch_bounds__(BJ) adj_pass_c(Consts k, const StageDev *stp, const double *p,
-                                                 const double *lam_d, const double *fx, const double *fy,
-                                                 double *lam_g, double *lam_p, double *par_out)
+__constant__ double kZeroFace[10] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+
+// C: zones of [-1, ni] x [-1, nj]: gather the four faces, rho * strain, sources,
+// the u_n adjoint.
+template <int BJ, bool CHAIN>
+__global__ void __launch_bounds__(BJ) adj_zones(Consts k, AdjArgs a)
 {
     __shared__ StageDev st;
     if (threadIdx.x == 0)
-        st = *stp;
+        st = *a.st;
     __syncthreads();
     const int ni = k.ni, nj = k.nj;
     const long wi = ni + 2, wj = nj + 2;
@@ -532,56 +546,66 @@ __global__ void __launch_bounds__(BJ) adj_pass_c(Consts k, const StageDev *stp, 
     if (z < wi * wj) {
         const int i = (int)(z / wj) - 1, j = (int)(z % wj) - 1;
         const size_t c = zi(i, j, nj);
-        const double *xe = fx + c * 10;                 // x-face i + 1/2 (zone is its minus side)
-        const double *xw = fx + zi(i - 1, j, nj) * 10;  // x-face i - 1/2 (plus side)
-        const double *ys = fy + c * 10;                 // y-face j - 1/2 (plus side)
-        const double *yn = fy + zi(i, j + 1, nj) * 10;  // y-face j + 1/2 (minus side)
+        // faces that pass B wrote; the others carry no adjoint
+        const bool row = j >= 0 && j < nj, col = i >= 0 && i < ni;
+        const double *xe = row && i < ni ? a.fx + c * 10 : kZeroFace;
+        const double *xw = row && i >= 0 ? a.fx + zi(i - 1, j, nj) * 10 : kZeroFace;
+        const double *ys = col && j >= 0 ? a.fy + c * 10 : kZeroFace;
+        const double *yn = col && j < nj ? a.fy + zi(i, j + 1, nj) * 10 : kZeroFace;
         double lp[3], lgx[3], lgy[3];
         for (int q = 0; q < 3; ++q) {
             lp[q] = xe[q] + xw[3 + q] + yn[q] + ys[3 + q];
             lgx[q] = 0.5 * xe[q] - 0.5 * xw[3 + q];
             lgy[q] = 0.5 * yn[q] - 0.5 * ys[3 + q];
         }
+        const double *sl = a.sl + c * 9;
         if (k.nu > 0.0) {
             const double lxx = xe[6] + xw[8];
             const double lxy = xe[7] + xw[9] + yn[6] + ys[8];
             const double lyy = yn[7] + ys[9];
-            double gx[3], gy[3], rs[3];
-            slopes_at(k, p, i, j, gx, gy, nullptr);
-            const double rho = p[c * 3];
-            rho_strain_generic(1.0, gx, gy, k, rs);  // strain itself
-            lp[0] += rs[0] * lxx + rs[1] * lxy + rs[2] * lyy;
+            const double rho = a.p[c * 3];
+            double s[3];
+            rho_strain_generic(1.0, sl, sl + 3, k, s);
+            lp[0] += s[0] * lxx + s[1] * lxy + s[2] * lyy;
             lgx[1] += rho * (4.0 / 3.0 * lxx - 2.0 / 3.0 * lyy) / k.dx;
             lgy[2] += rho * (-2.0 / 3.0 * lxx + 4.0 / 3.0 * lyy) / k.dy;
             lgx[2] += rho * lxy / k.dx;
             lgy[1] += rho * lxy / k.dy;
         }
-        if (i >= 0 && i < ni && j >= 0 && j < nj) {
-            const double *pc = p + c * 3;
-            const double *ld = lam_d + c * 3;
+        double lu[3];
+        if (lam_rk(k, a, i, j, lu)) {
+            const double *pc = a.p + c * 3;
+            double ld[3];
+            for (int q = 0; q < 3; ++q)
+                ld[q] = st.one_minus_a * lu[q];
             const double xc = k.xl + (i + 0.5) * k.dx, yc = k.yl + (j + 0.5) * k.dy;
             const double dt = st.dt;
-            // u' = (1 - a)(u + du): the direct u term and the buffer's -(u - u0) rate dt
             const double rate = buffer_rate(k, st, xc, yc);
-            double lu[3];
+            double luu[3];
             for (int q = 0; q < 3; ++q)
-                lu[q] = ld[q] * (1.0 - rate * dt);
+                luu[q] = ld[q] * (1.0 - rate * dt);
             for (int q = 0; q < 2; ++q) {
                 gravity_vjp(st.m[q], xc, yc, dt, pc, ld, lp, par + 5 * q);
                 sink_vjp(st.m[q], xc, yc, dt, pc, ld, lp, par + 5 * q, par + 11);
             }
-            // u = (rho, vx rho, vy rho)
-            lp[0] += lu[0] + lu[1] * pc[1] + lu[2] * pc[2];
-            lp[1] += lu[1] * pc[0];
-            lp[2] += lu[2] * pc[0];
+            lp[0] += luu[0] + luu[1] * pc[1] + luu[2] * pc[2];
+            lp[1] += luu[1] * pc[0];
+            lp[2] += luu[2] * pc[0];
+            if (a.pn && st.a != 0.0) {
+                const double *pn = a.pn + c * 3;
+                const double l0 = st.a * lu[0], l1 = st.a * lu[1], l2 = st.a * lu[2];
+                a.lam_n[c * 3 + 0] += l0 + l1 * pn[1] + l2 * pn[2];
+                a.lam_n[c * 3 + 1] += l1 * pn[0];
+                a.lam_n[c * 3 + 2] += l2 * pn[0];
+            }
         }
         for (int q = 0; q < 3; ++q) {
-            lam_g[c * 6 + q] = lgx[q];
-            lam_g[c * 6 + 3 + q] = lgy[q];
-            lam_p[c * 3 + q] = lp[q];
+            a.lg[c * 6 + q] = lgx[q];
+            a.lg[c * 6 + 3 + q] = lgy[q];
+            a.lp[c * 3 + q] = lp[q];
         }
     }
-    block_sum_params<BJ>(par, par_out);
+    store_params<BJ, CHAIN>(a, par);
 }
 
 __device__ __forceinline__ void slope_weights(unsigned sel, double theta, double *w)
@@ -600,28 +624,25 @@ __device__ __forceinline__ void slope_weights(unsigned sel, double theta, double
     }
 }
 
-// D: zones of [-2, ni + 1] x [-2, nj + 1]: slope products to their three zones.
-__global__ void adj_pass_d(Consts k, const unsigned *words, const double *lam_g, double *lam_p)
+// the full input adjoint at padded position (i, j): its direct part plus its
+// share of the slopes of its x- and y-neighbours (slopes live on [-1, ni] x [-1, nj])
+__device__ __forceinline__ void input_adjoint_at(const Consts &k, const AdjArgs &a, int i, int j, double *acc)
 {
     const int ni = k.ni, nj = k.nj;
-    const long wi = ni + 4, wj = nj + 4;
-    const long z = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (z >= wi * wj)
-        return;
-    const int i = (int)(z / wj) - 2, j = (int)(z % wj) - 2;
     const size_t c = zi(i, j, nj);
-    double acc[3] = {0.0, 0.0, 0.0};
-    // x-slopes of zones i - 1, i, i + 1 (defined on [-1, ni] x [-1, nj])
+    const bool in_range = i >= -1 && i <= ni && j >= -1 && j <= nj;
+    for (int q = 0; q < 3; ++q)
+        acc[q] = in_range ? a.lp[c * 3 + q] : 0.0;
     for (int d = -1; d <= 1; ++d) {
         const int ii = i + d;
         if (ii < -1 || ii > ni || j < -1 || j > nj)
             continue;
         const size_t o = zi(ii, j, nj);
-        const unsigned w = words[o];
+        const unsigned w = a.words[o];
         for (int q = 0; q < 3; ++q) {
             double wt[3];
             slope_weights((w >> (2 * q)) & 3u, k.theta, wt);
-            acc[q] += wt[1 - d] * lam_g[o * 6 + q];  // zone i sits at position (i - ii) + 1 of the slope ii
+            acc[q] += wt[1 - d] * a.lg[o * 6 + q];
         }
     }
     for (int d = -1; d <= 1; ++d) {
@@ -629,44 +650,46 @@ __global__ void adj_pass_d(Consts k, const unsigned *words, const double *lam_g,
         if (jj < -1 || jj > nj || i < -1 || i > ni)
             continue;
         const size_t o = zi(i, jj, nj);
-        const unsigned w = words[o];
+        const unsigned w = a.words[o];
         for (int q = 0; q < 3; ++q) {
             double wt[3];
             slope_weights((w >> (6 + 2 * q)) & 3u, k.theta, wt);
-            acc[q] += wt[1 - d] * lam_g[o * 6 + 3 + q];
+            acc[q] += wt[1 - d] * a.lg[o * 6 + 3 + q];
         }
     }
-    for (int q = 0; q < 3; ++q)
-        lam_p[c * 3 + q] += acc[q];
 }
 
-// E: interior zones gather the adjoints of their guard images.
-__global__ void adj_fold_guards(int ni, int nj, const double *lam_p, double *lam_rd)
+// D: interior zones: slope products and the guard images folded into the
+// zones they copy (zero-gradient boundary)
+__global__ void adj_inputs(Consts k, AdjArgs a)
 {
-    const long n = (long)ni * nj;
+    const int ni = k.ni, nj = k.nj;
     const long z = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (z >= n)
+    if (z >= (long)ni * nj)
         return;
     const int i = (int)(z / nj), j = (int)(z - (long)i * nj);
     const int ilo = i == 0 ? -2 : i, ihi = i == ni - 1 ? ni + 1 : i;
     const int jlo = j == 0 ? -2 : j, jhi = j == nj - 1 ? nj + 1 : j;
-    double acc[3] = {0.0, 0.0, 0.0};
+    double tot[3] = {0.0, 0.0, 0.0};
     for (int ii = ilo; ii <= ihi; ++ii)
-        for (int jj = jlo; jj <= jhi; ++jj)
+        for (int jj = jlo; jj <= jhi; ++jj) {
+            double v[3];
+            input_adjoint_at(k, a, ii, jj, v);
             for (int q = 0; q < 3; ++q)
-                acc[q] += lam_p[zi(ii, jj, nj) * 3 + q];
+                tot[q] += v[q];
+        }
     for (int q = 0; q < 3; ++q)
-        lam_rd[zi(i, j, nj) * 3 + q] += acc[q];
+        a.lam_rd[zi(i, j, nj) * 3 + q] += tot[q];
 }
 
 // fixed-order sum of block partials into one parameter row
-__global__ void sum_params(const double *blocks, int nblocks, double *out)
+__global__ void sum_params(const double *blocks, int nblocks, int width, double *out)
 {
-    if (threadIdx.x >= NPAR)
+    if ((int)threadIdx.x >= width)
         return;
     double s = 0.0;
     for (int b = 0; b < nblocks; ++b)
-        s += blocks[(size_t)b * NPAR + threadIdx.x];
+        s += blocks[(size_t)b * width + threadIdx.x];
     out[threadIdx.x] += s;
 }
 
@@ -738,15 +761,15 @@ __global__ void objective_tangent_kernel(Consts k, const StageDev *stp, TangentP
 }
 
 // lambda_p += dF/dp per zone; parameter derivatives to blocks
-template <int BJ>
-__global__ void __launch_bounds__(BJ) objective_adjoint_kernel(Consts k, const StageDev *stp, const double *p,
-                                                               double wm, double wt, double *lam,
-                                                               double *par_out)
+template <int BJ, bool CHAIN>
+__global__ void __launch_bounds__(BJ) objective_adjoint_kernel(Consts k, AdjArgs args, double wm, double wt)
 {
     __shared__ StageDev st;
     if (threadIdx.x == 0)
-        st = *stp;
+        st = *args.st;
     __syncthreads();
+    const double *p = args.p;
+    double *lam = args.lam_rd;
     double par[NPAR];
     for (int v = 0; v < NPAR; ++v)
         par[v] = 0.0;
@@ -792,7 +815,7 @@ __global__ void __launch_bounds__(BJ) objective_adjoint_kernel(Consts k, const S
             }
         }
     }
-    block_sum_params<BJ>(par, par_out);
+    store_params<BJ, CHAIN>(args, par);
 }
 
 inline int nblocks(long n, int bs) { return (int)((n + bs - 1) / bs); }
@@ -809,9 +832,92 @@ using namespace cbd;
 
 namespace {
 
+constexpr size_t WS_PER_ZONE = 9 + 10 + 10 + 6 + 3;
+
 bool grid_ok(const cbd_grid_t *g)
 {
     return g && g->ni > 0 && g->nj > 0 && g->xr > g->xl && g->yr > g->yl && (g->eos_type == 1 || g->eos_type == 2);
+}
+
+AdjArgs adj_args(const cbd_grid_t *grid, const void *stage_dev, void *workspace, const double *jac)
+{
+    AdjArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.st = static_cast<const StageDev *>(stage_dev);
+    const size_t zones = (size_t)(grid->ni + 4) * (grid->nj + 4);
+    double *ws = static_cast<double *>(workspace);
+    a.sl = ws;
+    a.fx = a.sl + zones * 9;
+    a.fy = a.fx + zones * 10;
+    a.lg = a.fy + zones * 10;
+    a.lp = a.lg + zones * 6;
+    a.jac = jac;
+    return a;
+}
+
+// With `jac` null: 12 parameter derivatives of this stage ADDED into
+// params_out. Otherwise the chained (q, e, nu, rate) sums are accumulated
+// per block into params_out (blocks x 4), reduced by adjoint_chain_finish.
+int stage_adjoint_impl(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
+                       const double *primitive_n, const double *primitive_out, const unsigned int *words,
+                       const double *lam_out, double *lam_rd, double *lam_n, const double *jac, double *params_out,
+                       void *workspace, void *stream)
+{
+    if (!grid_ok(grid) || !stage_dev || !primitive_rd || !primitive_out || !words || !lam_out || !lam_rd ||
+        !params_out || !workspace || (primitive_n && !lam_n))
+        return CBD_ERR_ARGUMENT;
+    const Consts k = consts_from_grid(grid);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int ni = grid->ni, nj = grid->nj;
+    const size_t zones = (size_t)(ni + 4) * (nj + 4);
+    AdjArgs a = adj_args(grid, stage_dev, workspace, jac);
+    a.p = primitive_rd;
+    a.pn = primitive_n;
+    a.pout = primitive_out;
+    a.words = words;
+    a.lam_out = lam_out;
+    a.lam_rd = lam_rd;
+    a.lam_n = lam_n;
+    double *parts = static_cast<double *>(workspace) + zones * WS_PER_ZONE;
+    a.par = jac ? params_out : parts;
+    const long nwide = (long)(ni + 2) * (nj + 2);
+    const int nb = nblocks(nwide, 128);
+    adj_slopes<<<nb, 128, 0, s>>>(k, a);
+    if (jac) {
+        adj_faces<128, true><<<nb, 128, 0, s>>>(k, a);
+        adj_zones<128, true><<<nb, 128, 0, s>>>(k, a);
+    } else {
+        adj_faces<128, false><<<nb, 128, 0, s>>>(k, a);
+        sum_params<<<1, 32, 0, s>>>(parts, nb, NPAR, params_out);
+        adj_zones<128, false><<<nb, 128, 0, s>>>(k, a);
+        sum_params<<<1, 32, 0, s>>>(parts, nb, NPAR, params_out);
+    }
+    adj_inputs<<<nblocks((long)ni * nj, 128), 128, 0, s>>>(k, a);
+    return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
+}
+
+int objective_adjoint_impl(const cbd_grid_t *grid, const void *stage_dev, const double *primitive, double w_mdot,
+                           double w_torque, double *lam, const double *jac, double *params_out, void *workspace,
+                           void *stream)
+{
+    if (!grid_ok(grid) || !stage_dev || !primitive || !lam || !params_out || !workspace)
+        return CBD_ERR_ARGUMENT;
+    const Consts k = consts_from_grid(grid);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t zones = (size_t)(grid->ni + 4) * (grid->nj + 4);
+    AdjArgs a = adj_args(grid, stage_dev, workspace, jac);
+    a.p = primitive;
+    a.lam_rd = lam;
+    double *parts = static_cast<double *>(workspace) + zones * WS_PER_ZONE;
+    a.par = jac ? params_out : parts;
+    const int nb = nblocks((long)grid->ni * grid->nj, 128);
+    if (jac) {
+        objective_adjoint_kernel<128, true><<<nb, 128, 0, s>>>(k, a, w_mdot, w_torque);
+    } else {
+        objective_adjoint_kernel<128, false><<<nb, 128, 0, s>>>(k, a, w_mdot, w_torque);
+        sum_params<<<1, 32, 0, s>>>(parts, nb, NPAR, params_out);
+    }
+    return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
 }
 
 }  // namespace
@@ -824,8 +930,8 @@ size_t cbdiso_b200_adjoint_workspace_bytes(const cbd_grid_t *grid)
         return 0;
     const size_t zones = (size_t)(grid->ni + 4) * (grid->nj + 4);
     const size_t blocks = (size_t)nblocks((long)(grid->ni + 2) * (grid->nj + 2), 128) + 1;
-    // lam_d (3) + fx (10) + fy (10) + lam_g (6) + lam_p (3) doubles per zone, 3 x blocks x NPAR partials
-    return zones * (3 + 10 + 10 + 6 + 3) * sizeof(double) + 3 * blocks * NPAR * sizeof(double) + 256;
+    // sl (9) + fx (10) + fy (10) + lg (6) + lp (3) doubles per zone, then block partials
+    return zones * WS_PER_ZONE * sizeof(double) + blocks * NPAR * sizeof(double) + 256;
 }
 
 int cbdiso_b200_stage_record_branches(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
@@ -875,33 +981,34 @@ int cbdiso_b200_stage_adjoint(const cbd_grid_t *grid, const void *stage_dev, con
                               const double *lam_out, double *lam_rd, double *lam_n, double *params_out,
                               void *workspace, void *stream)
 {
-    if (!grid_ok(grid) || !stage_dev || !primitive_rd || !primitive_out || !words || !lam_out || !lam_rd ||
-        !params_out || !workspace || (primitive_n && !lam_n))
+    return stage_adjoint_impl(grid, stage_dev, primitive_rd, primitive_n, primitive_out, words, lam_out, lam_rd,
+                              lam_n, nullptr, params_out, workspace, stream);
+}
+
+int cbdiso_b200_stage_adjoint_chained(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
+                                      const double *primitive_n, const double *primitive_out,
+                                      const unsigned int *words, const double *lam_out, double *lam_rd,
+                                      double *lam_n, const double *jacobian, double *chain_acc, void *workspace,
+                                      void *stream)
+{
+    if (!jacobian || !chain_acc)
         return CBD_ERR_ARGUMENT;
-    const Consts k = consts_from_grid(grid);
-    const StageDev *st = static_cast<const StageDev *>(stage_dev);
-    const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int ni = grid->ni, nj = grid->nj;
-    const size_t zones = (size_t)(ni + 4) * (nj + 4);
-    double *ws = static_cast<double *>(workspace);
-    double *lam_d = ws;
-    double *fx = lam_d + zones * 3;
-    double *fy = fx + zones * 10;
-    double *lam_g = fy + zones * 10;
-    double *lam_p = lam_g + zones * 6;
-    double *parts = lam_p + zones * 3;
-    const long nwide = (long)(ni + 2) * (nj + 2);
-    const int nb = nblocks(nwide, 128);
-    if (cudaMemsetAsync(ws, 0, zones * (3 + 10 + 10 + 6 + 3) * sizeof(double), s) != cudaSuccess)
-        return CBD_ERR_CUDA;
-    adj_pass_a<<<nblocks((long)ni * nj, 128), 128, 0, s>>>(k, st, primitive_out, words, lam_out, primitive_n,
-                                                           lam_d, lam_n);
-    adj_pass_b<128><<<nb, 128, 0, s>>>(k, st, primitive_rd, words, lam_d, fx, fy, parts);
-    sum_params<<<1, 32, 0, s>>>(parts, nb, params_out);
-    adj_pass_c<128><<<nb, 128, 0, s>>>(k, st, primitive_rd, lam_d, fx, fy, lam_g, lam_p, parts);
-    sum_params<<<1, 32, 0, s>>>(parts, nb, params_out);
-    adj_pass_d<<<nblocks((long)zones, 128), 128, 0, s>>>(k, words, lam_g, lam_p);
-    adj_fold_guards<<<nblocks((long)ni * nj, 128), 128, 0, s>>>(ni, nj, lam_p, lam_rd);
+    return stage_adjoint_impl(grid, stage_dev, primitive_rd, primitive_n, primitive_out, words, lam_out, lam_rd,
+                              lam_n, jacobian, chain_acc, workspace, stream);
+}
+
+size_t cbdiso_b200_adjoint_chain_blocks(const cbd_grid_t *grid)
+{
+    if (!grid_ok(grid))
+        return 0;
+    return (size_t)nblocks((long)(grid->ni + 2) * (grid->nj + 2), 128);
+}
+
+int cbdiso_b200_adjoint_chain_finish(const double *chain_acc, int num_blocks, double *out4, void *stream)
+{
+    if (!chain_acc || num_blocks <= 0 || !out4)
+        return CBD_ERR_ARGUMENT;
+    sum_params<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(chain_acc, num_blocks, 4, out4);
     return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
 }
 
@@ -928,17 +1035,18 @@ int cbdiso_b200_objective_adjoint(const cbd_grid_t *grid, const void *stage_dev,
                                   double w_mdot, double w_torque, double *lam, double *params_out, void *workspace,
                                   void *stream)
 {
-    if (!grid_ok(grid) || !stage_dev || !primitive || !lam || !params_out || !workspace)
+    return objective_adjoint_impl(grid, stage_dev, primitive, w_mdot, w_torque, lam, nullptr, params_out,
+                                  workspace, stream);
+}
+
+int cbdiso_b200_objective_adjoint_chained(const cbd_grid_t *grid, const void *stage_dev, const double *primitive,
+                                          double w_mdot, double w_torque, double *lam, const double *jacobian,
+                                          double *chain_acc, void *workspace, void *stream)
+{
+    if (!jacobian || !chain_acc)
         return CBD_ERR_ARGUMENT;
-    const Consts k = consts_from_grid(grid);
-    const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const size_t zones = (size_t)(grid->ni + 4) * (grid->nj + 4);
-    double *parts = static_cast<double *>(workspace) + zones * (3 + 10 + 10 + 6 + 3);
-    const int nb = nblocks((long)grid->ni * grid->nj, 128);
-    objective_adjoint_kernel<128><<<nb, 128, 0, s>>>(k, static_cast<const StageDev *>(stage_dev), primitive, w_mdot,
-                                                     w_torque, lam, parts);
-    sum_params<<<1, 32, 0, s>>>(parts, nb, params_out);
-    return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
+    return objective_adjoint_impl(grid, stage_dev, primitive, w_mdot, w_torque, lam, jacobian, chain_acc,
+                                  workspace, stream);
 }
 
 }  // extern "C"

@@ -39,7 +39,12 @@ __global__ void step_prologue_kernel(StepperDev *steppers, int n, const double *
     }
     if (finalize)
         return;
-    const double dt = s->fixed_dt > 0.0 ? s->fixed_dt : s->min_spacing / result[0] * s->cfl;
+    if (s->dt_sequence && s->step >= s->dt_count) {
+        s->status = CBD_ERR_ARGUMENT;
+        return;
+    }
+    const double dt = s->dt_sequence ? s->dt_sequence[s->step]
+                                     : (s->fixed_dt > 0.0 ? s->fixed_dt : s->min_spacing / result[0] * s->cfl);
     const double time0 = s->time;
     double t = time0;
     double times[3];
@@ -66,6 +71,8 @@ __global__ void step_prologue_kernel(StepperDev *steppers, int n, const double *
         r.dt = dt;
         r.buffer_mass = r.m[0].mass + r.m[1].mass;
         r.buffer_k = s->buffer_k;
+        if (s->history && s->step < s->history_capacity)
+            s->history[(size_t)s->step * s->num_stages + k] = r;
     }
     s->dt = dt;
     s->time = t;
@@ -120,6 +127,21 @@ int cbdiso_b200_stepper_init(const cbd_grid_t *grid, const cbd_orbit_t *orbit, i
                      : 0.0;
     s.series_capacity = series_capacity;
     s.status = CBD_OK;
+    std::memcpy(stepper, &s, sizeof(s));
+    return CBD_OK;
+}
+
+int cbdiso_b200_stepper_attach(void *stepper, const double *dt_sequence, int dt_count, void *history,
+                               int history_capacity)
+{
+    if (!stepper || dt_count < 0 || history_capacity < 0 || (dt_sequence && dt_count == 0))
+        return CBD_ERR_ARGUMENT;
+    StepperDev s;
+    std::memcpy(&s, stepper, sizeof(s));
+    s.dt_sequence = dt_sequence;
+    s.dt_count = dt_count;
+    s.history = static_cast<StageDev *>(history);
+    s.history_capacity = history ? history_capacity : 0;
     std::memcpy(stepper, &s, sizeof(s));
     return CBD_OK;
 }

@@ -18,6 +18,10 @@ struct StepperDev {
     int step;            // steps taken
     int status;          // CBD_OK, or CBD_ERR_KEPLER once a solve failed (then no further steps)
     int series_capacity; // rows available in the time-series buffer
+    const double *dt_sequence;  // if set: dt of step n is dt_sequence[n] (n < dt_count)
+    StageDev *history;          // if set: stage records of step n also go to history[n * num_stages ...]
+    int dt_count;
+    int history_capacity;       // steps the history holds
 };
 
 // Prologue of n grids' steps; grid d reads results + d * result_stride and
