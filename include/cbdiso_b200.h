@@ -354,19 +354,20 @@ int cbdiso_b200_objective_adjoint(const cbd_grid_t *grid, const void *stage_dev,
                                   double w_mdot, double w_torque, double *lam, double *params_out, void *workspace,
                                   void *stream);
 
-/* Chained forms for a whole reverse sweep: instead of 12 parameter
+/* Chained forms for a whole reverse sweep: the stage adjoint records the
+ * stage's branches itself (into the workspace); instead of 12 parameter
  * derivatives per call, the mass-parameter part is contracted on the device
  * with `jacobian` (device memory, 10 x 2 row-major: d(x, y, vx, vy, mass of
  * mass 1, then of mass 2) / d(q, e) at this stage's time) and ADDED per
  * block into `chain_acc` (device, cbdiso_b200_adjoint_chain_blocks(grid) x 4
  * doubles: d/dq, d/de, d/dnu, d/d(sink rate)), which the caller zeroes once
  * before the sweep. cbdiso_b200_adjoint_chain_finish ADDS the block sums, in
- * a fixed order, into out4 (device, 4 doubles). */
+ * a fixed order, into out4 (device, 4 doubles). The chained objective's
+ * weights are per unit time: each is multiplied by the record's dt. */
 int cbdiso_b200_stage_adjoint_chained(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
-                                      const double *primitive_n, const double *primitive_out,
-                                      const unsigned int *words, const double *lam_out, double *lam_rd,
-                                      double *lam_n, const double *jacobian, double *chain_acc, void *workspace,
-                                      void *stream);
+                                      const double *primitive_n, const double *primitive_out, const double *lam_out,
+                                      double *lam_rd, double *lam_n, const double *jacobian, double *chain_acc,
+                                      void *workspace, void *stream);
 int cbdiso_b200_objective_adjoint_chained(const cbd_grid_t *grid, const void *stage_dev, const double *primitive,
                                           double w_mdot, double w_torque, double *lam, const double *jacobian,
                                           double *chain_acc, void *workspace, void *stream);

@@ -140,7 +140,7 @@ def _declare(lib):
         "cbdiso_b200_stage_adjoint": [POINTER(Grid), V, V, V, V, V, V, V, V, V, V, V],
         "cbdiso_b200_objective_tangent": [POINTER(Grid), V, V, D, V, V, D, D, V, c_int, V],
         "cbdiso_b200_objective_adjoint": [POINTER(Grid), V, V, D, D, V, V, V, V],
-        "cbdiso_b200_stage_adjoint_chained": [POINTER(Grid), V, V, V, V, V, V, V, V, V, V, V, V],
+        "cbdiso_b200_stage_adjoint_chained": [POINTER(Grid), V, V, V, V, V, V, V, V, V, V, V],
         "cbdiso_b200_objective_adjoint_chained": [POINTER(Grid), V, V, D, D, V, V, V, V, V],
         "cbdiso_b200_adjoint_chain_finish": [V, c_int, V, V],
     }.items():

@@ -127,10 +127,13 @@ class AdjointRun:
     """
 
     def __init__(self, resolution=512, steps=400, checkpoint_every=20, cfl=0.3, plm_theta=1.5, mach=10.0,
-                 domain_radius=8.0):
+                 domain_radius=8.0, store_states=None):
         self.n = resolution
         self.steps = steps
         self.checkpoint_every = checkpoint_every
+        # keep every stage state of the forward run (no recompute) when it
+        # fits: None = when it takes under half the free device memory
+        self.store_states = store_states
         self.cfl = cfl
         self.plm_theta = plm_theta
         self.mach = mach
@@ -177,14 +180,19 @@ class AdjointRun:
         nb = int(self._lib.cbdiso_b200_stage_record_bytes())
         history = torch.empty(steps * 2 * nb, dtype=torch.uint8, device=s.device) if keep else None
         t_start = s.time
-        rows, cps = [], {}
-        for start in range(0, steps, K):
-            stop = min(start + K, steps)
-            if keep:
-                cps[start] = s._buf[0].clone()
-            rows += s.run(stop - start, cfl=self.cfl, steps_per_graph=K,
-                          dt_sequence=None if fresh else dts_dev[start:stop],
-                          history=history[start * 2 * nb:stop * 2 * nb] if keep else None)
+        rows, cps, trajectory = [], {}, None
+        if keep and self._keep_all(s):
+            trajectory = torch.empty((2 * steps + 1,) + tuple(s._buf[0].shape), dtype=torch.float64,
+                                     device=s.device)
+            rows = s.run(steps, cfl=self.cfl, dt_sequence=dts_dev, history=history, trajectory=trajectory)
+        else:
+            for start in range(0, steps, K):
+                stop = min(start + K, steps)
+                if keep:
+                    cps[start] = s._buf[0].clone()
+                rows += s.run(stop - start, cfl=self.cfl, steps_per_graph=K,
+                              dt_sequence=None if fresh else dts_dev[start:stop],
+                              history=history[start * 2 * nb:stop * 2 * nb] if keep else None)
         dts = np.array([r[-1] for r in rows])
         if fresh:
             self.dts = dts
@@ -194,8 +202,17 @@ class AdjointRun:
         J = np.array([np.dot(w, mdot), np.dot(w, torque)])
         if keep:
             self._fwd = dict(solver=s, t_start=t_start, checkpoints=cps, params=params, history=history,
-                             record_bytes=nb)
+                             record_bytes=nb, trajectory=trajectory)
         return J
+
+    def _keep_all(self, s):
+        if self.store_states is not None:
+            return bool(self.store_states)
+        import torch
+
+        need = (2 * self.steps + 1) * s._buf[0].numel() * 8
+        free, _ = torch.cuda.mem_get_info(s.device)
+        return need < free // 2
 
     def stage_times(self, t_start):
         """(t0, t1, t_end) of every step, from the frozen dt sequence with the
@@ -236,11 +253,13 @@ class AdjointRun:
         dev = torch.frombuffer(host, dtype=torch.uint8).to(s.device)
         return dev, nb, (t0, t1, t_end)
 
-    def gradient(self, weights=(1.0, 0.0)):
+    def gradient(self, weights=(1.0, 0.0), graph=True):
         """
         dJ/dprim0 (ni, nj, 3) and dJ/d(q, e, nu, sink_rate) for
         J = weights[0] * mean accretion + weights[1] * mean torque, at the
-        last forward(keep=True) run.
+        last forward(keep=True) run. With `graph`, the reverse sweep of a full
+        segment is captured once in a CUDA graph and replayed for every full
+        segment (its stage records and Jacobians staged into fixed buffers).
         """
         import torch
 
@@ -248,75 +267,41 @@ class AdjointRun:
         f = self._fwd
         s: Solver = f["solver"]
         params: Params = f["params"]
-        g = ctypes.byref(s._grid)
-        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-        P = lambda t: ctypes.c_void_p(t.data_ptr())
-        shape = s._buf[0].shape
-        f64 = dict(dtype=torch.float64, device=s.device)
         steps, K = self.steps, self.checkpoint_every
         history, nb = f["history"], f["record_bytes"]
-        rec = lambda n, k: ctypes.c_void_p(history.data_ptr() + (2 * n + k) * nb)
-
+        c = s.mesh.dx * s.mesh.dy / self.dts.sum()
+        w = (weights[0] * c, weights[1] * c)
         times = self.stage_times(f["t_start"])
         jac = torch.from_numpy(mass_jacobians(times.reshape(-1), params.mass_ratio,
-                                              params.eccentricity).reshape(steps, 3, 20)).to(s.device)
-        row = jac.stride(0) * 8
-        jp = lambda n, k: ctypes.c_void_p(jac.data_ptr() + n * row + k * 20 * 8)
-
-        ws = torch.empty(int(lib.cbdiso_b200_adjoint_workspace_bytes(g)) // 8 + 8, **f64)
-        nblk = int(lib.cbdiso_b200_adjoint_chain_blocks(g))
-        chain = torch.zeros(nblk * 4, **f64)
-        words = [torch.empty(shape[:2], dtype=torch.int32, device=s.device) for _ in range(2)]
-        total = self.dts.sum()
-        da = s.mesh.dx * s.mesh.dy
-        lam = torch.zeros(shape, **f64)
-        lam_n = torch.zeros(shape, **f64)
-        lam_star = torch.empty(shape, **f64)
-        seg = min(K, steps)
-        p = [torch.empty(shape, **f64) for _ in range(seg + 1)]
-        stars = [torch.empty(shape, **f64) for _ in range(seg)]
-        s1, s2 = _capi.Stage(), _capi.Stage()
-        s2.a = 0.5
-        scratch, result = P(s._scratch), P(s._result)
-        check = _capi.check
+                                              params.eccentricity).reshape(steps, 60)).to(s.device)
+        trajectory = f["trajectory"]
+        sweep = self._sweep(s, 0 if trajectory is not None else min(K, steps), w)
+        sweep.chain.zero_()
+        sweep.lam.zero_()
+        sweep.lam_n.zero_()
+        if trajectory is not None:
+            # every state of the forward run is at hand: no recompute
+            sweep.run(history, jac, steps, states=trajectory)
+            return sweep.finish()
         for start in reversed(range(0, steps, K)):
             stop = min(start + K, steps)
-            # recompute the segment from its checkpoint with the recorded stage
-            # records, keeping every state (the in-place final stage is
-            # replayed out of place: inputs star, p[idx] -> p[idx + 1])
-            p[0].copy_(f["checkpoints"][start])
-            for idx, n in enumerate(range(start, stop)):
-                check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s1), rec(n, 0), P(p[idx]), None,
-                                                    P(stars[idx]), None, scratch, result, stream), "advance_stage")
-                check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s2), rec(n, 1), P(stars[idx]), P(p[idx]),
-                                                    P(p[idx + 1]), None, scratch, result, stream), "advance_stage")
-            for n in reversed(range(start, stop)):
-                idx = n - start
-                pn, star, out = p[idx], stars[idx], p[idx + 1]
-                c = float(self.dts[n]) / total * da
-                # objective term of step n (state after the step, end masses)
-                check(lib.cbdiso_b200_objective_adjoint_chained(g, rec(n, 1), P(out), weights[0] * c,
-                                                                weights[1] * c, P(lam), jp(n, 2), P(chain),
-                                                                P(ws), stream), "objective_adjoint")
-                # stage 2: inputs star (read), pn (u_n)
-                check(lib.cbdiso_b200_stage_record_branches(g, rec(n, 1), P(star), P(out), P(words[1]), stream),
-                      "record")
-                lam_star.zero_()
-                check(lib.cbdiso_b200_stage_adjoint_chained(g, rec(n, 1), P(star), P(pn), P(out), P(words[1]),
-                                                            P(lam), P(lam_star), P(lam_n), jp(n, 1), P(chain),
-                                                            P(ws), stream), "stage_adjoint")
-                # stage 1: input pn
-                check(lib.cbdiso_b200_stage_record_branches(g, rec(n, 0), P(pn), P(star), P(words[0]), stream),
-                      "record")
-                check(lib.cbdiso_b200_stage_adjoint_chained(g, rec(n, 0), P(pn), None, P(star), P(words[0]),
-                                                            P(lam_star), P(lam_n), None, jp(n, 0), P(chain),
-                                                            P(ws), stream), "stage_adjoint")
-                lam, lam_n = lam_n, lam
-                lam_n.zero_()
-        out4 = torch.zeros(4, **f64)
-        check(lib.cbdiso_b200_adjoint_chain_finish(P(chain), nblk, P(out4), stream), "chain_finish")
-        grad_state = lam[NG:-NG, NG:-NG].cpu().numpy()
-        return grad_state, out4.cpu().numpy()
+            sweep.p[0].copy_(f["checkpoints"][start])
+            if graph and stop - start == sweep.k:
+                sweep.hist.copy_(history[start * 2 * nb:stop * 2 * nb])
+                sweep.jac.copy_(jac[start:stop])
+                sweep.replay()
+            else:
+                sweep.run(history[start * 2 * nb:stop * 2 * nb], jac[start:stop], stop - start)
+        return sweep.finish()
+
+    def _sweep(self, s, k, w):
+        """The reverse-sweep buffers and graph for segments of k steps, cached
+        on the run while the grid (its Consts), k and the weights stay."""
+        key = (bytes(s._grid), k, w)
+        cached = getattr(self, "_sweep_cache", None)
+        if cached is None or cached.key != key:
+            self._sweep_cache = _ReverseSweep(self._lib, s, k, w, key)
+        return self._sweep_cache
 
     # ------------------------------------------------------------------
     def tangent(self, prim0, params: Params, dprim0, dparams, weights=(1.0, 0.0)):
@@ -368,6 +353,114 @@ class AdjointRun:
             p, dp = out, dout
             t = t_end
         return acc
+
+
+class _ReverseSweep:
+    """
+    Buffers of the reverse sweep over one segment of k steps: the recomputed
+    states p[0..k] and stage-1 outputs (none for k = 0: the states come
+    from a recorded trajectory), the adjoint states, the adjoint workspace
+    and the chained parameter accumulator; and the CUDA graph of a full
+    segment, reading its stage records and Jacobians from `hist` and `jac`.
+    """
+
+    def __init__(self, lib, s, k, w, key):
+        import torch
+
+        self.key, self.k, self.w, self.lib = key, k, w, lib
+        self.grid = _capi.Grid.from_buffer_copy(s._grid)
+        g = ctypes.byref(self.grid)
+        shape = s._buf[0].shape
+        f64 = dict(dtype=torch.float64, device=s.device)
+        self.nb = int(lib.cbdiso_b200_stage_record_bytes())
+        self.p = [torch.empty(shape, **f64) for _ in range(k + 1)]
+        self.stars = [torch.empty(shape, **f64) for _ in range(k)]
+        self.lam = torch.zeros(shape, **f64)
+        self.lam_n = torch.zeros(shape, **f64)
+        self.lam_star = torch.empty(shape, **f64)
+        self.ws = torch.empty(int(lib.cbdiso_b200_adjoint_workspace_bytes(g)) // 8 + 8, **f64)
+        self.rows = int(lib.cbdiso_b200_adjoint_chain_blocks(g))
+        self.chain = torch.zeros(self.rows * 4, **f64)
+        self.scratch = torch.zeros(int(lib.cbdiso_b200_scratch_bytes(g)) // 8 + 8, **f64)
+        self.result = torch.zeros(64, **f64)
+        self.hist = torch.empty(max(k, 1) * 2 * self.nb, dtype=torch.uint8, device=s.device)
+        self.jac = torch.empty((max(k, 1), 60), **f64)
+        self.graph = None
+
+    def run(self, hist, jac, count, states=None):
+        """The recompute and reverse sweep of one segment of `count` steps,
+        with stage records `hist` (2 per step) and Jacobians `jac`
+        (count x 60: stage 1, stage 2, end of step, 10 x 2 each). With
+        `states` (a recorded trajectory: u_n at 2n, the first stage's output
+        at 2n + 1) nothing is recomputed."""
+        import torch
+
+        lib, g, nb = self.lib, ctypes.byref(self.grid), self.nb
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        P = lambda t: ctypes.c_void_p(t.data_ptr())
+        rec = lambda n, k: ctypes.c_void_p(hist.data_ptr() + (2 * n + k) * nb)
+        jp = lambda n, k: ctypes.c_void_p(jac.data_ptr() + (60 * n + 20 * k) * 8)
+        s1, s2 = _capi.Stage(), _capi.Stage()
+        s2.a = 0.5
+        if states is not None:
+            p, stars = states[0::2], states[1::2]
+        else:
+            p, stars = self.p, self.stars
+        scratch, result, ws, chain = P(self.scratch), P(self.result), P(self.ws), P(self.chain)
+        check = _capi.check
+        # recompute the segment from p[0] with the recorded stage records,
+        # keeping every state (the in-place final stage is replayed out of
+        # place: inputs star, p[n] -> p[n + 1])
+        for n in range(count if states is None else 0):
+            check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s1), rec(n, 0), P(p[n]), None, P(stars[n]), None,
+                                                scratch, result, stream), "advance_stage")
+            check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s2), rec(n, 1), P(stars[n]), P(p[n]), P(p[n + 1]),
+                                                None, scratch, result, stream), "advance_stage")
+        lam, lam_n, lam_star = self.lam, self.lam_n, self.lam_star
+        for n in reversed(range(count)):
+            pn, star, out = p[n], stars[n], p[n + 1]
+            # objective term of step n (state after the step, end masses;
+            # the chained weights are per unit time: dt_n / sum(dt) * dA)
+            check(lib.cbdiso_b200_objective_adjoint_chained(g, rec(n, 1), P(out), self.w[0], self.w[1], P(lam),
+                                                            jp(n, 2), chain, ws, stream), "objective_adjoint")
+            # stage 2: inputs star (read), pn (u_n)
+            lam_star.zero_()
+            check(lib.cbdiso_b200_stage_adjoint_chained(g, rec(n, 1), P(star), P(pn), P(out), P(lam), P(lam_star),
+                                                        P(lam_n), jp(n, 1), chain, ws, stream), "stage_adjoint")
+            # stage 1: input pn
+            check(lib.cbdiso_b200_stage_adjoint_chained(g, rec(n, 0), P(pn), None, P(star), P(lam_star), P(lam_n),
+                                                        None, jp(n, 0), chain, ws, stream), "stage_adjoint")
+            lam, lam_n = lam_n, lam
+            lam_n.zero_()
+        if lam is not self.lam:
+            # an odd count leaves the adjoint in the other buffer
+            self.lam.copy_(lam)
+            self.lam_n.zero_()
+
+    def replay(self):
+        import torch
+
+        if self.graph is None:
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            graph = torch.cuda.CUDAGraph()
+            # capture records the launches without running them
+            with torch.cuda.graph(graph, stream=side):
+                self.run(self.hist, self.jac, self.k)
+            torch.cuda.current_stream().wait_stream(side)
+            self.graph = graph
+        self.graph.replay()
+
+    def finish(self):
+        import torch
+
+        out4 = torch.zeros(4, dtype=torch.float64, device=self.chain.device)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _capi.check(self.lib.cbdiso_b200_adjoint_chain_finish(ctypes.c_void_p(self.chain.data_ptr()), self.rows,
+                                                              ctypes.c_void_p(out4.data_ptr()), stream),
+                    "chain_finish")
+        grad_state = self.lam[NG:-NG, NG:-NG].cpu().numpy()
+        return grad_state, out4.cpu().numpy()
 
 
 def make_solver_exact(setup, mesh, physics, prim0, plm_theta):

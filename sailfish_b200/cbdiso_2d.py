@@ -401,7 +401,7 @@ class Solver(SolverBase):
         return o
 
     def run(self, steps, cfl=None, fixed_dt=None, graph=True, steps_per_graph=16, dt_sequence=None,
-            history=None):
+            history=None, trajectory=None):
         """
         Advance `steps` iterations entirely on the device: each step's dt is
         min(dx, dy) / max wavespeed * cfl (driver.py:508-510) from the previous
@@ -411,8 +411,12 @@ class Solver(SolverBase):
         `steps_per_graph` steps is captured once in a CUDA graph (cached on
         the solver) and replayed. `history` (a device uint8 tensor of
         steps * rk_order stage records) receives every step's stage records.
-        Returns the time series: one row per step, the `reductions()` row
-        followed by dt.
+        `trajectory` (RK2 only; a device float64 tensor of 2 * steps + 1
+        padded states) receives the whole run instead of the two solver
+        buffers: [0] the current state, then per step n the first stage's
+        output [2n + 1] and the step's result [2n + 2]; the last is copied
+        back into the solver. Returns the time series: one row per step, the
+        `reductions()` row followed by dt.
         """
         import torch
 
@@ -456,15 +460,30 @@ class Solver(SolverBase):
         epilogue = self._epilogue(self._time, True, self._device_diags if self._fused else [])
         weights = RK_WEIGHTS[self._options.rk_order]
 
-        def one_step():
+        def one_step(n=None):
             stream = self._stream()
             self._check(lib.cbdiso_b200_step_prologue(self._ptr(stepper), self._ptr(self._result),
                                                       self._ptr(self._records), self._ptr(series), nvals, 0,
                                                       stream), "step_prologue")
-            self._launch_stages(weights, epilogue, stream)
+            if n is None:
+                self._launch_stages(weights, epilogue, stream)
+            else:
+                self._launch_stages(weights, epilogue, stream,
+                                    (trajectory[2 * n], trajectory[2 * n + 1], trajectory[2 * n + 2]))
 
         remaining = steps
-        if graph and steps >= steps_per_graph:
+        if trajectory is not None:
+            if self._options.rk_order != 2:
+                raise ValueError("a trajectory is recorded for RK2 only")
+            if trajectory.shape[0] < 2 * steps + 1 or trajectory.shape[1:] != self._buf[0].shape or \
+                    trajectory.dtype != self._buf[0].dtype or not trajectory.is_contiguous():
+                raise ValueError("trajectory must hold 2 * steps + 1 padded float64 states")
+            trajectory[0].copy_(self._buf[0])
+            for n in range(steps):
+                one_step(n)
+            self._buf[0].copy_(trajectory[2 * steps])
+            remaining = 0
+        if graph and remaining >= steps_per_graph:
             # the graph bakes in buffer addresses: RK1 alternates two assignments
             key = (steps_per_graph, nvals, self._buf[0].data_ptr())
             cuda_graph = self._graphs.get(key)
@@ -534,15 +553,19 @@ class Solver(SolverBase):
             out.append(vals + [dt])
         return out
 
-    def _launch_stages(self, weights, epilogue, stream):
+    def _launch_stages(self, weights, epilogue, stream, rk2_buffers=None):
         """The RK stages of one step, reading the stage records in
         self._records; the last stage carries the epilogue. Buffers: RK1
         A -> B (then swapped), RK2 A -> B, B (+A) -> A, RK3 A -> B,
-        B (+A) -> C, C (+A) -> A."""
+        B (+A) -> C, C (+A) -> A; or, for RK2, the given (u_n, stage 1
+        output, result)."""
         lib, g = self._lib, self._grid
         A = self._buf[0]
         B = self._buf[1]
-        if len(weights) == 1:
+        if rk2_buffers is not None:
+            un, mid, out = rk2_buffers
+            plan = [(un, None, mid, None), (mid, un, out, epilogue)]
+        elif len(weights) == 1:
             plan = [(A, None, B, epilogue)]
         elif len(weights) == 2:
             plan = [(A, None, B, None), (B, A, A, epilogue)]
@@ -559,7 +582,7 @@ class Solver(SolverBase):
                 ctypes.byref(ep) if ep is not None else None, self._ptr(self._scratch), self._ptr(self._result),
                 stream)
             self._check(status, "advance_stage")
-        if len(weights) == 1:
+        if len(weights) == 1 and rk2_buffers is None:
             self._buf[0], self._buf[1] = B, A
 
     def reductions(self):

@@ -208,29 +208,74 @@ __global__ void record_kernel(Consts k, const StageDev *stp, const double *p, co
 // adjoint building blocks
 // ---------------------------------------------------------------------------
 
-// d(cs^2)/d(mass parameters) at (x, y), times lam, into par[0..9]
+// Derivative values need no correct rounding (the branches they follow are
+// fixed): the vector-Jacobian products below use reciprocal square roots and
+// reciprocals.
+
+// Parameter-derivative accumulator of one thread. Indices: 5 p + (x, y, vx,
+// vy, mass) of mass p, 10 = nu, 11 = sink rate. The per-stage form keeps the
+// 12 sums; the chained form contracts the mass part with the stage's Kepler
+// Jacobian (shared memory) as it goes and keeps 4: d/dq, d/de, d/dnu, d/drate.
+template <bool CHAIN>
+struct ParAcc;
+
+template <>
+struct ParAcc<false> {
+    static constexpr int N = NPAR;
+    double v[NPAR];
+    __device__ explicit ParAcc(const double *)
+    {
+        for (int r = 0; r < NPAR; ++r)
+            v[r] = 0.0;
+    }
+    __device__ __forceinline__ void add(int r, double x) { v[r] += x; }
+};
+
+template <>
+struct ParAcc<true> {
+    static constexpr int N = 4;
+    double v[4];
+    const double *jac;
+    __device__ explicit ParAcc(const double *j) : jac(j)
+    {
+        for (int r = 0; r < 4; ++r)
+            v[r] = 0.0;
+    }
+    __device__ __forceinline__ void add(int r, double x)
+    {
+        if (r < 10) {
+            v[0] += x * jac[2 * r];
+            v[1] += x * jac[2 * r + 1];
+        } else {
+            v[r - 8] += x;
+        }
+    }
+};
+
+// d(cs^2)/d(mass parameters) at (x, y), times lam, into the accumulator
+template <class Acc>
 __device__ __forceinline__ void cs2_param_vjp(const Consts &k, const StageDev &st, double x, double y, double lam,
-                                              double *par)
+                                              Acc &par)
 {
     if (k.eos != 2 || lam == 0.0)
         return;
+    const double l = lam * k.inv_mach2;
     for (int p = 0; p < 2; ++p) {
         const MassDev &m = st.m[p];
         if (!(m.mass > 0.0))
             continue;
         const double dx = x - m.x, dy = y - m.y;
-        const double S = dx * dx + dy * dy + m.soft2;
-        const double s12 = 1.0 / sqrt(S);
-        const double s32 = s12 / S;
-        par[5 * p + 0] += lam * m.mass * dx * s32 / k.mach2;
-        par[5 * p + 1] += lam * m.mass * dy * s32 / k.mach2;
-        par[5 * p + 4] += lam * s12 / k.mach2;
+        const double s12 = rsqrt(dx * dx + dy * dy + m.soft2);
+        const double w = l * m.mass * s12 * s12 * s12;
+        par.add(5 * p + 0, w * dx);
+        par.add(5 * p + 1, w * dy);
+        par.add(5 * p + 4, l * s12);
     }
 }
 
 // HLLE vector-Jacobian product for the recorded am / ap choice `sel`.
 template <int DIR>
-__device__ __forceinline__ void hlle_vjp(const double *pl, const double *pr, double cs2, unsigned sel,
+__device__ __forceinline__ void hlle_vjp(const double *pl, const double *pr, double cs2, double cs, unsigned sel,
                                          const double *lf, double *lpl, double *lpr, double *lcs2)
 {
     const double ul[3] = {pl[0], pl[1] * pl[0], pl[2] * pl[0]};
@@ -241,15 +286,14 @@ __device__ __forceinline__ void hlle_vjp(const double *pl, const double *pr, dou
     double fr[3] = {vr * ur[0], vr * ur[1], vr * ur[2]};
     fl[1 + DIR] += pl[0] * cs2;
     fr[1 + DIR] += pr[0] * cs2;
-    const double cs = sqrt(cs2);
     const unsigned s_am = sel & 3u, s_ap = (sel >> 2) & 3u;
     const double am = s_am == 0 ? 0.0 : (s_am == 1 ? vl - cs : vr - cs);
     const double ap = s_ap == 0 ? 0.0 : (s_ap == 1 ? vl + cs : vr + cs);
-    const double D = ap - am;
+    const double inv_d = 1.0 / (ap - am);
     double lfl[3], lfr[3], lul[3], lur[3], lap = 0.0, lam = 0.0;
     for (int q = 0; q < 3; ++q) {
-        const double F = (fl[q] * ap - fr[q] * am - (ul[q] - ur[q]) * ap * am) / D;
-        const double w = lf[q] / D;
+        const double F = (fl[q] * ap - fr[q] * am - (ul[q] - ur[q]) * ap * am) * inv_d;
+        const double w = lf[q] * inv_d;
         lfl[q] = w * ap;
         lfr[q] = -w * am;
         lul[q] = -w * ap * am;
@@ -273,7 +317,7 @@ __device__ __forceinline__ void hlle_vjp(const double *pl, const double *pr, dou
         lcs += lap;
     }
     if (cs > 0.0)
-        *lcs2 += lcs / (2.0 * cs);
+        *lcs2 += lcs * (0.5 / cs);
     // fluxes: f0 = v u0, f1 = v u1 (+ rho cs2 if DIR == 0), f2 = v u2 (+ rho cs2 if DIR == 1)
     lvl += lfl[0] * ul[0] + lfl[1] * ul[1] + lfl[2] * ul[2];
     lvr += lfr[0] * ur[0] + lfr[1] * ur[1] + lfr[2] * ur[2];
@@ -303,50 +347,23 @@ __device__ __forceinline__ void hlle_vjp(const double *pl, const double *pr, dou
     lpr[2] += lvyr;
 }
 
-// Gravity of one mass: d(du)/d(sigma) and d(du)/d(mass parameters).
-__device__ __forceinline__ void gravity_vjp(const MassDev &m, double x, double y, double dt, const double *pc,
-                                            const double *ld, double *lp, double *par5)
+// Gravity of mass p: d(du)/d(sigma) and d(du)/d(mass parameters).
+template <class Acc>
+__device__ __forceinline__ void gravity_vjp(const MassDev &m, int p, double x, double y, double dt, const double *pc,
+                                            const double *ld, double *lp, Acc &par)
 {
     if (m.mass == 0.0)
         return;
     const double dx = x - m.x, dy = y - m.y;
-    const double S = dx * dx + dy * dy + m.soft2;
-    const double g = inv_pow15<false>(S);
-    const double h = g / S;
+    const double r = rsqrt(dx * dx + dy * dy + m.soft2);
+    const double g = r * r * r;
+    const double h = g * r * r;
     const double sig = pc[0];
     const double a = ld[1] * dx + ld[2] * dy;
     lp[0] += -m.mass * g * a * dt;
-    par5[4] += -sig * g * a * dt;
-    par5[0] += -sig * m.mass * dt * (ld[1] * (3.0 * dx * dx * h - g) + ld[2] * (3.0 * dx * dy * h));
-    par5[1] += -sig * m.mass * dt * (ld[1] * (3.0 * dx * dy * h) + ld[2] * (3.0 * dy * dy * h - g));
-}
-
-// Sink of one mass, direction by direction through the dual-number sink:
-// inputs (sigma, vx, vy, xp, yp, vxp, vyp, rate).
-__device__ void sink_vjp(const MassDev &m, double x, double y, double dt, const double *pc, const double *ld,
-                         double *lp, double *par5, double *lrate)
-{
-    if (m.sink_rate == 0.0 || m.sink_model < 1 || m.sink_model > 3)
-        return;
-    const double dx = x - m.x, dy = y - m.y;
-    if (!(dx * dx + dy * dy < m.sink_hi2))
-        return;
-    double seed[8];
-    for (int dir = 0; dir < 8; ++dir) {
-        for (int s = 0; s < 8; ++s)
-            seed[s] = s == dir ? 1.0 : 0.0;
-        Dual du[3] = {dual(0.0), dual(0.0), dual(0.0)};
-        sink_generic<Dual>(m, dual(m.x, seed[3]), dual(m.y, seed[4]), dual(m.vx, seed[5]), dual(m.vy, seed[6]),
-                           dual(m.sink_rate, seed[7]), x, y, dt, dual(pc[0], seed[0]), dual(pc[1], seed[1]),
-                           dual(pc[2], seed[2]), du);
-        const double v = ld[0] * du[0].d + ld[1] * du[1].d + ld[2] * du[2].d;
-        if (dir < 3)
-            lp[dir] += v;
-        else if (dir < 7)
-            par5[dir - 3] += v;
-        else
-            *lrate += v;
-    }
+    par.add(5 * p + 4, -sig * g * a * dt);
+    par.add(5 * p + 0, -sig * m.mass * dt * (ld[1] * (3.0 * dx * dx * h - g) + ld[2] * (3.0 * dx * dy * h)));
+    par.add(5 * p + 1, -sig * m.mass * dt * (ld[1] * (3.0 * dx * dy * h) + ld[2] * (3.0 * dy * dy * h - g)));
 }
 
 // ---------------------------------------------------------------------------
@@ -358,7 +375,7 @@ struct AdjArgs {
     const double *p;        // stage input (read by the stencil)
     const double *pn;       // u_n source (null for a = 0)
     const double *pout;     // stage output
-    const unsigned *words;  // recorded branches
+    unsigned *words;        // branch words (read; written by the recording slope pass)
     const double *lam_out;  // adjoint of the output (interior)
     double *lam_rd;         // += adjoint of the input (interior, guards folded)
     double *lam_n;          // += adjoint of the u_n source (interior)
@@ -370,7 +387,7 @@ struct AdjArgs {
 };
 
 // lambda of the RK sum u' of zone (i, j): conserved-to-primitive with the
-// recorded floor / ceiling flags; ld = (1 - a) lambda_u'.
+// recorded floor / ceiling flags; zero outside the interior.
 __device__ __forceinline__ bool lam_rk(const Consts &k, const AdjArgs &a, int i, int j, double *lu)
 {
     if (i < 0 || i >= k.ni || j < 0 || j >= k.nj) {
@@ -381,168 +398,186 @@ __device__ __forceinline__ bool lam_rk(const Consts &k, const AdjArgs &a, int i,
     const unsigned w = a.words[c];
     const double *o = a.pout + c * 3;
     const double *l = a.lam_out + c * 3;
+    const double inv_rho = 1.0 / o[0];
     const double lvx = (w & BW_CEIL_X) ? 0.0 : l[1];
     const double lvy = (w & BW_CEIL_Y) ? 0.0 : l[2];
-    lu[1] = lvx / o[0];
-    lu[2] = lvy / o[0];
-    lu[0] = (w & BW_FLOOR) ? 0.0 : l[0] - (o[1] * lvx + o[2] * lvy) / o[0];
+    lu[1] = lvx * inv_rho;
+    lu[2] = lvy * inv_rho;
+    lu[0] = (w & BW_FLOOR) ? 0.0 : l[0] - (o[1] * lvx + o[2] * lvy) * inv_rho;
     return true;
 }
 
-template <int BJ, bool CHAIN>
-__device__ __forceinline__ void store_params(const AdjArgs &a, double (&par)[NPAR])
+// The stage record in shared memory, and in the chained form the stage's
+// Kepler Jacobian (10 x 2).
+struct StageShared {
+    StageDev st;
+    double jac[20];
+};
+
+template <bool CHAIN>
+__device__ __forceinline__ void load_stage(const AdjArgs &a, StageShared &sh)
 {
-    __shared__ double sm[NPAR * (BJ / 32)];
+    if (threadIdx.x == 0)
+        sh.st = *a.st;
+    if (CHAIN && threadIdx.x >= 32 && threadIdx.x < 52)
+        sh.jac[threadIdx.x - 32] = a.jac[threadIdx.x - 32];
+    __syncthreads();
+}
+
+// Block sum of the accumulators, in a fixed order: the per-stage form stores
+// the block's 12 sums as its row; the chained form adds its 4 sums to its row.
+template <int NT, bool CHAIN>
+__device__ __forceinline__ void store_params(const AdjArgs &a, const ParAcc<CHAIN> &acc)
+{
+    constexpr int NV = ParAcc<CHAIN>::N;
+    constexpr int NW = NT / 32;
+    __shared__ double sm[NV * NW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int v = 0; v < NPAR; ++v) {
-        double x = par[v];
+    for (int r = 0; r < NV; ++r) {
+        double x = acc.v[r];
         for (int o = 16; o > 0; o >>= 1)
             x += __shfl_down_sync(0xffffffffu, x, o);
         if (lane == 0)
-            sm[v * (BJ / 32) + warp] = x;
+            sm[r * NW + warp] = x;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double tot[NPAR];
-        for (int v = 0; v < NPAR; ++v) {
-            double x = 0.0;
-            for (int w = 0; w < BJ / 32; ++w)
-                x += sm[v * (BJ / 32) + w];
-            tot[v] = x;
-        }
-        if (CHAIN) {
-            double q = 0.0, e = 0.0;
-            for (int v = 0; v < 10; ++v) {
-                q += tot[v] * a.jac[2 * v];
-                e += tot[v] * a.jac[2 * v + 1];
-            }
-            double *out = a.par + (size_t)blockIdx.x * 4;
-            out[0] += q;
-            out[1] += e;
-            out[2] += tot[10];
-            out[3] += tot[11];
-        } else {
-            for (int v = 0; v < NPAR; ++v)
-                a.par[(size_t)blockIdx.x * NPAR + v] = tot[v];
-        }
+    if ((int)threadIdx.x < NV) {
+        double x = 0.0;
+        for (int w = 0; w < NW; ++w)
+            x += sm[threadIdx.x * NW + w];
+        double *out = a.par + (size_t)blockIdx.x * NV + threadIdx.x;
+        if (CHAIN)
+            *out += x;
+        else
+            *out = x;
     }
 }
 
-// S: slopes and rho * strain of the zones of [-1, ni] x [-1, nj]
-__global__ void adj_slopes(Consts k, AdjArgs a)
+__device__ __forceinline__ long grid_start(int nt) { return blockIdx.x * (long)nt + threadIdx.x; }
+__device__ __forceinline__ long grid_step(int nt) { return (long)gridDim.x * nt; }
+
+constexpr int ADJ_THREADS = 128;
+constexpr int ADJ_MIN_BLOCKS = 5;  // resident blocks per SM the register budget allows
+
+// S: slopes and rho * strain of the zones of [-1, ni] x [-1, nj]; with
+// RECORD also the branch word (limiter choices; floor and ceiling flags of
+// interior zones) that cbdiso_b200_stage_record_branches would write, less
+// the HLLE choices, which pass B recomputes.
+template <bool RECORD>
+__global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_slopes(Consts k, AdjArgs a)
 {
     const long wi = k.ni + 2, wj = k.nj + 2;
-    const long z = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (z >= wi * wj)
-        return;
-    const int i = (int)(z / wj) - 1, j = (int)(z % wj) - 1;
-    double *o = a.sl + zi(i, j, k.nj) * 9;
-    slopes_at(k, a.p, i, j, o, o + 3, nullptr);
-    if (k.nu > 0.0)
-        rho_strain_generic(a.p[zi(i, j, k.nj) * 3], o, o + 3, k, o + 6);
-    else
-        o[6] = o[7] = o[8] = 0.0;
-}
-
-// B: faces. fx[c] is the x-face i + 1/2 of zone c = (i, j), fy[c] the y-face
-// j - 1/2. Per face: lambda of the minus-side state (3), of the plus-side
-// state (3), of the two rho*strain components of the minus side (2) and of
-// the plus side (2).
-template <int BJ, bool CHAIN>
-__global__ void __launch_bounds__(BJ) adj_faces(Consts k, AdjArgs a)
-{
-    __shared__ StageDev st;
-    if (threadIdx.x == 0)
-        st = *a.st;
-    __syncthreads();
-    const int ni = k.ni, nj = k.nj;
-    const long wi = ni + 2, wj = nj + 2;
-    const long z = blockIdx.x * (long)BJ + threadIdx.x;
-    double par[NPAR];
-    for (int v = 0; v < NPAR; ++v)
-        par[v] = 0.0;
-    MassT<double> m[2];
-    masses_t<double>(st, nullptr, m);
-    const double dt = st.dt, hn = 0.5 * k.nu, b = st.one_minus_a;
+    const long z = grid_start(ADJ_THREADS);
     if (z < wi * wj) {
         const int i = (int)(z / wj) - 1, j = (int)(z % wj) - 1;
-        const size_t c = zi(i, j, nj);
-        const unsigned w = a.words[c];
-        double luc[3];
-        lam_rk(k, a, i, j, luc);
-        if (i <= ni - 1 && j >= 0 && j < nj) {  // x-face i + 1/2: L = (i, j), R = (i + 1, j)
-            const size_t cr = zi(i + 1, j, nj);
-            const double *sl = a.sl + c * 9, *sr = a.sl + cr * 9;
-            double lur[3];
-            lam_rk(k, a, i + 1, j, lur);
-            double pl[3], pr[3], lf[3];
-            for (int q = 0; q < 3; ++q) {
-                pl[q] = a.p[c * 3 + q] + 0.5 * sl[q];
-                pr[q] = a.p[cr * 3 + q] - 0.5 * sr[q];
-                lf[q] = (b * lur[q] - b * luc[q]) * dt / k.dx;
-            }
-            const double xf = k.xl + (i + 1.0) * k.dx, yc = k.yl + (j + 0.5) * k.dy;
-            double lpl[3] = {0, 0, 0}, lpr[3] = {0, 0, 0}, lcs2 = 0.0;
-            hlle_vjp<0>(pl, pr, cs2_generic(k, m, xf, yc), (w >> BW_XFACE) & 15u, lf, lpl, lpr, &lcs2);
-            cs2_param_vjp(k, st, xf, yc, lcs2, par);
-            double *o = a.fx + c * 10;
-            for (int q = 0; q < 3; ++q) {
-                o[q] = lpl[q];
-                o[3 + q] = lpr[q];
-            }
-            if (k.nu > 0.0) {
-                o[6] = o[8] = -hn * lf[1];
-                o[7] = o[9] = -hn * lf[2];
-                par[10] += -0.5 * (sl[6] + sr[6]) * lf[1] - 0.5 * (sl[7] + sr[7]) * lf[2];
-            }
+        const size_t c = zi(i, j, k.nj);
+        double *o = a.sl + c * 9;
+        unsigned w = 0;
+        slopes_at(k, a.p, i, j, o, o + 3, RECORD ? &w : nullptr);
+        if (k.nu > 0.0) {
+            const double rho = a.p[c * 3];
+            const double sxx = 4.0 / 3.0 * o[1] * k.inv_dx - 2.0 / 3.0 * o[5] * k.inv_dy;
+            const double syy = -2.0 / 3.0 * o[1] * k.inv_dx + 4.0 / 3.0 * o[5] * k.inv_dy;
+            const double sxy = o[2] * k.inv_dx + o[4] * k.inv_dy;
+            o[6] = rho * sxx;
+            o[7] = rho * sxy;
+            o[8] = rho * syy;
+        } else {
+            o[6] = o[7] = o[8] = 0.0;
         }
-        if (i >= 0 && i < ni && j >= 0 && j <= nj) {  // y-face j - 1/2: L = (i, j - 1), R = (i, j)
-            const size_t cl = zi(i, j - 1, nj);
-            const double *sl = a.sl + cl * 9, *sr = a.sl + c * 9;
-            double lul[3];
-            lam_rk(k, a, i, j - 1, lul);
-            double pl[3], pr[3], lf[3];
-            for (int q = 0; q < 3; ++q) {
-                pl[q] = a.p[cl * 3 + q] + 0.5 * sl[3 + q];
-                pr[q] = a.p[c * 3 + q] - 0.5 * sr[3 + q];
-                lf[q] = (b * luc[q] - b * lul[q]) * dt / k.dy;
+        if (RECORD) {
+            if (i >= 0 && i < k.ni && j >= 0 && j < k.nj) {
+                const double *q = a.pout + c * 3;
+                if (!(q[0] > k.rho_min))
+                    w |= BW_FLOOR;
+                if (!(fabs(q[1]) < k.vmax))
+                    w |= BW_CEIL_X;
+                if (!(fabs(q[2]) < k.vmax))
+                    w |= BW_CEIL_Y;
             }
-            const double xc = k.xl + (i + 0.5) * k.dx, yf = k.yl + (j + 0.0) * k.dy;
-            double lpl[3] = {0, 0, 0}, lpr[3] = {0, 0, 0}, lcs2 = 0.0;
-            hlle_vjp<1>(pl, pr, cs2_generic(k, m, xc, yf), (w >> BW_YFACE) & 15u, lf, lpl, lpr, &lcs2);
-            cs2_param_vjp(k, st, xc, yf, lcs2, par);
-            double *o = a.fy + c * 10;
-            for (int q = 0; q < 3; ++q) {
-                o[q] = lpl[q];
-                o[3 + q] = lpr[q];
-            }
-            if (k.nu > 0.0) {
-                o[6] = o[8] = -hn * lf[1];
-                o[7] = o[9] = -hn * lf[2];
-                par[10] += -0.5 * (sl[7] + sr[7]) * lf[1] - 0.5 * (sl[8] + sr[8]) * lf[2];
-            }
+            a.words[c] = w;
         }
     }
-    store_params<BJ, CHAIN>(a, par);
+}
+
+// B: faces, one per thread: items [0, n) are the x-faces, [n, 2 n) the
+// y-faces, n = (ni + 2)(nj + 2). fx[c] is the x-face i + 1/2 of zone
+// c = (i, j), fy[c] the y-face j - 1/2. Per face: lambda of the minus-side
+// state (3), of the plus-side state (3), of the two rho*strain components of
+// the minus side (2) and of the plus side (2). The HLLE wave choice is
+// recomputed with the stage's own (correctly rounded) face sound speed.
+template <bool CHAIN>
+__global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_faces(Consts k, AdjArgs a)
+{
+    __shared__ StageShared sh;
+    load_stage<CHAIN>(a, sh);
+    const StageDev &st = sh.st;
+    const int ni = k.ni, nj = k.nj;
+    const long wi = ni + 2, wj = nj + 2, n = wi * wj;
+    ParAcc<CHAIN> par(sh.jac);
+    MassT<double> m[2];
+    masses_t<double>(st, nullptr, m);
+    const double hn = 0.5 * k.nu, b = st.one_minus_a;
+    const long f = grid_start(ADJ_THREADS);
+    const bool ydir = f >= n;
+    const long z = ydir ? f - n : f;
+    const int i = (int)(z / wj) - 1, j = (int)(z % wj) - 1;
+    // x-face i + 1/2: L = (i, j), R = (i + 1, j); y-face j - 1/2: L = (i, j - 1), R = (i, j)
+    const bool live = f < 2 * n &&
+                      (ydir ? (i >= 0 && i < ni && j >= 0 && j <= nj) : (i <= ni - 1 && j >= 0 && j < nj));
+    if (live) {
+        const int il = i, jl = ydir ? j - 1 : j, ir = ydir ? i : i + 1, jr = j;
+        const size_t cl = zi(il, jl, nj), cr = zi(ir, jr, nj);
+        const double *sl = a.sl + cl * 9 + (ydir ? 3 : 0), *sr = a.sl + cr * 9 + (ydir ? 3 : 0);
+        double lul[3], lur[3];
+        lam_rk(k, a, il, jl, lul);
+        lam_rk(k, a, ir, jr, lur);
+        const double cf = b * st.dt * (ydir ? k.inv_dy : k.inv_dx);
+        double pl[3], pr[3], lf[3];
+        for (int q = 0; q < 3; ++q) {
+            pl[q] = a.p[cl * 3 + q] + 0.5 * sl[q];
+            pr[q] = a.p[cr * 3 + q] - 0.5 * sr[q];
+            lf[q] = (lur[q] - lul[q]) * cf;
+        }
+        const double xf = ydir ? k.xl + (i + 0.5) * k.dx : k.xl + (i + 1.0) * k.dx;
+        const double yf = ydir ? k.yl + (j + 0.0) * k.dy : k.yl + (j + 0.5) * k.dy;
+        const double cs2 = cs2_generic(k, m, xf, yf), cs = sqrt(cs2);
+        double lpl[3] = {0, 0, 0}, lpr[3] = {0, 0, 0}, lcs2 = 0.0;
+        if (ydir)
+            hlle_vjp<1>(pl, pr, cs2, cs, hlle_select(pl[2], pr[2], cs), lf, lpl, lpr, &lcs2);
+        else
+            hlle_vjp<0>(pl, pr, cs2, cs, hlle_select(pl[1], pr[1], cs), lf, lpl, lpr, &lcs2);
+        cs2_param_vjp(k, st, xf, yf, lcs2, par);
+        double *o = (ydir ? a.fy : a.fx) + zi(i, j, nj) * 10;
+        for (int q = 0; q < 3; ++q) {
+            o[q] = lpl[q];
+            o[3 + q] = lpr[q];
+        }
+        if (k.nu > 0.0) {
+            // x: f1 -= hn (rs_xx L + R), f2 -= hn (rs_xy L + R); y: rs_xy, rs_yy
+            const double *rl = a.sl + cl * 9 + (ydir ? 7 : 6), *rr = a.sl + cr * 9 + (ydir ? 7 : 6);
+            o[6] = o[8] = -hn * lf[1];
+            o[7] = o[9] = -hn * lf[2];
+            par.add(10, -0.5 * (rl[0] + rr[0]) * lf[1] - 0.5 * (rl[1] + rr[1]) * lf[2]);
+        }
+    }
+    store_params<ADJ_THREADS, CHAIN>(a, par);
 }
 
 __constant__ double kZeroFace[10] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 
-// C: zones of [-1, ni] x [-1, nj]: gather the four faces, rho * strain, sources,
-// the u_n adjoint.
-template <int BJ, bool CHAIN>
-__global__ void __launch_bounds__(BJ) adj_zones(Consts k, AdjArgs a)
+// C: zones of [-1, ni] x [-1, nj]: gather the four faces, rho * strain,
+// gravity and buffer sources, the u_n adjoint (sinks: adj_sinks).
+template <bool CHAIN>
+__global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_zones(Consts k, AdjArgs a)
 {
-    __shared__ StageDev st;
-    if (threadIdx.x == 0)
-        st = *a.st;
-    __syncthreads();
+    __shared__ StageShared sh;
+    load_stage<CHAIN>(a, sh);
+    const StageDev &st = sh.st;
     const int ni = k.ni, nj = k.nj;
     const long wi = ni + 2, wj = nj + 2;
-    const long z = blockIdx.x * (long)BJ + threadIdx.x;
-    double par[NPAR];
-    for (int v = 0; v < NPAR; ++v)
-        par[v] = 0.0;
+    ParAcc<CHAIN> par(sh.jac);
+    const long z = grid_start(ADJ_THREADS);
     if (z < wi * wj) {
         const int i = (int)(z / wj) - 1, j = (int)(z % wj) - 1;
         const size_t c = zi(i, j, nj);
@@ -558,19 +593,20 @@ __global__ void __launch_bounds__(BJ) adj_zones(Consts k, AdjArgs a)
             lgx[q] = 0.5 * xe[q] - 0.5 * xw[3 + q];
             lgy[q] = 0.5 * yn[q] - 0.5 * ys[3 + q];
         }
-        const double *sl = a.sl + c * 9;
         if (k.nu > 0.0) {
+            const double *sl = a.sl + c * 9;
             const double lxx = xe[6] + xw[8];
             const double lxy = xe[7] + xw[9] + yn[6] + ys[8];
             const double lyy = yn[7] + ys[9];
             const double rho = a.p[c * 3];
-            double s[3];
-            rho_strain_generic(1.0, sl, sl + 3, k, s);
-            lp[0] += s[0] * lxx + s[1] * lxy + s[2] * lyy;
-            lgx[1] += rho * (4.0 / 3.0 * lxx - 2.0 / 3.0 * lyy) / k.dx;
-            lgy[2] += rho * (-2.0 / 3.0 * lxx + 4.0 / 3.0 * lyy) / k.dy;
-            lgx[2] += rho * lxy / k.dx;
-            lgy[1] += rho * lxy / k.dy;
+            const double sxx = 4.0 / 3.0 * sl[1] * k.inv_dx - 2.0 / 3.0 * sl[5] * k.inv_dy;
+            const double syy = -2.0 / 3.0 * sl[1] * k.inv_dx + 4.0 / 3.0 * sl[5] * k.inv_dy;
+            const double sxy = sl[2] * k.inv_dx + sl[4] * k.inv_dy;
+            lp[0] += sxx * lxx + sxy * lxy + syy * lyy;
+            lgx[1] += rho * (4.0 / 3.0 * lxx - 2.0 / 3.0 * lyy) * k.inv_dx;
+            lgy[2] += rho * (-2.0 / 3.0 * lxx + 4.0 / 3.0 * lyy) * k.inv_dy;
+            lgx[2] += rho * lxy * k.inv_dx;
+            lgy[1] += rho * lxy * k.inv_dy;
         }
         double lu[3];
         if (lam_rk(k, a, i, j, lu)) {
@@ -584,10 +620,8 @@ __global__ void __launch_bounds__(BJ) adj_zones(Consts k, AdjArgs a)
             double luu[3];
             for (int q = 0; q < 3; ++q)
                 luu[q] = ld[q] * (1.0 - rate * dt);
-            for (int q = 0; q < 2; ++q) {
-                gravity_vjp(st.m[q], xc, yc, dt, pc, ld, lp, par + 5 * q);
-                sink_vjp(st.m[q], xc, yc, dt, pc, ld, lp, par + 5 * q, par + 11);
-            }
+            for (int q = 0; q < 2; ++q)
+                gravity_vjp(st.m[q], q, xc, yc, dt, pc, ld, lp, par);
             lp[0] += luu[0] + luu[1] * pc[1] + luu[2] * pc[2];
             lp[1] += luu[1] * pc[0];
             lp[2] += luu[2] * pc[0];
@@ -605,7 +639,70 @@ __global__ void __launch_bounds__(BJ) adj_zones(Consts k, AdjArgs a)
             a.lp[c * 3 + q] = lp[q];
         }
     }
-    store_params<BJ, CHAIN>(a, par);
+    store_params<ADJ_THREADS, CHAIN>(a, par);
+}
+
+// Interior zones near a mass that its sink can reach: an index box around
+// the mass, one zone wider than the sink's reach on each side.
+__device__ __forceinline__ void sink_box(const Consts &k, const MassDev &m, int *i0, int *i1, int *j0, int *j1)
+{
+    const double reach = m.sink_r4 * 1.0000001;
+    *i0 = max(0, (int)floor((m.x - reach - k.xl) * k.inv_dx) - 1);
+    *i1 = min(k.ni - 1, (int)floor((m.x + reach - k.xl) * k.inv_dx) + 1);
+    *j0 = max(0, (int)floor((m.y - reach - k.yl) * k.inv_dy) - 1);
+    *j1 = min(k.nj - 1, (int)floor((m.y + reach - k.yl) * k.inv_dy) + 1);
+}
+
+// One directional derivative of a mass's sink term at a zone: direction
+// dir of (sigma, vx, vy, x_p, y_p, vx_p, vy_p, rate), weighted by ld.
+__device__ __forceinline__ double sink_direction(const MassDev &m, double x, double y, double dt, const double *pc,
+                                                 const double *ld, int dir)
+{
+    Dual du[3] = {dual(0.0), dual(0.0), dual(0.0)};
+    sink_generic<Dual>(m, dual(m.x, dir == 3), dual(m.y, dir == 4), dual(m.vx, dir == 5), dual(m.vy, dir == 6),
+                       dual(m.sink_rate, dir == 7), x, y, dt, dual(pc[0], dir == 0), dual(pc[1], dir == 1),
+                       dual(pc[2], dir == 2), du);
+    return ld[0] * du[0].d + ld[1] * du[1].d + ld[2] * du[2].d;
+}
+
+// Sinks of the stage (after pass C): lambda_p and the parameter sums of the
+// zones in each mass's sink box, one thread per (zone, direction).
+template <bool CHAIN>
+__global__ void __launch_bounds__(ADJ_THREADS) adj_sinks(Consts k, AdjArgs a)
+{
+    __shared__ StageShared sh;
+    load_stage<CHAIN>(a, sh);
+    const StageDev &st = sh.st;
+    ParAcc<CHAIN> par(sh.jac);
+    for (int q = 0; q < 2; ++q) {
+        const MassDev &m = st.m[q];
+        if (m.sink_rate == 0.0 || m.sink_model < 1 || m.sink_model > 3)
+            continue;
+        int i0, i1, j0, j1;
+        sink_box(k, m, &i0, &i1, &j0, &j1);
+        if (i1 < i0 || j1 < j0)
+            continue;
+        const long bw = j1 - j0 + 1, n = (long)(i1 - i0 + 1) * bw * 8;
+        for (long t = grid_start(ADJ_THREADS); t < n; t += grid_step(ADJ_THREADS)) {
+            const long z = t >> 3;
+            const int dir = (int)(t & 7);
+            const int i = i0 + (int)(z / bw), j = j0 + (int)(z % bw);
+            const double x = k.xl + (i + 0.5) * k.dx, y = k.yl + (j + 0.5) * k.dy;
+            const double dx = x - m.x, dy = y - m.y;
+            if (!(dx * dx + dy * dy < m.sink_hi2))
+                continue;
+            double lu[3];
+            lam_rk(k, a, i, j, lu);
+            const size_t c = zi(i, j, k.nj);
+            const double ld[3] = {st.one_minus_a * lu[0], st.one_minus_a * lu[1], st.one_minus_a * lu[2]};
+            const double v = sink_direction(m, x, y, st.dt, a.p + c * 3, ld, dir);
+            if (dir < 3)
+                a.lp[c * 3 + dir] += v;
+            else
+                par.add(dir < 7 ? 5 * q + dir - 3 : 11, v);
+        }
+    }
+    store_params<ADJ_THREADS, CHAIN>(a, par);
 }
 
 __device__ __forceinline__ void slope_weights(unsigned sel, double theta, double *w)
@@ -661,25 +758,25 @@ __device__ __forceinline__ void input_adjoint_at(const Consts &k, const AdjArgs 
 
 // D: interior zones: slope products and the guard images folded into the
 // zones they copy (zero-gradient boundary)
-__global__ void adj_inputs(Consts k, AdjArgs a)
+__global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_inputs(Consts k, AdjArgs a)
 {
     const int ni = k.ni, nj = k.nj;
-    const long z = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (z >= (long)ni * nj)
-        return;
-    const int i = (int)(z / nj), j = (int)(z - (long)i * nj);
-    const int ilo = i == 0 ? -2 : i, ihi = i == ni - 1 ? ni + 1 : i;
-    const int jlo = j == 0 ? -2 : j, jhi = j == nj - 1 ? nj + 1 : j;
-    double tot[3] = {0.0, 0.0, 0.0};
-    for (int ii = ilo; ii <= ihi; ++ii)
-        for (int jj = jlo; jj <= jhi; ++jj) {
-            double v[3];
-            input_adjoint_at(k, a, ii, jj, v);
-            for (int q = 0; q < 3; ++q)
-                tot[q] += v[q];
-        }
-    for (int q = 0; q < 3; ++q)
-        a.lam_rd[zi(i, j, nj) * 3 + q] += tot[q];
+    const long z = grid_start(ADJ_THREADS);
+    if (z < (long)ni * nj) {
+        const int i = (int)(z / nj), j = (int)(z - (long)i * nj);
+        const int ilo = i == 0 ? -2 : i, ihi = i == ni - 1 ? ni + 1 : i;
+        const int jlo = j == 0 ? -2 : j, jhi = j == nj - 1 ? nj + 1 : j;
+        double tot[3] = {0.0, 0.0, 0.0};
+        for (int ii = ilo; ii <= ihi; ++ii)
+            for (int jj = jlo; jj <= jhi; ++jj) {
+                double v[3];
+                input_adjoint_at(k, a, ii, jj, v);
+                for (int q = 0; q < 3; ++q)
+                    tot[q] += v[q];
+            }
+        for (int q = 0; q < 3; ++q)
+            a.lam_rd[zi(i, j, nj) * 3 + q] += tot[q];
+    }
 }
 
 // fixed-order sum of block partials into one parameter row
@@ -760,21 +857,21 @@ __global__ void objective_tangent_kernel(Consts k, const StageDev *stp, TangentP
     }
 }
 
-// lambda_p += dF/dp per zone; parameter derivatives to blocks
-template <int BJ, bool CHAIN>
-__global__ void __launch_bounds__(BJ) objective_adjoint_kernel(Consts k, AdjArgs args, double wm, double wt)
+// lambda_p += dF/dp per zone (torque part); parameter derivatives to blocks.
+// With per_time the weight is multiplied by the record's dt.
+template <bool CHAIN>
+__global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) objective_adjoint_kernel(Consts k, AdjArgs args, double wt,
+                                                                        bool per_time)
 {
-    __shared__ StageDev st;
-    if (threadIdx.x == 0)
-        st = *args.st;
-    __syncthreads();
+    __shared__ StageShared sh;
+    load_stage<CHAIN>(args, sh);
+    const StageDev &st = sh.st;
     const double *p = args.p;
     double *lam = args.lam_rd;
-    double par[NPAR];
-    for (int v = 0; v < NPAR; ++v)
-        par[v] = 0.0;
-    const long n = (long)k.ni * k.nj;
-    const long z = blockIdx.x * (long)BJ + threadIdx.x;
+    ParAcc<CHAIN> par(sh.jac);
+    const double w = per_time ? wt * st.dt : wt;
+    const long n = w != 0.0 ? (long)k.ni * k.nj : 0;
+    const long z = grid_start(ADJ_THREADS);
     if (z < n) {
         const int i = (int)(z / k.nj), j = (int)(z - (long)i * k.nj);
         const size_t c = zi(i, j, k.nj) * 3;
@@ -782,40 +879,61 @@ __global__ void __launch_bounds__(BJ) objective_adjoint_kernel(Consts k, AdjArgs
         const double sig = p[c];
         for (int q = 0; q < 2; ++q) {
             const MassDev &b = st.e[q];
-            // torque part: T = -sigma m g (x dy - y dx)
+            // T = -sigma m g (x dy - y dx)
             if (b.mass != 0.0) {
                 const double dx = x - b.x, dy = y - b.y;
-                const double S = dx * dx + dy * dy + b.soft2;
-                const double g = inv_pow15<false>(S), h = g / S;
+                const double r = rsqrt(dx * dx + dy * dy + b.soft2);
+                const double g = r * r * r, h = g * r * r;
                 const double cr = x * dy - y * dx;
-                lam[c] += wt * (-b.mass * g * cr);
-                par[5 * q + 4] += wt * (-sig * g * cr);
-                par[5 * q + 0] += wt * (-sig * b.mass) * (3.0 * dx * h * cr + g * y);
-                par[5 * q + 1] += wt * (-sig * b.mass) * (3.0 * dy * h * cr - g * x);
-            }
-            // accretion part: -mdot, through the dual sink (rare zones)
-            const double dx = x - b.x, dy = y - b.y;
-            if (b.sink_rate != 0.0 && dx * dx + dy * dy < b.sink_hi2) {
-                for (int dir = 0; dir < 8; ++dir) {
-                    double s[8];
-                    for (int t = 0; t < 8; ++t)
-                        s[t] = t == dir ? 1.0 : 0.0;
-                    Dual du[3] = {dual(0.0), dual(0.0), dual(0.0)};
-                    sink_generic<Dual>(b, dual(b.x, s[3]), dual(b.y, s[4]), dual(b.vx, s[5]), dual(b.vy, s[6]),
-                                       dual(b.sink_rate, s[7]), x, y, 1.0, dual(p[c], s[0]), dual(p[c + 1], s[1]),
-                                       dual(p[c + 2], s[2]), du);
-                    const double v = -wm * du[0].d;
-                    if (dir < 3)
-                        lam[c + dir] += v;
-                    else if (dir < 7)
-                        par[5 * q + dir - 3] += v;
-                    else
-                        par[11] += v;
-                }
+                lam[c] += w * (-b.mass * g * cr);
+                par.add(5 * q + 4, w * (-sig * g * cr));
+                par.add(5 * q + 0, w * (-sig * b.mass) * (3.0 * dx * h * cr + g * y));
+                par.add(5 * q + 1, w * (-sig * b.mass) * (3.0 * dy * h * cr - g * x));
             }
         }
     }
-    store_params<BJ, CHAIN>(args, par);
+    store_params<ADJ_THREADS, CHAIN>(args, par);
+}
+
+// accretion part of the objective (-mdot), through the dual sink, over the
+// sink boxes of the end-of-step masses, one thread per (zone, direction)
+template <bool CHAIN>
+__global__ void __launch_bounds__(ADJ_THREADS) objective_sinks(Consts k, AdjArgs args, double wm, bool per_time)
+{
+    __shared__ StageShared sh;
+    load_stage<CHAIN>(args, sh);
+    const StageDev &st = sh.st;
+    const double *p = args.p;
+    double *lam = args.lam_rd;
+    ParAcc<CHAIN> par(sh.jac);
+    const double w = per_time ? wm * st.dt : wm;
+    const double ld[3] = {-w, 0.0, 0.0};
+    for (int q = 0; q < 2 && w != 0.0; ++q) {
+        const MassDev &b = st.e[q];
+        if (b.sink_rate == 0.0 || b.sink_model < 1 || b.sink_model > 3)
+            continue;
+        int i0, i1, j0, j1;
+        sink_box(k, b, &i0, &i1, &j0, &j1);
+        if (i1 < i0 || j1 < j0)
+            continue;
+        const long bw = j1 - j0 + 1, n = (long)(i1 - i0 + 1) * bw * 8;
+        for (long t = grid_start(ADJ_THREADS); t < n; t += grid_step(ADJ_THREADS)) {
+            const long z = t >> 3;
+            const int dir = (int)(t & 7);
+            const int i = i0 + (int)(z / bw), j = j0 + (int)(z % bw);
+            const size_t c = zi(i, j, k.nj) * 3;
+            const double x = k.xl + (i + 0.5) * k.dx, y = k.yl + (j + 0.5) * k.dy;
+            const double dx = x - b.x, dy = y - b.y;
+            if (!(dx * dx + dy * dy < b.sink_hi2))
+                continue;
+            const double v = sink_direction(b, x, y, 1.0, p + c, ld, dir);
+            if (dir < 3)
+                lam[c + dir] += v;
+            else
+                par.add(dir < 7 ? 5 * q + dir - 3 : 11, v);
+        }
+    }
+    store_params<ADJ_THREADS, CHAIN>(args, par);
 }
 
 inline int nblocks(long n, int bs) { return (int)((n + bs - 1) / bs); }
@@ -832,7 +950,9 @@ using namespace cbd;
 
 namespace {
 
-constexpr size_t WS_PER_ZONE = 9 + 10 + 10 + 6 + 3;
+// per zone: slopes and rho * strain (9), x-face (10), y-face (10), slope
+// adjoints (6), direct adjoints (3), the branch word (one slot)
+constexpr size_t WS_PER_ZONE = 9 + 10 + 10 + 6 + 3 + 1;
 
 bool grid_ok(const cbd_grid_t *g)
 {
@@ -851,48 +971,72 @@ AdjArgs adj_args(const cbd_grid_t *grid, const void *stage_dev, void *workspace,
     a.fy = a.fx + zones * 10;
     a.lg = a.fy + zones * 10;
     a.lp = a.lg + zones * 6;
+    a.words = reinterpret_cast<unsigned *>(a.lp + zones * 3);
+    a.par = ws + zones * WS_PER_ZONE;  // per-block partials of the per-stage form
     a.jac = jac;
     return a;
 }
 
-// With `jac` null: 12 parameter derivatives of this stage ADDED into
-// params_out. Otherwise the chained (q, e, nu, rate) sums are accumulated
-// per block into params_out (blocks x 4), reduced by adjoint_chain_finish.
+// Blocks of the adjoint passes: one item (zone or face) per thread; the face
+// pass is the widest. Rows of the chained accumulator and of the per-block
+// partials.
+int adj_rows(const cbd_grid_t *grid)
+{
+    const long faces = 2L * (grid->ni + 2) * (grid->nj + 2);
+    return (int)((faces + ADJ_THREADS - 1) / ADJ_THREADS);
+}
+
+int pass_blocks(long items) { return items > 0 ? (int)((items + ADJ_THREADS - 1) / ADJ_THREADS) : 1; }
+
+constexpr int SINK_PASS_BLOCKS = 16;
+
+// With `jac` null: `words` is the recorded branch record and the 12
+// parameter derivatives of this stage are ADDED into params_out. Otherwise
+// the branch words are recorded here (into the workspace) and the chained
+// (q, e, nu, rate) sums are accumulated per block into params_out
+// (adj_rows() x 4), reduced by cbdiso_b200_adjoint_chain_finish.
 int stage_adjoint_impl(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
                        const double *primitive_n, const double *primitive_out, const unsigned int *words,
                        const double *lam_out, double *lam_rd, double *lam_n, const double *jac, double *params_out,
                        void *workspace, void *stream)
 {
-    if (!grid_ok(grid) || !stage_dev || !primitive_rd || !primitive_out || !words || !lam_out || !lam_rd ||
-        !params_out || !workspace || (primitive_n && !lam_n))
+    if (!grid_ok(grid) || !stage_dev || !primitive_rd || !primitive_out || (!jac && !words) || !lam_out ||
+        !lam_rd || !params_out || !workspace || (primitive_n && !lam_n))
         return CBD_ERR_ARGUMENT;
     const Consts k = consts_from_grid(grid);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int ni = grid->ni, nj = grid->nj;
-    const size_t zones = (size_t)(ni + 4) * (nj + 4);
     AdjArgs a = adj_args(grid, stage_dev, workspace, jac);
     a.p = primitive_rd;
     a.pn = primitive_n;
     a.pout = primitive_out;
-    a.words = words;
+    if (!jac)
+        a.words = const_cast<unsigned *>(words);  // read only: RECORD is off
     a.lam_out = lam_out;
     a.lam_rd = lam_rd;
     a.lam_n = lam_n;
-    double *parts = static_cast<double *>(workspace) + zones * WS_PER_ZONE;
-    a.par = jac ? params_out : parts;
-    const long nwide = (long)(ni + 2) * (nj + 2);
-    const int nb = nblocks(nwide, 128);
-    adj_slopes<<<nb, 128, 0, s>>>(k, a);
+    double *parts = a.par;
+    if (jac)
+        a.par = params_out;
+    const long wide = (long)(ni + 2) * (nj + 2);
+    const int bw = pass_blocks(wide), bf = pass_blocks(2 * wide), bi = pass_blocks((long)ni * nj);
+    const int bs = SINK_PASS_BLOCKS;
+    constexpr int T = ADJ_THREADS;
     if (jac) {
-        adj_faces<128, true><<<nb, 128, 0, s>>>(k, a);
-        adj_zones<128, true><<<nb, 128, 0, s>>>(k, a);
+        adj_slopes<true><<<bw, T, 0, s>>>(k, a);
+        adj_faces<true><<<bf, T, 0, s>>>(k, a);
+        adj_zones<true><<<bw, T, 0, s>>>(k, a);
+        adj_sinks<true><<<bs, T, 0, s>>>(k, a);
     } else {
-        adj_faces<128, false><<<nb, 128, 0, s>>>(k, a);
-        sum_params<<<1, 32, 0, s>>>(parts, nb, NPAR, params_out);
-        adj_zones<128, false><<<nb, 128, 0, s>>>(k, a);
-        sum_params<<<1, 32, 0, s>>>(parts, nb, NPAR, params_out);
+        adj_slopes<false><<<bw, T, 0, s>>>(k, a);
+        adj_faces<false><<<bf, T, 0, s>>>(k, a);
+        sum_params<<<1, 32, 0, s>>>(parts, bf, NPAR, params_out);
+        adj_zones<false><<<bw, T, 0, s>>>(k, a);
+        sum_params<<<1, 32, 0, s>>>(parts, bw, NPAR, params_out);
+        adj_sinks<false><<<bs, T, 0, s>>>(k, a);
+        sum_params<<<1, 32, 0, s>>>(parts, bs, NPAR, params_out);
     }
-    adj_inputs<<<nblocks((long)ni * nj, 128), 128, 0, s>>>(k, a);
+    adj_inputs<<<bi, T, 0, s>>>(k, a);
     return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
 }
 
@@ -904,18 +1048,21 @@ int objective_adjoint_impl(const cbd_grid_t *grid, const void *stage_dev, const 
         return CBD_ERR_ARGUMENT;
     const Consts k = consts_from_grid(grid);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const size_t zones = (size_t)(grid->ni + 4) * (grid->nj + 4);
     AdjArgs a = adj_args(grid, stage_dev, workspace, jac);
     a.p = primitive;
     a.lam_rd = lam;
-    double *parts = static_cast<double *>(workspace) + zones * WS_PER_ZONE;
-    a.par = jac ? params_out : parts;
-    const int nb = nblocks((long)grid->ni * grid->nj, 128);
+    double *parts = a.par;
+    const int bz = pass_blocks((long)grid->ni * grid->nj), bs = SINK_PASS_BLOCKS;
+    constexpr int T = ADJ_THREADS;
     if (jac) {
-        objective_adjoint_kernel<128, true><<<nb, 128, 0, s>>>(k, a, w_mdot, w_torque);
+        a.par = params_out;
+        objective_adjoint_kernel<true><<<bz, T, 0, s>>>(k, a, w_torque, true);
+        objective_sinks<true><<<bs, T, 0, s>>>(k, a, w_mdot, true);
     } else {
-        objective_adjoint_kernel<128, false><<<nb, 128, 0, s>>>(k, a, w_mdot, w_torque);
-        sum_params<<<1, 32, 0, s>>>(parts, nb, NPAR, params_out);
+        objective_adjoint_kernel<false><<<bz, T, 0, s>>>(k, a, w_torque, false);
+        sum_params<<<1, 32, 0, s>>>(parts, bz, NPAR, params_out);
+        objective_sinks<false><<<bs, T, 0, s>>>(k, a, w_mdot, false);
+        sum_params<<<1, 32, 0, s>>>(parts, bs, NPAR, params_out);
     }
     return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
 }
@@ -929,9 +1076,8 @@ size_t cbdiso_b200_adjoint_workspace_bytes(const cbd_grid_t *grid)
     if (!grid_ok(grid))
         return 0;
     const size_t zones = (size_t)(grid->ni + 4) * (grid->nj + 4);
-    const size_t blocks = (size_t)nblocks((long)(grid->ni + 2) * (grid->nj + 2), 128) + 1;
-    // sl (9) + fx (10) + fy (10) + lg (6) + lp (3) doubles per zone, then block partials
-    return zones * WS_PER_ZONE * sizeof(double) + blocks * NPAR * sizeof(double) + 256;
+    // WS_PER_ZONE doubles per zone, then the block partials
+    return zones * WS_PER_ZONE * sizeof(double) + (size_t)adj_rows(grid) * NPAR * sizeof(double) + 256;
 }
 
 int cbdiso_b200_stage_record_branches(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
@@ -986,14 +1132,13 @@ int cbdiso_b200_stage_adjoint(const cbd_grid_t *grid, const void *stage_dev, con
 }
 
 int cbdiso_b200_stage_adjoint_chained(const cbd_grid_t *grid, const void *stage_dev, const double *primitive_rd,
-                                      const double *primitive_n, const double *primitive_out,
-                                      const unsigned int *words, const double *lam_out, double *lam_rd,
-                                      double *lam_n, const double *jacobian, double *chain_acc, void *workspace,
-                                      void *stream)
+                                      const double *primitive_n, const double *primitive_out, const double *lam_out,
+                                      double *lam_rd, double *lam_n, const double *jacobian, double *chain_acc,
+                                      void *workspace, void *stream)
 {
     if (!jacobian || !chain_acc)
         return CBD_ERR_ARGUMENT;
-    return stage_adjoint_impl(grid, stage_dev, primitive_rd, primitive_n, primitive_out, words, lam_out, lam_rd,
+    return stage_adjoint_impl(grid, stage_dev, primitive_rd, primitive_n, primitive_out, nullptr, lam_out, lam_rd,
                               lam_n, jacobian, chain_acc, workspace, stream);
 }
 
@@ -1001,7 +1146,7 @@ size_t cbdiso_b200_adjoint_chain_blocks(const cbd_grid_t *grid)
 {
     if (!grid_ok(grid))
         return 0;
-    return (size_t)nblocks((long)(grid->ni + 2) * (grid->nj + 2), 128);
+    return (size_t)adj_rows(grid);
 }
 
 int cbdiso_b200_adjoint_chain_finish(const double *chain_acc, int num_blocks, double *out4, void *stream)

@@ -163,6 +163,19 @@ __device__ __forceinline__ T cs2_generic(const Consts &k, const MassT<T> *m, con
     return T{} * 0.0 + 1.0;
 }
 
+// The HLLE wave choice (cbdiso_2d.c:370-373) from the face velocities and the
+// sound speed: am in bits 0-1, ap in bits 2-3 (0 = zero, 1 = the left
+// state's wave, 2 = the right state's).
+__device__ __forceinline__ unsigned hlle_select(double vl, double vr, double cs)
+{
+    const double lm = vl - cs, rm = vr - cs, lp = vl + cs, rp = vr + cs;
+    const unsigned s_in_m = lm < rm ? 1u : 2u;
+    const double in_m = lm < rm ? lm : rm;
+    const unsigned s_in_p = lp > rp ? 1u : 2u;
+    const double in_p = lp > rp ? lp : rp;
+    return (0.0 < in_m ? 0u : s_in_m) | ((0.0 > in_p ? 0u : s_in_p) << 2);
+}
+
 // HLLE flux (cbdiso_2d.c:352-380); sel receives am (bits 0-1) and ap (2-3).
 template <class T, int DIR>
 __device__ __forceinline__ void hlle_generic(const T *pl, const T *pr, const T &cs2, T *f, unsigned *sel)
