@@ -276,3 +276,50 @@ def test_torch_autograd_function():
     J.backward()
     assert sigma0.grad.shape == sigma0.shape and params.grad.shape == (4,)
     assert torch.isfinite(sigma0.grad).all() and torch.isfinite(params.grad).all()
+
+
+@pytest.fixture(scope="module")
+def full_run():
+    """The full-size adjoint case: 512^2, config-0 physics with q = 0.5,
+    e = 0.1, 400 RK2 steps at CFL 0.3, dt frozen, checkpoints every 20."""
+    run = AdjointRun(resolution=512, steps=400, checkpoint_every=20)
+    params = Params(0.5, 0.1, 1e-3, 10.0)
+    prim = run.initial_state(seed=0)
+    run.forward(prim, params, freeze=True, keep=True)
+    return run, params, prim
+
+
+def test_full_size_gradient_matches_central_differences(full_run):
+    """Eight seeded directions, each a smooth surface-density bump plus a
+    parameter direction, central differences with h = 1e-6."""
+    run, params, prim = full_run
+    run.forward(prim, params, keep=True)
+    gs, gp = run.gradient((1.0, 0.0))
+    rng = np.random.default_rng(8)
+    scale = np.array([0.1, 0.05, 1e-3, 1.0])
+    for k in range(8):
+        dprim = np.zeros_like(prim)
+        dprim[..., 0] = _bump(run, rng)
+        dpar = rng.uniform(-1.0, 1.0, 4) * scale
+        adj = float((gs * dprim).sum()) + float(gp @ dpar)
+        h = 1e-6
+        jp = run.forward(prim + h * dprim, Params(*(np.array(params) + h * dpar)))[0]
+        jm = run.forward(prim - h * dprim, Params(*(np.array(params) - h * dpar)))[0]
+        fd = (jp - jm) / (2 * h)
+        assert abs(fd - adj) <= 1e-4 * abs(adj) + 1e-10 * abs(jp), (k, fd, adj)
+
+
+def test_full_size_gradient_matches_tangent(full_run):
+    """The dot-product test <lambda, du> = <grad J, d> against the
+    forward-mode tangent at full size, for both objectives."""
+    run, params, prim = full_run
+    rng = np.random.default_rng(9)
+    for weights in ((1.0, 0.0), (0.0, 1.0)):
+        run.forward(prim, params, keep=True)
+        gs, gp = run.gradient(weights)
+        dprim = np.zeros_like(prim)
+        dprim[..., 0] = rng.uniform(-1, 1, prim.shape[:2]) * 1e-2
+        dpar = rng.uniform(-1, 1, 4) * np.array([0.1, 0.05, 1e-4, 1.0])
+        tan = run.tangent(prim, params, dprim, dpar, weights)
+        adj = float((gs * dprim).sum()) + float(gp @ dpar)
+        assert abs(tan - adj) <= 1e-9 * abs(tan), (weights, tan, adj)
