@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--tile", default=None, help="columns,rows,occupancy of the stage kernel (default: library)")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the batched-disk and adjoint measurements added to the line at N=1")
     return p.parse_args()
 
 
@@ -255,6 +257,108 @@ def run_ours(args, rank, world):
     return line
 
 
+def batched_extra(plain_value):
+    """Many-disk throughput: 64 seeded disks of 128^2 to 1024^2 (about 19.8 M
+    zones), each with its own dt, q, e, Mach and nu, advanced together by the
+    persistent tile-queue kernel; 48 timed steps after 16."""
+    import torch
+
+    from sailfish_b200.batched import BatchedSolver, config2_disks
+
+    b = BatchedSolver(config2_disks(64, seed=2024), diagnostics=DIAGNOSTICS)
+    b.run(16)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    b.run(48)
+    stop.record()
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop) / 48
+    value = b.total_zones / (ms * 1e-3)
+    return {"workload": "64 disks 128^2..1024^2, own dt / q / e / Mach / nu, RK2 FP64", "zones": b.total_zones,
+            "value": value, "unit": "zone-updates/s", "ms_per_step": ms,
+            "vs_single_disk_value": value / plain_value}
+
+
+def adjoint_extra():
+    """Forward + gradient of the time-averaged accretion rate at 512^2 over
+    400 RK2 steps (dt frozen), per step, against a plain device step."""
+    import torch
+
+    from sailfish_b200.adjoint import AdjointRun, Params
+
+    run = AdjointRun(resolution=512, steps=400, checkpoint_every=20)
+    params = Params(0.5, 0.1, 1e-3, 10.0)
+    prim = run.initial_state(seed=0)
+    run.forward(prim, params, freeze=True, keep=True)
+    run.gradient((1.0, 0.0))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    run.forward(prim, params, keep=True)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    run.gradient((1.0, 0.0))
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    solver = run._solver(params, prim)
+    solver.run(16, cfl=run.cfl)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    solver.run(run.steps, cfl=run.cfl)
+    stop.record()
+    torch.cuda.synchronize()
+    plain = start.elapsed_time(stop) / run.steps
+    fwd, adj = (t1 - t0) * 1e3 / run.steps, (t2 - t1) * 1e3 / run.steps
+    return {"workload": "512^2, q 0.5, e 0.1, 400 RK2 steps, d(mean accretion)/d(Sigma_0, q, e, nu, sink rate)",
+            "forward_ms_per_step": fwd, "gradient_ms_per_step": adj, "plain_ms_per_step": plain,
+            "forward_plus_gradient_vs_plain": (fwd + adj) / plain,
+            "stored_states": run._fwd["trajectory"] is not None, "timing": "host wall clock around each call"}
+
+
+def batched_adjoint_extra():
+    """32 disks (half 256^2, half 512^2; own q, e, nu), 200 steps: forward
+    with stored states plus gradient over 8 streams, against the batched
+    forward of the same disks."""
+    import torch
+
+    from sailfish_b200.adjoint import BatchedAdjoint, config4_disks
+    from sailfish_b200.batched import BatchedSolver, Disk
+
+    disks = config4_disks(32)
+    batch = BatchedAdjoint(disks, steps=200, streams=8)
+    batch.forward(freeze=True, keep=True)
+    batch.gradient((1.0, 0.0))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch.forward(keep=True)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    batch.gradient((1.0, 0.0))
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    members = []
+    for d, r, p in zip(disks, batch.runs, batch.prims):
+        setup = r.setup(d.params)
+        members.append(Disk(setup, setup.mesh(d.resolution), p))
+    b = BatchedSolver(members, diagnostics=[dict(quantity="mdot", which_mass=1, accretion=True),
+                                            dict(quantity="mdot", which_mass=2, accretion=True),
+                                            dict(quantity="torque", which_mass="both", gravity=True)])
+    b.run(16)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    b.run(200)
+    stop.record()
+    torch.cuda.synchronize()
+    fwd = start.elapsed_time(stop) * 1e-3
+    return {"workload": "32 disks (16 x 256^2, 16 x 512^2), own q / e / nu, 200 RK2 steps, gradients of the "
+                        "mean accretion rate", "forward_stored_s": t1 - t0, "gradient_s": t2 - t1,
+            "batched_forward_s": fwd, "gradient_vs_batched_forward": (t2 - t1) / fwd,
+            "forward_plus_gradient_vs_batched_forward": (t2 - t0) / fwd,
+            "timing": "host wall clock (forward + gradient), CUDA events (batched forward)"}
+
+
 # ---------------------------------------------------------------------------
 # the reference's CPU kernels (oracle/_ref) and the oracle port
 # ---------------------------------------------------------------------------
@@ -337,6 +441,10 @@ def main():
         line = run_reference(args, rank, world)
     else:
         line = run_ours(args, rank, world)
+        if world == 1 and not args.no_extras:
+            line["batched"] = batched_extra(line["value"])
+            line["adjoint"] = adjoint_extra()
+            line["adjoint_batched"] = batched_adjoint_extra()
         if rank == 0 and not args.no_cpu_baseline:
             n = args.size
             v, kind, el = time_cpu(n, 2 if n >= 2048 else 5, 1, args.seed)

@@ -186,10 +186,12 @@ class AdjointRun:
                                      device=s.device)
             rows = s.run(steps, cfl=self.cfl, dt_sequence=dts_dev, history=history, trajectory=trajectory)
         else:
+            store = self._checkpoint_store(s) if keep else None
             for start in range(0, steps, K):
                 stop = min(start + K, steps)
                 if keep:
-                    cps[start] = s._buf[0].clone()
+                    cps[start] = store[start // K]
+                    cps[start].copy_(s._buf[0])
                 rows += s.run(stop - start, cfl=self.cfl, steps_per_graph=K,
                               dt_sequence=None if fresh else dts_dev[start:stop],
                               history=history[start * 2 * nb:stop * 2 * nb] if keep else None)
@@ -204,6 +206,16 @@ class AdjointRun:
             self._fwd = dict(solver=s, t_start=t_start, checkpoints=cps, params=params, history=history,
                              record_bytes=nb, trajectory=trajectory)
         return J
+
+    def _checkpoint_store(self, s):
+        """Checkpoint slots (one per segment), kept on the run and reused."""
+        import torch
+
+        shape = (-(-self.steps // self.checkpoint_every),) + tuple(s._buf[0].shape)
+        store = getattr(self, "_checkpoints", None)
+        if store is None or tuple(store.shape) != shape or store.device != s._buf[0].device:
+            store = self._checkpoints = torch.empty(shape, dtype=torch.float64, device=s._buf[0].device)
+        return store
 
     def _keep_all(self, s):
         if self.store_states is not None:
@@ -466,6 +478,104 @@ class _ReverseSweep:
 def make_solver_exact(setup, mesh, physics, prim0, plm_theta):
     return Solver(setup=setup, mesh=mesh, solution=prim0, physics=physics,
                   options=dict(rk_order=2, plm_theta=plm_theta, precision="exact"))
+
+
+# ---------------------------------------------------------------------------
+# many disks
+# ---------------------------------------------------------------------------
+
+
+class AdjointDisk(NamedTuple):
+    """One disk of a batched adjoint: grid size, parameters, Mach number and
+    the initial primitive state (ni, nj, 3) (None: the setup's disk with
+    seeded noise)."""
+
+    resolution: int
+    params: Params
+    mach: float = 10.0
+    prim0: Optional[np.ndarray] = None
+
+
+class BatchedAdjoint:
+    """
+    Forward runs and gradients of many independent disks on one GPU. Each
+    disk is an AdjointRun (its own dt sequence, stage records and adjoint
+    buffers); the disks are spread over `streams` CUDA streams, each driven
+    by its own host thread, so that the kernels of different disks overlap
+    on the device and their host-side launch work overlaps on the CPU. Each
+    disk's results are identical to running its AdjointRun alone.
+    """
+
+    def __init__(self, disks, steps=200, checkpoint_every=20, cfl=0.3, plm_theta=1.5, streams=8,
+                 store_states=None):
+        self.disks = list(disks)
+        self.runs = [AdjointRun(resolution=d.resolution, steps=steps, checkpoint_every=checkpoint_every, cfl=cfl,
+                                plm_theta=plm_theta, mach=d.mach, store_states=store_states) for d in self.disks]
+        self.prims = [d.prim0 if d.prim0 is not None else r.initial_state(seed=i)
+                      for i, (d, r) in enumerate(zip(self.disks, self.runs))]
+        self.num_streams = max(1, min(int(streams), len(self.disks)))
+        self._streams = None
+
+    def _each(self, fn):
+        """fn(i) for every disk, disk i on stream i % num_streams; returns the
+        results in disk order."""
+        import threading
+
+        import torch
+
+        if self._streams is None:
+            self._streams = [torch.cuda.Stream() for _ in range(self.num_streams)]
+        device = torch.cuda.current_device()
+        out = [None] * len(self.disks)
+        errors = []
+        start = torch.cuda.current_stream()
+
+        def worker(w):
+            try:
+                torch.cuda.set_device(device)
+                st = self._streams[w]
+                st.wait_stream(start)
+                with torch.cuda.stream(st):
+                    for i in range(w, len(self.disks), self.num_streams):
+                        out[i] = fn(i)
+            except BaseException as exc:  # re-raised on the calling thread
+                errors.append(exc)
+
+        threads = [threading.Thread(target=worker, args=(w,)) for w in range(self.num_streams)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        for st in self._streams:
+            start.wait_stream(st)
+        if errors:
+            raise errors[0]
+        return out
+
+    def forward(self, freeze=False, keep=False):
+        """J of every disk (list of (mean accretion, mean torque))."""
+        return self._each(lambda i: self.runs[i].forward(self.prims[i], self.disks[i].params, freeze=freeze,
+                                                         keep=keep))
+
+    def gradient(self, weights=(1.0, 0.0)):
+        """(dJ/dprim0, dJ/d(q, e, nu, sink_rate)) of every disk, after
+        forward(keep=True)."""
+        return self._each(lambda i: self.runs[i].gradient(weights))
+
+
+def config4_disks(num=32, seed=4096, sizes=(256, 512)):
+    """The batched adjoint workload: `num` disks, half of each size in
+    `sizes` (seeded order), q ~ U[0.1, 1], e ~ U[0, 0.5], nu ~ logU[1e-4,
+    1e-2], sink rate 10, Mach 10, on [-8, 8]^2 with the config-0 physics."""
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(np.repeat(np.array(sizes), -(-num // len(sizes)))[:num])
+    out = []
+    for n in order:
+        q = float(rng.uniform(0.1, 1.0))
+        e = float(rng.uniform(0.0, 0.5))
+        nu = float(10.0 ** rng.uniform(-4.0, -2.0))
+        out.append(AdjointDisk(int(n), Params(q, e, nu, 10.0)))
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -113,8 +113,10 @@ LaunchShape stage_shape(int ni, int nj, int bj, int rows, int occupancy = 0)
     const int strips = (nj + bj - 1) / bj;
     if (rows <= 0) {
         const int slots = 148 * (s.minb > 1 ? s.minb : 4);
+        // small grids: shorter segments for more CTAs (a CTA's run time is
+        // about its rows + 4 dependent row steps)
         rows = 32;
-        while (rows > 8 && (long)strips * ((ni + rows - 1) / rows) < 2L * slots)
+        while (rows > 4 && (long)strips * ((ni + rows - 1) / rows) < 2L * slots)
             rows /= 2;
     }
     if (rows < 4)

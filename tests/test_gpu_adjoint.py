@@ -323,3 +323,22 @@ def test_full_size_gradient_matches_tangent(full_run):
         tan = run.tangent(prim, params, dprim, dpar, weights)
         adj = float((gs * dprim).sum()) + float(gp @ dpar)
         assert abs(tan - adj) <= 1e-9 * abs(tan), (weights, tan, adj)
+
+
+def test_batched_adjoint_matches_each_disk_alone():
+    """Disks run concurrently on several streams and host threads give the
+    J and gradients of each disk run alone, bit for bit."""
+    from sailfish_b200.adjoint import AdjointDisk, BatchedAdjoint
+
+    disks = [AdjointDisk(32, Params(0.3, 0.2, 1e-3, 10.0)), AdjointDisk(48, Params(0.9, 0.0, 3e-4, 10.0), 20.0),
+             AdjointDisk(40, Params(0.5, 0.4, 5e-3, 10.0)), AdjointDisk(32, Params(0.7, 0.1, 1e-4, 10.0), 15.0)]
+    batch = BatchedAdjoint(disks, steps=12, checkpoint_every=5, streams=3)
+    J = batch.forward(freeze=True, keep=True)
+    grads = batch.gradient((1.0, 0.5))
+    for i, d in enumerate(disks):
+        run = AdjointRun(resolution=d.resolution, steps=12, checkpoint_every=5, mach=d.mach)
+        j = run.forward(batch.prims[i], d.params, freeze=True, keep=True)
+        gs, gp = run.gradient((1.0, 0.5))
+        np.testing.assert_array_equal(j, J[i])
+        np.testing.assert_array_equal(gs, grads[i][0])
+        np.testing.assert_array_equal(gp, grads[i][1])
