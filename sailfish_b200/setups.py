@@ -59,6 +59,21 @@ class SetupBase:
     def validate(self):
         pass
 
+    def model_parameters(self):
+        """(key, value, about) of every model parameter (setup_base.py:146-155)."""
+        for key, _, about in type(self).default_model_parameters():
+            yield key, getattr(self, key), about
+
+    def model_parameter_dict(self):
+        """The model parameters as a dict (setup_base.py:157-161)."""
+        return {key: val for key, val, _ in self.model_parameters()}
+
+    @classmethod
+    def dash_case_class_name(cls):
+        """The class name in dash case, as setups are named in configuration and
+        checkpoint files (setup_base.py:94-103)."""
+        return "".join("-" + c.lower() if c.isupper() else c for c in cls.__name__).lstrip("-")
+
     @property
     def boundary_condition(self):
         return "outflow"
@@ -103,8 +118,14 @@ class CircumbinaryDisk(SetupBase):
     buffer_is_enabled = param(True, "whether the buffer zone is enabled", mutable=True)
     sink_model = param("torque_free", "sink [acceleration_free|force_free|torque_free]", mutable=True)
     initial_sigma = param(1.0, "initial disk surface density")
+    # gamma-law parameters, kept so that parameter sets (and checkpoints) of
+    # the reference setup load unchanged; the isothermal solver ignores them
+    initial_pressure = param(1e-2, "initial disk surface pressure at r=a (gamma-law)")
+    cooling_coefficient = param(0.0, "strength of the cooling term (gamma-law)")
+    alpha = param(0.1, "alpha-viscosity parameter (gamma-law)")
     nu = param(0.001, "kinematic viscosity parameter (isothermal)")
     constant_softening = param(True, "whether to use constant softening")
+    gamma_law_index = param(5.0 / 3.0, "adiabatic index (gamma-law)")
     which_diagnostics = param("none", "diagnostics set to get from solver [none|mdots]")
 
     def validate(self):
