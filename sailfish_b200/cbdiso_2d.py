@@ -116,7 +116,14 @@ class Solver(SolverBase):
     """Adapter driving the fused sm_100a kernels of libcbdiso_b200.so."""
 
     def __init__(self, setup=None, mesh=None, time=0.0, solution=None, num_patches=1, mode="gpu",
-                 physics=dict(), options=dict()):
+                 physics=dict(), options=dict(), index_range=None):
+        """
+        `index_range` (a, b) makes this solver one patch of the mesh: rows
+        a <= i < b, with the patch's own edge coordinates as the reference's
+        Patch has them (cbdiso_2d.py:69-80); `solution` is then the whole
+        mesh's or the patch's. The multi-GPU solver (distributed.py) runs one
+        patch per rank and exchanges the guard rows between stages.
+        """
         import torch
 
         physics = dict(physics)
@@ -153,7 +160,16 @@ class Solver(SolverBase):
         self.num_cons = NQ
         self.num_patches = num_patches
         self.device = torch.device("cuda", torch.cuda.current_device())
-        ni, nj = mesh.shape
+        ni_mesh, nj = mesh.shape
+        a, b = index_range if index_range is not None else (0, ni_mesh)
+        if not 0 <= a < b <= ni_mesh:
+            raise ValueError(f"index_range {index_range} is outside the mesh's {ni_mesh} rows")
+        self.index_range = (a, b)
+        ni = b - a
+        # called after each RK stage with (stage, output buffer) and after each
+        # step, on the launching stream (the multi-GPU solver's exchanges)
+        self._stage_hook = None
+        self._step_hook = None
 
         logger.info(f"initiate with time={time:0.4f}")
         logger.info(f"mesh is {mesh}")
@@ -163,6 +179,8 @@ class Solver(SolverBase):
             primitive = initial_condition(setup, mesh, time)
         else:
             primitive = np.asarray(solution, dtype=np.float64)
+        if primitive.shape == (ni_mesh, nj, NQ) and ni != ni_mesh:
+            primitive = primitive[a:b]
         if primitive.shape != (ni, nj, NQ):
             raise ValueError(f"solution has shape {primitive.shape}, expected {(ni, nj, NQ)}")
 
@@ -180,8 +198,8 @@ class Solver(SolverBase):
 
         g = _capi.Grid()
         g.ni, g.nj = ni, nj
-        g.xl, g.yl = mesh.vertex_coordinates(0, 0)
-        g.xr, g.yr = mesh.vertex_coordinates(ni, nj)
+        g.xl, g.yl = mesh.vertex_coordinates(a, 0)
+        g.xr, g.yr = mesh.vertex_coordinates(b, nj)
         g.plm_theta = options.plm_theta
         g.eos_type = enum_value(physics.eos_type)
         g.precision = _capi.PRECISION[options.precision]
@@ -428,6 +446,10 @@ class Solver(SolverBase):
         orbit = self._device_orbit()
         if not self._result_valid:
             self._reduce_now(True, self._device_diags if self._fused else [])
+            if self._step_hook is not None:
+                self._step_hook()
+        if self._stage_hook is not None or self._step_hook is not None:
+            graph = False  # the hooks' collectives stay outside graph capture
         nvals = 2 * len(self._device_diags) if self._fused else 0
         if self._options.rk_order == 1 and steps_per_graph % 2:
             steps_per_graph += 1  # RK1 swaps the two buffers each step: capture whole pairs
@@ -513,6 +535,7 @@ class Solver(SolverBase):
         self._result_valid = True
         rows = series[:steps].cpu().numpy()
         self.d2h_bytes += rows.nbytes + state.numel()
+        self.last_series = rows  # raw device rows (time, dt, wavespeed, sums)
         return self._series_rows(rows)
 
     def _stepper_fields(self, state):
@@ -582,8 +605,49 @@ class Solver(SolverBase):
                 ctypes.byref(ep) if ep is not None else None, self._ptr(self._scratch), self._ptr(self._result),
                 stream)
             self._check(status, "advance_stage")
+            if self._stage_hook is not None:
+                self._stage_hook(s, wr)
         if len(weights) == 1 and rk2_buffers is None:
             self._buf[0], self._buf[1] = B, A
+        if self._step_hook is not None:
+            self._step_hook()
+
+    # hooks of the multi-GPU solver (distributed.py)
+
+    def state_buffer(self):
+        """The padded device state (its guard rows are exchanged in place)."""
+        return self._buf[0]
+
+    def wavespeed_buffer(self):
+        """One-element device view holding the wavespeed maximum of the
+        current state once ensure_wavespeed() has run."""
+        return self._result[0:1]
+
+    def ensure_wavespeed(self):
+        """Compute the wavespeed maximum of the current state if it is not
+        already known; True if it was computed now."""
+        if self._result_valid:
+            return False
+        self._reduce_now(True, self._device_diags if self._fused else [])
+        return True
+
+    def wavespeed_changed(self):
+        """The wavespeed buffer was rewritten on the device (all-reduced)."""
+        self._cached = None
+
+    def reduction_sums(self):
+        """The diagnostic sums over this solver's zones before the dx dy
+        factor (float or complex per non-time diagnostic)."""
+        if not self._device_diags:
+            return []
+        if not (self._fused and self._result_valid):
+            self._reduce_now(True, self._device_diags)
+        res = self._read_result()
+        out = []
+        for k, d in enumerate(self._device_diags):
+            re, im = res[1 + 2 * k], res[2 + 2 * k]
+            out.append(complex(re, im) if d.quantity in COMPLEX_QUANTITIES else float(re))
+        return out
 
     def reductions(self):
         """
