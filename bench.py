@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--tile", default=None, help="columns,rows,occupancy of the stage kernel (default: library)")
+    p.add_argument("--mode", default="auto", choices=["auto", "slab", "replicas"],
+                   help="slab: one mesh split into N row slabs (guard rows exchanged over NCCL); replicas: N "
+                        "independent runs; auto: slab for N > 1")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the batched-disk and adjoint measurements added to the line at N=1")
     return p.parse_args()
@@ -157,6 +160,88 @@ def stage_kernel_time(solver, repeats=20):
     stop.record()
     torch.cuda.synchronize()
     return start.elapsed_time(stop) * 1e-3 / (2 * repeats)
+
+
+def slab_size(n, world):
+    """Weak scaling: a square mesh with about n^2 zones per GPU (multiple of 64)."""
+    return int(round(n * math.sqrt(world) / 64.0)) * 64
+
+
+def run_slabs(args, rank, world):
+    """N GPUs on one mesh of about N * n^2 zones, one row slab per rank
+    (sailfish_b200.distributed): guard rows exchanged between stages, the
+    wavespeed all-reduced each step."""
+    import torch
+    import torch.distributed as tdist
+
+    from sailfish_b200.cbdiso_2d import initial_condition
+    from sailfish_b200.distributed import DistributedSolver, subdivide
+    from sailfish_b200.setups import CircumbinaryDisk
+
+    n = slab_size(args.size, world)
+    setup = CircumbinaryDisk(**SETUP_PARAMS)
+    mesh = setup.mesh(n)
+    physics = setup.physics
+    physics["diagnostics"] = DIAGNOSTICS
+    a, b = list(subdivide(n, world))[rank]
+    prim = initial_condition(setup, mesh, 0.0, rows=(a, b))
+    prim[..., 0] += 1e-3 * np.random.default_rng(args.seed + rank).uniform(-1.0, 1.0, size=(b - a, n))
+    opts = dict(rk_order=2, plm_theta=THETA, precision=args.precision)
+    solver = DistributedSolver(setup=setup, mesh=mesh, solution=prim, physics=physics, options=opts)
+    solver.run(max(args.warmup, 3), cfl=CFL)
+    tdist.barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        start.record()
+        rows = solver.run(args.steps, cfl=CFL)
+        stop.record()
+        torch.cuda.synchronize()
+    assert len(rows) == args.steps and all(np.isfinite(r[-1]) for r in rows)
+    t = torch.tensor([start.elapsed_time(stop) * 1e-3], device="cuda", dtype=torch.float64)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    elapsed = float(t.item())
+    value = n * n * args.steps / elapsed
+
+    # end to end: host data in, the public driver loop, the whole state out
+    e2e_steps = max(1, min(args.steps, 20))
+    tdist.barrier()
+    t0 = time.perf_counter()
+    s2 = DistributedSolver(setup=setup, mesh=mesh, solution=prim, physics=physics, options=opts)
+    for _ in range(e2e_steps):
+        s2.advance(mesh.min_spacing() / s2.maximum_wavespeed() * CFL)
+        s2.reductions()
+    final = s2.local.solution
+    t1 = time.perf_counter()
+    t = torch.tensor([t1 - t0], device="cuda", dtype=torch.float64)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    e2e_value = n * n * e2e_steps / float(t.item())
+    # per step, summed over the ranks: the slab upload and download
+    e2e_bytes = torch.tensor([float(prim.nbytes + final.nbytes)], device="cuda", dtype=torch.float64)
+    tdist.all_reduce(e2e_bytes)
+    del s2
+    peak, peak_kind = measured_peaks()
+    if rank != 0:
+        return None
+    return {
+        "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"cbdiso_2d circumbinary disk {n}x{n} FP64 RK2 theta {THETA} CFL {CFL} "
+                               f"split into {world} row slabs, per-step mdot/torque reductions",
+                   "zones": n * n, "zones_per_gpu": n * n / world, "precision": args.precision,
+                   "timed": "DistributedSolver.run: device dt / Kepler per rank, NCCL guard-row exchange "
+                            "per stage, wavespeed all-reduce per step",
+                   "l2": "state arrays exceed L2; no flush", "parallelism": f"slab{world}"},
+        "e2e": {"value": e2e_value, "unit": "zone-updates/s",
+                "h2d_bytes_per_step": int(float(e2e_bytes.item()) / 2 / e2e_steps),
+                "d2h_bytes_per_step": int(float(e2e_bytes.item()) / 2 / e2e_steps), "steps": e2e_steps,
+                "includes": "slab upload, public-API driver loop (host dt each step), slab download"},
+        "gpu_launches": 3 * args.steps + 1,
+        "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_source": peak_kind,
+                     "note": "per-kernel roofline is reported by the N = 1 line"},
+        "clocks": clocks.summary(),
+    }
 
 
 def run_ours(args, rank, world):
@@ -429,29 +514,39 @@ def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    if world > 1 and args.impl == "ours":
+    slabs = args.mode == "slab" or (args.mode == "auto" and world > 1)
+    group = args.impl == "ours" and (world > 1 or slabs)
+    if group:
         import datetime
+        import socket
 
         import torch
         import torch.distributed as tdist
 
+        if world == 1 and "MASTER_PORT" not in os.environ:
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(sk.getsockname()[1]), RANK="0",
+                                  WORLD_SIZE="1")
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     if args.impl == "reference":
         line = run_reference(args, rank, world)
+    elif slabs:
+        line = run_slabs(args, rank, world)
     else:
         line = run_ours(args, rank, world)
         if world == 1 and not args.no_extras:
             line["batched"] = batched_extra(line["value"])
             line["adjoint"] = adjoint_extra()
             line["adjoint_batched"] = batched_adjoint_extra()
-        if rank == 0 and not args.no_cpu_baseline:
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
             n = args.size
             v, kind, el = time_cpu(n, 2 if n >= 2048 else 5, 1, args.seed)
             line["cpu_baseline"] = {"value": v, "unit": "zone-updates/s",
                                     "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())), "kind": kind,
                                     "sample": f"{2 if n >= 2048 else 5} driver steps at {n}^2"}
-    if world > 1 and args.impl == "ours":
+    if group:
         import torch.distributed as tdist
 
         tdist.destroy_process_group()

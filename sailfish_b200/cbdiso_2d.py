@@ -59,23 +59,25 @@ class Options(NamedTuple):
     tile: Optional[tuple] = None
 
 
-def initial_condition(setup, mesh, time):
+def initial_condition(setup, mesh, time, rows=None):
     """
-    Primitive data (ni, nj, 3) from a setup (cbdiso_2d.py:33-46). Setups with a
-    vectorised `primitive_array(t, x, y)` are evaluated on the whole grid at
-    once; others zone by zone as the reference does.
+    Primitive data (ni, nj, 3) from a setup (cbdiso_2d.py:33-46), or only the
+    rows a <= i < b of it for rows=(a, b). Setups with a vectorised
+    `primitive_array(t, x, y)` are evaluated on the whole block at once;
+    others zone by zone as the reference does.
     """
     ni, nj = mesh.shape
+    a, b = rows if rows is not None else (0, ni)
     if hasattr(setup, "primitive_array"):
-        i = np.arange(ni, dtype=np.float64)[:, None]
+        i = np.arange(a, b, dtype=np.float64)[:, None]
         j = np.arange(nj, dtype=np.float64)[None, :]
-        x = np.broadcast_to(mesh.x0 + (i + 0.5) * mesh.dx, (ni, nj))
-        y = np.broadcast_to(mesh.y0 + (j + 0.5) * mesh.dy, (ni, nj))
+        x = np.broadcast_to(mesh.x0 + (i + 0.5) * mesh.dx, (b - a, nj))
+        y = np.broadcast_to(mesh.y0 + (j + 0.5) * mesh.dy, (b - a, nj))
         return np.ascontiguousarray(setup.primitive_array(time, x, y), dtype=np.float64)
-    primitive = np.zeros([ni, nj, 3])
-    for i in range(ni):
+    primitive = np.zeros([b - a, nj, 3])
+    for i in range(a, b):
         for j in range(nj):
-            setup.primitive(time, mesh.cell_coordinates(i, j), primitive[i, j])
+            setup.primitive(time, mesh.cell_coordinates(i, j), primitive[i - a, j])
     return primitive
 
 
@@ -176,7 +178,7 @@ class Solver(SolverBase):
         logger.info("boundary condition is outflow")
 
         if solution is None:
-            primitive = initial_condition(setup, mesh, time)
+            primitive = initial_condition(setup, mesh, time, rows=(a, b))
         else:
             primitive = np.asarray(solution, dtype=np.float64)
         if primitive.shape == (ni_mesh, nj, NQ) and ni != ni_mesh:
