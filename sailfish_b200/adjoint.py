@@ -178,12 +178,12 @@ class AdjointRun:
         fresh = self.dts is None or freeze
         dts_dev = None if fresh else torch.from_numpy(np.ascontiguousarray(self.dts)).to(s.device)
         nb = int(self._lib.cbdiso_b200_stage_record_bytes())
-        history = torch.empty(steps * 2 * nb, dtype=torch.uint8, device=s.device) if keep else None
+        history = self._kept("_history", (steps * 2 * nb,), torch.uint8, s.device) if keep else None
         t_start = s.time
         rows, cps, trajectory = [], {}, None
         if keep and self._keep_all(s):
-            trajectory = torch.empty((2 * steps + 1,) + tuple(s._buf[0].shape), dtype=torch.float64,
-                                     device=s.device)
+            trajectory = self._kept("_trajectory", (2 * steps + 1,) + tuple(s._buf[0].shape), torch.float64,
+                                    s.device)
             rows = s.run(steps, cfl=self.cfl, dt_sequence=dts_dev, history=history, trajectory=trajectory)
         else:
             store = self._checkpoint_store(s) if keep else None
@@ -206,6 +206,18 @@ class AdjointRun:
             self._fwd = dict(solver=s, t_start=t_start, checkpoints=cps, params=params, history=history,
                              record_bytes=nb, trajectory=trajectory)
         return J
+
+    def _kept(self, name, shape, dtype, device):
+        """A device buffer kept on the run and reused by later forward runs
+        of the same shape (so that the reverse sweep's graph stays valid)."""
+        import torch
+
+        t = getattr(self, name, None)
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype or t.device != device:
+            setattr(self, name, None)
+            t = torch.empty(shape, dtype=dtype, device=device)
+            setattr(self, name, t)
+        return t
 
     def _checkpoint_store(self, s):
         """Checkpoint slots (one per segment), kept on the run and reused."""
@@ -293,7 +305,10 @@ class AdjointRun:
         sweep.lam_n.zero_()
         if trajectory is not None:
             # every state of the forward run is at hand: no recompute
-            sweep.run(history, jac, steps, states=trajectory)
+            if graph:
+                sweep.replay_stored(history, jac, steps, trajectory)
+            else:
+                sweep.run(history, jac, steps, states=trajectory)
             return sweep.finish()
         for start in reversed(range(0, steps, K)):
             stop = min(start + K, steps)
@@ -463,6 +478,28 @@ class _ReverseSweep:
             self.graph = graph
         self.graph.replay()
 
+    def replay_stored(self, hist, jac, count, states):
+        """The whole sweep over a stored trajectory from one CUDA graph,
+        captured on the first call for these trajectory and record buffers;
+        the Jacobians are staged into a buffer of the sweep."""
+        import torch
+
+        key = (hist.data_ptr(), states.data_ptr(), count, tuple(states.shape))
+        if getattr(self, "_stored_key", None) != key:
+            self._stored_graph = None
+            self._stored_jac = torch.empty_like(jac)
+            self._stored_jac.copy_(jac)
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=side):
+                self.run(hist, self._stored_jac, count, states=states)
+            torch.cuda.current_stream().wait_stream(side)
+            self._stored_graph, self._stored_key = graph, key
+        else:
+            self._stored_jac.copy_(jac)
+        self._stored_graph.replay()
+
     def finish(self):
         import torch
 
@@ -559,8 +596,10 @@ class BatchedAdjoint:
 
     def gradient(self, weights=(1.0, 0.0)):
         """(dJ/dprim0, dJ/d(q, e, nu, sink_rate)) of every disk, after
-        forward(keep=True)."""
-        return self._each(lambda i: self.runs[i].gradient(weights))
+        forward(keep=True). No CUDA graphs here: a capture in one host thread
+        does not admit the device-wide synchronisation another thread's
+        capture starts with."""
+        return self._each(lambda i: self.runs[i].gradient(weights, graph=False))
 
 
 def config4_disks(num=32, seed=4096, sizes=(256, 512)):
@@ -607,3 +646,32 @@ def objective_function(run: AdjointRun, weights=(1.0, 0.0)):
             return (torch.from_numpy(grad_state[..., 0] * g), torch.from_numpy(grad_params * g))
 
     return CircumbinaryObjective
+
+
+def main(argv=None):
+    """One forward run and gradient on the device (a profiling / smoke case):
+    python -m sailfish_b200.adjoint --resolution 512 --steps 20"""
+    import argparse
+
+    import torch
+
+    p = argparse.ArgumentParser(description=main.__doc__)
+    p.add_argument("--resolution", type=int, default=512)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--checkpoint-every", type=int, default=20)
+    p.add_argument("--store-states", choices=["auto", "yes", "no"], default="auto")
+    a = p.parse_args(argv)
+    store = dict(auto=None, yes=True, no=False)[a.store_states]
+    run = AdjointRun(resolution=a.resolution, steps=a.steps, checkpoint_every=a.checkpoint_every,
+                     store_states=store)
+    prim = run.initial_state(seed=0)
+    params = Params(0.5, 0.1, 1e-3, 10.0)
+    run.forward(prim, params, freeze=True, keep=True)
+    J = run.forward(prim, params, keep=True)
+    _, grad = run.gradient((1.0, 0.0))
+    torch.cuda.synchronize()
+    print("J", J, "dJ/d(q, e, nu, sink_rate)", grad)
+
+
+if __name__ == "__main__":
+    main()

@@ -299,3 +299,29 @@ def config2_disks(num=64, seed=2024, sizes=(128, 192, 256, 384, 512, 768, 1024))
         prim[..., 0] += 1e-3 * rng.uniform(-1.0, 1.0, size=(n, n))
         out.append(Disk(setup, mesh, prim))
     return out
+
+
+def main(argv=None):
+    """A few steps of a seeded batch of disks without graphs (a profiling /
+    smoke case): python -m sailfish_b200.batched --disks 16 --sizes 256,512"""
+    import argparse
+
+    import torch
+
+    p = argparse.ArgumentParser(description=main.__doc__)
+    p.add_argument("--disks", type=int, default=16)
+    p.add_argument("--sizes", default="256,512")
+    p.add_argument("--steps", type=int, default=4)
+    p.add_argument("--seed", type=int, default=2024)
+    a = p.parse_args(argv)
+    sizes = tuple(int(v) for v in a.sizes.split(","))
+    diags = [dict(quantity="mdot", which_mass=1, accretion=True), dict(quantity="mdot", which_mass=2, accretion=True),
+             dict(quantity="torque", which_mass="both", gravity=True)]
+    b = BatchedSolver(config2_disks(a.disks, seed=a.seed, sizes=sizes), diagnostics=diags)
+    b.run(a.steps, graph=False)
+    torch.cuda.synchronize()
+    print("zones", b.total_zones)
+
+
+if __name__ == "__main__":
+    main()
