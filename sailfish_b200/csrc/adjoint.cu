@@ -779,15 +779,21 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_inputs(Consts
     }
 }
 
-// fixed-order sum of block partials into one parameter row
+// Fixed-order sum of block partials into one parameter row: warp v sums
+// column v, lane l the rows l, l + 32, ... in order, then the lanes in a
+// fixed shuffle tree (deterministic, independent of timing).
 __global__ void sum_params(const double *blocks, int nblocks, int width, double *out)
 {
-    if ((int)threadIdx.x >= width)
+    const int v = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (v >= width)
         return;
     double s = 0.0;
-    for (int b = 0; b < nblocks; ++b)
-        s += blocks[(size_t)b * width + threadIdx.x];
-    out[threadIdx.x] += s;
+    for (int b = lane; b < nblocks; b += 32)
+        s += blocks[(size_t)b * width + v];
+    for (int o = 16; o > 0; o >>= 1)
+        s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0)
+        out[v] += s;
 }
 
 // ---------------------------------------------------------------------------
@@ -1030,11 +1036,11 @@ int stage_adjoint_impl(const cbd_grid_t *grid, const void *stage_dev, const doub
     } else {
         adj_slopes<false><<<bw, T, 0, s>>>(k, a);
         adj_faces<false><<<bf, T, 0, s>>>(k, a);
-        sum_params<<<1, 32, 0, s>>>(parts, bf, NPAR, params_out);
+        sum_params<<<1, 32 * NPAR, 0, s>>>(parts, bf, NPAR, params_out);
         adj_zones<false><<<bw, T, 0, s>>>(k, a);
-        sum_params<<<1, 32, 0, s>>>(parts, bw, NPAR, params_out);
+        sum_params<<<1, 32 * NPAR, 0, s>>>(parts, bw, NPAR, params_out);
         adj_sinks<false><<<bs, T, 0, s>>>(k, a);
-        sum_params<<<1, 32, 0, s>>>(parts, bs, NPAR, params_out);
+        sum_params<<<1, 32 * NPAR, 0, s>>>(parts, bs, NPAR, params_out);
     }
     adj_inputs<<<bi, T, 0, s>>>(k, a);
     return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
@@ -1060,9 +1066,9 @@ int objective_adjoint_impl(const cbd_grid_t *grid, const void *stage_dev, const 
         objective_sinks<true><<<bs, T, 0, s>>>(k, a, w_mdot, true);
     } else {
         objective_adjoint_kernel<false><<<bz, T, 0, s>>>(k, a, w_torque, false);
-        sum_params<<<1, 32, 0, s>>>(parts, bz, NPAR, params_out);
+        sum_params<<<1, 32 * NPAR, 0, s>>>(parts, bz, NPAR, params_out);
         objective_sinks<false><<<bs, T, 0, s>>>(k, a, w_mdot, false);
-        sum_params<<<1, 32, 0, s>>>(parts, bs, NPAR, params_out);
+        sum_params<<<1, 32 * NPAR, 0, s>>>(parts, bs, NPAR, params_out);
     }
     return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
 }
@@ -1153,7 +1159,7 @@ int cbdiso_b200_adjoint_chain_finish(const double *chain_acc, int num_blocks, do
 {
     if (!chain_acc || num_blocks <= 0 || !out4)
         return CBD_ERR_ARGUMENT;
-    sum_params<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(chain_acc, num_blocks, 4, out4);
+    sum_params<<<1, 32 * 4, 0, static_cast<cudaStream_t>(stream)>>>(chain_acc, num_blocks, 4, out4);
     return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
 }
 

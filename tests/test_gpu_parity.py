@@ -287,3 +287,33 @@ def test_one_step_full_grid_against_oracle(n):
              dict(quantity="torque", which_mass="both", gravity=True)]
     scale = np.array(ref.reductions(diags, absolute=True))
     assert np.all(np.abs(np.array(s.reductions()) - np.array(ref.reductions(diags))) <= 1e-12 * scale)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("precision", ["exact", "fma", "fast"])
+def test_config0_256_1000_steps(precision):
+    """1000 RK2 steps of config 0 (256^2, theta 1.5, CFL 0.3, dt from each
+    run's own wavespeed): every precision stays within 1e-10 of the oracle
+    (C restatement, OpenMP) in each field's maximum norm."""
+    n, steps = 256, 1000
+    setup = CircumbinaryDisk(domain_radius=8.0, mach_number=10.0, mass_ratio=1.0, eccentricity=0.0, sink_rate=10.0,
+                             sink_radius=0.05, softening_length=0.05, nu=0.001)
+    mesh = setup.mesh(n)
+    from sailfish_b200.cbdiso_2d import initial_condition
+
+    prim = initial_condition(setup, mesh, 0.0)
+    prim[..., 0] += oh.seeded_noise(n, n, 0)
+    physics = setup.physics
+    s = make_solver("cbdiso_2d", physics, dict(rk_order=2, plm_theta=1.5, precision=precision), setup=setup,
+                    mesh=mesh, solution=prim)
+    meta = dict(setup="circumbinary-disk", mesh=[-8.0, -8.0, 8.0, 8.0, n, n], rk=2, theta=1.5,
+                params=dict(domain_radius=8.0, mach_number=10.0, mass_ratio=1.0, eccentricity=0.0,
+                            sink_rate=10.0, sink_radius=0.05, softening_length=0.05, nu=0.001))
+    cfg = oracle_config(meta)
+    o = oh.OracleSolver(cfg, prim, 0.0, oh.Kernels("oracle", 1.5, threads="omp"))
+    for _ in range(steps):
+        s.advance(mesh.min_spacing() / s.maximum_wavespeed() * 0.3)
+        o.advance(mesh.min_spacing() / o.maximum_wavespeed() * 0.3)
+    assert s.time == pytest.approx(o.time, rel=1e-12)
+    err = field_error(s.solution, o.solution)
+    assert err <= 1e-10, err
