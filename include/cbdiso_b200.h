@@ -372,6 +372,12 @@ int cbdiso_b200_objective_adjoint_chained(const cbd_grid_t *grid, const void *st
                                           double w_mdot, double w_torque, double *lam, const double *jacobian,
                                           double *chain_acc, void *workspace, void *stream);
 size_t cbdiso_b200_adjoint_chain_blocks(const cbd_grid_t *grid);
+
+/* Test hook (no counterpart in the reference): 1 (default) runs each stage
+ * adjoint as one fused row-marching kernel, 0 as separate passes over the
+ * zones and faces; lambda_rd and lambda_n agree bit for bit, the parameter
+ * sums to rounding. Process-wide. */
+int cbdiso_b200_set_adjoint_variant(int fused);
 int cbdiso_b200_adjoint_chain_finish(const double *chain_acc, int num_blocks, double *out4, void *stream);
 
 /* The epilogue quantities alone, on a given state (guards not needed). */

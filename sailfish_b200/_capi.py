@@ -130,6 +130,8 @@ def _declare(lib):
     lib.cbdiso_b200_batched_prologue.restype = c_int
     lib.cbdiso_b200_adjoint_workspace_bytes.argtypes = [POINTER(Grid)]
     lib.cbdiso_b200_adjoint_workspace_bytes.restype = c_size_t
+    lib.cbdiso_b200_set_adjoint_variant.argtypes = [c_int]
+    lib.cbdiso_b200_set_adjoint_variant.restype = c_int
     lib.cbdiso_b200_adjoint_chain_blocks.argtypes = [POINTER(Grid)]
     lib.cbdiso_b200_adjoint_chain_blocks.restype = c_size_t
     V = c_void_p
@@ -186,6 +188,7 @@ def exported_symbols():
         "cbdiso_b200_stage_adjoint", "cbdiso_b200_objective_tangent", "cbdiso_b200_objective_adjoint",
         "cbdiso_b200_stepper_attach", "cbdiso_b200_stage_adjoint_chained", "cbdiso_b200_objective_adjoint_chained",
         "cbdiso_b200_adjoint_chain_finish", "cbdiso_b200_adjoint_chain_blocks",
+        "cbdiso_b200_set_adjoint_variant",
     ]
 
 

@@ -252,6 +252,19 @@ struct ParAcc<true> {
     }
 };
 
+// An accumulator that counts only when `on` (halo work recomputed by a
+// neighbouring CTA must not be counted twice).
+template <class Acc>
+struct GatedAcc {
+    Acc &acc;
+    bool on;
+    __device__ __forceinline__ void add(int r, double x)
+    {
+        if (on)
+            acc.add(r, x);
+    }
+};
+
 // d(cs^2)/d(mass parameters) at (x, y), times lam, into the accumulator
 template <class Acc>
 __device__ __forceinline__ void cs2_param_vjp(const Consts &k, const StageDev &st, double x, double y, double lam,
@@ -386,8 +399,22 @@ struct AdjArgs {
     const double *jac;      // d(mass parameters)/d(q, e) of this stage, 10 x 2 (chained form)
 };
 
-// lambda of the RK sum u' of zone (i, j): conserved-to-primitive with the
-// recorded floor / ceiling flags; zero outside the interior.
+// lambda of the RK sum u' of a zone from its output primitives o and their
+// adjoint l: the conserved-to-primitive VJP with the floor / ceiling flags
+// the stage took (decided from the output as the branch record does).
+__device__ __forceinline__ void lam_rk_zone(const Consts &k, const double *o, const double *l, double *lu)
+{
+    const bool floor = !(o[0] > k.rho_min);
+    const bool ceil_x = !(fabs(o[1]) < k.vmax), ceil_y = !(fabs(o[2]) < k.vmax);
+    const double inv_rho = 1.0 / o[0];
+    const double lvx = ceil_x ? 0.0 : l[1];
+    const double lvy = ceil_y ? 0.0 : l[2];
+    lu[1] = lvx * inv_rho;
+    lu[2] = lvy * inv_rho;
+    lu[0] = floor ? 0.0 : l[0] - (o[1] * lvx + o[2] * lvy) * inv_rho;
+}
+
+// lambda of the RK sum u' of zone (i, j); zero outside the interior.
 __device__ __forceinline__ bool lam_rk(const Consts &k, const AdjArgs &a, int i, int j, double *lu)
 {
     if (i < 0 || i >= k.ni || j < 0 || j >= k.nj) {
@@ -395,15 +422,7 @@ __device__ __forceinline__ bool lam_rk(const Consts &k, const AdjArgs &a, int i,
         return false;
     }
     const size_t c = zi(i, j, k.nj);
-    const unsigned w = a.words[c];
-    const double *o = a.pout + c * 3;
-    const double *l = a.lam_out + c * 3;
-    const double inv_rho = 1.0 / o[0];
-    const double lvx = (w & BW_CEIL_X) ? 0.0 : l[1];
-    const double lvy = (w & BW_CEIL_Y) ? 0.0 : l[2];
-    lu[1] = lvx * inv_rho;
-    lu[2] = lvy * inv_rho;
-    lu[0] = (w & BW_FLOOR) ? 0.0 : l[0] - (o[1] * lvx + o[2] * lvy) * inv_rho;
+    lam_rk_zone(k, a.pout + c * 3, a.lam_out + c * 3, lu);
     return true;
 }
 
@@ -427,8 +446,10 @@ __device__ __forceinline__ void load_stage(const AdjArgs &a, StageShared &sh)
 // Block sum of the accumulators, in a fixed order: the per-stage form stores
 // the block's 12 sums as its row; the chained form adds its 4 sums to its row.
 template <int NT, bool CHAIN>
-__device__ __forceinline__ void store_params(const AdjArgs &a, const ParAcc<CHAIN> &acc)
+__device__ __forceinline__ void store_params(const AdjArgs &a, const ParAcc<CHAIN> &acc, int row = -1)
 {
+    if (row < 0)
+        row = blockIdx.x;
     constexpr int NV = ParAcc<CHAIN>::N;
     constexpr int NW = NT / 32;
     __shared__ double sm[NV * NW];
@@ -445,7 +466,7 @@ __device__ __forceinline__ void store_params(const AdjArgs &a, const ParAcc<CHAI
         double x = 0.0;
         for (int w = 0; w < NW; ++w)
             x += sm[threadIdx.x * NW + w];
-        double *out = a.par + (size_t)blockIdx.x * NV + threadIdx.x;
+        double *out = a.par + (size_t)row * NV + threadIdx.x;
         if (CHAIN)
             *out += x;
         else
@@ -458,6 +479,115 @@ __device__ __forceinline__ long grid_step(int nt) { return (long)gridDim.x * nt;
 
 constexpr int ADJ_THREADS = 128;
 constexpr int ADJ_MIN_BLOCKS = 5;  // resident blocks per SM the register budget allows
+
+// rho * strain (xx, xy, yy) of a zone from its slopes gx, gy (shear_strain,
+// cbdiso_2d.c:248-263, with the constant divisors as reciprocals: derivative
+// arithmetic needs no correct rounding)
+__device__ __forceinline__ void rho_strain_of(const Consts &k, double rho, const double *gx, const double *gy,
+                                              double *rs)
+{
+    const double sxx = 4.0 / 3.0 * gx[1] * k.inv_dx - 2.0 / 3.0 * gy[2] * k.inv_dy;
+    const double syy = -2.0 / 3.0 * gx[1] * k.inv_dx + 4.0 / 3.0 * gy[2] * k.inv_dy;
+    const double sxy = gx[2] * k.inv_dx + gy[1] * k.inv_dy;
+    rs[0] = rho * sxx;
+    rs[1] = rho * sxy;
+    rs[2] = rho * syy;
+}
+
+// The adjoint of one face. L / R: primitives, slopes along the face normal,
+// the two rho * strain components of the viscous flux (x: xx, xy; y: xy,
+// yy), and the adjoint of the zones' RK sums. Out, 8 doubles: lambda of
+// the minus-side face state (3), of the plus-side state (3), and of the
+// viscous flux's two rho * strain sums (2, the same for both sides).
+template <int DIR, class Acc>
+__device__ __forceinline__ void face_vjp(const Consts &k, const StageDev &st, const MassT<double> *m,
+                                         const double *pL, const double *pR, const double *gL, const double *gR,
+                                         const double *rL, const double *rR, const double *lul, const double *lur,
+                                         double xf, double yf, Acc &par, double *o)
+{
+    const double hn = 0.5 * k.nu, b = st.one_minus_a;
+    const double cf = b * st.dt * (DIR ? k.inv_dy : k.inv_dx);
+    double pl[3], pr[3], lf[3];
+    for (int q = 0; q < 3; ++q) {
+        pl[q] = pL[q] + 0.5 * gL[q];
+        pr[q] = pR[q] - 0.5 * gR[q];
+        lf[q] = (lur[q] - lul[q]) * cf;
+    }
+    const double cs2 = cs2_generic(k, m, xf, yf), cs = sqrt(cs2);
+    double lpl[3] = {0, 0, 0}, lpr[3] = {0, 0, 0}, lcs2 = 0.0;
+    hlle_vjp<DIR>(pl, pr, cs2, cs, hlle_select(pl[1 + DIR], pr[1 + DIR], cs), lf, lpl, lpr, &lcs2);
+    cs2_param_vjp(k, st, xf, yf, lcs2, par);
+    for (int q = 0; q < 3; ++q) {
+        o[q] = lpl[q];
+        o[3 + q] = lpr[q];
+    }
+    if (k.nu > 0.0) {
+        o[6] = -hn * lf[1];
+        o[7] = -hn * lf[2];
+        par.add(10, -0.5 * (rL[0] + rR[0]) * lf[1] - 0.5 * (rL[1] + rR[1]) * lf[2]);
+    } else {
+        o[6] = o[7] = 0.0;
+    }
+}
+
+// The adjoint gathered at one zone of [-1, ni] x [-1, nj] from its four
+// faces (8-double records; a face that does not exist reads as zeros): the
+// direct adjoint lp, the slope adjoints lgx, lgy, the rho * strain products,
+// and for interior zones the gravity and buffer sources and the u_n term.
+// Out: g[0..2] = lgx, g[3..5] = lgy, g[6..8] = lp.
+template <class Acc>
+__device__ __forceinline__ void zone_gather(const Consts &k, const StageDev &st, int i, int j, const double *xe,
+                                            const double *xw, const double *ys, const double *yn, const double *gx,
+                                            const double *gy, const double *pc, const double *lu, bool interior,
+                                            const double *pn, double *lam_n, Acc &par, double *g)
+{
+    double lp[3], lgx[3], lgy[3];
+    for (int q = 0; q < 3; ++q) {
+        lp[q] = xe[q] + xw[3 + q] + yn[q] + ys[3 + q];
+        lgx[q] = 0.5 * xe[q] - 0.5 * xw[3 + q];
+        lgy[q] = 0.5 * yn[q] - 0.5 * ys[3 + q];
+    }
+    if (k.nu > 0.0) {
+        const double lxx = xe[6] + xw[6];
+        const double lxy = xe[7] + xw[7] + yn[6] + ys[6];
+        const double lyy = yn[7] + ys[7];
+        const double rho = pc[0];
+        double s[3];
+        rho_strain_of(k, 1.0, gx, gy, s);
+        lp[0] += s[0] * lxx + s[1] * lxy + s[2] * lyy;
+        lgx[1] += rho * (4.0 / 3.0 * lxx - 2.0 / 3.0 * lyy) * k.inv_dx;
+        lgy[2] += rho * (-2.0 / 3.0 * lxx + 4.0 / 3.0 * lyy) * k.inv_dy;
+        lgx[2] += rho * lxy * k.inv_dx;
+        lgy[1] += rho * lxy * k.inv_dy;
+    }
+    if (interior) {
+        double ld[3];
+        for (int q = 0; q < 3; ++q)
+            ld[q] = st.one_minus_a * lu[q];
+        const double xc = k.xl + (i + 0.5) * k.dx, yc = k.yl + (j + 0.5) * k.dy;
+        const double dt = st.dt;
+        const double rate = buffer_rate(k, st, xc, yc);
+        double luu[3];
+        for (int q = 0; q < 3; ++q)
+            luu[q] = ld[q] * (1.0 - rate * dt);
+        for (int q = 0; q < 2; ++q)
+            gravity_vjp(st.m[q], q, xc, yc, dt, pc, ld, lp, par);
+        lp[0] += luu[0] + luu[1] * pc[1] + luu[2] * pc[2];
+        lp[1] += luu[1] * pc[0];
+        lp[2] += luu[2] * pc[0];
+        if (pn && st.a != 0.0) {
+            const double l0 = st.a * lu[0], l1 = st.a * lu[1], l2 = st.a * lu[2];
+            lam_n[0] += l0 + l1 * pn[1] + l2 * pn[2];
+            lam_n[1] += l1 * pn[0];
+            lam_n[2] += l2 * pn[0];
+        }
+    }
+    for (int q = 0; q < 3; ++q) {
+        g[q] = lgx[q];
+        g[3 + q] = lgy[q];
+        g[6 + q] = lp[q];
+    }
+}
 
 // S: slopes and rho * strain of the zones of [-1, ni] x [-1, nj]; with
 // RECORD also the branch word (limiter choices; floor and ceiling flags of
@@ -474,17 +604,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_slopes(Consts
         double *o = a.sl + c * 9;
         unsigned w = 0;
         slopes_at(k, a.p, i, j, o, o + 3, RECORD ? &w : nullptr);
-        if (k.nu > 0.0) {
-            const double rho = a.p[c * 3];
-            const double sxx = 4.0 / 3.0 * o[1] * k.inv_dx - 2.0 / 3.0 * o[5] * k.inv_dy;
-            const double syy = -2.0 / 3.0 * o[1] * k.inv_dx + 4.0 / 3.0 * o[5] * k.inv_dy;
-            const double sxy = o[2] * k.inv_dx + o[4] * k.inv_dy;
-            o[6] = rho * sxx;
-            o[7] = rho * sxy;
-            o[8] = rho * syy;
-        } else {
+        if (k.nu > 0.0)
+            rho_strain_of(k, a.p[c * 3], o, o + 3, o + 6);
+        else
             o[6] = o[7] = o[8] = 0.0;
-        }
         if (RECORD) {
             if (i >= 0 && i < k.ni && j >= 0 && j < k.nj) {
                 const double *q = a.pout + c * 3;
@@ -502,10 +625,9 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_slopes(Consts
 
 // B: faces, one per thread: items [0, n) are the x-faces, [n, 2 n) the
 // y-faces, n = (ni + 2)(nj + 2). fx[c] is the x-face i + 1/2 of zone
-// c = (i, j), fy[c] the y-face j - 1/2. Per face: lambda of the minus-side
-// state (3), of the plus-side state (3), of the two rho*strain components of
-// the minus side (2) and of the plus side (2). The HLLE wave choice is
-// recomputed with the stage's own (correctly rounded) face sound speed.
+// c = (i, j), fy[c] the y-face j - 1/2, 8 doubles each (face_vjp). The HLLE
+// wave choice is recomputed with the stage's own (correctly rounded) face
+// sound speed.
 template <bool CHAIN>
 __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_faces(Consts k, AdjArgs a)
 {
@@ -517,7 +639,6 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_faces(Consts 
     ParAcc<CHAIN> par(sh.jac);
     MassT<double> m[2];
     masses_t<double>(st, nullptr, m);
-    const double hn = 0.5 * k.nu, b = st.one_minus_a;
     const long f = grid_start(ADJ_THREADS);
     const bool ydir = f >= n;
     const long z = ydir ? f - n : f;
@@ -528,46 +649,25 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_faces(Consts 
     if (live) {
         const int il = i, jl = ydir ? j - 1 : j, ir = ydir ? i : i + 1, jr = j;
         const size_t cl = zi(il, jl, nj), cr = zi(ir, jr, nj);
-        const double *sl = a.sl + cl * 9 + (ydir ? 3 : 0), *sr = a.sl + cr * 9 + (ydir ? 3 : 0);
         double lul[3], lur[3];
         lam_rk(k, a, il, jl, lul);
         lam_rk(k, a, ir, jr, lur);
-        const double cf = b * st.dt * (ydir ? k.inv_dy : k.inv_dx);
-        double pl[3], pr[3], lf[3];
-        for (int q = 0; q < 3; ++q) {
-            pl[q] = a.p[cl * 3 + q] + 0.5 * sl[q];
-            pr[q] = a.p[cr * 3 + q] - 0.5 * sr[q];
-            lf[q] = (lur[q] - lul[q]) * cf;
-        }
-        const double xf = ydir ? k.xl + (i + 0.5) * k.dx : k.xl + (i + 1.0) * k.dx;
-        const double yf = ydir ? k.yl + (j + 0.0) * k.dy : k.yl + (j + 0.5) * k.dy;
-        const double cs2 = cs2_generic(k, m, xf, yf), cs = sqrt(cs2);
-        double lpl[3] = {0, 0, 0}, lpr[3] = {0, 0, 0}, lcs2 = 0.0;
+        const double *sl = a.sl + cl * 9, *sr = a.sl + cr * 9;
+        double *o = (ydir ? a.fy : a.fx) + zi(i, j, nj) * 8;
         if (ydir)
-            hlle_vjp<1>(pl, pr, cs2, cs, hlle_select(pl[2], pr[2], cs), lf, lpl, lpr, &lcs2);
+            face_vjp<1>(k, st, m, a.p + cl * 3, a.p + cr * 3, sl + 3, sr + 3, sl + 7, sr + 7, lul, lur,
+                        k.xl + (i + 0.5) * k.dx, k.yl + (j + 0.0) * k.dy, par, o);
         else
-            hlle_vjp<0>(pl, pr, cs2, cs, hlle_select(pl[1], pr[1], cs), lf, lpl, lpr, &lcs2);
-        cs2_param_vjp(k, st, xf, yf, lcs2, par);
-        double *o = (ydir ? a.fy : a.fx) + zi(i, j, nj) * 10;
-        for (int q = 0; q < 3; ++q) {
-            o[q] = lpl[q];
-            o[3 + q] = lpr[q];
-        }
-        if (k.nu > 0.0) {
-            // x: f1 -= hn (rs_xx L + R), f2 -= hn (rs_xy L + R); y: rs_xy, rs_yy
-            const double *rl = a.sl + cl * 9 + (ydir ? 7 : 6), *rr = a.sl + cr * 9 + (ydir ? 7 : 6);
-            o[6] = o[8] = -hn * lf[1];
-            o[7] = o[9] = -hn * lf[2];
-            par.add(10, -0.5 * (rl[0] + rr[0]) * lf[1] - 0.5 * (rl[1] + rr[1]) * lf[2]);
-        }
+            face_vjp<0>(k, st, m, a.p + cl * 3, a.p + cr * 3, sl, sr, sl + 6, sr + 6, lul, lur,
+                        k.xl + (i + 1.0) * k.dx, k.yl + (j + 0.5) * k.dy, par, o);
     }
     store_params<ADJ_THREADS, CHAIN>(a, par);
 }
 
-__constant__ double kZeroFace[10] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+__constant__ double kZeroFace[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 
-// C: zones of [-1, ni] x [-1, nj]: gather the four faces, rho * strain,
-// gravity and buffer sources, the u_n adjoint (sinks: adj_sinks).
+// C: zones of [-1, ni] x [-1, nj]: zone_gather of the four faces pass B wrote
+// (sinks: adj_sinks).
 template <bool CHAIN>
 __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_zones(Consts k, AdjArgs a)
 {
@@ -581,62 +681,21 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_zones(Consts 
     if (z < wi * wj) {
         const int i = (int)(z / wj) - 1, j = (int)(z % wj) - 1;
         const size_t c = zi(i, j, nj);
-        // faces that pass B wrote; the others carry no adjoint
         const bool row = j >= 0 && j < nj, col = i >= 0 && i < ni;
-        const double *xe = row && i < ni ? a.fx + c * 10 : kZeroFace;
-        const double *xw = row && i >= 0 ? a.fx + zi(i - 1, j, nj) * 10 : kZeroFace;
-        const double *ys = col && j >= 0 ? a.fy + c * 10 : kZeroFace;
-        const double *yn = col && j < nj ? a.fy + zi(i, j + 1, nj) * 10 : kZeroFace;
-        double lp[3], lgx[3], lgy[3];
-        for (int q = 0; q < 3; ++q) {
-            lp[q] = xe[q] + xw[3 + q] + yn[q] + ys[3 + q];
-            lgx[q] = 0.5 * xe[q] - 0.5 * xw[3 + q];
-            lgy[q] = 0.5 * yn[q] - 0.5 * ys[3 + q];
-        }
-        if (k.nu > 0.0) {
-            const double *sl = a.sl + c * 9;
-            const double lxx = xe[6] + xw[8];
-            const double lxy = xe[7] + xw[9] + yn[6] + ys[8];
-            const double lyy = yn[7] + ys[9];
-            const double rho = a.p[c * 3];
-            const double sxx = 4.0 / 3.0 * sl[1] * k.inv_dx - 2.0 / 3.0 * sl[5] * k.inv_dy;
-            const double syy = -2.0 / 3.0 * sl[1] * k.inv_dx + 4.0 / 3.0 * sl[5] * k.inv_dy;
-            const double sxy = sl[2] * k.inv_dx + sl[4] * k.inv_dy;
-            lp[0] += sxx * lxx + sxy * lxy + syy * lyy;
-            lgx[1] += rho * (4.0 / 3.0 * lxx - 2.0 / 3.0 * lyy) * k.inv_dx;
-            lgy[2] += rho * (-2.0 / 3.0 * lxx + 4.0 / 3.0 * lyy) * k.inv_dy;
-            lgx[2] += rho * lxy * k.inv_dx;
-            lgy[1] += rho * lxy * k.inv_dy;
-        }
+        const double *xe = row && i < ni ? a.fx + c * 8 : kZeroFace;
+        const double *xw = row && i >= 0 ? a.fx + zi(i - 1, j, nj) * 8 : kZeroFace;
+        const double *ys = col && j >= 0 ? a.fy + c * 8 : kZeroFace;
+        const double *yn = col && j < nj ? a.fy + zi(i, j + 1, nj) * 8 : kZeroFace;
         double lu[3];
-        if (lam_rk(k, a, i, j, lu)) {
-            const double *pc = a.p + c * 3;
-            double ld[3];
-            for (int q = 0; q < 3; ++q)
-                ld[q] = st.one_minus_a * lu[q];
-            const double xc = k.xl + (i + 0.5) * k.dx, yc = k.yl + (j + 0.5) * k.dy;
-            const double dt = st.dt;
-            const double rate = buffer_rate(k, st, xc, yc);
-            double luu[3];
-            for (int q = 0; q < 3; ++q)
-                luu[q] = ld[q] * (1.0 - rate * dt);
-            for (int q = 0; q < 2; ++q)
-                gravity_vjp(st.m[q], q, xc, yc, dt, pc, ld, lp, par);
-            lp[0] += luu[0] + luu[1] * pc[1] + luu[2] * pc[2];
-            lp[1] += luu[1] * pc[0];
-            lp[2] += luu[2] * pc[0];
-            if (a.pn && st.a != 0.0) {
-                const double *pn = a.pn + c * 3;
-                const double l0 = st.a * lu[0], l1 = st.a * lu[1], l2 = st.a * lu[2];
-                a.lam_n[c * 3 + 0] += l0 + l1 * pn[1] + l2 * pn[2];
-                a.lam_n[c * 3 + 1] += l1 * pn[0];
-                a.lam_n[c * 3 + 2] += l2 * pn[0];
-            }
-        }
+        const bool interior = lam_rk(k, a, i, j, lu);
+        const double *sl = a.sl + c * 9;
+        double g[9];
+        zone_gather(k, st, i, j, xe, xw, ys, yn, sl, sl + 3, a.p + c * 3, lu, interior,
+                    a.pn ? a.pn + c * 3 : nullptr, a.lam_n ? a.lam_n + c * 3 : nullptr, par, g);
         for (int q = 0; q < 3; ++q) {
-            a.lg[c * 6 + q] = lgx[q];
-            a.lg[c * 6 + 3 + q] = lgy[q];
-            a.lp[c * 3 + q] = lp[q];
+            a.lg[c * 6 + q] = g[q];
+            a.lg[c * 6 + 3 + q] = g[3 + q];
+            a.lp[c * 3 + q] = g[6 + q];
         }
     }
     store_params<ADJ_THREADS, CHAIN>(a, par);
@@ -665,8 +724,16 @@ __device__ __forceinline__ double sink_direction(const MassDev &m, double x, dou
     return ld[0] * du[0].d + ld[1] * du[1].d + ld[2] * du[2].d;
 }
 
-// Sinks of the stage (after pass C): lambda_p and the parameter sums of the
-// zones in each mass's sink box, one thread per (zone, direction).
+__device__ __forceinline__ bool in_box(int i, int j, int i0, int i1, int j0, int j1)
+{
+    return i >= i0 && i <= i1 && j >= j0 && j <= j1;
+}
+
+// Sinks of the stage, after the input pass: their adjoint goes straight into
+// lambda_rd (sink zones are interior zones, which no guard image reaches),
+// one thread per (zone, direction) of the union of the masses' sink boxes;
+// a zone in both boxes adds mass 1's term to mass 0's before the store, so
+// no two threads write one element.
 template <bool CHAIN>
 __global__ void __launch_bounds__(ADJ_THREADS) adj_sinks(Consts k, AdjArgs a)
 {
@@ -674,32 +741,51 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_sinks(Consts k, AdjArgs a)
     load_stage<CHAIN>(a, sh);
     const StageDev &st = sh.st;
     ParAcc<CHAIN> par(sh.jac);
+    int box[2][4];
+    bool on[2];
     for (int q = 0; q < 2; ++q) {
         const MassDev &m = st.m[q];
-        if (m.sink_rate == 0.0 || m.sink_model < 1 || m.sink_model > 3)
+        on[q] = !(m.sink_rate == 0.0 || m.sink_model < 1 || m.sink_model > 3);
+        if (on[q]) {
+            sink_box(k, m, &box[q][0], &box[q][1], &box[q][2], &box[q][3]);
+            on[q] = box[q][1] >= box[q][0] && box[q][3] >= box[q][2];
+        }
+    }
+    for (int q = 0; q < 2; ++q) {
+        if (!on[q])
             continue;
-        int i0, i1, j0, j1;
-        sink_box(k, m, &i0, &i1, &j0, &j1);
-        if (i1 < i0 || j1 < j0)
-            continue;
-        const long bw = j1 - j0 + 1, n = (long)(i1 - i0 + 1) * bw * 8;
+        const int i0 = box[q][0], j0 = box[q][2];
+        const long bw = box[q][3] - j0 + 1, n = (long)(box[q][1] - i0 + 1) * bw * 8;
         for (long t = grid_start(ADJ_THREADS); t < n; t += grid_step(ADJ_THREADS)) {
             const long z = t >> 3;
             const int dir = (int)(t & 7);
             const int i = i0 + (int)(z / bw), j = j0 + (int)(z % bw);
+            if (q == 1 && on[0] && in_box(i, j, box[0][0], box[0][1], box[0][2], box[0][3]))
+                continue;  // done with mass 0's box
             const double x = k.xl + (i + 0.5) * k.dx, y = k.yl + (j + 0.5) * k.dy;
-            const double dx = x - m.x, dy = y - m.y;
-            if (!(dx * dx + dy * dy < m.sink_hi2))
-                continue;
+            const size_t c = zi(i, j, k.nj);
             double lu[3];
             lam_rk(k, a, i, j, lu);
-            const size_t c = zi(i, j, k.nj);
             const double ld[3] = {st.one_minus_a * lu[0], st.one_minus_a * lu[1], st.one_minus_a * lu[2]};
-            const double v = sink_direction(m, x, y, st.dt, a.p + c * 3, ld, dir);
-            if (dir < 3)
-                a.lp[c * 3 + dir] += v;
-            else
-                par.add(dir < 7 ? 5 * q + dir - 3 : 11, v);
+            double vsum = 0.0;
+            bool any = false;
+            for (int p = q; p < 2; ++p) {
+                const MassDev &m = st.m[p];
+                if (!on[p] || !in_box(i, j, box[p][0], box[p][1], box[p][2], box[p][3]))
+                    continue;
+                const double dx = x - m.x, dy = y - m.y;
+                if (!(dx * dx + dy * dy < m.sink_hi2))
+                    continue;
+                const double v = sink_direction(m, x, y, st.dt, a.p + c * 3, ld, dir);
+                if (dir < 3) {
+                    vsum = any ? vsum + v : v;
+                    any = true;
+                } else {
+                    par.add(dir < 7 ? 5 * p + dir - 3 : 11, v);
+                }
+            }
+            if (dir < 3 && any)
+                a.lam_rd[c * 3 + dir] += vsum;
         }
     }
     store_params<ADJ_THREADS, CHAIN>(a, par);
@@ -766,17 +852,283 @@ __global__ void __launch_bounds__(ADJ_THREADS, ADJ_MIN_BLOCKS) adj_inputs(Consts
         const int i = (int)(z / nj), j = (int)(z - (long)i * nj);
         const int ilo = i == 0 ? -2 : i, ihi = i == ni - 1 ? ni + 1 : i;
         const int jlo = j == 0 ? -2 : j, jhi = j == nj - 1 ? nj + 1 : j;
+        // row sums of the folded images first, then the rows in order
         double tot[3] = {0.0, 0.0, 0.0};
-        for (int ii = ilo; ii <= ihi; ++ii)
+        for (int ii = ilo; ii <= ihi; ++ii) {
+            double row[3] = {0.0, 0.0, 0.0};
             for (int jj = jlo; jj <= jhi; ++jj) {
                 double v[3];
                 input_adjoint_at(k, a, ii, jj, v);
                 for (int q = 0; q < 3; ++q)
-                    tot[q] += v[q];
+                    row[q] += v[q];
             }
+            for (int q = 0; q < 3; ++q)
+                tot[q] += row[q];
+        }
         for (int q = 0; q < 3; ++q)
             a.lam_rd[zi(i, j, nj) * 3 + q] += tot[q];
     }
+}
+
+// ---------------------------------------------------------------------------
+// fused adjoint stage: one row-marching pass (the passes S, B, C and D above
+// in one kernel, their intermediate results kept in shared-memory rings)
+// ---------------------------------------------------------------------------
+//
+// A CTA of AM_NT threads owns AM_BJ output columns [j0, j0 + AM_BJ) and a
+// segment of output rows, and marches down the rows. At iteration r it
+//   1. stages row r + 3 of the input primitives and the RK-sum adjoint of
+//      row r + 2 (prefetched into registers one iteration ahead),
+//   2. computes the slopes, rho * strain and limiter choices of row r + 2,
+//   3. the x-face adjoint between rows r + 1 and r + 2 (one per column, kept
+//      in registers) and the y-face adjoints of row r + 1,
+//   4. the zone gather of row r + 1,
+//   5. the input adjoint of row r (slope products of rows r - 1 .. r + 1,
+//      guard images folded in) and adds it to lambda_rd.
+// Each quantity is computed once per zone or face with the same functions
+// and operation order as the separate passes, so the two agree bit for bit
+// in lambda_rd and lambda_n. Column spans relative to j0: primitives
+// [j0 - 3, j0 + BJ + 2], slopes and RK-sum adjoints [j0 - 2, j0 + BJ + 1],
+// gathers [j0 - 1, j0 + BJ], y-faces j - 1/2 for j in [j0 - 1, j0 + BJ + 1].
+
+constexpr int AM_NT = 128;
+constexpr int AM_BJ = AM_NT - 8;
+constexpr int AM_NP = AM_BJ + 6, AM_NS = AM_BJ + 4, AM_NG = AM_BJ + 2, AM_NY = AM_BJ + 3;
+
+struct MarchSmem {
+    double p[4][AM_NP][3];   // rows mod 4
+    double sl[2][AM_NS][9];  // rows mod 2: gx (3), gy (3), rho * strain (3)
+    double lr[2][AM_NS][3];  // RK-sum adjoint, rows mod 2
+    double yf[AM_NY][8];     // y-faces of the gathered row
+    double lg[3][AM_NG][9];  // rows mod 3: lgx (3), lgy (3), lp (3)
+    unsigned wd[4][AM_NS];   // limiter choices, rows mod 4
+};
+
+__device__ __forceinline__ int mod(int r, int m) { return ((r % m) + m) % m; }
+
+// input_adjoint_at on the shared rings (row r must be in [r0 - 1 ..] of the
+// rings; c any padded column the strip covers)
+__device__ __forceinline__ void march_input_adjoint(const Consts &k, const MarchSmem &sm, int r, int c, int j0,
+                                                    double *acc)
+{
+    const int ni = k.ni, nj = k.nj;
+    const bool in_range = r >= -1 && r <= ni && c >= -1 && c <= nj;
+    const int cg = c - (j0 - 1), cs = c - (j0 - 2);
+    for (int q = 0; q < 3; ++q)
+        acc[q] = in_range ? sm.lg[mod(r, 3)][cg][6 + q] : 0.0;
+    for (int d = -1; d <= 1; ++d) {
+        const int ii = r + d;
+        if (ii < -1 || ii > ni || c < -1 || c > nj)
+            continue;
+        const unsigned w = sm.wd[mod(ii, 4)][cs];
+        for (int q = 0; q < 3; ++q) {
+            double wt[3];
+            slope_weights((w >> (2 * q)) & 3u, k.theta, wt);
+            acc[q] += wt[1 - d] * sm.lg[mod(ii, 3)][cg][q];
+        }
+    }
+    for (int d = -1; d <= 1; ++d) {
+        const int jj = c + d;
+        if (jj < -1 || jj > nj || r < -1 || r > ni)
+            continue;
+        const unsigned w = sm.wd[mod(r, 4)][cs + d];
+        for (int q = 0; q < 3; ++q) {
+            double wt[3];
+            slope_weights((w >> (6 + 2 * q)) & 3u, k.theta, wt);
+            acc[q] += wt[1 - d] * sm.lg[mod(r, 3)][cg + d][3 + q];
+        }
+    }
+}
+
+template <bool CHAIN>
+__global__ void __launch_bounds__(AM_NT, 3) adj_march(Consts k, AdjArgs a, int seg_rows)
+{
+    extern __shared__ __align__(16) unsigned char am_raw[];
+    MarchSmem &sm = *reinterpret_cast<MarchSmem *>(am_raw);
+    __shared__ StageShared sh;
+    load_stage<CHAIN>(a, sh);
+    const StageDev &st = sh.st;
+    ParAcc<CHAIN> par(sh.jac);
+    MassT<double> m[2];
+    masses_t<double>(st, nullptr, m);
+
+    const int ni = k.ni, nj = k.nj, t = threadIdx.x;
+    const int j0 = blockIdx.x * AM_BJ;
+    const int R0 = blockIdx.y * seg_rows, R1 = min(R0 + seg_rows, ni);
+    // output rows, with the guard rows that fold into the edge rows
+    const int r_first = R0 == 0 ? -2 : R0, r_last = R1 == ni ? ni + 1 : R1 - 1;
+
+    // own columns of each span
+    const int cP = j0 - 3 + t, cS = j0 - 2 + t, cG = j0 - 1 + t, cY = j0 - 1 + t, cO = j0 + t;
+    const bool onP = t < AM_NP && cP >= -2 && cP <= nj + 1;
+    const bool onS = t < AM_NS && cS >= -2 && cS <= nj + 1;
+    const bool onG = t < AM_NG && cG >= -1 && cG <= nj;
+    const bool onY = t < AM_NY;
+    const bool onO = t < AM_BJ && cO < nj;
+
+    // registers: prefetched row, the previous x-face's plus side, output sums
+    double pre_p[3] = {0.0, 0.0, 0.0}, pre_o[3] = {0.0, 0.0, 0.0}, pre_l[3] = {0.0, 0.0, 0.0};
+    double xprev[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double acc[3] = {0.0, 0.0, 0.0};
+
+    auto fetch = [&](int r) {
+        // primitives of row r + 3, output and its adjoint of row r + 2
+        const int L = r + 3, R = r + 2;
+        if (onP && L >= -2 && L <= ni + 1 && L >= r_first - 3 && L <= r_last + 3) {
+            const double *src = a.p + zi(L, cP, nj) * 3;
+            pre_p[0] = src[0];
+            pre_p[1] = src[1];
+            pre_p[2] = src[2];
+        }
+        if (onS && R >= 0 && R < ni && cS >= 0 && cS < nj && R >= r_first - 2 && R <= r_last + 2) {
+            const size_t c = zi(R, cS, nj) * 3;
+            for (int q = 0; q < 3; ++q) {
+                pre_o[q] = a.pout[c + q];
+                pre_l[q] = a.lam_out[c + q];
+            }
+        }
+    };
+
+    fetch(r_first - 6);
+    for (int r = r_first - 6; r <= r_last; ++r) {
+        // 1. stage the prefetched row, prefetch the next
+        {
+            const int L = r + 3, R = r + 2;
+            if (t < AM_NP) {
+                double *d = sm.p[mod(L, 4)][t];
+                const bool live = onP && L >= -2 && L <= ni + 1;
+                d[0] = live ? pre_p[0] : 0.0;
+                d[1] = live ? pre_p[1] : 0.0;
+                d[2] = live ? pre_p[2] : 0.0;
+            }
+            if (t < AM_NS) {
+                double *d = sm.lr[mod(R, 2)][t];
+                if (onS && R >= 0 && R < ni && cS >= 0 && cS < nj && R >= r_first - 2) {
+                    lam_rk_zone(k, pre_o, pre_l, d);
+                } else {
+                    d[0] = d[1] = d[2] = 0.0;
+                }
+            }
+        }
+        if (r < r_last)
+            fetch(r + 1);
+        __syncthreads();
+
+        // 2. slopes, rho * strain and limiter choices of row r + 2
+        {
+            const int R = r + 2;
+            if (t < AM_NS && R >= -1 && R <= ni && R >= r_first - 2) {
+                double *o = sm.sl[mod(R, 2)][t];
+                unsigned w = 0;
+                if (onS && cS >= -1 && cS <= nj) {
+                    const double *pm = sm.p[mod(R - 1, 4)][t + 1], *p0 = sm.p[mod(R, 4)][t + 1];
+                    const double *pp = sm.p[mod(R + 1, 4)][t + 1];
+                    const double *pw = sm.p[mod(R, 4)][t], *pe = sm.p[mod(R, 4)][t + 2];
+                    for (int q = 0; q < 3; ++q) {
+                        const unsigned sx = slope_select(pm[q], p0[q], pp[q], k.theta);
+                        const unsigned sy = slope_select(pw[q], p0[q], pe[q], k.theta);
+                        o[q] = slope_generic(pm[q], p0[q], pp[q], k.theta);
+                        o[3 + q] = slope_generic(pw[q], p0[q], pe[q], k.theta);
+                        w |= sx << (2 * q);
+                        w |= sy << (6 + 2 * q);
+                    }
+                    if (k.nu > 0.0)
+                        rho_strain_of(k, p0[0], o, o + 3, o + 6);
+                    else
+                        o[6] = o[7] = o[8] = 0.0;
+                } else {
+                    for (int q = 0; q < 9; ++q)
+                        o[q] = 0.0;
+                }
+                sm.wd[mod(R, 4)][t] = w;
+            }
+        }
+        __syncthreads();
+
+        // 3. x-face (r + 1) + 1/2 in registers, y-faces of row r + 1
+        double xnew[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        {
+            const int A = r + 1;
+            if (onG && A >= -1 && A <= ni - 1 && A >= r_first - 2 && cG >= 0 && cG < nj) {
+                const int s = t + 1, pc = t + 2;  // this column in the S and P spans
+                const double *sA = sm.sl[mod(A, 2)][s], *sB = sm.sl[mod(A + 1, 2)][s];
+                // the face A + 1/2 belongs to the CTA owning row min(A + 1, ni - 1) and its column
+                const int orow = A + 1 < ni ? A + 1 : ni - 1;
+                GatedAcc<ParAcc<CHAIN>> gp{par, orow >= R0 && orow < R1 && cG >= j0 && cG < j0 + AM_BJ};
+                face_vjp<0>(k, st, m, sm.p[mod(A, 4)][pc], sm.p[mod(A + 1, 4)][pc], sA, sB, sA + 6, sB + 6,
+                            sm.lr[mod(A, 2)][s], sm.lr[mod(A + 1, 2)][s], k.xl + (A + 1.0) * k.dx,
+                            k.yl + (cG + 0.5) * k.dy, gp, xnew);
+            }
+            if (onY) {
+                double *o = sm.yf[t];
+                const int j = cY;  // face j - 1/2: L = (A, j - 1), R = (A, j)
+                if (A >= 0 && A < ni && j >= 0 && j <= nj && A >= r_first - 1 && A <= r_last + 1) {
+                    const int sl_ = t, sr_ = t + 1;  // S-span indices of j - 1 and j
+                    const double *gL = sm.sl[mod(A, 2)][sl_], *gR = sm.sl[mod(A, 2)][sr_];
+                    // the face j - 1/2 belongs to the CTA owning row A and column min(j, nj - 1)
+                    const int ocol = j < nj ? j : nj - 1;
+                    GatedAcc<ParAcc<CHAIN>> gp{par, A >= R0 && A < R1 && ocol >= j0 && ocol < j0 + AM_BJ};
+                    face_vjp<1>(k, st, m, sm.p[mod(A, 4)][t + 1], sm.p[mod(A, 4)][t + 2], gL + 3, gR + 3, gL + 7,
+                                gR + 7, sm.lr[mod(A, 2)][sl_], sm.lr[mod(A, 2)][sr_], k.xl + (A + 0.5) * k.dx,
+                                k.yl + (j + 0.0) * k.dy, gp, o);
+                } else {
+                    for (int q = 0; q < 8; ++q)
+                        o[q] = 0.0;
+                }
+            }
+        }
+        __syncthreads();
+
+        // 4. zone gather of row r + 1
+        {
+            const int A = r + 1;
+            if (t < AM_NG && A >= -1 && A <= ni && A >= r_first - 1) {
+                double *g = sm.lg[mod(A, 3)][t];
+                if (onG) {
+                    const bool interior = A >= 0 && A < ni && cG >= 0 && cG < nj;
+                    // sources and the u_n term count once: in the CTA owning the zone
+                    const bool own = interior && A >= R0 && A < R1 && cG >= j0 && cG < j0 + AM_BJ;
+                    const size_t c = zi(A, cG, nj);
+                    const double *sl = sm.sl[mod(A, 2)][t + 1];
+                    GatedAcc<ParAcc<CHAIN>> gp{par, own};
+                    zone_gather(k, st, A, cG, xnew, xprev, sm.yf[t], sm.yf[t + 1], sl, sl + 3,
+                                sm.p[mod(A, 4)][t + 2], sm.lr[mod(A, 2)][t + 1], interior,
+                                own && a.pn ? a.pn + c * 3 : nullptr, own && a.lam_n ? a.lam_n + c * 3 : nullptr,
+                                gp, g);
+                } else {
+                    for (int q = 0; q < 9; ++q)
+                        g[q] = 0.0;
+                }
+            }
+            for (int q = 0; q < 8; ++q)
+                xprev[q] = xnew[q];
+        }
+        __syncthreads();
+
+        // 5. input adjoint of row r, guard images folded into the edge zones
+        if (onO && r >= r_first) {
+            double row[3] = {0.0, 0.0, 0.0}, v[3];
+            const int clo = cO == 0 ? -2 : cO, chi = cO == nj - 1 ? nj + 1 : cO;
+            for (int c = clo; c <= chi; ++c) {
+                march_input_adjoint(k, sm, r, c, j0, v);
+                for (int q = 0; q < 3; ++q)
+                    row[q] += v[q];
+            }
+            const int z = r < 0 ? 0 : (r >= ni ? ni - 1 : r);
+            const int start = z == 0 ? -2 : z, end = z == ni - 1 ? ni + 1 : z;
+            if (r == start)
+                acc[0] = acc[1] = acc[2] = 0.0;
+            for (int q = 0; q < 3; ++q)
+                acc[q] += row[q];
+            if (r == end) {
+                double *dst = a.lam_rd + zi(z, cO, nj) * 3;
+                for (int q = 0; q < 3; ++q)
+                    dst[q] += acc[q];
+            }
+        }
+        __syncthreads();
+    }
+    store_params<AM_NT, CHAIN>(a, par, blockIdx.y * gridDim.x + blockIdx.x);
 }
 
 // Fixed-order sum of block partials into one parameter row: warp v sums
@@ -956,9 +1308,9 @@ using namespace cbd;
 
 namespace {
 
-// per zone: slopes and rho * strain (9), x-face (10), y-face (10), slope
+// per zone: slopes and rho * strain (9), x-face (8), y-face (8), slope
 // adjoints (6), direct adjoints (3), the branch word (one slot)
-constexpr size_t WS_PER_ZONE = 9 + 10 + 10 + 6 + 3 + 1;
+constexpr size_t WS_PER_ZONE = 9 + 8 + 8 + 6 + 3 + 1;
 
 bool grid_ok(const cbd_grid_t *g)
 {
@@ -974,8 +1326,8 @@ AdjArgs adj_args(const cbd_grid_t *grid, const void *stage_dev, void *workspace,
     double *ws = static_cast<double *>(workspace);
     a.sl = ws;
     a.fx = a.sl + zones * 9;
-    a.fy = a.fx + zones * 10;
-    a.lg = a.fy + zones * 10;
+    a.fy = a.fx + zones * 8;
+    a.lg = a.fy + zones * 8;
     a.lp = a.lg + zones * 6;
     a.words = reinterpret_cast<unsigned *>(a.lp + zones * 3);
     a.par = ws + zones * WS_PER_ZONE;  // per-block partials of the per-stage form
@@ -989,12 +1341,43 @@ AdjArgs adj_args(const cbd_grid_t *grid, const void *stage_dev, void *workspace,
 int adj_rows(const cbd_grid_t *grid)
 {
     const long faces = 2L * (grid->ni + 2) * (grid->nj + 2);
-    return (int)((faces + ADJ_THREADS - 1) / ADJ_THREADS);
+    const long pass = (faces + ADJ_THREADS - 1) / ADJ_THREADS;
+    // the fused kernel's CTAs at its shortest (8-row) segments
+    const long march = (long)((grid->nj + AM_BJ - 1) / AM_BJ) * ((grid->ni + 7) / 8);
+    return (int)(pass > march ? pass : march);
 }
 
 int pass_blocks(long items) { return items > 0 ? (int)((items + ADJ_THREADS - 1) / ADJ_THREADS) : 1; }
 
 constexpr int SINK_PASS_BLOCKS = 16;
+
+// the fused row-marching stage adjoint (default) or the separate passes
+int g_fused_adjoint = 1;
+
+// Strips of AM_BJ columns x segments of rows: 32-row segments, halved down to
+// 8 while the grid is under two waves of three CTAs per SM.
+dim3 march_grid(int ni, int nj)
+{
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                   cudaSuccess)
+        cudaGetLastError();
+    const int strips = (nj + AM_BJ - 1) / AM_BJ;
+    int rows = 32;
+    while (rows > 8 && (long)strips * ((ni + rows - 1) / rows) < 2L * 3 * sms)
+        rows /= 2;
+    return dim3(strips, (ni + rows - 1) / rows, 1);
+}
+
+template <bool CHAIN>
+bool march_ready()
+{
+    static int ok = -1;
+    if (ok < 0)
+        ok = cudaFuncSetAttribute(adj_march<CHAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(MarchSmem)) == cudaSuccess;
+    return ok == 1;
+}
 
 // With `jac` null: `words` is the recorded branch record and the 12
 // parameter derivatives of this stage are ADDED into params_out. Otherwise
@@ -1028,10 +1411,30 @@ int stage_adjoint_impl(const cbd_grid_t *grid, const void *stage_dev, const doub
     const int bw = pass_blocks(wide), bf = pass_blocks(2 * wide), bi = pass_blocks((long)ni * nj);
     const int bs = SINK_PASS_BLOCKS;
     constexpr int T = ADJ_THREADS;
+    if (g_fused_adjoint) {
+        const dim3 grid = march_grid(ni, nj);
+        const int seg = (ni + (int)grid.y - 1) / (int)grid.y;
+        const size_t smem = sizeof(MarchSmem);
+        if (jac) {
+            if (!march_ready<true>())
+                return CBD_ERR_CUDA;
+            adj_march<true><<<grid, AM_NT, smem, s>>>(k, a, seg);
+            adj_sinks<true><<<bs, T, 0, s>>>(k, a);
+        } else {
+            if (!march_ready<false>())
+                return CBD_ERR_CUDA;
+            adj_march<false><<<grid, AM_NT, smem, s>>>(k, a, seg);
+            sum_params<<<1, 32 * NPAR, 0, s>>>(parts, (int)(grid.x * grid.y), NPAR, params_out);
+            adj_sinks<false><<<bs, T, 0, s>>>(k, a);
+            sum_params<<<1, 32 * NPAR, 0, s>>>(parts, bs, NPAR, params_out);
+        }
+        return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
+    }
     if (jac) {
         adj_slopes<true><<<bw, T, 0, s>>>(k, a);
         adj_faces<true><<<bf, T, 0, s>>>(k, a);
         adj_zones<true><<<bw, T, 0, s>>>(k, a);
+        adj_inputs<<<bi, T, 0, s>>>(k, a);
         adj_sinks<true><<<bs, T, 0, s>>>(k, a);
     } else {
         adj_slopes<false><<<bw, T, 0, s>>>(k, a);
@@ -1039,10 +1442,10 @@ int stage_adjoint_impl(const cbd_grid_t *grid, const void *stage_dev, const doub
         sum_params<<<1, 32 * NPAR, 0, s>>>(parts, bf, NPAR, params_out);
         adj_zones<false><<<bw, T, 0, s>>>(k, a);
         sum_params<<<1, 32 * NPAR, 0, s>>>(parts, bw, NPAR, params_out);
+        adj_inputs<<<bi, T, 0, s>>>(k, a);
         adj_sinks<false><<<bs, T, 0, s>>>(k, a);
         sum_params<<<1, 32 * NPAR, 0, s>>>(parts, bs, NPAR, params_out);
     }
-    adj_inputs<<<bi, T, 0, s>>>(k, a);
     return cudaGetLastError() == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
 }
 
@@ -1146,6 +1549,14 @@ int cbdiso_b200_stage_adjoint_chained(const cbd_grid_t *grid, const void *stage_
         return CBD_ERR_ARGUMENT;
     return stage_adjoint_impl(grid, stage_dev, primitive_rd, primitive_n, primitive_out, nullptr, lam_out, lam_rd,
                               lam_n, jacobian, chain_acc, workspace, stream);
+}
+
+int cbdiso_b200_set_adjoint_variant(int fused)
+{
+    if (fused != 0 && fused != 1)
+        return CBD_ERR_ARGUMENT;
+    g_fused_adjoint = fused;
+    return CBD_OK;
 }
 
 size_t cbdiso_b200_adjoint_chain_blocks(const cbd_grid_t *grid)

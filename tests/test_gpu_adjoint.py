@@ -342,3 +342,66 @@ def test_batched_adjoint_matches_each_disk_alone():
         np.testing.assert_array_equal(j, J[i])
         np.testing.assert_array_equal(gs, grads[i][0])
         np.testing.assert_array_equal(gp, grads[i][1])
+
+
+def _stage_adjoint(s, dev, nb, stage, p, pn, out, lam, variant, chained):
+    lib = s._lib
+    g = ctypes.byref(s._grid)
+    _capi.check(lib.cbdiso_b200_set_adjoint_variant(variant), "variant")
+    try:
+        rec = ctypes.c_void_p(dev.data_ptr() + stage * nb)
+        lam_rd, lam_n = torch.zeros_like(p), torch.zeros_like(p)
+        ws = torch.zeros(int(lib.cbdiso_b200_adjoint_workspace_bytes(g)) // 8 + 8, dtype=torch.float64,
+                         device=p.device)
+        pnp = P(pn) if pn is not None else None
+        lnp = P(lam_n) if pn is not None else None
+        if chained:
+            rows = int(lib.cbdiso_b200_adjoint_chain_blocks(g))
+            chain = torch.zeros(rows * 4, dtype=torch.float64, device=p.device)
+            jac = torch.from_numpy(np.random.default_rng(5).uniform(-1, 1, 20)).to(p.device)
+            _capi.check(lib.cbdiso_b200_stage_adjoint_chained(g, rec, P(p), pnp, P(out), P(lam), P(lam_rd), lnp,
+                                                              P(jac), P(chain), P(ws), _stream()), "chained")
+            pars = torch.zeros(4, dtype=torch.float64, device=p.device)
+            _capi.check(lib.cbdiso_b200_adjoint_chain_finish(P(chain), rows, P(pars), _stream()), "finish")
+        else:
+            words = torch.zeros(p.shape[:2], dtype=torch.int32, device=p.device)
+            _capi.check(lib.cbdiso_b200_stage_record_branches(g, rec, P(p), P(out), P(words), _stream()), "rec")
+            pars = torch.zeros(12, dtype=torch.float64, device=p.device)
+            _capi.check(lib.cbdiso_b200_stage_adjoint(g, rec, P(p), pnp, P(out), P(words), P(lam), P(lam_rd), lnp,
+                                                      P(pars), P(ws), _stream()), "adjoint")
+        torch.cuda.synchronize()
+        return lam_rd.cpu().numpy(), lam_n.cpu().numpy(), pars.cpu().numpy()
+    finally:
+        lib.cbdiso_b200_set_adjoint_variant(1)
+
+
+@pytest.fixture(scope="module")
+def wide_case():
+    """256^2 (three column strips of the fused kernel, several row segments)."""
+    run = AdjointRun(resolution=256, steps=1)
+    params = Params(0.6, 0.2, 2e-3, 10.0)
+    s = _state(run, params, steps=2)
+    dt = 0.8 * s.mesh.min_spacing() / s.maximum_wavespeed() * 0.3
+    dev, nb, _ = run._records(s, s.time, dt)
+    return s, dev, nb
+
+
+@pytest.mark.parametrize("chained", [False, True])
+@pytest.mark.parametrize("stage", [0, 1])
+@pytest.mark.parametrize("case", ["stage_case", "wide_case"])
+def test_fused_stage_adjoint_matches_the_separate_passes(request, case, stage, chained):
+    """The row-marching adjoint kernel gives the separate passes' lambda_rd and
+    lambda_n bit for bit; the parameter sums (added in another order) to
+    rounding."""
+    c = request.getfixturevalue(case)
+    s, dev, nb = (c[2], c[3], c[4]) if case == "stage_case" else c
+    p = s._buf[0]
+    pn = p.clone() if stage == 1 else None
+    out = _stage(s, dev, stage * nb, 0.5 * stage, p, pn)
+    lam = torch.zeros_like(p)
+    lam[2:-2, 2:-2] = _rand_like(lam[2:-2, 2:-2], 31 + stage)
+    a = _stage_adjoint(s, dev, nb, stage, p, pn, out, lam, 0, chained)
+    b = _stage_adjoint(s, dev, nb, stage, p, pn, out, lam, 1, chained)
+    np.testing.assert_array_equal(b[0], a[0])
+    np.testing.assert_array_equal(b[1], a[1])
+    np.testing.assert_allclose(b[2], a[2], rtol=1e-12, atol=1e-12 * np.abs(a[2]).max())
