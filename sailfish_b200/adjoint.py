@@ -40,6 +40,7 @@ from typing import NamedTuple, Optional
 import numpy as np
 
 from . import _capi
+from ._graphs import capture
 from .cbdiso_2d import NG, NQ, Solver, initial_condition
 from .kepler import OrbitalElements
 from .setups import CircumbinaryDisk
@@ -154,6 +155,19 @@ class AdjointRun:
         prim[..., 0] += 1e-3 * np.random.default_rng(seed).uniform(-1.0, 1.0, size=(self.n, self.n))
         return prim
 
+    def _forward_solver(self, params, prim0):
+        """The solver of forward runs, kept while the parameters stay (its
+        buffers, and the CUDA graphs recorded on them, are reused)."""
+        key = tuple(float(v) for v in params)
+        cached = getattr(self, "_fwd_solver", None)
+        if cached is not None and cached[0] == key:
+            cached[1].reset(prim0, 0.0)
+            return cached[1]
+        self._fwd_solver = None
+        s = self._solver(params, prim0)
+        self._fwd_solver = (key, s)
+        return s
+
     def _solver(self, params, prim0):
         setup = self.setup(params)
         mesh = setup.mesh(self.n)
@@ -173,10 +187,13 @@ class AdjointRun:
         """
         import torch
 
-        s = self._solver(params, prim0)
+        s = self._forward_solver(params, prim0)
         steps, K = self.steps, self.checkpoint_every
         fresh = self.dts is None or freeze
-        dts_dev = None if fresh else torch.from_numpy(np.ascontiguousarray(self.dts)).to(s.device)
+        dts_dev = None
+        if not fresh:
+            dts_dev = self._kept("_dts_dev", (steps,), torch.float64, s.device)
+            dts_dev.copy_(torch.from_numpy(np.ascontiguousarray(self.dts)))
         nb = int(self._lib.cbdiso_b200_stage_record_bytes())
         history = self._kept("_history", (steps * 2 * nb,), torch.uint8, s.device) if keep else None
         t_start = s.time
@@ -472,7 +489,7 @@ class _ReverseSweep:
             side.wait_stream(torch.cuda.current_stream())
             graph = torch.cuda.CUDAGraph()
             # capture records the launches without running them
-            with torch.cuda.graph(graph, stream=side):
+            with capture(graph, side):
                 self.run(self.hist, self.jac, self.k)
             torch.cuda.current_stream().wait_stream(side)
             self.graph = graph
@@ -492,7 +509,7 @@ class _ReverseSweep:
             side = torch.cuda.Stream()
             side.wait_stream(torch.cuda.current_stream())
             graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(graph, stream=side):
+            with capture(graph, side):
                 self.run(hist, self._stored_jac, count, states=states)
             torch.cuda.current_stream().wait_stream(side)
             self._stored_graph, self._stored_key = graph, key
@@ -561,7 +578,10 @@ class BatchedAdjoint:
         import torch
 
         if self._streams is None:
-            self._streams = [torch.cuda.Stream() for _ in range(self.num_streams)]
+            # torch hands out pooled streams round-robin; the workers take theirs
+            # from the high-priority pool so that no graph capture (whose side
+            # streams come from the default pool) can land on a worker's stream
+            self._streams = [torch.cuda.Stream(priority=-1) for _ in range(self.num_streams)]
         device = torch.cuda.current_device()
         out = [None] * len(self.disks)
         errors = []
@@ -596,10 +616,8 @@ class BatchedAdjoint:
 
     def gradient(self, weights=(1.0, 0.0)):
         """(dJ/dprim0, dJ/d(q, e, nu, sink_rate)) of every disk, after
-        forward(keep=True). No CUDA graphs here: a capture in one host thread
-        does not admit the device-wide synchronisation another thread's
-        capture starts with."""
-        return self._each(lambda i: self.runs[i].gradient(weights, graph=False))
+        forward(keep=True)."""
+        return self._each(lambda i: self.runs[i].gradient(weights))
 
 
 def config4_disks(num=32, seed=4096, sizes=(256, 512)):

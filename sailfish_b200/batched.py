@@ -25,6 +25,7 @@ from typing import List, NamedTuple, Optional, Sequence
 import numpy as np
 
 from . import _capi
+from ._graphs import capture
 from .cbdiso_2d import COMPLEX_QUANTITIES, NG, NQ, RK_WEIGHTS, Options, Solver, _diag_struct
 from .physics import Diagnostic, Physics, enum_value
 
@@ -223,7 +224,7 @@ class BatchedSolver:
                 side = torch.cuda.Stream()
                 side.wait_stream(torch.cuda.current_stream())
                 g = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(g, stream=side):
+                with capture(g, side):
                     for _ in range(steps_per_graph):
                         self._one_step(nvals)
                 torch.cuda.current_stream().wait_stream(side)

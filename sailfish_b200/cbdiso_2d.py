@@ -35,6 +35,7 @@ from typing import NamedTuple, Optional
 import numpy as np
 
 from . import _capi
+from ._graphs import capture
 from .mesh import is_planar_cartesian_2d
 from .physics import Diagnostic, Physics, enum_value
 from .solver_base import SolverBase
@@ -503,8 +504,23 @@ class Solver(SolverBase):
                     trajectory.dtype != self._buf[0].dtype or not trajectory.is_contiguous():
                 raise ValueError("trajectory must hold 2 * steps + 1 padded float64 states")
             trajectory[0].copy_(self._buf[0])
-            for n in range(steps):
-                one_step(n)
+            if graph:
+                # one graph for the whole run: every step writes its own slots
+                key = ("trajectory", steps, trajectory.data_ptr(), nvals)
+                cuda_graph = self._graphs.get(key)
+                if cuda_graph is None:
+                    side = torch.cuda.Stream()
+                    side.wait_stream(torch.cuda.current_stream())
+                    cuda_graph = torch.cuda.CUDAGraph()
+                    with capture(cuda_graph, side):
+                        for n in range(steps):
+                            one_step(n)
+                    torch.cuda.current_stream().wait_stream(side)
+                    self._graphs[key] = cuda_graph
+                cuda_graph.replay()
+            else:
+                for n in range(steps):
+                    one_step(n)
             self._buf[0].copy_(trajectory[2 * steps])
             remaining = 0
         if graph and remaining >= steps_per_graph:
@@ -515,7 +531,7 @@ class Solver(SolverBase):
                 side = torch.cuda.Stream()
                 side.wait_stream(torch.cuda.current_stream())
                 cuda_graph = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(cuda_graph, stream=side):
+                with capture(cuda_graph, side):
                     for _ in range(steps_per_graph):
                         one_step()
                 torch.cuda.current_stream().wait_stream(side)
@@ -613,6 +629,22 @@ class Solver(SolverBase):
             self._buf[0], self._buf[1] = B, A
         if self._step_hook is not None:
             self._step_hook()
+
+    def reset(self, solution, time=0.0):
+        """Start again from `solution` (host (ni, nj, 3)) at `time`, keeping
+        the device buffers (and the CUDA graphs that refer to them)."""
+        import torch
+
+        primitive = np.asarray(solution, dtype=np.float64)
+        ni, nj = self._grid.ni, self._grid.nj
+        if primitive.shape != (ni, nj, NQ):
+            raise ValueError(f"solution has shape {primitive.shape}, expected {(ni, nj, NQ)}")
+        self._buf[0][NG:-NG, NG:-NG] = torch.from_numpy(primitive).to(self.device)
+        self._check(self._lib.cbdiso_b200_fill_guards(ctypes.byref(self._grid), self._ptr(self._buf[0]),
+                                                      self._stream()), "fill_guards")
+        self._time = float(time)
+        self._cached = None
+        self._result_valid = False
 
     # hooks of the multi-GPU solver (distributed.py)
 
