@@ -377,6 +377,9 @@ def adjoint_extra():
     prim = run.initial_state(seed=0)
     run.forward(prim, params, freeze=True, keep=True)
     run.gradient((1.0, 0.0))
+    # warm-up with the frozen dt sequence (records this form's CUDA graphs)
+    run.forward(prim, params, keep=True)
+    run.gradient((1.0, 0.0))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     run.forward(prim, params, keep=True)
@@ -413,6 +416,9 @@ def batched_adjoint_extra():
     disks = config4_disks(32)
     batch = BatchedAdjoint(disks, steps=200, streams=8)
     batch.forward(freeze=True, keep=True)
+    batch.gradient((1.0, 0.0))
+    # warm-up with the frozen dt sequences (records this form's CUDA graphs)
+    batch.forward(keep=True)
     batch.gradient((1.0, 0.0))
     torch.cuda.synchronize()
     t0 = time.perf_counter()

@@ -1349,7 +1349,9 @@ int adj_rows(const cbd_grid_t *grid)
 
 int pass_blocks(long items) { return items > 0 ? (int)((items + ADJ_THREADS - 1) / ADJ_THREADS) : 1; }
 
-constexpr int SINK_PASS_BLOCKS = 16;
+// grid-stride over the sink boxes' (zone, direction) items: about one pass at
+// 2048^2 (a box of ~3k zones per mass); never more than the accumulator rows
+constexpr int SINK_PASS_BLOCKS = 148;
 
 // the fused row-marching stage adjoint (default) or the separate passes
 int g_fused_adjoint = 1;
@@ -1409,7 +1411,7 @@ int stage_adjoint_impl(const cbd_grid_t *grid, const void *stage_dev, const doub
         a.par = params_out;
     const long wide = (long)(ni + 2) * (nj + 2);
     const int bw = pass_blocks(wide), bf = pass_blocks(2 * wide), bi = pass_blocks((long)ni * nj);
-    const int bs = SINK_PASS_BLOCKS;
+    const int bs = adj_rows(grid) < SINK_PASS_BLOCKS ? adj_rows(grid) : SINK_PASS_BLOCKS;
     constexpr int T = ADJ_THREADS;
     if (g_fused_adjoint) {
         const dim3 grid = march_grid(ni, nj);
@@ -1461,7 +1463,8 @@ int objective_adjoint_impl(const cbd_grid_t *grid, const void *stage_dev, const 
     a.p = primitive;
     a.lam_rd = lam;
     double *parts = a.par;
-    const int bz = pass_blocks((long)grid->ni * grid->nj), bs = SINK_PASS_BLOCKS;
+    const int bz = pass_blocks((long)grid->ni * grid->nj);
+    const int bs = adj_rows(grid) < SINK_PASS_BLOCKS ? adj_rows(grid) : SINK_PASS_BLOCKS;
     constexpr int T = ADJ_THREADS;
     if (jac) {
         a.par = params_out;
