@@ -7,6 +7,8 @@
 #   libref_t18_omp.so  theta = 1.8, OpenMP
 #   libref_t15_cpu.so  theta = 1.5 (line `#define PLM_THETA 1.8` rewritten
 #   libref_t15_omp.so  on the fly, as a solver option would), serial / OpenMP
+#   libref_gam_cpu.so  the gamma-law kernels (sailfish/solvers/cbdgam_2d.c,
+#   libref_gam_omp.so  theta 1.5 as written), serial / OpenMP
 #
 # Flags mirror what cffi uses for sailfish's JIT build (-O2 -fwrapv, plus
 # -fopenmp -std=c99 in omp mode; sailfish/kernel/system.py:78-81). The
@@ -32,4 +34,13 @@ for theta in 1.8 1.5; do
     done
 done
 grep -q "^#define PLM_THETA 1\.8$" "$src" || { echo "build_ref.sh: PLM_THETA line not found" >&2; exit 1; }
+# the gamma-law kernels (sailfish/solvers/cbdgam_2d.c, theta 1.5 as written)
+gsrc="$ref_root/sailfish/solvers/cbdgam_2d.c"
+if [[ -f "$gsrc" ]]; then
+    for mode in cpu omp; do
+        if [[ $mode == omp ]]; then flags="-DEXEC_MODE=1 -fopenmp -std=c99"; else flags="-DEXEC_MODE=0"; fi
+        $cc -O2 -fwrapv -fPIC -shared $flags -include "$here/ref_macros.h" -x c "$gsrc" \
+            -o "$out/libref_gam_${mode}.so" -lm
+    done
+fi
 echo "built reference kernels into $out"

@@ -18,10 +18,16 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def golden_names():
-    """The solver-run fixtures (make_golden.py); the checkpoint fixtures
-    (chkpt_*, make_checkpoint.py) have their own tests."""
+    """The isothermal solver-run fixtures (make_golden.py); the gamma-law ones
+    (gam_*) and the checkpoint fixtures (chkpt_*, make_checkpoint.py) have
+    their own tests."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith("chkpt_"))
+                  if not os.path.basename(p).startswith(("chkpt_", "gam_")))
+
+
+def gam_names():
+    """The gamma-law (cbdgam_2d) solver-run fixtures."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "gam_*.npz")))
 
 
 def load(name):
@@ -99,3 +105,64 @@ def diagnostics(meta):
             d["radial_cut"] = tuple(d["radial_cut"])
         out.append(d)
     return out
+
+
+GAM_DEFAULTS = dict(domain_radius=12.0, eccentricity=0.0, mass_ratio=1.0, sink_rate=10.0, sink_radius=0.05,
+                    softening_length=0.05, buffer_is_enabled=True, sink_model="torque_free", initial_sigma=1.0,
+                    initial_pressure=1e-2, cooling_coefficient=0.0, alpha=0.1, constant_softening=True,
+                    gamma_law_index=5.0 / 3.0)
+
+
+def gam_oracle_config(meta):
+    """Gamma-law oracle configuration for one golden case: the physics the
+    gamma-law CircumbinaryDisk hands to cbdgam_2d (circumbinary_disk.py:137-152)
+    and the buffer state sampled at the onset radius (cbdgam_2d.py:291-303)."""
+    from oracle import host_gam as og
+
+    x0, y0, x1, y1, ni, nj = meta["mesh"]
+    p = dict(GAM_DEFAULTS, **meta["params"])
+    onset = 0.1
+    bs, _, _, bp = og.gamma_disk_primitive(x1 - onset, 0.0, p["softening_length"], p["initial_sigma"],
+                                           p["initial_pressure"])
+    on = p["buffer_is_enabled"]
+    return og.GamConfig(
+        x0=x0, x1=x1, y0=y0, y1=y1, ni=int(ni), nj=int(nj), gamma_law_index=p["gamma_law_index"],
+        alpha=p["alpha"], cooling_coefficient=p["cooling_coefficient"], constant_softening=p["constant_softening"],
+        buffer_is_enabled=on, buffer_driving_rate=1000.0, buffer_onset_width=onset,
+        buffer_surface_density=bs if on else 0.0, buffer_surface_pressure=bp if on else 0.0,
+        masses=oh.binary_masses(1.0, 1.0, p["mass_ratio"], p["eccentricity"], p["softening_length"],
+                                p["sink_model"], p["sink_rate"], p["sink_radius"]),
+        plm_theta=meta["theta"])
+
+
+def gam_initial_data(meta):
+    """The gamma-law CircumbinaryDisk's initial data on the fixture's mesh,
+    zone by zone through the oracle's restatement."""
+    from oracle import host_gam as og
+
+    x0, y0, x1, y1, ni, nj = meta["mesh"]
+    ni, nj = int(ni), int(nj)
+    p = dict(GAM_DEFAULTS, **meta["params"])
+    dx, dy = (x1 - x0) / ni, (y1 - y0) / nj
+    out = np.empty((ni, nj, 4))
+    for i in range(ni):
+        for j in range(nj):
+            out[i, j] = og.gamma_disk_primitive(x0 + (i + 0.5) * dx, y0 + (j + 0.5) * dy, p["softening_length"],
+                                                p["initial_sigma"], p["initial_pressure"])
+    return out
+
+
+def gam_initial_state(data):
+    """A gamma-law fixture's starting state: setup data times (1 + seeded noise).
+    Fixtures stored subsampled get their initial data rebuilt (and checked
+    against the stored subsample)."""
+    meta = data["meta"]
+    prim = np.array(data["ic"], dtype=np.float64)
+    if prim.shape[0] != int(meta["mesh"][4]):
+        full = gam_initial_data(meta)
+        assert np.array_equal(full[::8, ::8], prim)
+        prim = full
+    if meta["seed"] is not None:
+        ni, nj = prim.shape[:2]
+        prim[..., 0] *= 1.0 + oh.seeded_noise(ni, nj, meta["seed"])
+    return prim

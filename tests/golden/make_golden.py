@@ -1,6 +1,7 @@
 """
 Generates the golden fixtures in this directory by running the reference
-sailfish cbdiso_2d solver itself (CPU mode, its own cffi-built kernels).
+sailfish cbdiso_2d and cbdgam_2d solvers themselves (CPU mode, their own
+cffi-built kernels).
 
 Usage (needs the reference tree, by default at /root/reference, or set
 REFERENCE_ROOT):
@@ -50,6 +51,15 @@ FORCE_DIAG = [
     dict(quantity="mass"),
     dict(quantity="power", which_mass=1, gravity=True),
     dict(quantity="power", which_mass=2, gravity=True),
+]
+GAM_DIAG = [
+    dict(quantity="time"),
+    dict(quantity="mdot", which_mass=1, accretion=True),
+    dict(quantity="mdot", which_mass=2, accretion=True),
+    dict(quantity="torque", which_mass="both", gravity=True),
+    dict(quantity="torque", which_mass=1, gravity=True, radial_cut=(1.0, 4.0)),
+    dict(quantity="sigma_m1"),
+    dict(quantity="eccentricity_vector", radial_cut=(1.0, 4.0)),
 ]
 CBD_DIAG = [
     dict(quantity="time"),
@@ -106,6 +116,28 @@ CASES = {
     "explosion_t15_n40": dict(
         setup="cylindrical-explosion", theta=1.5, resolution=40, steps=10, seed=None, patches=1, rk=2,
         params=dict(), diagnostics=[dict(quantity="time"), dict(quantity="mass")]),
+    # gamma-law (cbdgam_2d, theta 1.5 as the reference fixes it): alpha viscosity, constant softening
+    "gam_n64": dict(
+        setup="circumbinary-disk", solver="cbdgam_2d", noise="relative", theta=1.5, resolution=64, steps=20, seed=11, patches=1,
+        cfl=0.1, params=dict(eos="gamma-law", domain_radius=8.0, mass_ratio=1.0, eccentricity=0.0, alpha=0.1),
+        diagnostics=CBD_DIAG),
+    # eccentric, unequal, cooling, acceleration-free sinks, two patches, all four gamma-law diagnostics
+    "gam_n48_cool_p2": dict(
+        setup="circumbinary-disk", solver="cbdgam_2d", noise="relative", theta=1.5, resolution=48, steps=15, seed=12, patches=2,
+        cfl=0.1, params=dict(eos="gamma-law", domain_radius=6.0, mass_ratio=0.5, eccentricity=0.3, alpha=0.05,
+                             cooling_coefficient=10.0, sink_model="acceleration_free"),
+        diagnostics=GAM_DIAG),
+    # softening that follows the disk height, force-free sinks, inviscid, no buffer
+    "gam_n40_soft_inviscid": dict(
+        setup="circumbinary-disk", solver="cbdgam_2d", noise="relative", theta=1.5, resolution=40, steps=12, seed=13, patches=1,
+        cfl=0.1, params=dict(eos="gamma-law", domain_radius=4.0, mass_ratio=0.8, eccentricity=0.1, alpha=0.0,
+                             constant_softening=False, sink_model="force_free", buffer_is_enabled=False),
+        diagnostics=GAM_DIAG),
+    # 256^2, 60 steps (state stored subsampled)
+    "gam_n256": dict(
+        setup="circumbinary-disk", solver="cbdgam_2d", noise="relative", theta=1.5, resolution=256, steps=60, seed=14, patches=1,
+        cfl=0.1, params=dict(eos="gamma-law", domain_radius=8.0, mass_ratio=1.0, eccentricity=0.0, alpha=0.1),
+        diagnostics=CBD_DIAG, store="subsample8"),
     # config 0 as stated: 256^2, theta = 1.5, 100 steps (state stored subsampled, see `store`)
     "config0_t15_n256": dict(
         setup="circumbinary-disk", theta=1.5, resolution=256, steps=100, seed=0, patches=1, rk=2,
@@ -141,22 +173,31 @@ def run_case(name, out_path):
         else:
             mesh = setup.mesh(case["resolution"])
         ni, nj = mesh.shape
-        ic = np.zeros((ni, nj, 3))
+        solver_name = case.get("solver", "cbdiso_2d")
+        nq = 4 if solver_name == "cbdgam_2d" else 3
+        ic = np.zeros((ni, nj, nq))
         for i in range(ni):
             for j in range(nj):
                 setup.primitive(0.0, mesh.cell_coordinates(i, j), ic[i, j])
         prim = ic.copy()
         if case["seed"] is not None:
             rng = np.random.default_rng(case["seed"])
-            prim[..., 0] += 1e-3 * rng.uniform(-1.0, 1.0, size=(ni, nj))
+            noise = 1e-3 * rng.uniform(-1.0, 1.0, size=(ni, nj))
+            if case.get("noise") == "relative":
+                # the gamma-law disk's cavity density (~1e-4) is below the absolute amplitude
+                prim[..., 0] *= 1.0 + noise
+            else:
+                prim[..., 0] += noise
         physics = setup.physics
         physics["diagnostics"] = case["diagnostics"]
+        options = dict(rk_order=case["rk"]) if solver_name == "cbdiso_2d" else dict()
         solver = make_solver(
-            "cbdiso_2d", physics, dict(rk_order=case["rk"]), setup=setup, mesh=mesh, time=0.0, solution=prim,
+            solver_name, physics, options, setup=setup, mesh=mesh, time=0.0, solution=prim,
             num_patches=case["patches"], mode="cpu")
+        cfl = case.get("cfl", 0.3)
         dts, series, first = [], [], None
         for n in range(case["steps"]):
-            dt = mesh.min_spacing(0.0) / solver.maximum_wavespeed() * 0.3
+            dt = mesh.min_spacing(0.0) / solver.maximum_wavespeed() * cfl
             solver.advance(dt)
             dts.append(dt)
             series.append([complex(v) for v in solver.reductions()])
@@ -164,12 +205,12 @@ def run_case(name, out_path):
                 first = solver.solution
         last = solver.solution
         ws = solver.maximum_wavespeed()
-        meta = dict(case, name=name, mesh=list(mesh), cfl=0.3)
+        meta = dict(case, name=name, mesh=list(mesh), cfl=cfl, rk=case.get("rk", 2))
         out = dict(meta=json.dumps(meta), ic=ic, dts=np.array(dts), series=np.array(series, dtype=complex),
                    max_wavespeed=np.float64(ws), time=np.float64(solver.time))
         if case.get("store") == "subsample8":
             out.update(first_sub=first[::8, ::8], last_sub=last[::8, ::8],
-                       last_sums=np.array([last[..., q].sum() for q in range(3)]),
+                       last_sums=np.array([last[..., q].sum() for q in range(nq)]),
                        ic=ic[::8, ::8])
         else:
             out.update(first=first, last=last)
