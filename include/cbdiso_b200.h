@@ -19,6 +19,9 @@
  *     the next step's CFL wavespeed and the diagnostics reductions fused in;
  *     plus the batched many-disk form and the tangent / adjoint kernels.
  *
+ *  3. The gamma-law sibling, cbdgam_2d: its four drop-in kernels
+ *     (sailfish/solvers/cbdgam_2d.c) and a product stage with fused guards.
+ *
  * Arrays use the reference layout: C-contiguous (ni + 4, nj + 4, 3) float64,
  * two guard zones per side, j fastest, then the field (Sigma, vx, vy) or
  * (Sigma, Sigma vx, Sigma vy).
@@ -390,6 +393,114 @@ int cbdiso_b200_reduce(
  * elements: out[4i] = a/b, out[4i+1] = a^-1.5, out[4i+2] = a^4,
  * out[4i+3] = PLM slope of (a, b, a + b) with theta 1.5. */
 int cbdiso_b200_eval_primitives(long n, const double *a, const double *b, double *out, void *stream);
+
+/* ------------------------------------------------------------------------
+ * 3. the gamma-law sibling, cbdgam_2d (sailfish/solvers/cbdgam_2d.c)
+ *
+ * Arrays: C-contiguous (ni + 4, nj + 4, 4) float64, fields (Sigma, vx, vy,
+ * pressure) or (Sigma, Sigma vx, Sigma vy, energy). Arithmetic is the
+ * reference's, operation for operation and without FMA contraction; results
+ * differ from a CPU build only where CUDA's pow / exp round differently.
+ * ---------------------------------------------------------------------- */
+
+/* Drop-in kernels: the reference's symbol names and positional arguments,
+ * DEVICE pointers, the library's current stream, an int status. */
+
+/* replaces cbdgam_2d_advance_rk, sailfish/solvers/cbdgam_2d.c:439-683
+ * (writes the interior of primitive_wr; theta from cbdgam_b200_set_plm_theta) */
+int cbdgam_2d_advance_rk(int ni, int nj, double patch_xl, double patch_xr, double patch_yl, double patch_yr,
+                         double *conserved_rk, double *primitive_rd, double *primitive_wr, double gamma_law_index,
+                         double buffer_surface_density, double buffer_surface_pressure, double buffer_central_mass,
+                         double buffer_driving_rate, double buffer_outer_radius, double buffer_onset_width,
+                         int buffer_is_enabled, double x1, double y1, double vx1, double vy1, double mass1,
+                         double softening_length1, double sink_rate1, double sink_radius1, int sink_model1, double x2,
+                         double y2, double vx2, double vy2, double mass2, double softening_length2,
+                         double sink_rate2, double sink_radius2, int sink_model2, double alpha, double a, double dt,
+                         double velocity_ceiling, double cooling_coefficient, double mach_ceiling,
+                         double density_floor, double pressure_floor, int constant_softening);
+
+/* replaces cbdgam_2d_wavespeed, sailfish/solvers/cbdgam_2d.c:685-708 */
+int cbdgam_2d_wavespeed(int ni, int nj, double *primitive, double *wavespeed, double gamma_law_index);
+
+/* replaces cbdgam_2d_primitive_to_conserved, sailfish/solvers/cbdgam_2d.c:710-729 */
+int cbdgam_2d_primitive_to_conserved(int ni, int nj, double *primitive, double *conserved, double gamma_law_index);
+
+/* replaces cbdgam_2d_point_mass_source_term, sailfish/solvers/cbdgam_2d.c:731-784 */
+int cbdgam_2d_point_mass_source_term(int ni, int nj, double patch_xl, double patch_xr, double patch_yl,
+                                     double patch_yr, double x1, double y1, double vx1, double vy1, double mass1,
+                                     double softening_length1, double sink_rate1, double sink_radius1,
+                                     int sink_model1, double x2, double y2, double vx2, double vy2, double mass2,
+                                     double softening_length2, double sink_rate2, double sink_radius2,
+                                     int sink_model2, int which_mass, double *primitive, double *cons_rate,
+                                     int constant_softening, double gamma_law_index);
+
+/* PLM theta of the gamma-law drop-in kernels, in [1, 2]; default 1.5 as in
+ * sailfish/solvers/cbdgam_2d.c:15. Process-wide. */
+int cbdgam_b200_set_plm_theta(double theta);
+
+/* Mesh, equation of state, physics and options of a gamma-law run
+ * (cbdgam_2d.py:23-27 Options; the Physics fields it reads). */
+typedef struct cbdgam_grid {
+    int ni, nj;
+    double xl, xr, yl, yr;  /* patch extent (vertex coordinates) */
+    double plm_theta;
+    double gamma_law_index;
+    double alpha;
+    double cooling_coefficient;
+    double mach_ceiling;
+    double velocity_ceiling;
+    double density_floor;
+    double pressure_floor;
+    int constant_softening;
+    int buffer_is_enabled;
+    double buffer_surface_density;
+    double buffer_surface_pressure;
+    double buffer_driving_rate;
+    double buffer_outer_radius;
+    double buffer_onset_width;
+} cbdgam_grid_t;
+
+typedef struct cbdgam_stage {
+    cbd_mass_t mass[2];          /* point masses at the stage's start time */
+    double buffer_central_mass;  /* m1 + m2 */
+    double a;                    /* RK weight of u_n */
+    double dt;
+} cbdgam_stage_t;
+
+/* One RK stage of the product path (cbdgam_2d.c:439-683 with
+ * cbdgam_2d.py:473-520): u_n is rebuilt in the kernel from primitive_n
+ * (null when a = 0: u_n is then the state read, as in the reference's first
+ * stage) and the zero-gradient guard zones of primitive_wr are written with
+ * its edge zones. primitive_wr may be primitive_n (each zone reads only its
+ * own u_n); it must not be primitive_rd. wavespeed_max (device, may be null):
+ * the largest signal speed of the written state is max-ed into it, so the
+ * caller zeroes it first; a NaN state leaves a NaN there. */
+int cbdgam_b200_advance_stage(const cbdgam_grid_t *grid, const cbdgam_stage_t *stage, const double *primitive_rd,
+                              const double *primitive_n, double *primitive_wr, double *wavespeed_max, void *stream);
+
+/* Writes the zero-gradient guard zones of a state from its edge zones
+ * (cbdgam_2d.py:491-520 on one patch). */
+int cbdgam_b200_fill_guards(const cbdgam_grid_t *grid, double *primitive, void *stream);
+
+/* The CFL wavespeed maximum and up to 4 diagnostic sums (cbdgam_2d.py:
+ * 341-447: mdot, torque, sigma_m1, eccentricity_vector, with radial cuts) on
+ * a state, with point masses `masses[2]`. mdot and torque take the
+ * accretion rates when the diagnostic's accretion flag is set, else the
+ * gravity rates (the gravity flag must then be set). result[0] = max
+ * wavespeed, result[1 + 2k], result[2 + 2k] = real and imaginary part of
+ * sum_cells f_k (not multiplied by dx dy); the summation order is fixed.
+ * scratch: cbdgam_b200_scratch_bytes(grid) bytes of device memory. */
+size_t cbdgam_b200_scratch_bytes(const cbdgam_grid_t *grid);
+int cbdgam_b200_reduce(const cbdgam_grid_t *grid, const cbd_mass_t *masses, const cbd_diag_t *diags, int num_diags,
+                       const double *primitive, double *scratch, double *result, void *stream);
+
+/* sizeof of cbdgam_grid_t and cbdgam_stage_t, for bindings to check. */
+void cbdgam_b200_abi_sizes(size_t out[2]);
+
+/* Test hook (no counterpart in the reference): the correctly rounded powers
+ * the gamma-law kernels use, on device arrays of n elements: out[8i + 0..6]
+ * = x^3, x^-2, x^-3, x^4, x^-1.5, (1 + x)^RN(-1/3), exp(-x); out[8i + 7] = 0. */
+int cbdgam_b200_eval_powers(long n, const double *x, double *out, void *stream);
 
 #ifdef __cplusplus
 }

@@ -73,6 +73,27 @@ class Epilogue(Structure):
     _fields_ = [("mass", Mass * 2), ("want_wavespeed", c_int), ("num_diag", c_int), ("diag", Diag * MAX_DIAG)]
 
 
+class GamGrid(Structure):
+    """cbdgam_grid_t: a gamma-law run's mesh, physics and options."""
+
+    _fields_ = [("ni", c_int), ("nj", c_int), ("xl", c_double), ("xr", c_double), ("yl", c_double),
+                ("yr", c_double), ("plm_theta", c_double), ("gamma_law_index", c_double), ("alpha", c_double),
+                ("cooling_coefficient", c_double), ("mach_ceiling", c_double), ("velocity_ceiling", c_double),
+                ("density_floor", c_double), ("pressure_floor", c_double), ("constant_softening", c_int),
+                ("buffer_is_enabled", c_int), ("buffer_surface_density", c_double),
+                ("buffer_surface_pressure", c_double), ("buffer_driving_rate", c_double),
+                ("buffer_outer_radius", c_double), ("buffer_onset_width", c_double)]
+
+
+class GamStage(Structure):
+    """cbdgam_stage_t: what changes per gamma-law RK stage."""
+
+    _fields_ = [("mass", Mass * 2), ("buffer_central_mass", c_double), ("a", c_double), ("dt", c_double)]
+
+
+GAM_MAX_DIAG = 4
+
+
 _lib = None
 _DP = POINTER(c_double)
 
@@ -149,6 +170,26 @@ def _declare(lib):
         f = getattr(lib, name)
         f.argtypes = args
         f.restype = c_int
+    m9 = [D] * 8 + [I]
+    for name, args in {
+        "cbdgam_2d_advance_rk": [I, I, D, D, D, D, V, V, V, D, D, D, D, D, D, D, I] + m9 + m9
+        + [D, D, D, D, D, D, D, D, I],
+        "cbdgam_2d_wavespeed": [I, I, V, V, D],
+        "cbdgam_2d_primitive_to_conserved": [I, I, V, V, D],
+        "cbdgam_2d_point_mass_source_term": [I, I, D, D, D, D] + m9 + m9 + [I, V, V, I, D],
+        "cbdgam_b200_set_plm_theta": [D],
+        "cbdgam_b200_advance_stage": [POINTER(GamGrid), POINTER(GamStage), V, V, V, V, V],
+        "cbdgam_b200_fill_guards": [POINTER(GamGrid), V, V],
+        "cbdgam_b200_reduce": [POINTER(GamGrid), POINTER(Mass), POINTER(Diag), c_int, V, V, V, V],
+        "cbdgam_b200_eval_powers": [ctypes.c_long, V, V, V],
+    }.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = c_int
+    lib.cbdgam_b200_scratch_bytes.argtypes = [POINTER(GamGrid)]
+    lib.cbdgam_b200_scratch_bytes.restype = c_size_t
+    lib.cbdgam_b200_abi_sizes.argtypes = [POINTER(c_size_t)]
+    lib.cbdgam_b200_abi_sizes.restype = None
     lib.cbdiso_b200_abi_sizes.argtypes = [POINTER(c_size_t)]
     lib.cbdiso_b200_abi_sizes.restype = None
     lib.cbdiso_b200_status_string.argtypes = [c_int]
@@ -189,11 +230,18 @@ def exported_symbols():
         "cbdiso_b200_stepper_attach", "cbdiso_b200_stage_adjoint_chained", "cbdiso_b200_objective_adjoint_chained",
         "cbdiso_b200_adjoint_chain_finish", "cbdiso_b200_adjoint_chain_blocks",
         "cbdiso_b200_set_adjoint_variant",
+        "cbdgam_2d_advance_rk", "cbdgam_2d_wavespeed", "cbdgam_2d_primitive_to_conserved",
+        "cbdgam_2d_point_mass_source_term", "cbdgam_b200_set_plm_theta", "cbdgam_b200_advance_stage",
+        "cbdgam_b200_fill_guards", "cbdgam_b200_scratch_bytes", "cbdgam_b200_reduce", "cbdgam_b200_abi_sizes",
+        "cbdgam_b200_eval_powers",
     ]
 
 
 def abi_sizes():
-    """(C sizes, ctypes sizes) of the four public structs."""
+    """(C sizes, ctypes sizes) of the public structs: cbd_mass_t,
+    cbd_grid_t, cbd_stage_t, cbd_epilogue_t, cbdgam_grid_t, cbdgam_stage_t."""
     out = (c_size_t * 4)()
     lib().cbdiso_b200_abi_sizes(out)
-    return list(out), [ctypes.sizeof(t) for t in (Mass, Grid, Stage, Epilogue)]
+    gam = (c_size_t * 2)()
+    lib().cbdgam_b200_abi_sizes(gam)
+    return list(out) + list(gam), [ctypes.sizeof(t) for t in (Mass, Grid, Stage, Epilogue, GamGrid, GamStage)]

@@ -180,6 +180,9 @@ int cbd::set_diagnostics(Consts &k, const cbd_epilogue_t *ep, int first, int cou
     return CBD_OK;
 }
 
+namespace cbd {
+cudaStream_t drop_in_stream() { return g_stream; }
+}  // namespace cbd
 
 extern "C" {
 

@@ -26,4 +26,7 @@ cudaError_t launch_stage_fast(const LaunchShape &s, const Consts &k, const Stage
 Consts consts_from_grid(const cbd_grid_t *g);
 int set_diagnostics(Consts &k, const cbd_epilogue_t *ep, int first, int count);
 
+// The stream the drop-in kernels launch on (cbdiso_b200_set_stream).
+cudaStream_t drop_in_stream();
+
 }  // namespace cbd

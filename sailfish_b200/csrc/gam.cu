@@ -1,0 +1,1010 @@
+// The gamma-law circumbinary-disk stage (cbdgam_2d): the reference's
+// energy-equation sibling of cbdiso_2d (sailfish/solvers/cbdgam_2d.c), with
+// four fields (sigma, vx, vy, pressure), alpha viscosity with the disk's
+// scale height, softening that may follow the scale height, cooling, a
+// pressure floor and a Mach ceiling.
+//
+// Built with -fmad=false: every +, -, *, / and sqrt is the IEEE operation
+// the reference's CPU build performs, in the reference's order, so results
+// differ from it only where CUDA's pow / exp round differently from glibc's.
+//
+// One thread per zone over a CTA tile of 8 x 32 zones whose primitives (with
+// a two-zone halo) are staged in shared memory. The reference's face fluxes
+// are not shareable between the two zones of a face (each zone takes the
+// sound speed of the neighbour across the face, cbdgam_2d.c:608-611, and the
+// viscous flux the neighbour's scale height), so each zone computes its four
+// faces, as the reference does.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "cbdiso_b200.h"
+
+namespace cbd {
+cudaStream_t drop_in_stream();  // capi.cu: the stream set by cbdiso_b200_set_stream
+}
+
+namespace gam {
+
+constexpr int NF = 4;
+constexpr int NG = 2;
+constexpr int TI = 8, TJ = 32;  // CTA tile (rows i, columns j)
+constexpr int HI = TI + 2 * NG, HJ = TJ + 2 * NG;
+
+struct Mass {
+    double x, y, vx, vy, mass, soft, rate, radius;
+    int model;
+};
+
+struct Consts {
+    int ni, nj;
+    double xl, yl, dx, dy;
+    double theta, gamma, alpha, cooling, mach_ceiling, vmax, rho_floor, p_floor;
+    int constant_softening;
+    int buffer_on;
+    double buf_sigma, buf_pressure, buf_rate, buf_outer, buf_width;
+    double buf_onset_m3;  // pow(buf_outer - buf_width, -3.0), glibc's on the host
+    double mach_m2;       // pow(mach_ceiling, -2.0), glibc's on the host
+};
+
+struct Stage {
+    Mass m[2];
+    double buf_mass, a, dt;
+    int write_guards;
+    int un_from_primitive;  // u_n = cons(primitive_n) in-kernel (else: a conserved array)
+};
+
+// ---------------------------------------------------------------------------
+// Correctly rounded powers and exponential. The reference's CPU build takes
+// these from glibc, whose results are the correctly rounded ones in all but
+// rare cases near a rounding midpoint; CUDA's pow / exp may be an ulp off. In
+// a near-vacuum zone an ulp in the energy update is amplified by the
+// cancellation between total and kinetic energy, so the kernels compute each
+// power as a double-double value (error-free products via FMA, Dekker /
+// Knuth) rounded once, which is the correctly rounded result except within
+// about 2^-100 of a midpoint. Arguments outside a safe normal range fall back
+// to pow / exp.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ bool in_range(double x) { return x > 1e-90 && x < 1e90; }
+
+// RN(x^3): x^2 = h + l exactly, x^3 = h x + l x with h x an exact pair
+__device__ __forceinline__ double cube_rn(double x)
+{
+    if (!in_range(fabs(x)))
+        return pow(x, 3.0);
+    const double h = x * x, l = fma(x, x, -h);
+    const double p = h * x, e = fma(h, x, -p);
+    return p + (e + l * x);
+}
+
+// RN(1 / (h + l)) for a double-double h + l: q = RN(1 / h) leaves the exact
+// residual 1 - q h, and one correction step rounds once
+__device__ __forceinline__ double recip_dd_rn(double h, double l)
+{
+    const double q = 1.0 / h;
+    const double r = fma(-q, h, 1.0) - q * l;
+    return q + q * r;
+}
+
+// RN(x^-2)
+__device__ __forceinline__ double inv_square_rn(double x)
+{
+    if (!in_range(fabs(x)))
+        return pow(x, -2.0);
+    const double h = x * x, l = fma(x, x, -h);
+    return recip_dd_rn(h, l);
+}
+
+// RN(x^-3)
+__device__ __forceinline__ double inv_cube_rn(double x)
+{
+    if (!in_range(fabs(x)))
+        return pow(x, -3.0);
+    const double h = x * x, l = fma(x, x, -h);
+    const double p = h * x, e = fma(h, x, -p) + l * x;
+    return recip_dd_rn(p, e);
+}
+
+// RN(x^4): x^2 as an exact pair, squared, rounded once
+__device__ __forceinline__ double fourth_rn(double x)
+{
+    if (!in_range(fabs(x)))
+        return pow(x, 4.0);
+    const double h = x * x, l = fma(x, x, -h);
+    const double r = h * h;
+    return r + (fma(h, h, -r) + 2.0 * h * l);
+}
+
+// RN(x^-1.5) for positive x: 1/x and its square root as double-double pairs
+// (one Newton correction of the root), their product rounded once
+__device__ __forceinline__ double inv_pow15_rn(double x)
+{
+    if (!in_range(x))
+        return pow(x, -1.5);
+    const double u = 1.0 / x;
+    const double u_lo = u * fma(-u, x, 1.0);
+    const double w = sqrt(u);
+    const double w_lo = (fma(-w, w, u) + u_lo) * (0.5 * w * x);
+    const double h = u * w;
+    return h + (fma(u, w, -h) + (u * w_lo + u_lo * w));
+}
+
+// RN(pow(x, RN(-1/3))) for x >= 1. The exponent -1/3 rounded to a double is
+// -1/3 + d with d = 2^-54 / 3, so the power is x^(-1/3) (1 + d ln x) to far
+// below an ulp. x^(-1/3) comes from one Newton step y + y (1 - x y^3) / 3 on
+// rcbrt(x), with the residual 1 - x y^3 in double-double.
+__device__ __forceinline__ double pow_m13_rn(double x)
+{
+    if (!(x >= 1.0 && x < 1e90))
+        return pow(x, -1.0 / 3.0);
+    const double y = rcbrt(x);
+    const double h = y * y, l = fma(y, y, -h);
+    const double p = h * y, e = fma(h, y, -p) + l * y;  // y^3 = p + e
+    const double s = x * p, s_lo = fma(x, p, -s) + x * e;  // x y^3 = s + s_lo
+    const double resid = (1.0 - s) - s_lo;  // 1 - s is exact: s is within an ulp or so of 1
+    const double d = 0x1.5555555555555p-56;
+    return y + y * (resid / 3.0 + d * log(x));
+}
+
+// RN(exp(x)) for -745 < x <= 0: x = k ln2 + r with r carried as a
+// double-double (ln 2 = LN2_HI + LN2_LO), exp(r) by its Taylor series to
+// degree 23 in double-double Horner form (|r| <= 0.35: truncation below
+// 2^-103), scaled by 2^k.
+__device__ __forceinline__ double exp_rn(double x)
+{
+    if (!(x > -700.0 && x <= 0.0))
+        return exp(x);
+    constexpr double LN2_HI = 0x1.62e42fefa39efp-1, LN2_LO = 0x1.abc9e3b39803fp-56;
+    const double k = rint(x * 0x1.71547652b82fep+0);
+    const double t = k * LN2_HI, t_lo = fma(k, LN2_HI, -t);  // k LN2_HI exactly
+    const double a = x - t;  // exact: x and t agree to within a factor of two, or k = 0
+    const double b = -t_lo - k * LN2_LO;
+    double r = a + b;
+    double r_lo = b - (r - a);  // r + r_lo = a + b (Fast2Sum, |a| >= |b|)
+    // Horner: s <- 1 + s r / n for n = 23 .. 1, s as a double-double
+    double sh = 1.0, sl = 0.0;
+    for (int n = 23; n >= 1; --n) {
+        // (sh + sl)(r + r_lo)
+        const double m = sh * r;
+        const double m_lo = fma(sh, r, -m) + (sh * r_lo + sl * r);
+        // divided by n: q = RN(m / n), exact remainder m - q n
+        const double q = m / n;
+        const double q_lo = (fma(-q, (double)n, m) + m_lo) / n;
+        // 1 + q + q_lo
+        const double u = 1.0 + q;
+        const double u_lo = (1.0 - u) + q + q_lo;  // |q| < 1: Fast2Sum
+        sh = u + u_lo;
+        sl = u_lo - (sh - u);
+    }
+    return ldexp(sh + sl, (int)k);
+}
+
+__device__ __forceinline__ double lesser(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double greater(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double sign_of(double x) { return copysign(1.0, x); }
+__device__ __forceinline__ size_t at(int i, int j, int nj) { return ((size_t)(i + NG) * (nj + 2 * NG) + (j + NG)) * NF; }
+
+// cbdgam_2d.c:27-33
+__device__ __forceinline__ double slope(double yl, double y0, double yr, double theta)
+{
+    const double a = (y0 - yl) * theta;
+    const double b = (yr - yl) * 0.5;
+    const double c = (yr - y0) * theta;
+    const double m = lesser(fabs(a), lesser(fabs(b), fabs(c)));
+    return 0.25 * fabs(sign_of(a) + sign_of(b)) * (sign_of(a) + sign_of(c)) * m;
+}
+
+template <class A, class B, class C>
+__device__ __forceinline__ void slopes(const A &yl, const B &y0, const C &yr, double theta, double *g)
+{
+#pragma unroll
+    for (int q = 0; q < NF; ++q)
+        g[q] = slope(yl[q], y0[q], yr[q], theta);
+}
+
+// cbdgam_2d.c:75-106
+template <class V>
+__device__ __forceinline__ double scale_height(const Mass *m, double x, double y, const V &p)
+{
+    if (m[0].mass == 0.0 && m[1].mass == 0.0)
+        return 1.0;
+    double w2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        if (m[k].mass > 0.0) {
+            const double dx = x - m[k].x, dy = y - m[k].y;
+            const double r = sqrt(dx * dx + dy * dy + 1e-12);
+            w2 += m[k].mass * inv_cube_rn(r);
+        }
+    }
+    return sqrt(p[3] / p[0]) / sqrt(w2);
+}
+
+// cbdgam_2d.c:108-203
+template <class V>
+__device__ __forceinline__ void mass_source(const Mass &m, double x, double y, double dt, const V &p, double h,
+                                            int constant_softening, double gamma, double *du)
+{
+    const double sigma = p[0];
+    const double eps = p[3] / sigma / (gamma - 1.0);
+    const double dx = x - m.x, dy = y - m.y;
+    const double r2 = dx * dx + dy * dy;
+    const double dr = sqrt(r2);
+    const double rs = m.radius;
+    double soft;
+    if (constant_softening) {
+        soft = m.soft;
+    } else if (dr > rs) {
+        soft = 0.5 * h;
+    } else {
+        const double q = dr / rs;
+        const double w = (1.0 - q * q) * (1.0 - q * q);  // pow(., 2.0) is the correctly rounded square
+        soft = w * rs + (1.0 - w) * 0.5 * h;
+    }
+    const double rate = (dr < 4.0 * rs) ? m.rate * exp_rn(-fourth_rn(dr / rs)) : 0.0;
+    const double fnum = sigma * m.mass * inv_pow15_rn(r2 + soft * soft);
+    const double fx = -fnum * dx, fy = -fnum * dy;
+    const double mdot = sigma * rate * -1.0;
+    const double vx = p[1], vy = p[2];
+    if (m.model == 1) {
+        du[0] = dt * mdot;
+        du[1] = dt * mdot * p[1] + dt * fx;
+        du[2] = dt * mdot * p[2] + dt * fy;
+        du[3] = dt * (mdot * eps + 0.5 * mdot * (vx * vx + vy * vy)) + dt * (fx * vx + fy * vy);
+    } else if (m.model == 2) {
+        const double ex = dx / (dr + 1e-12), ey = dy / (dr + 1e-12);
+        const double dvr = (vx - m.vx) * ex + (vy - m.vy) * ey;
+        const double wx = dvr * ex + m.vx, wy = dvr * ey + m.vy;
+        du[0] = dt * mdot;
+        du[1] = dt * mdot * wx + dt * fx;
+        du[2] = dt * mdot * wy + dt * fy;
+        du[3] = dt * (mdot * eps + 0.5 * mdot * (wx * wx + wy * wy)) + dt * (fx * vx + fy * vy);
+    } else if (m.model == 3) {
+        du[0] = dt * mdot;
+        du[1] = dt * fx;
+        du[2] = dt * fy;
+        du[3] = dt * (fx * vx + fy * vy);
+    } else {
+        du[0] = du[1] = du[2] = du[3] = 0.0;
+    }
+}
+
+template <class V>
+__device__ __forceinline__ double cs2_of(double gamma, const V &p) { return p[3] / p[0] * gamma; }
+
+// cbdgam_2d.c:238-276
+__device__ __forceinline__ void buffer_source(const Consts &k, double buf_mass, double x, double y, double dt,
+                                              double *u)
+{
+    if (!k.buffer_on)
+        return;
+    const double rc = sqrt(x * x + y * y);
+    const double onset = k.buf_outer - k.buf_width;
+    if (rc > onset) {
+        const double pf = k.buf_sigma * sqrt(buf_mass / rc);
+        const double px = pf * (-y / rc), py = pf * (x / rc);
+        const double ek = 0.5 * (px * px + py * py) / k.buf_sigma;
+        const double target[NF] = {k.buf_sigma, px, py, k.buf_pressure / (k.gamma - 1.0) + ek};
+        const double omega = sqrt(buf_mass * k.buf_onset_m3);  // pow(onset, -3.0), from the host
+        const double rate = k.buf_rate * omega * (rc - onset) / (k.buf_outer - onset);
+#pragma unroll
+        for (int q = 0; q < NF; ++q)
+            u[q] -= (u[q] - target[q]) * rate * dt;
+    }
+}
+
+// cbdgam_2d.c:278-294 (xx, xy, yx, yy)
+__device__ __forceinline__ void strain(const double *gx, const double *gy, double dx, double dy, double *s)
+{
+    const double sxx = 4.0 / 3.0 * gx[1] / dx - 2.0 / 3.0 * gy[2] / dy;
+    const double syy = -2.0 / 3.0 * gx[1] / dx + 4.0 / 3.0 * gy[2] / dy;
+    const double sxy = 1.0 / 1.0 * gx[2] / dx + 1.0 / 1.0 * gy[1] / dy;
+    s[0] = sxx;
+    s[1] = sxy;
+    s[2] = sxy;
+    s[3] = syy;
+}
+
+// cbdgam_2d.c:298-317
+template <class V>
+__device__ __forceinline__ void cooling(const Consts &k, double dt, const V &p, double *u)
+{
+    const double gamma = k.gamma, sigma = p[0];
+    const double eps = p[3] / p[0] / (gamma - 1.0);
+    double cooled = eps * pow_m13_rn(1.0 + 3.0 * k.cooling * inv_square_rn(sigma) * cube_rn(eps) * dt);
+    const double ek = 0.5 * (p[1] * p[1] + p[2] * p[2]);
+    cooled = greater(cooled, 2.0 * ek / gamma / (gamma - 1.0) * k.mach_m2);  // pow(mach_ceiling, -2.0), host
+    u[3] += sigma * (cooled - eps);
+}
+
+// cbdgam_2d.c:319-345
+__device__ __forceinline__ void cons_to_prim(const Consts &k, const double *u, double *p)
+{
+    double pres = greater(k.p_floor, (u[3] - 0.5 * (u[1] * u[1] + u[2] * u[2]) / u[0]) * (k.gamma - 1.0));
+    double vx = sign_of(u[1]) * lesser(fabs(u[1] / u[0]), k.vmax);
+    double vy = sign_of(u[2]) * lesser(fabs(u[2] / u[0]), k.vmax);
+    double rho = u[0];
+    if (u[0] < k.rho_floor) {
+        rho = k.rho_floor;
+        vx = 0.0;
+        vy = 0.0;
+        pres = k.p_floor;
+    }
+    p[0] = rho;
+    p[1] = vx;
+    p[2] = vy;
+    p[3] = pres;
+}
+
+// cbdgam_2d.c:347-362
+template <class V>
+__device__ __forceinline__ void prim_to_cons(const V &p, double *u, double gamma)
+{
+    const double rho = p[0], vx = p[1], vy = p[2], pres = p[3];
+    u[0] = rho;
+    u[1] = vx * rho;
+    u[2] = vy * rho;
+    u[3] = pres / (gamma - 1.0) + 0.5 * rho * (vx * vx + vy * vy);
+}
+
+// cbdgam_2d.c:364-434: HLLE flux across a face with normal DIR
+template <int DIR>
+__device__ __forceinline__ void hlle(const double *pl, const double *pr, double cs2, double gamma, double *f)
+{
+    double ul[NF], ur[NF];
+    prim_to_cons(pl, ul, gamma);
+    prim_to_cons(pr, ur, gamma);
+    const double vl = DIR == 0 ? pl[1] : pl[2], vr = DIR == 0 ? pr[1] : pr[2];
+    const double fl[NF] = {vl * ul[0], vl * ul[1] + pl[3] * (double)(DIR == 0), vl * ul[2] + pl[3] * (double)(DIR == 1),
+                           vl * (ul[3] + pl[3])};
+    const double fr[NF] = {vr * ur[0], vr * ur[1] + pr[3] * (double)(DIR == 0), vr * ur[2] + pr[3] * (double)(DIR == 1),
+                           vr * (ur[3] + pr[3])};
+    const double cs = sqrt(cs2);
+    const double am = lesser(0.0, lesser(vl - cs, vr - cs));
+    const double ap = greater(0.0, greater(vl + cs, vr + cs));
+#pragma unroll
+    for (int q = 0; q < NF; ++q)
+        f[q] = (fl[q] * ap - fr[q] * am - (ul[q] - ur[q]) * ap * am) / (ap - am);
+}
+
+// cbdgam_2d.c:401-409
+template <class V>
+__device__ __forceinline__ double max_wavespeed(const V &p, double cs2)
+{
+    const double cs = sqrt(cs2);
+    const double ax = greater(fabs(p[1] - cs), fabs(p[1] + cs));
+    const double ay = greater(fabs(p[2] - cs), fabs(p[2] + cs));
+    return greater(ax, ay);
+}
+
+// One zone's stage update (cbdgam_2d.c:499-682); P(di, dj) gives the input
+// primitives of the zone (i + di, j + dj), indexed by field.
+template <class Load>
+__device__ void zone_update(const Consts &k, const Stage &st, int i, int j, const Load &P, const double *un,
+                            double *out)
+{
+    const double dx = k.dx, dy = k.dy, theta = k.theta, gamma = k.gamma;
+    const double xl = k.xl + (i + 0.0) * dx, xc = k.xl + (i + 0.5) * dx, xr = k.xl + (i + 1.0) * dx;
+    const double yl = k.yl + (j + 0.0) * dy, yc = k.yl + (j + 0.5) * dy, yr = k.yl + (j + 1.0) * dy;
+    const auto c = P(0, 0), w1 = P(-1, 0), e1 = P(1, 0), s1 = P(0, -1), n1 = P(0, 1);
+
+    double gxw[NF], gxc[NF], gxe[NF], gys[NF], gyc[NF], gyn[NF];
+    slopes(P(-2, 0), w1, c, theta, gxw);
+    slopes(w1, c, e1, theta, gxc);
+    slopes(c, e1, P(2, 0), theta, gxe);
+    slopes(P(0, -2), s1, c, theta, gys);
+    slopes(s1, c, n1, theta, gyc);
+    slopes(c, n1, P(0, 2), theta, gyn);
+
+    const double cs2w = cs2_of(gamma, w1), cs2e = cs2_of(gamma, e1);
+    const double cs2s = cs2_of(gamma, s1), cs2n = cs2_of(gamma, n1);
+    const double hc = scale_height(st.m, xc, yc, c);
+
+    double fw[NF], fe[NF], fs[NF], fn[NF];
+    {
+        double lo[NF], hi[NF];
+#pragma unroll
+        for (int q = 0; q < NF; ++q) {
+            lo[q] = w1[q] + 0.5 * gxw[q];
+            hi[q] = c[q] - 0.5 * gxc[q];
+        }
+        hlle<0>(lo, hi, cs2w, gamma, fw);
+#pragma unroll
+        for (int q = 0; q < NF; ++q) {
+            lo[q] = c[q] + 0.5 * gxc[q];
+            hi[q] = e1[q] - 0.5 * gxe[q];
+        }
+        hlle<0>(lo, hi, cs2e, gamma, fe);
+#pragma unroll
+        for (int q = 0; q < NF; ++q) {
+            lo[q] = s1[q] + 0.5 * gys[q];
+            hi[q] = c[q] - 0.5 * gyc[q];
+        }
+        hlle<1>(lo, hi, cs2s, gamma, fs);
+#pragma unroll
+        for (int q = 0; q < NF; ++q) {
+            lo[q] = c[q] + 0.5 * gyc[q];
+            hi[q] = n1[q] - 0.5 * gyn[q];
+        }
+        hlle<1>(lo, hi, cs2n, gamma, fn);
+    }
+
+    if (k.alpha > 0.0) {
+        double gyw[NF], gye[NF], gxs[NF], gxn[NF];
+        slopes(P(-1, -1), w1, P(-1, 1), theta, gyw);
+        slopes(P(1, -1), e1, P(1, 1), theta, gye);
+        slopes(P(-1, -1), s1, P(1, -1), theta, gxs);
+        slopes(P(-1, 1), n1, P(1, 1), theta, gxn);
+        double tw[4], te[4], ts[4], tn[4], tc[4];
+        strain(gxw, gyw, dx, dy, tw);
+        strain(gxe, gye, dx, dy, te);
+        strain(gxs, gys, dx, dy, ts);
+        strain(gxn, gyn, dx, dy, tn);
+        strain(gxc, gyc, dx, dy, tc);
+        const double cs2c = cs2_of(gamma, c);
+        const double hw = scale_height(st.m, xl, yc, w1), he = scale_height(st.m, xr, yc, e1);
+        const double hs = scale_height(st.m, xc, yl, s1), hn = scale_height(st.m, xc, yr, n1);
+        const double nuc = k.alpha * hc * sqrt(cs2c);
+        const double nuw = k.alpha * hw * sqrt(cs2w), nue = k.alpha * he * sqrt(cs2e);
+        const double nus = k.alpha * hs * sqrt(cs2s), nun = k.alpha * hn * sqrt(cs2n);
+
+        fw[1] -= 0.5 * (nuw * w1[0] * tw[0] + nuc * c[0] * tc[0]);
+        fw[2] -= 0.5 * (nuw * w1[0] * tw[1] + nuc * c[0] * tc[1]);
+        fe[1] -= 0.5 * (nuc * c[0] * tc[0] + nue * e1[0] * te[0]);
+        fe[2] -= 0.5 * (nuc * c[0] * tc[1] + nue * e1[0] * te[1]);
+        fs[1] -= 0.5 * (nus * s1[0] * ts[2] + nuc * c[0] * tc[2]);
+        fs[2] -= 0.5 * (nus * s1[0] * ts[3] + nuc * c[0] * tc[3]);
+        fn[1] -= 0.5 * (nuc * c[0] * tc[2] + nun * n1[0] * tn[2]);
+        fn[2] -= 0.5 * (nuc * c[0] * tc[3] + nun * n1[0] * tn[3]);
+
+        fw[3] -= 0.5 * (nuw * w1[0] * tw[0] * w1[1] + nuc * c[0] * tc[0] * c[1]);
+        fe[3] -= 0.5 * (nuc * c[0] * tc[0] * c[1] + nue * e1[0] * te[0] * e1[1]);
+        fw[3] -= 0.5 * (nuw * w1[0] * tw[1] * w1[2] + nuc * c[0] * tc[1] * c[2]);
+        fe[3] -= 0.5 * (nuc * c[0] * tc[1] * c[2] + nue * e1[0] * te[1] * e1[2]);
+        fs[3] -= 0.5 * (nus * s1[0] * ts[2] * s1[1] + nuc * c[0] * tc[2] * c[1]);
+        fn[3] -= 0.5 * (nuc * c[0] * tc[2] * c[1] + nun * n1[0] * tn[2] * n1[1]);
+        fs[3] -= 0.5 * (nus * s1[0] * ts[3] * s1[2] + nuc * c[0] * tc[3] * c[2]);
+        fn[3] -= 0.5 * (nuc * c[0] * tc[3] * c[2] + nun * n1[0] * tn[3] * n1[2]);
+    }
+
+    double u[NF];
+    prim_to_cons(c, u, gamma);
+    buffer_source(k, st.buf_mass, xc, yc, st.dt, u);
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        double du[NF];
+        mass_source(st.m[m], xc, yc, st.dt, c, hc, k.constant_softening, gamma, du);
+#pragma unroll
+        for (int q = 0; q < NF; ++q)
+            u[q] += du[q];
+    }
+    cooling(k, st.dt, c, u);
+#pragma unroll
+    for (int q = 0; q < NF; ++q) {
+        u[q] -= ((fe[q] - fw[q]) / dx + (fn[q] - fs[q]) / dy) * st.dt;
+        u[q] = (1.0 - st.a) * u[q] + st.a * un[q];
+    }
+    cons_to_prim(k, u, out);
+}
+
+// a maximum that keeps a NaN operand, so that a NaN wavespeed reaches the host
+__device__ __forceinline__ double max_nan(double a, double b) { return (a > b || a != a) ? a : b; }
+
+// The primitives of one zone in the field-major shared tile.
+struct TileZone {
+    const double *p;
+    __device__ double operator[](int q) const { return p[q * (HI * HJ)]; }
+};
+
+// One RK stage. primitive_n supplies u_n (cons of it, rebuilt in the kernel)
+// or un_all does (the reference's conserved_rk array). With ws_max set, the
+// largest wavespeed of the written zones is max-ed into it (non-negative
+// doubles order as their bit patterns do).
+__global__ void __launch_bounds__(TI * TJ) stage_kernel(Consts k, Stage st, const double *__restrict__ prd,
+                                                         const double *pn,
+                                                         const double *__restrict__ un_all, double *pwr,
+                                                         unsigned long long *ws_max)
+{
+    __shared__ double tile[NF][HI][HJ];
+    __shared__ double warp_max[TI * TJ / 32];
+    const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
+    const int ni = k.ni, nj = k.nj;
+    const int tid = threadIdx.y * TJ + threadIdx.x;
+    for (int s = tid; s < HI * HJ; s += TI * TJ) {
+        const int ii = i0 - NG + s / HJ, jj = j0 - NG + s % HJ;
+        if (ii <= ni + 1 && jj <= nj + 1) {
+            const double *src = prd + at(ii, jj, nj);
+#pragma unroll
+            for (int q = 0; q < NF; ++q)
+                tile[q][s / HJ][s % HJ] = src[q];
+        }
+    }
+    __syncthreads();
+    const int i = i0 + threadIdx.y, j = j0 + threadIdx.x;
+    double ws = 0.0;
+    if (i < ni && j < nj) {
+        auto P = [&](int di, int dj) { return TileZone{&tile[0][threadIdx.y + NG + di][threadIdx.x + NG + dj]}; };
+        // u_n enters as (1 - a) u + a u_n even when a = 0, as in the reference
+        double un[NF];
+        if (st.un_from_primitive) {
+            double pn_z[NF];
+#pragma unroll
+            for (int q = 0; q < NF; ++q)
+                pn_z[q] = pn[at(i, j, nj) + q];
+            prim_to_cons(pn_z, un, k.gamma);
+        } else {
+#pragma unroll
+            for (int q = 0; q < NF; ++q)
+                un[q] = un_all[at(i, j, nj) + q];
+        }
+        double out[NF];
+        zone_update(k, st, i, j, P, un, out);
+        // the zone and, on the edges, its zero-gradient guard images
+        const int ilo = (st.write_guards && i == 0) ? -NG : i, ihi = (st.write_guards && i == ni - 1) ? ni + 1 : i;
+        const int jlo = (st.write_guards && j == 0) ? -NG : j, jhi = (st.write_guards && j == nj - 1) ? nj + 1 : j;
+        for (int ii = ilo; ii <= ihi; ++ii)
+            for (int jj = jlo; jj <= jhi; ++jj) {
+                double *dst = pwr + at(ii, jj, nj);
+#pragma unroll
+                for (int q = 0; q < NF; ++q)
+                    dst[q] = out[q];
+            }
+        if (ws_max)
+            ws = max_wavespeed(out, cs2_of(k.gamma, out));
+    }
+    if (ws_max) {  // uniform over the block
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            ws = max_nan(ws, __shfl_xor_sync(0xffffffffu, ws, o));
+        if ((tid & 31) == 0)
+            warp_max[tid >> 5] = ws;
+        __syncthreads();
+        if (tid == 0) {
+            double m = warp_max[0];
+            for (int w = 1; w < TI * TJ / 32; ++w)
+                m = max_nan(m, warp_max[w]);
+            atomicMax(ws_max, (unsigned long long)__double_as_longlong(m));
+        }
+    }
+}
+
+__global__ void p2c_kernel(int ni, int nj, double gamma, const double *prim, double *cons)
+{
+    const long n = (long)ni * nj;
+    for (long z = blockIdx.x * (long)blockDim.x + threadIdx.x; z < n; z += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(z / nj), j = (int)(z % nj);
+        prim_to_cons(prim + at(i, j, nj), cons + at(i, j, nj), gamma);
+    }
+}
+
+__global__ void wavespeed_kernel(int ni, int nj, double gamma, const double *prim, double *ws)
+{
+    const long n = (long)ni * nj;
+    for (long z = blockIdx.x * (long)blockDim.x + threadIdx.x; z < n; z += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(z / nj), j = (int)(z % nj);
+        const double *p = prim + at(i, j, nj);
+        ws[(size_t)(i + NG) * (nj + 2 * NG) + (j + NG)] = max_wavespeed(p, cs2_of(gamma, p));
+    }
+}
+
+__global__ void source_kernel(int ni, int nj, double xl, double yl, double dx, double dy, Mass m1, Mass m2,
+                              int which, int constant_softening, double gamma, const double *prim, double *rate)
+{
+    const Mass ms[2] = {m1, m2};
+    const long n = (long)ni * nj;
+    for (long z = blockIdx.x * (long)blockDim.x + threadIdx.x; z < n; z += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(z / nj), j = (int)(z % nj);
+        const double xc = xl + (i + 0.5) * dx, yc = yl + (j + 0.5) * dy;
+        const double *p = prim + at(i, j, nj);
+        const double h = scale_height(ms, xc, yc, p);
+        mass_source(ms[which - 1], xc, yc, 1.0, p, h, constant_softening, gamma, rate + at(i, j, nj));
+    }
+}
+
+// zero-gradient guard images of a state (the reference's outflow set_bc)
+__global__ void guards_kernel(int ni, int nj, double *a)
+{
+    const long wi = ni + 2 * NG, wj = nj + 2 * NG;
+    for (long z = blockIdx.x * (long)blockDim.x + threadIdx.x; z < wi * wj; z += (long)gridDim.x * blockDim.x) {
+        const int ii = (int)(z / wj) - NG, jj = (int)(z % wj) - NG;
+        if (ii >= 0 && ii < ni && jj >= 0 && jj < nj)
+            continue;
+        const int ci = ii < 0 ? 0 : (ii >= ni ? ni - 1 : ii);
+        const int cj = jj < 0 ? 0 : (jj >= nj ? nj - 1 : jj);
+#pragma unroll
+        for (int q = 0; q < NF; ++q)
+            a[at(ii, jj, nj) + q] = a[at(ci, cj, nj) + q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// reductions: the CFL wavespeed maximum and the diagnostic sums
+// ---------------------------------------------------------------------------
+
+constexpr int RED_THREADS = 256;
+constexpr int MAX_DIAG = 4;
+constexpr int RED_VALUES = 1 + 2 * MAX_DIAG;
+
+struct Diag {
+    int quantity, which_mass, gravity, accretion, has_cut;
+    double r0, r1;
+};
+
+struct RedArgs {
+    Consts k;
+    Mass m[2];
+    Diag d[MAX_DIAG];
+    int nd;
+};
+
+// a mass's source rates (dt = 1) for a diagnostic: the accretion rates
+// (masses zero) when its accretion flag is set, else the gravity rates
+// (sink rates zero), as the reference's reductions pass mass * gravity and
+// sink_rate * accretion (cbdgam_2d.py:104-139, 346-349, 397-402)
+__device__ __forceinline__ void diag_rates(const RedArgs &r, const Diag &d, int which, double xc, double yc,
+                                           const double *p, double *rate)
+{
+    Mass ms[2] = {r.m[0], r.m[1]};
+    const double gravity = d.accretion ? 0.0 : 1.0, accretion = d.accretion ? 1.0 : 0.0;
+    for (int k = 0; k < 2; ++k) {
+        ms[k].mass = ms[k].mass * gravity;
+        ms[k].rate = ms[k].rate * accretion;
+    }
+    const double h = scale_height(ms, xc, yc, p);
+    mass_source(ms[which - 1], xc, yc, 1.0, p, h, r.k.constant_softening, r.k.gamma, rate);
+}
+
+__device__ __forceinline__ void diag_value(const RedArgs &r, const Diag &d, double x, double y, const double *p,
+                                           double *re, double *im)
+{
+    const double rr = sqrt(x * x + y * y);
+    const double cut = d.has_cut ? (double)((d.r0 < rr) * (rr < d.r1)) : 1.0;
+    *im = 0.0;
+    if (d.quantity == CBD_Q_SIGMA_M1) {
+        const double s = p[0] * cut;
+        *re = s * (x / rr);
+        *im = s * (y / rr);
+        return;
+    }
+    if (d.quantity == CBD_Q_ECCENTRICITY_VECTOR) {
+        const double s = p[0] * cut, vx = p[1] * cut, vy = p[2] * cut;
+        const double vv = vx * vx + vy * vy, vr = vx * x + vy * y;
+        *re = s * ((vv * x - vr * vx) / 1.0 - x / rr);
+        *im = s * ((vv * y - vr * vy) / 1.0 - y / rr);
+        return;
+    }
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int which = 1; which <= 2; ++which) {
+        if (d.which_mass != 3 && d.which_mass != which)
+            continue;
+        double rate[NF];
+        diag_rates(r, d, which, x, y, p, rate);
+        for (int q = 0; q < 3; ++q)
+            f[q] += rate[q];
+    }
+    if (d.quantity == CBD_Q_MDOT)
+        *re = f[0] * cut;
+    else  // torque
+        *re = x * (f[2] * cut) - y * (f[1] * cut);
+}
+
+// per-block partial sums in a fixed tree order; the wavespeed maximum
+__global__ void __launch_bounds__(RED_THREADS) reduce_kernel(RedArgs r, const double *prim, double *partials)
+{
+    __shared__ double sm[RED_VALUES][RED_THREADS];
+    const Consts &k = r.k;
+    double v[RED_VALUES];
+    for (int q = 0; q < RED_VALUES; ++q)
+        v[q] = 0.0;
+    const long n = (long)k.ni * k.nj;
+    for (long z = blockIdx.x * (long)RED_THREADS + threadIdx.x; z < n; z += (long)gridDim.x * RED_THREADS) {
+        const int i = (int)(z / k.nj), j = (int)(z % k.nj);
+        const double *p = prim + at(i, j, k.nj);
+        v[0] = greater(v[0], max_wavespeed(p, cs2_of(k.gamma, p)));
+        const double x = k.xl + (i + 0.5) * k.dx, y = k.yl + (j + 0.5) * k.dy;
+        for (int d = 0; d < r.nd; ++d) {
+            double re, im;
+            diag_value(r, r.d[d], x, y, p, &re, &im);
+            v[1 + 2 * d] += re;
+            v[2 + 2 * d] += im;
+        }
+    }
+    for (int q = 0; q < RED_VALUES; ++q)
+        sm[q][threadIdx.x] = v[q];
+    __syncthreads();
+    for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            sm[0][threadIdx.x] = greater(sm[0][threadIdx.x], sm[0][threadIdx.x + w]);
+            for (int q = 1; q < RED_VALUES; ++q)
+                sm[q][threadIdx.x] += sm[q][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < RED_VALUES)
+        partials[(size_t)blockIdx.x * RED_VALUES + threadIdx.x] = sm[threadIdx.x][0];
+}
+
+__global__ void finish_kernel(const double *partials, int nblocks, double *result)
+{
+    const int q = threadIdx.x;
+    if (q >= RED_VALUES)
+        return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) {
+        const double x = partials[(size_t)b * RED_VALUES + q];
+        s = q == 0 ? greater(s, x) : s + x;
+    }
+    result[q] = s;
+}
+
+// the correctly rounded helpers on device arrays (a test hook)
+__global__ void eval_powers_kernel(long n, const double *x, double *out)
+{
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        const double v = x[t];
+        double *o = out + 8 * t;
+        o[0] = cube_rn(v);
+        o[1] = inv_square_rn(v);
+        o[2] = inv_cube_rn(v);
+        o[3] = fourth_rn(v);
+        o[4] = inv_pow15_rn(v);
+        o[5] = pow_m13_rn(1.0 + v);
+        o[6] = exp_rn(-v);
+        o[7] = 0.0;
+    }
+}
+
+constexpr int RED_BLOCKS = 592;  // 4 per SM on a B200; fixed so the summation order is too
+
+double g_theta = 1.5;  // the drop-in kernels' PLM theta (the reference fixes 1.5)
+
+bool grid_ok(const cbdgam_grid_t *g)
+{
+    return g && g->ni > 0 && g->nj > 0 && g->xr > g->xl && g->yr > g->yl && g->gamma_law_index != 1.0;
+}
+
+Consts consts_of(const cbdgam_grid_t *g)
+{
+    Consts k;
+    std::memset(&k, 0, sizeof(k));
+    k.ni = g->ni;
+    k.nj = g->nj;
+    k.xl = g->xl;
+    k.yl = g->yl;
+    k.dx = (g->xr - g->xl) / g->ni;
+    k.dy = (g->yr - g->yl) / g->nj;
+    k.theta = g->plm_theta;
+    k.gamma = g->gamma_law_index;
+    k.alpha = g->alpha;
+    k.cooling = g->cooling_coefficient;
+    k.mach_ceiling = g->mach_ceiling;
+    k.vmax = g->velocity_ceiling;
+    k.rho_floor = g->density_floor;
+    k.p_floor = g->pressure_floor;
+    k.constant_softening = g->constant_softening;
+    k.buffer_on = g->buffer_is_enabled;
+    k.buf_sigma = g->buffer_surface_density;
+    k.buf_pressure = g->buffer_surface_pressure;
+    k.buf_rate = g->buffer_driving_rate;
+    k.buf_outer = g->buffer_outer_radius;
+    k.buf_width = g->buffer_onset_width;
+    k.buf_onset_m3 = std::pow(g->buffer_outer_radius - g->buffer_onset_width, -3.0);
+    k.mach_m2 = std::pow(g->mach_ceiling, -2.0);
+    return k;
+}
+
+Mass mass_of(const cbd_mass_t &m)
+{
+    return Mass{m.x, m.y, m.vx, m.vy, m.mass, m.softening_length, m.sink_rate, m.sink_radius, m.sink_model};
+}
+
+Mass mass_args(double x, double y, double vx, double vy, double mass, double soft, double rate, double radius,
+               int model)
+{
+    return Mass{x, y, vx, vy, mass, soft, rate, radius, model};
+}
+
+int status_of(cudaError_t e) { return e == cudaSuccess ? CBD_OK : CBD_ERR_CUDA; }
+
+int launch_stage(const Consts &k, const Stage &st, const double *prd, const double *pn, const double *un,
+                 double *pwr, double *ws_max, cudaStream_t s)
+{
+    const dim3 grid((k.nj + TJ - 1) / TJ, (k.ni + TI - 1) / TI), block(TJ, TI);
+    stage_kernel<<<grid, block, 0, s>>>(k, st, prd, pn, un, pwr, reinterpret_cast<unsigned long long *>(ws_max));
+    return status_of(cudaGetLastError());
+}
+
+int blocks_for(long n, int t)
+{
+    const long b = (n + t - 1) / t;
+    return (int)(b < 2048 ? (b > 0 ? b : 1) : 2048);
+}
+
+}  // namespace gam
+
+using namespace gam;
+
+extern "C" {
+
+int cbdgam_b200_eval_powers(long n, const double *x, double *out, void *stream)
+{
+    if (n < 0 || (n > 0 && (!x || !out)))
+        return CBD_ERR_ARGUMENT;
+    if (n == 0)
+        return CBD_OK;
+    eval_powers_kernel<<<blocks_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(n, x, out);
+    return status_of(cudaGetLastError());
+}
+
+void cbdgam_b200_abi_sizes(size_t out[2])
+{
+    out[0] = sizeof(cbdgam_grid_t);
+    out[1] = sizeof(cbdgam_stage_t);
+}
+
+int cbdgam_b200_set_plm_theta(double theta)
+{
+    if (!(theta >= 1.0 && theta <= 2.0))
+        return CBD_ERR_ARGUMENT;
+    g_theta = theta;
+    return CBD_OK;
+}
+
+int cbdgam_2d_advance_rk(int ni, int nj, double xl, double xr, double yl, double yr, double *conserved_rk,
+                         double *primitive_rd, double *primitive_wr, double gamma_law_index,
+                         double buffer_surface_density, double buffer_surface_pressure, double buffer_central_mass,
+                         double buffer_driving_rate, double buffer_outer_radius, double buffer_onset_width,
+                         int buffer_is_enabled, double x1, double y1, double vx1, double vy1, double mass1,
+                         double softening_length1, double sink_rate1, double sink_radius1, int sink_model1, double x2,
+                         double y2, double vx2, double vy2, double mass2, double softening_length2,
+                         double sink_rate2, double sink_radius2, int sink_model2, double alpha, double a, double dt,
+                         double velocity_ceiling, double cooling_coefficient, double mach_ceiling,
+                         double density_floor, double pressure_floor, int constant_softening)
+{
+    if (ni <= 0 || nj <= 0 || !conserved_rk || !primitive_rd || !primitive_wr)
+        return CBD_ERR_ARGUMENT;
+    cbdgam_grid_t g;
+    std::memset(&g, 0, sizeof(g));
+    g.ni = ni;
+    g.nj = nj;
+    g.xl = xl;
+    g.xr = xr;
+    g.yl = yl;
+    g.yr = yr;
+    g.plm_theta = g_theta;
+    g.gamma_law_index = gamma_law_index;
+    g.alpha = alpha;
+    g.cooling_coefficient = cooling_coefficient;
+    g.mach_ceiling = mach_ceiling;
+    g.velocity_ceiling = velocity_ceiling;
+    g.density_floor = density_floor;
+    g.pressure_floor = pressure_floor;
+    g.constant_softening = constant_softening;
+    g.buffer_is_enabled = buffer_is_enabled;
+    g.buffer_surface_density = buffer_surface_density;
+    g.buffer_surface_pressure = buffer_surface_pressure;
+    g.buffer_driving_rate = buffer_driving_rate;
+    g.buffer_outer_radius = buffer_outer_radius;
+    g.buffer_onset_width = buffer_onset_width;
+    Stage st;
+    std::memset(&st, 0, sizeof(st));
+    st.m[0] = mass_args(x1, y1, vx1, vy1, mass1, softening_length1, sink_rate1, sink_radius1, sink_model1);
+    st.m[1] = mass_args(x2, y2, vx2, vy2, mass2, softening_length2, sink_rate2, sink_radius2, sink_model2);
+    st.buf_mass = buffer_central_mass;
+    st.a = a;
+    st.dt = dt;
+    st.write_guards = 0;
+    st.un_from_primitive = 0;
+    return launch_stage(consts_of(&g), st, primitive_rd, nullptr, conserved_rk, primitive_wr, nullptr,
+                        cbd::drop_in_stream());
+}
+
+int cbdgam_2d_wavespeed(int ni, int nj, double *primitive, double *wavespeed, double gamma_law_index)
+{
+    if (ni <= 0 || nj <= 0 || !primitive || !wavespeed)
+        return CBD_ERR_ARGUMENT;
+    wavespeed_kernel<<<blocks_for((long)ni * nj, 256), 256, 0,
+                       cbd::drop_in_stream()>>>(ni, nj, gamma_law_index,
+                                                                                   primitive, wavespeed);
+    return status_of(cudaGetLastError());
+}
+
+int cbdgam_2d_primitive_to_conserved(int ni, int nj, double *primitive, double *conserved, double gamma_law_index)
+{
+    if (ni <= 0 || nj <= 0 || !primitive || !conserved)
+        return CBD_ERR_ARGUMENT;
+    p2c_kernel<<<blocks_for((long)ni * nj, 256), 256, 0, cbd::drop_in_stream()>>>(
+        ni, nj, gamma_law_index, primitive, conserved);
+    return status_of(cudaGetLastError());
+}
+
+int cbdgam_2d_point_mass_source_term(int ni, int nj, double xl, double xr, double yl, double yr, double x1,
+                                     double y1, double vx1, double vy1, double mass1, double softening_length1,
+                                     double sink_rate1, double sink_radius1, int sink_model1, double x2, double y2,
+                                     double vx2, double vy2, double mass2, double softening_length2,
+                                     double sink_rate2, double sink_radius2, int sink_model2, int which_mass,
+                                     double *primitive, double *cons_rate, int constant_softening,
+                                     double gamma_law_index)
+{
+    if (ni <= 0 || nj <= 0 || !primitive || !cons_rate || (which_mass != 1 && which_mass != 2))
+        return CBD_ERR_ARGUMENT;
+    const Mass m1 = mass_args(x1, y1, vx1, vy1, mass1, softening_length1, sink_rate1, sink_radius1, sink_model1);
+    const Mass m2 = mass_args(x2, y2, vx2, vy2, mass2, softening_length2, sink_rate2, sink_radius2, sink_model2);
+    source_kernel<<<blocks_for((long)ni * nj, 256), 256, 0,
+                    cbd::drop_in_stream()>>>(
+        ni, nj, xl, yl, (xr - xl) / ni, (yr - yl) / nj, m1, m2, which_mass, constant_softening, gamma_law_index,
+        primitive, cons_rate);
+    return status_of(cudaGetLastError());
+}
+
+int cbdgam_b200_advance_stage(const cbdgam_grid_t *grid, const cbdgam_stage_t *stage, const double *primitive_rd,
+                              const double *primitive_n, double *primitive_wr, double *wavespeed_max, void *stream)
+{
+    if (!grid_ok(grid) || !stage || !primitive_rd || !primitive_wr || primitive_wr == primitive_rd)
+        return CBD_ERR_ARGUMENT;
+    if (!primitive_n) {
+        if (stage->a != 0.0)
+            return CBD_ERR_ARGUMENT;
+        primitive_n = primitive_rd;  // the first stage's u_n is the state it reads
+    }
+    Stage st;
+    std::memset(&st, 0, sizeof(st));
+    st.m[0] = mass_of(stage->mass[0]);
+    st.m[1] = mass_of(stage->mass[1]);
+    st.buf_mass = stage->buffer_central_mass;
+    st.a = stage->a;
+    st.dt = stage->dt;
+    st.write_guards = 1;
+    st.un_from_primitive = 1;
+    return launch_stage(consts_of(grid), st, primitive_rd, primitive_n, nullptr, primitive_wr, wavespeed_max,
+                        static_cast<cudaStream_t>(stream));
+}
+
+int cbdgam_b200_fill_guards(const cbdgam_grid_t *grid, double *primitive, void *stream)
+{
+    if (!grid_ok(grid) || !primitive)
+        return CBD_ERR_ARGUMENT;
+    const long n = (long)(grid->ni + 4) * (grid->nj + 4);
+    guards_kernel<<<blocks_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(grid->ni, grid->nj,
+                                                                                      primitive);
+    return status_of(cudaGetLastError());
+}
+
+size_t cbdgam_b200_scratch_bytes(const cbdgam_grid_t *grid)
+{
+    if (!grid_ok(grid))
+        return 0;
+    return (size_t)RED_BLOCKS * RED_VALUES * sizeof(double);
+}
+
+int cbdgam_b200_reduce(const cbdgam_grid_t *grid, const cbd_mass_t *masses, const cbd_diag_t *diags, int num_diags,
+                       const double *primitive, double *scratch, double *result, void *stream)
+{
+    if (!grid_ok(grid) || !masses || !primitive || !scratch || !result || num_diags < 0 ||
+        num_diags > MAX_DIAG || (num_diags > 0 && !diags))
+        return CBD_ERR_ARGUMENT;
+    RedArgs r;
+    std::memset(&r, 0, sizeof(r));
+    r.k = consts_of(grid);
+    r.m[0] = mass_of(masses[0]);
+    r.m[1] = mass_of(masses[1]);
+    for (int d = 0; d < num_diags; ++d) {
+        const cbd_diag_t &src = diags[d];
+        if (src.quantity != CBD_Q_MDOT && src.quantity != CBD_Q_TORQUE && src.quantity != CBD_Q_SIGMA_M1 &&
+            src.quantity != CBD_Q_ECCENTRICITY_VECTOR)
+            return CBD_ERR_ARGUMENT;
+        const bool rates = src.quantity == CBD_Q_MDOT || src.quantity == CBD_Q_TORQUE;
+        if (rates && ((!src.accretion && !src.gravity) || src.which_mass < 1 || src.which_mass > 3))
+            return CBD_ERR_ARGUMENT;
+        r.d[d] = Diag{src.quantity, src.which_mass, src.gravity, src.accretion, src.has_cut, src.r0, src.r1};
+    }
+    r.nd = num_diags;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    reduce_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(r, primitive, scratch);
+    finish_kernel<<<1, 32, 0, s>>>(scratch, RED_BLOCKS, result);
+    return status_of(cudaGetLastError());
+}
+
+}  // extern "C"

@@ -101,13 +101,15 @@ def _binary_point_masses(setup, time, x_offset=None):
 
 class CircumbinaryDisk(SetupBase):
     """
-    Isothermal circumbinary disk (sailfish/setups/circumbinary_disk.py:17-215):
-    uniform surface density, Keplerian rotation about the origin with a
-    softened radius, a binary on a Kepler orbit, Keplerian buffer beyond
-    domain_radius - 1.
+    Circumbinary disk, isothermal or gamma-law
+    (sailfish/setups/circumbinary_disk.py:17-215): Keplerian rotation about
+    the origin with a softened radius and a binary on a Kepler orbit. The
+    isothermal disk has uniform surface density (cbdiso_2d); the gamma-law
+    disk the power laws Sigma ~ r^-3/5, P ~ r^-3/2 with an inner taper
+    (cbdgam_2d).
     """
 
-    eos = param("isothermal", "EOS type (only isothermal uses cbdiso_2d)")
+    eos = param("isothermal", "EOS type: either isothermal or gamma-law")
     domain_radius = param(12.0, "half side length of the square computational domain")
     mach_number = param(10.0, "orbital Mach number (isothermal)", mutable=True)
     eccentricity = param(0.0, "orbital eccentricity of the binary", mutable=True)
@@ -117,22 +119,28 @@ class CircumbinaryDisk(SetupBase):
     softening_length = param(0.05, "gravitational softening length", mutable=True)
     buffer_is_enabled = param(True, "whether the buffer zone is enabled", mutable=True)
     sink_model = param("torque_free", "sink [acceleration_free|force_free|torque_free]", mutable=True)
-    initial_sigma = param(1.0, "initial disk surface density")
-    # gamma-law parameters, kept so that parameter sets (and checkpoints) of
-    # the reference setup load unchanged; the isothermal solver ignores them
+    initial_sigma = param(1.0, "initial disk surface density at r=a (gamma-law)")
     initial_pressure = param(1e-2, "initial disk surface pressure at r=a (gamma-law)")
     cooling_coefficient = param(0.0, "strength of the cooling term (gamma-law)")
     alpha = param(0.1, "alpha-viscosity parameter (gamma-law)")
     nu = param(0.001, "kinematic viscosity parameter (isothermal)")
-    constant_softening = param(True, "whether to use constant softening")
+    constant_softening = param(True, "whether to use constant softening (gamma-law)")
     gamma_law_index = param(5.0 / 3.0, "adiabatic index (gamma-law)")
     which_diagnostics = param("none", "diagnostics set to get from solver [none|mdots]")
 
     def validate(self):
-        if self.eos != "isothermal":
-            raise SetupError(f"this build supports eos=isothermal only, got {self.eos}")
+        if not self.is_isothermal and not self.is_gamma_law:
+            raise SetupError(f"eos must be isothermal or gamma-law, got {self.eos}")
         if self.which_diagnostics not in ["none", "mdots"]:
             raise SetupError(f"which_diagnostics must be none or mdots, got {self.which_diagnostics}")
+
+    @property
+    def is_isothermal(self):
+        return self.eos == "isothermal"
+
+    @property
+    def is_gamma_law(self):
+        return self.eos == "gamma-law"
 
     def primitive(self, t, coords, primitive):
         GM = 1.0
@@ -141,18 +149,36 @@ class CircumbinaryDisk(SetupBase):
         r_softened = sqrt(x * x + y * y + self.softening_length * self.softening_length)
         phi_hat_x = -y / max(r, 1e-12)
         phi_hat_y = +x / max(r, 1e-12)
-        primitive[0] = self.initial_sigma
-        primitive[1] = sqrt(GM / r_softened) * phi_hat_x
-        primitive[2] = sqrt(GM / r_softened) * phi_hat_y
+        if self.is_isothermal:
+            primitive[0] = self.initial_sigma
+            primitive[1] = sqrt(GM / r_softened) * phi_hat_x
+            primitive[2] = sqrt(GM / r_softened) * phi_hat_y
+        elif self.is_gamma_law:
+            # Goodman (2003) eq. (A2): power laws with an inner taper
+            taper = 0.0001 + 0.9999 * exp(-((1.0 / r_softened) ** 30))
+            primitive[0] = self.initial_sigma * r_softened ** (-3.0 / 5.0) * taper
+            primitive[1] = sqrt(GM / r_softened) * phi_hat_x
+            primitive[2] = sqrt(GM / r_softened) * phi_hat_y
+            primitive[3] = self.initial_pressure * r_softened ** (-3.0 / 2.0) * taper
 
     def primitive_array(self, t, x, y):
+        """primitive() on whole arrays of zone centres. The isothermal fields
+        match primitive() bit for bit; the gamma-law power laws and taper go
+        through numpy's pow / exp, which may differ from Python's math in
+        the last place."""
         GM = 1.0
         r = np.sqrt(x * x + y * y)
         r_softened = np.sqrt(x * x + y * y + self.softening_length * self.softening_length)
-        out = np.empty(np.broadcast(x, y).shape + (3,))
-        out[..., 0] = self.initial_sigma
+        nq = 4 if self.is_gamma_law else 3
+        out = np.empty(np.broadcast(x, y).shape + (nq,))
         out[..., 1] = np.sqrt(GM / r_softened) * (-y / np.maximum(r, 1e-12))
         out[..., 2] = np.sqrt(GM / r_softened) * (+x / np.maximum(r, 1e-12))
+        if self.is_gamma_law:
+            taper = 0.0001 + 0.9999 * np.exp(-((1.0 / r_softened) ** 30))
+            out[..., 0] = self.initial_sigma * r_softened ** (-3.0 / 5.0) * taper
+            out[..., 3] = self.initial_pressure * r_softened ** (-3.0 / 2.0) * taper
+        else:
+            out[..., 0] = self.initial_sigma
         return out
 
     def mesh(self, resolution):
@@ -164,6 +190,21 @@ class CircumbinaryDisk(SetupBase):
 
     @property
     def physics(self):
+        if self.is_gamma_law:
+            return dict(
+                eos_type=EquationOfState.GAMMA_LAW,
+                gamma_law_index=self.gamma_law_index,
+                point_mass_function=self.point_masses,
+                buffer_is_enabled=self.buffer_is_enabled,
+                buffer_driving_rate=1000.0,
+                buffer_onset_width=0.1,
+                cooling_coefficient=self.cooling_coefficient,
+                constant_softening=self.constant_softening,
+                viscosity_model=ViscosityModel.CONSTANT_ALPHA if self.alpha > 0.0 else ViscosityModel.NONE,
+                viscosity_coefficient=0.0,
+                alpha=self.alpha,
+                diagnostics=self.diagnostics,
+            )
         return dict(
             eos_type=EquationOfState.LOCALLY_ISOTHERMAL,
             mach_number=self.mach_number,
@@ -191,7 +232,7 @@ class CircumbinaryDisk(SetupBase):
 
     @property
     def solver(self):
-        return "cbdiso_2d"
+        return "cbdgam_2d" if self.is_gamma_law else "cbdiso_2d"
 
     @property
     def default_end_time(self):

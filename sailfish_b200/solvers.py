@@ -21,9 +21,9 @@ def register_solver_extension(solver_name):
 
 
 def make_solver(name, physics, options, **kwargs):
-    from . import cbdiso_2d
+    from . import cbdgam_2d, cbdiso_2d
 
-    solvers = dict(cbdiso_2d=cbdiso_2d)
+    solvers = dict(cbdiso_2d=cbdiso_2d, cbdgam_2d=cbdgam_2d)
     for ext_name in _extension_modules:
         solvers[ext_name] = import_module(ext_name)
     try:

@@ -1,0 +1,379 @@
+"""
+Parity of the gamma-law CUDA path (cbdgam_2d) with the gamma-law oracle and
+the fixtures the reference solver wrote (tests/golden/gam_*.npz).
+
+The kernels run the reference's arithmetic operation by operation without
+FMA contraction; they differ from the CPU build only where CUDA's pow / exp
+round differently from glibc's (about one ulp). Tolerances, per field as
+max|a - b| / max|b|:
+  * one stage or one step: 1e-13;
+  * the fixtures' runs (12 to 60 steps) and 1000 steps at 48^2: 1e-12 and
+    1e-10 (the parity bar: 1e-12 per step, 1e-10 after 1000 steps);
+  * diagnostic sums, which cancel: 1e-12 of sum |f| dA.
+"""
+
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+from cases import diagnostics, gam_initial_state, gam_names, gam_oracle_config, load
+from oracle import host_gam as og
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from sailfish_b200 import _capi, make_solver  # noqa: E402
+from sailfish_b200.mesh import PlanarCartesian2DMesh  # noqa: E402
+from sailfish_b200.physics import Diagnostic  # noqa: E402
+from sailfish_b200.setups import CircumbinaryDisk  # noqa: E402
+
+NG = 2
+
+
+def field_error(a, b):
+    return max(float(np.abs(a[..., q] - b[..., q]).max() / max(np.abs(b[..., q]).max(), 1e-300))
+               for q in range(a.shape[-1]))
+
+
+def gam_solver(d, **options):
+    meta = d["meta"]
+    x0, y0, x1, y1, ni, nj = meta["mesh"]
+    setup = CircumbinaryDisk(**meta["params"])
+    mesh = PlanarCartesian2DMesh(x0, y0, x1, y1, int(ni), int(nj))
+    physics = setup.physics
+    physics["diagnostics"] = diagnostics(meta)
+    opts = dict(plm_theta=meta["theta"])
+    opts.update(options)
+    return make_solver("cbdgam_2d", physics, opts, setup=setup, mesh=mesh, solution=gam_initial_state(d),
+                       num_patches=meta["patches"])
+
+
+def sums_scale(meta, state, time, want):
+    """sum |f| dA of each diagnostic on `state` (the oracle), or the largest
+    recorded value when that is larger."""
+    cfg = gam_oracle_config(meta)
+    o = og.GamOracleSolver(cfg, state, time)
+    scale = np.abs(np.array(o.reductions(diagnostics(meta), num_patches=1, absolute=True), dtype=complex))
+    return np.maximum(scale, np.abs(want).max(axis=0))
+
+
+@pytest.mark.parametrize("name", gam_names())
+def test_gamma_solver_matches_reference_fixtures(name):
+    d = load(name)
+    meta = d["meta"]
+    s = gam_solver(d)
+    assert s.recommended_cfl == 0.1 and s.maximum_cfl == 0.4
+    dts, series, first = [], [], None
+    for n in range(meta["steps"]):
+        dt = s.mesh.min_spacing() / s.maximum_wavespeed() * meta["cfl"]
+        s.advance(dt)
+        dts.append(dt)
+        series.append(s.reductions())
+        if n == 0:
+            first = s.solution
+    np.testing.assert_allclose(dts, d["dts"], rtol=1e-13, atol=0)
+    assert s.time == pytest.approx(float(d["time"]), rel=1e-14)
+    last = s.solution
+    if "last" in d:
+        assert field_error(first, d["first"]) <= 1e-13
+        assert field_error(last, d["last"]) <= 1e-12
+        state = d["last"]
+    else:
+        assert field_error(first[::8, ::8], d["first_sub"]) <= 1e-13
+        assert field_error(last[::8, ::8], d["last_sub"]) <= 1e-12
+        state = last
+    got = np.array(series, dtype=complex)
+    want = d["series"]
+    scale = sums_scale(meta, state, float(d["time"]), want)
+    assert (np.abs(got - want).max(axis=0) / np.maximum(scale, 1e-300)).max() <= 1e-12
+
+
+def test_gamma_1000_steps_against_oracle():
+    """48^2 with viscosity, cooling, the buffer and an eccentric binary:
+    1000 steps with the oracle's own dt sequence, states within 1e-10."""
+    d = load("gam_n48_cool_p2")
+    meta = dict(d["meta"])
+    cfg = gam_oracle_config(meta)
+    o = og.GamOracleSolver(cfg, gam_initial_state(d), 0.0)
+    s = gam_solver(d)
+    for n in range(1000):
+        dt = og.driver_dt(o, 0.1)
+        o.advance(dt)
+        s.advance(dt)
+        if n in (0, 99):
+            assert field_error(s.solution, o.solution) <= (1e-13 if n == 0 else 1e-11)
+    assert field_error(s.solution, o.solution) <= 1e-10
+    assert s.time == o.time
+
+
+# ---------------------------------------------------------------------------
+# the drop-in kernels through the C-ABI, on device arrays
+# ---------------------------------------------------------------------------
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _oracle_state(name, steps=2):
+    d = load(name)
+    cfg = gam_oracle_config(d["meta"])
+    s = og.GamOracleSolver(cfg, gam_initial_state(d), 0.0)
+    for _ in range(steps):
+        s.advance(og.driver_dt(s, 0.1))
+    s._set_bc()
+    return cfg, s
+
+
+def _buffer_args(cfg, s, m1, m2):
+    return (cfg.buffer_surface_density, cfg.buffer_surface_pressure, m1.mass + m2.mass, cfg.buffer_driving_rate,
+            s.buffer_outer_radius, cfg.buffer_onset_width, int(cfg.buffer_is_enabled))
+
+
+def _tail(cfg, a, dt):
+    return (cfg.alpha, a, dt, cfg.velocity_ceiling, cfg.cooling_coefficient, cfg.mach_ceiling, cfg.density_floor,
+            cfg.pressure_floor, int(cfg.constant_softening))
+
+
+def _set_stream(lib):
+    lib.cbdiso_b200_set_stream(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+
+
+@pytest.mark.parametrize("name", gam_names())
+@pytest.mark.parametrize("a", [0.0, 0.5])
+def test_dropin_advance_rk_matches_oracle(name, a):
+    cfg, s = _oracle_state(name)
+    lib = _capi.lib()
+    _set_stream(lib)
+    assert lib.cbdgam_b200_set_plm_theta(cfg.plm_theta) == 0
+    u0 = np.zeros_like(s.p1)
+    s.k.primitive_to_conserved(cfg.ni, cfg.nj, s.p1, u0, cfg.gamma_law_index)
+    m1, m2 = cfg.point_masses(s.time)
+    buf = _buffer_args(cfg, s, m1, m2)
+    dt = 0.7 * og.driver_dt(s, 0.1)
+    want = np.zeros_like(s.p1)
+    s.k.advance_rk(cfg, s.xl, s.xr, s.yl, s.yr, u0, s.p1, want, buf, m1, m2, a, dt)
+    du0, dp = _dev(u0), _dev(s.p1)
+    dw = torch.zeros(s.p1.shape, dtype=torch.float64, device="cuda")
+    st = lib.cbdgam_2d_advance_rk(cfg.ni, cfg.nj, s.xl, s.xr, s.yl, s.yr, _ptr(du0), _ptr(dp), _ptr(dw),
+                                  cfg.gamma_law_index, *buf, *m1.args(), *m2.args(), *_tail(cfg, a, dt))
+    assert st == 0
+    got = dw.cpu().numpy()
+    assert field_error(got[NG:-NG, NG:-NG], want[NG:-NG, NG:-NG]) <= 1e-13
+    # guard zones untouched, as in the reference
+    assert not got[:NG].any() and not got[:, :NG].any() and not got[-NG:].any() and not got[:, -NG:].any()
+
+
+@pytest.mark.parametrize("name", ["gam_n64", "gam_n40_soft_inviscid"])
+def test_dropin_small_kernels_match_oracle(name):
+    cfg, s = _oracle_state(name)
+    lib = _capi.lib()
+    _set_stream(lib)
+    g = cfg.gamma_law_index
+    dp = _dev(s.p1)
+    # wavespeed: sqrt and comparisons only, bit for bit
+    want = np.zeros(s.p1.shape[:2])
+    s.k.wavespeed(cfg.ni, cfg.nj, s.p1, want, g)
+    dws = torch.zeros(want.shape, dtype=torch.float64, device="cuda")
+    assert lib.cbdgam_2d_wavespeed(cfg.ni, cfg.nj, _ptr(dp), _ptr(dws), g) == 0
+    np.testing.assert_array_equal(dws.cpu().numpy(), want)
+    # primitive to conserved, bit for bit
+    want = np.zeros_like(s.p1)
+    s.k.primitive_to_conserved(cfg.ni, cfg.nj, s.p1, want, g)
+    du = torch.zeros(s.p1.shape, dtype=torch.float64, device="cuda")
+    assert lib.cbdgam_2d_primitive_to_conserved(cfg.ni, cfg.nj, _ptr(dp), _ptr(du), g) == 0
+    np.testing.assert_array_equal(du.cpu().numpy(), want)
+    # point-mass source terms for each mass, gravity and accretion parts
+    m1, m2 = cfg.point_masses(s.time)
+    for which in (1, 2):
+        for grav, acc in ((1.0, 0.0), (0.0, 1.0), (1.0, 1.0)):
+            a1, a2 = m1.args(grav, acc), m2.args(grav, acc)
+            want = np.zeros_like(s.p1)
+            s.k.point_mass_source_term(cfg.ni, cfg.nj, s.xl, s.xr, s.yl, s.yr, a1, a2, which, s.p1, want,
+                                       cfg.constant_softening, g)
+            dr = torch.zeros(s.p1.shape, dtype=torch.float64, device="cuda")
+            assert lib.cbdgam_2d_point_mass_source_term(cfg.ni, cfg.nj, s.xl, s.xr, s.yl, s.yr, *a1, *a2, which,
+                                                        _ptr(dp), _ptr(dr), int(cfg.constant_softening), g) == 0
+            got = dr.cpu().numpy()
+            for q in range(4):
+                scale = max(np.abs(want[..., q]).max(), 1e-300)
+                assert np.abs(got[..., q] - want[..., q]).max() <= 1e-14 * scale
+
+
+# ---------------------------------------------------------------------------
+# the product stage and reductions
+# ---------------------------------------------------------------------------
+
+
+def _grid(cfg, s):
+    g = _capi.GamGrid()
+    g.ni, g.nj = cfg.ni, cfg.nj
+    g.xl, g.xr, g.yl, g.yr = s.xl, s.xr, s.yl, s.yr
+    g.plm_theta = cfg.plm_theta
+    g.gamma_law_index = cfg.gamma_law_index
+    g.alpha = cfg.alpha
+    g.cooling_coefficient = cfg.cooling_coefficient
+    g.mach_ceiling = cfg.mach_ceiling
+    g.velocity_ceiling = cfg.velocity_ceiling
+    g.density_floor = cfg.density_floor
+    g.pressure_floor = cfg.pressure_floor
+    g.constant_softening = int(cfg.constant_softening)
+    g.buffer_is_enabled = int(cfg.buffer_is_enabled)
+    g.buffer_surface_density = cfg.buffer_surface_density
+    g.buffer_surface_pressure = cfg.buffer_surface_pressure
+    g.buffer_driving_rate = cfg.buffer_driving_rate
+    g.buffer_outer_radius = s.buffer_outer_radius
+    g.buffer_onset_width = cfg.buffer_onset_width
+    return g
+
+
+def _mass(m, out):
+    (out.x, out.y, out.vx, out.vy, out.mass, out.softening_length, out.sink_rate, out.sink_radius,
+     out.sink_model) = m.args()
+
+
+def _clamped_guards(a):
+    """Zero-gradient guard images of the interior of a padded array."""
+    ni, nj = a.shape[0] - 2 * NG, a.shape[1] - 2 * NG
+    ii = np.clip(np.arange(-NG, ni + NG), 0, ni - 1) + NG
+    jj = np.clip(np.arange(-NG, nj + NG), 0, nj - 1) + NG
+    return a[ii][:, jj]
+
+
+@pytest.mark.parametrize("name", ["gam_n48_cool_p2", "gam_n40_soft_inviscid"])
+def test_product_stage_equals_dropin_bit_for_bit(name):
+    """advance_stage rebuilds u_n from primitive_n in the kernel and writes
+    the guards; the drop-in kernel reads u_n from the conserved array: the
+    interiors agree bit for bit, the guards are the edge zones' images, and
+    the fused wavespeed maximum is the maximum over the written state."""
+    cfg, s = _oracle_state(name)
+    lib = _capi.lib()
+    _set_stream(lib)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert lib.cbdgam_b200_set_plm_theta(cfg.plm_theta) == 0
+    g = _grid(cfg, s)
+    m1, m2 = cfg.point_masses(s.time)
+    dt = 0.7 * og.driver_dt(s, 0.1)
+    pn = s.p1.copy()
+    prd = s.p1 * (1.0 + 1e-3 * np.cos(np.arange(s.p1.size).reshape(s.p1.shape)))  # a distinct stage input
+    prd = _clamped_guards(prd)
+    dpn, dprd = _dev(pn), _dev(prd)
+    du = torch.zeros_like(dpn)
+    assert lib.cbdgam_2d_primitive_to_conserved(cfg.ni, cfg.nj, _ptr(dpn), _ptr(du), cfg.gamma_law_index) == 0
+    for a in (0.0, 0.5):
+        # a = 0 reads the step's starting state, whose u_n is du; a = 0.5 a
+        # distinct stage input with u_n from the starting state
+        want = torch.zeros_like(dpn)
+        buf = _buffer_args(cfg, s, m1, m2)
+        src = dprd if a else dpn
+        assert lib.cbdgam_2d_advance_rk(cfg.ni, cfg.nj, s.xl, s.xr, s.yl, s.yr, _ptr(du), _ptr(src), _ptr(want),
+                                        cfg.gamma_law_index, *buf, *m1.args(), *m2.args(),
+                                        *_tail(cfg, a, dt)) == 0
+        st = _capi.GamStage()
+        _mass(m1, st.mass[0])
+        _mass(m2, st.mass[1])
+        st.buffer_central_mass = m1.mass + m2.mass
+        st.a, st.dt = a, dt
+        got = torch.full_like(dpn, float("nan"))
+        wsmax = torch.zeros(1, dtype=torch.float64, device="cuda")
+        assert lib.cbdgam_b200_advance_stage(ctypes.byref(g), ctypes.byref(st), _ptr(src),
+                                             _ptr(dpn) if a else None, _ptr(got), _ptr(wsmax), stream) == 0
+        got_h, want_h = got.cpu().numpy(), want.cpu().numpy()
+        np.testing.assert_array_equal(got_h[NG:-NG, NG:-NG], want_h[NG:-NG, NG:-NG])
+        np.testing.assert_array_equal(got_h, _clamped_guards(got_h))
+        ws = torch.zeros(got.shape[:2], dtype=torch.float64, device="cuda")
+        assert lib.cbdgam_2d_wavespeed(cfg.ni, cfg.nj, _ptr(got), _ptr(ws), cfg.gamma_law_index) == 0
+        assert float(wsmax.item()) == float(ws.max().item())
+    # in place over primitive_n (the RK2 step's second stage)
+    st.a = 0.5
+    inplace = dpn.clone()
+    assert lib.cbdgam_b200_advance_stage(ctypes.byref(g), ctypes.byref(st), _ptr(dprd), _ptr(inplace),
+                                         _ptr(inplace), None, stream) == 0
+    np.testing.assert_array_equal(inplace.cpu().numpy()[NG:-NG, NG:-NG], got.cpu().numpy()[NG:-NG, NG:-NG])
+
+
+@pytest.mark.parametrize("name", ["gam_n48_cool_p2", "gam_n40_soft_inviscid"])
+def test_reductions_match_oracle(name):
+    cfg, s = _oracle_state(name, steps=3)
+    d = load(name)
+    meta = d["meta"]
+    solver = gam_solver(d)
+    # load the oracle's state into the solver
+    solver._buf[0].copy_(_dev(s.p1))
+    solver._time = s.time
+    solver._ws_valid = False
+    assert solver.maximum_wavespeed() == s.maximum_wavespeed()
+    got = np.array(solver.reductions(), dtype=complex)
+    want = np.array(s.reductions(diagnostics(meta), num_patches=meta["patches"]), dtype=complex)
+    scale = np.abs(np.array(s.reductions(diagnostics(meta), absolute=True), dtype=complex))
+    assert (np.abs(got - want) / np.maximum(scale, 1e-300)).max() <= 1e-13
+
+
+def test_reductions_more_than_four_device_diagnostics():
+    """Five device sums run as two reduction launches."""
+    d = load("gam_n40_soft_inviscid")
+    meta = d["meta"]
+    cfg, s = _oracle_state("gam_n40_soft_inviscid", steps=1)
+    solver = gam_solver(d)
+    solver._buf[0].copy_(_dev(s.p1))
+    solver._time = s.time
+    diags = diagnostics(meta)[1:] + [dict(quantity="mdot", which_mass="both", accretion=True)]
+    solver._physics = solver._physics._replace(diagnostics=[Diagnostic(**x) for x in diags])
+    got = np.array(solver.reductions(), dtype=complex)
+    want = np.array(s.reductions(diags), dtype=complex)
+    scale = np.abs(np.array(s.reductions(diags, absolute=True), dtype=complex))
+    assert len(got) == 7
+    assert (np.abs(got - want) / np.maximum(scale, 1e-300)).max() <= 1e-13
+
+
+# ---------------------------------------------------------------------------
+# the correctly rounded powers
+# ---------------------------------------------------------------------------
+
+
+def _rn(value):
+    """A Decimal or Fraction rounded to the nearest double."""
+    return float(value)
+
+
+def test_powers_are_correctly_rounded():
+    """cube, x^-2, x^-3, x^4, x^-1.5, (1 + x)^RN(-1/3) and exp(-x) against
+    exact rationals or 60-digit decimals, rounded once."""
+    import decimal
+    from fractions import Fraction
+
+    decimal.getcontext().prec = 60
+    rng = np.random.default_rng(2024)
+    x = np.concatenate([rng.uniform(0.0, 1.0, 300), np.exp(rng.uniform(-20, 20, 300)),
+                        rng.uniform(0.0, 256.0, 200), [1.0, 2.0, 0.5, 1e-12, 3.0, 255.9]])
+    dx = _dev(x)
+    out = torch.zeros(8 * len(x), dtype=torch.float64, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert _capi.lib().cbdgam_b200_eval_powers(len(x), _ptr(dx), _ptr(out), stream) == 0
+    got = out.cpu().numpy().reshape(-1, 8)
+    y13 = decimal.Decimal(-1.0 / 3.0)
+    glibc_agree = 0
+    for v, g in zip(x, got):
+        v = float(v)
+        f = Fraction(v)
+        d = decimal.Decimal(v)
+        one_plus = 1.0 + v  # the kernel's argument is the rounded sum
+        want = [_rn(f ** 3), _rn(1 / f ** 2) if v else g[1], _rn(1 / f ** 3) if v else g[2], _rn(f ** 4),
+                _rn(1 / (d * d.sqrt())) if v else g[4], _rn((decimal.Decimal(one_plus).ln() * y13).exp()),
+                _rn((-d).exp()) if v < 700.0 else g[6]]
+        assert list(g[:7]) == want, (v, list(g[:7]), want)
+        glibc = [math.pow(v, 3.0), math.pow(v, -2.0) if v else g[1], math.pow(v, -3.0) if v else g[2],
+                 math.pow(v, 4.0), math.pow(v, -1.5) if v else g[4], math.pow(one_plus, -1.0 / 3.0),
+                 math.exp(-v)]
+        glibc_agree += list(g[:7]) == glibc
+    # the C library's pow / exp are correctly rounded in nearly every case
+    assert glibc_agree >= 0.99 * len(x)
