@@ -452,6 +452,109 @@ def batched_adjoint_extra():
             "timing": "host wall clock (forward + gradient), CUDA events (batched forward)"}
 
 
+GAM_SIZE = 2048
+GAM_BYTES_PER_ZONE_STEP = 160  # stage 1: read 32 B + write 32 B; stage 2: read 2 x 32 B + write 32 B
+
+
+def gamma_law_extra(steps=50, warmup=5):
+    """The gamma-law solver (cbdgam_2d): a 2048^2 gamma-law circumbinary disk
+    (alpha 0.1, buffer, constant softening, torque-free sinks, CFL 0.1), the
+    reference's driver loop through the public API (dt from the wavespeed
+    maximum every step), timed with CUDA events after warm-up; the stage
+    kernel alone for its roofline; the reference's own gamma-law CPU kernels
+    on a 512^2 sample beside it."""
+    import ctypes
+
+    import torch
+
+    from sailfish_b200 import _capi, make_solver
+
+    setup = _gamma_setup()
+    mesh = setup.mesh(GAM_SIZE)
+    s = make_solver("cbdgam_2d", setup.physics, {}, setup=setup, mesh=mesh)
+    zones = GAM_SIZE * GAM_SIZE
+    for _ in range(warmup):
+        s.advance(mesh.min_spacing() / s.maximum_wavespeed() * 0.1)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(steps):
+        s.advance(mesh.min_spacing() / s.maximum_wavespeed() * 0.1)
+    stop.record()
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop) / steps
+
+    # the second-stage kernel alone (reads two states, writes one)
+    lib, g = s._lib, s._grid
+    stage = s._stage(s.time, 0.5, mesh.min_spacing() / s.maximum_wavespeed() * 0.1)
+    out = torch.empty_like(s._buf[0])
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def launch():
+        _capi.check(lib.cbdgam_b200_advance_stage(ctypes.byref(g), ctypes.byref(stage), s._ptr(s._buf[0]),
+                                                  s._ptr(s._buf[1]), s._ptr(out), None, stream), "stage")
+
+    for _ in range(3):
+        launch()
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(20):
+        launch()
+    stop.record()
+    torch.cuda.synchronize()
+    kernel_s = start.elapsed_time(stop) * 1e-3 / 20
+    peak, peak_kind = measured_peaks()
+    achieved = 96.0 * zones / kernel_s / 1e9
+    line = {"workload": f"cbdgam_2d gamma-law circumbinary disk {GAM_SIZE}x{GAM_SIZE} FP64 RK2 theta 1.5 CFL 0.1, "
+                        "alpha 0.1, buffer on", "zones": zones, "value": zones / (ms * 1e-3),
+            "unit": "zone-updates/s", "ms_per_step": ms, "steps": steps, "warmup": warmup,
+            "timed": "Solver.advance + maximum_wavespeed per step (one 8-byte read back), CUDA events",
+            "roofline": {"bound": "fp64 issue (HBM shown for reference)", "kernel": "gam::stage_kernel (RK stage 2)",
+                         "kernel_ms": round(kernel_s * 1e3, 4), "bytes_per_launch": 96 * zones,
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind}}
+    del s, out
+    try:
+        line["cpu_baseline"] = gamma_cpu_baseline()
+    except (FileNotFoundError, OSError) as e:
+        line["cpu_baseline"] = {"unavailable": str(e)}
+    return line
+
+
+def _gamma_setup():
+    from sailfish_b200.setups import CircumbinaryDisk
+
+    return CircumbinaryDisk(eos="gamma-law")
+
+
+def gamma_cpu_baseline(n=512, steps=3):
+    """The reference's gamma-law kernels (oracle/_ref, OpenMP) driven as its
+    solver adapter does (oracle/host_gam.py), on n^2 zones."""
+    from oracle import host_gam as og
+    from sailfish_b200.cbdgam_2d import initial_condition
+
+    setup = _gamma_setup()
+    mesh = setup.mesh(n)
+    prim = initial_condition(setup, mesh, 0.0)
+    onset = [0.0] * 4
+    setup.primitive(0.0, [mesh.x1 - 0.1, 0.0], onset)
+    from oracle import host as oh
+
+    cfg = og.GamConfig(mesh.x0, mesh.x1, mesh.y0, mesh.y1, n, n, alpha=setup.alpha, buffer_is_enabled=True,
+                       buffer_surface_density=onset[0], buffer_surface_pressure=onset[3],
+                       masses=oh.binary_masses(1.0, 1.0, 1.0, 0.0, 0.05, "torque_free", 10.0, 0.05))
+    kernels = og.GamKernels("ref", 1.5, threads="omp")
+    solver = og.GamOracleSolver(cfg, prim, 0.0, kernels)
+    solver.advance(og.driver_dt(solver, 0.1))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        solver.advance(og.driver_dt(solver, 0.1))
+    el = time.perf_counter() - t0
+    return {"value": n * n * steps / el, "unit": "zone-updates/s",
+            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())), "kind": "reference",
+            "sample": f"{steps} driver steps at {n}^2 (advance + wavespeed)"}
+
+
 # ---------------------------------------------------------------------------
 # the reference's CPU kernels (oracle/_ref) and the oracle port
 # ---------------------------------------------------------------------------
@@ -548,6 +651,7 @@ def main():
             line["batched"] = batched_extra(line["value"])
             line["adjoint"] = adjoint_extra()
             line["adjoint_batched"] = batched_adjoint_extra()
+            line["gamma_law"] = gamma_law_extra()
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             n = args.size
             v, kind, el = time_cpu(n, 2 if n >= 2048 else 5, 1, args.seed)

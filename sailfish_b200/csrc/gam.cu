@@ -4,16 +4,20 @@
 // scale height, softening that may follow the scale height, cooling, a
 // pressure floor and a Mach ceiling.
 //
-// Built with -fmad=false: every +, -, *, / and sqrt is the IEEE operation
-// the reference's CPU build performs, in the reference's order, so results
-// differ from it only where CUDA's pow / exp round differently from glibc's.
+// Built with -fmad=false: every +, -, *, / and sqrt gives the IEEE result the
+// reference's CPU build computes, in the reference's order, and every power
+// and exponential is correctly rounded (see below), so results differ from
+// the reference only where glibc's pow / exp are not (about one call in a
+// thousand for the non-integer exponents).
 //
-// One thread per zone over a CTA tile of 8 x 32 zones whose primitives (with
-// a two-zone halo) are staged in shared memory. The reference's face fluxes
-// are not shareable between the two zones of a face (each zone takes the
-// sound speed of the neighbour across the face, cbdgam_2d.c:608-611, and the
-// viscous flux the neighbour's scale height), so each zone computes its four
-// faces, as the reference does.
+// One thread per zone over a CTA tile of 8 x 32 zones. The tile's primitives
+// (with a two-zone halo) are staged in shared memory; a first phase computes
+// the per-zone quantities every neighbouring update needs (slopes, p / Sigma,
+// sound speed, strain) and the scale heights' face geometry, a second the
+// zone updates. The reference's face fluxes are not shareable between the two
+// zones of a face (each zone takes the sound speed of the neighbour across
+// the face, cbdgam_2d.c:608-611, and the viscous flux the neighbour's scale
+// height), so each zone computes its four faces, as the reference does.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -31,6 +35,7 @@ constexpr int NF = 4;
 constexpr int NG = 2;
 constexpr int TI = 8, TJ = 32;  // CTA tile (rows i, columns j)
 constexpr int HI = TI + 2 * NG, HJ = TJ + 2 * NG;
+constexpr int STAGE_MIN_BLOCKS = 2;  // resident CTAs per SM the stage kernel is built for
 
 struct Mass {
     double x, y, vx, vy, mass, soft, rate, radius;
@@ -46,11 +51,13 @@ struct Consts {
     double buf_sigma, buf_pressure, buf_rate, buf_outer, buf_width;
     double buf_onset_m3;  // pow(buf_outer - buf_width, -3.0), glibc's on the host
     double mach_m2;       // pow(mach_ceiling, -2.0), glibc's on the host
+    double inv_dx, inv_dy, gm1, inv_gm1, inv_gamma;  // RN(1 / dx), ..., gamma - 1, RN(1 / (gamma - 1)), RN(1 / gamma)
 };
 
 struct Stage {
     Mass m[2];
     double buf_mass, a, dt;
+    int massless;  // both masses have zero mass: every scale height is 1
     int write_guards;
     int un_from_primitive;  // u_n = cons(primitive_n) in-kernel (else: a conserved array)
 };
@@ -196,14 +203,6 @@ __device__ __forceinline__ double slope(double yl, double y0, double yr, double 
     return 0.25 * fabs(sign_of(a) + sign_of(b)) * (sign_of(a) + sign_of(c)) * m;
 }
 
-template <class A, class B, class C>
-__device__ __forceinline__ void slopes(const A &yl, const B &y0, const C &yr, double theta, double *g)
-{
-#pragma unroll
-    for (int q = 0; q < NF; ++q)
-        g[q] = slope(yl[q], y0[q], yr[q], theta);
-}
-
 // cbdgam_2d.c:75-106
 template <class V>
 __device__ __forceinline__ double scale_height(const Mass *m, double x, double y, const V &p)
@@ -295,36 +294,177 @@ __device__ __forceinline__ void buffer_source(const Consts &k, double buf_mass, 
     }
 }
 
-// cbdgam_2d.c:278-294 (xx, xy, yx, yy)
-__device__ __forceinline__ void strain(const double *gx, const double *gy, double dx, double dy, double *s)
+// cbdgam_2d.c:347-362
+template <class V>
+__device__ __forceinline__ void prim_to_cons(const V &p, double *u, double gamma)
 {
-    const double sxx = 4.0 / 3.0 * gx[1] / dx - 2.0 / 3.0 * gy[2] / dy;
-    const double syy = -2.0 / 3.0 * gx[1] / dx + 4.0 / 3.0 * gy[2] / dy;
-    const double sxy = 1.0 / 1.0 * gx[2] / dx + 1.0 / 1.0 * gy[1] / dy;
-    s[0] = sxx;
-    s[1] = sxy;
-    s[2] = sxy;
-    s[3] = syy;
+    const double rho = p[0], vx = p[1], vy = p[2], pres = p[3];
+    u[0] = rho;
+    u[1] = vx * rho;
+    u[2] = vy * rho;
+    u[3] = pres / (gamma - 1.0) + 0.5 * rho * (vx * vx + vy * vy);
 }
 
-// cbdgam_2d.c:298-317
+// cbdgam_2d.c:401-409
 template <class V>
-__device__ __forceinline__ void cooling(const Consts &k, double dt, const V &p, double *u)
+__device__ __forceinline__ double max_wavespeed(const V &p, double cs2)
 {
-    const double gamma = k.gamma, sigma = p[0];
-    const double eps = p[3] / p[0] / (gamma - 1.0);
+    const double cs = sqrt(cs2);
+    const double ax = greater(fabs(p[1] - cs), fabs(p[1] + cs));
+    const double ay = greater(fabs(p[2] - cs), fabs(p[2] + cs));
+    return greater(ax, ay);
+}
+
+// ---------------------------------------------------------------------------
+// The stage kernel. The reference evaluates every quantity of a neighbour
+// inside each zone's update (cbdgam_2d.c:499-682): the x and y slopes of five
+// zones, four sound speeds, five scale heights and strain tensors. All of
+// these except the scale heights' geometry are per-zone values, and the
+// geometry is shared by the two zones of a face, so the kernel computes them
+// once per zone (per face) into shared memory in a first phase and the zone
+// updates read them in a second. Every value is computed by the same
+// operations in the same order as in the reference, so the split changes no
+// bit. Divisions by a constant (dx, dy, gamma - 1) or by one value several
+// times (the HLLE denominator, Sigma in the primitive recovery) use a
+// reciprocal rounded to nearest and a Markstein correction, which returns
+// the correctly rounded quotient.
+// ---------------------------------------------------------------------------
+
+// a / b rounded to nearest from y = RN(1 / b): the remainder a - q b of
+// q = RN(a y) is exact under FMA and one correction rounds to RN(a / b)
+__device__ __forceinline__ double div_by(double a, double b, double y)
+{
+    const double q = a * y;
+    return fma(fma(-q, b, a), y, q);
+}
+
+constexpr int ZI = TI + 2, ZJ = TJ + 2;  // zones with shared quantities: the tile and a ring of one
+// per-zone quantities: x and y slopes, p / Sigma, sound speed, sqrt(p / Sigma), strain xx, xy, yy
+enum { Q_GX = 0, Q_GY = 4, Q_T = 8, Q_CS = 9, Q_SQ = 10, Q_SXX = 11, Q_SXY = 12, Q_SYY = 13, NZQ = 14 };
+
+struct StageSmem {
+    double prim[NF][HI][HJ];
+    double z[NZQ][ZI][ZJ];
+    double fx[TI + 1][TJ];  // sqrt(sum_m M_m r^-3) at the x-faces (x_l of zone i0 + a, y_c of zone j0 + b)
+    double fy[TI][TJ + 1];  // the same at the y-faces (x_c of zone i0 + a, y_l of zone j0 + b)
+    double warp_max[TI * TJ / 32];
+};
+
+// sqrt(w2) of the scale height (cbdgam_2d.c:75-106) at (x, y)
+__device__ __forceinline__ double root_w2(const Mass *m, double x, double y)
+{
+    double w2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        if (m[k].mass > 0.0) {
+            const double dx = x - m[k].x, dy = y - m[k].y;
+            const double r = sqrt(dx * dx + dy * dy + 1e-12);
+            w2 += m[k].mass * inv_cube_rn(r);
+        }
+    }
+    return sqrt(w2);
+}
+
+// cbdgam_2d.c:347-362 with the constant divisor gamma - 1
+template <class V>
+__device__ __forceinline__ void p2c_fast(const Consts &k, const V &p, double *u)
+{
+    const double rho = p[0], vx = p[1], vy = p[2], pres = p[3];
+    u[0] = rho;
+    u[1] = vx * rho;
+    u[2] = vy * rho;
+    u[3] = div_by(pres, k.gm1, k.inv_gm1) + 0.5 * rho * (vx * vx + vy * vy);
+}
+
+// cbdgam_2d.c:411-434 given the neighbour's sound speed cs = sqrt(cs2)
+template <int DIR>
+__device__ __forceinline__ void hlle_fast(const Consts &k, const double *pl, const double *pr, double cs, double *f)
+{
+    double ul[NF], ur[NF];
+    p2c_fast(k, pl, ul);
+    p2c_fast(k, pr, ur);
+    const double vl = DIR == 0 ? pl[1] : pl[2], vr = DIR == 0 ? pr[1] : pr[2];
+    const double fl[NF] = {vl * ul[0], vl * ul[1] + pl[3] * (double)(DIR == 0), vl * ul[2] + pl[3] * (double)(DIR == 1),
+                           vl * (ul[3] + pl[3])};
+    const double fr[NF] = {vr * ur[0], vr * ur[1] + pr[3] * (double)(DIR == 0), vr * ur[2] + pr[3] * (double)(DIR == 1),
+                           vr * (ur[3] + pr[3])};
+    const double am = lesser(0.0, lesser(vl - cs, vr - cs));
+    const double ap = greater(0.0, greater(vl + cs, vr + cs));
+    const double den = ap - am, y = __drcp_rn(den);
+#pragma unroll
+    for (int q = 0; q < NF; ++q)
+        f[q] = div_by(fl[q] * ap - fr[q] * am - (ul[q] - ur[q]) * ap * am, den, y);
+}
+
+// cbdgam_2d.c:108-203 for the stage kernel: T = p / Sigma and h given
+template <class V>
+__device__ __forceinline__ void mass_source_fast(const Consts &k, const Mass &m, double x, double y, double dt,
+                                                 const V &p, double T, double h, double *du)
+{
+    const double sigma = p[0];
+    const double eps = div_by(T, k.gm1, k.inv_gm1);
+    const double dx = x - m.x, dy = y - m.y;
+    const double r2 = dx * dx + dy * dy;
+    const double dr = sqrt(r2);
+    const double rs = m.radius;
+    double soft;
+    if (k.constant_softening) {
+        soft = m.soft;
+    } else if (dr > rs) {
+        soft = 0.5 * h;
+    } else {
+        const double q = dr / rs;
+        const double w = (1.0 - q * q) * (1.0 - q * q);  // pow(., 2.0) is the correctly rounded square
+        soft = w * rs + (1.0 - w) * 0.5 * h;
+    }
+    const double rate = (dr < 4.0 * rs) ? m.rate * exp_rn(-fourth_rn(dr / rs)) : 0.0;
+    const double fnum = sigma * m.mass * inv_pow15_rn(r2 + soft * soft);
+    const double fx = -fnum * dx, fy = -fnum * dy;
+    const double mdot = sigma * rate * -1.0;
+    const double vx = p[1], vy = p[2];
+    if (m.model == 1) {
+        du[0] = dt * mdot;
+        du[1] = dt * mdot * p[1] + dt * fx;
+        du[2] = dt * mdot * p[2] + dt * fy;
+        du[3] = dt * (mdot * eps + 0.5 * mdot * (vx * vx + vy * vy)) + dt * (fx * vx + fy * vy);
+    } else if (m.model == 2) {
+        const double den = dr + 1e-12, yd = __drcp_rn(den);
+        const double ex = div_by(dx, den, yd), ey = div_by(dy, den, yd);
+        const double dvr = (vx - m.vx) * ex + (vy - m.vy) * ey;
+        const double wx = dvr * ex + m.vx, wy = dvr * ey + m.vy;
+        du[0] = dt * mdot;
+        du[1] = dt * mdot * wx + dt * fx;
+        du[2] = dt * mdot * wy + dt * fy;
+        du[3] = dt * (mdot * eps + 0.5 * mdot * (wx * wx + wy * wy)) + dt * (fx * vx + fy * vy);
+    } else if (m.model == 3) {
+        du[0] = dt * mdot;
+        du[1] = dt * fx;
+        du[2] = dt * fy;
+        du[3] = dt * (fx * vx + fy * vy);
+    } else {
+        du[0] = du[1] = du[2] = du[3] = 0.0;
+    }
+}
+
+// cbdgam_2d.c:298-317 with T = p / Sigma given
+template <class V>
+__device__ __forceinline__ void cooling_fast(const Consts &k, double dt, const V &p, double T, double *u)
+{
+    const double sigma = p[0];
+    const double eps = div_by(T, k.gm1, k.inv_gm1);
     double cooled = eps * pow_m13_rn(1.0 + 3.0 * k.cooling * inv_square_rn(sigma) * cube_rn(eps) * dt);
     const double ek = 0.5 * (p[1] * p[1] + p[2] * p[2]);
-    cooled = greater(cooled, 2.0 * ek / gamma / (gamma - 1.0) * k.mach_m2);  // pow(mach_ceiling, -2.0), host
+    cooled = greater(cooled, div_by(div_by(2.0 * ek, k.gamma, k.inv_gamma), k.gm1, k.inv_gm1) * k.mach_m2);
     u[3] += sigma * (cooled - eps);
 }
 
-// cbdgam_2d.c:319-345
-__device__ __forceinline__ void cons_to_prim(const Consts &k, const double *u, double *p)
+// cbdgam_2d.c:319-345 with one reciprocal of Sigma
+__device__ __forceinline__ void c2p_fast(const Consts &k, const double *u, double *p)
 {
-    double pres = greater(k.p_floor, (u[3] - 0.5 * (u[1] * u[1] + u[2] * u[2]) / u[0]) * (k.gamma - 1.0));
-    double vx = sign_of(u[1]) * lesser(fabs(u[1] / u[0]), k.vmax);
-    double vy = sign_of(u[2]) * lesser(fabs(u[2] / u[0]), k.vmax);
+    const double y = __drcp_rn(u[0]);
+    double pres = greater(k.p_floor, (u[3] - div_by(0.5 * (u[1] * u[1] + u[2] * u[2]), u[0], y)) * k.gm1);
+    double vx = sign_of(u[1]) * lesser(fabs(div_by(u[1], u[0], y)), k.vmax);
+    double vy = sign_of(u[2]) * lesser(fabs(div_by(u[2], u[0], y)), k.vmax);
     double rho = u[0];
     if (u[0] < k.rho_floor) {
         rho = k.rho_floor;
@@ -338,177 +478,164 @@ __device__ __forceinline__ void cons_to_prim(const Consts &k, const double *u, d
     p[3] = pres;
 }
 
-// cbdgam_2d.c:347-362
-template <class V>
-__device__ __forceinline__ void prim_to_cons(const V &p, double *u, double gamma)
+// a maximum that keeps a NaN operand, so that a NaN wavespeed reaches the host
+__device__ __forceinline__ double max_nan(double a, double b) { return (a > b || a != a) ? a : b; }
+
+// Phase 1: the per-zone quantities of zone (i0 - 1 + a, j0 - 1 + b) and the
+// face geometry of the tile.
+__device__ __forceinline__ void stage_phase1(const Consts &k, const Stage &st, StageSmem &sm, int i0, int j0, int tid)
 {
-    const double rho = p[0], vx = p[1], vy = p[2], pres = p[3];
-    u[0] = rho;
-    u[1] = vx * rho;
-    u[2] = vy * rho;
-    u[3] = pres / (gamma - 1.0) + 0.5 * rho * (vx * vx + vy * vy);
+    const double theta = k.theta;
+    for (int s = tid; s < ZI * ZJ; s += TI * TJ) {
+        const int a = s / ZJ, b = s % ZJ;
+        if (i0 - 1 + a > k.ni || j0 - 1 + b > k.nj)
+            continue;  // beyond the guard zones of the last tile: never read
+        double gx[NF], gy[NF];
+#pragma unroll
+        for (int q = 0; q < NF; ++q) {
+            gx[q] = slope(sm.prim[q][a][b + 1], sm.prim[q][a + 1][b + 1], sm.prim[q][a + 2][b + 1], theta);
+            gy[q] = slope(sm.prim[q][a + 1][b], sm.prim[q][a + 1][b + 1], sm.prim[q][a + 1][b + 2], theta);
+            sm.z[Q_GX + q][a][b] = gx[q];
+            sm.z[Q_GY + q][a][b] = gy[q];
+        }
+        const double T = sm.prim[3][a + 1][b + 1] / sm.prim[0][a + 1][b + 1];
+        sm.z[Q_T][a][b] = T;
+        sm.z[Q_CS][a][b] = sqrt(T * k.gamma);  // sqrt(cs2), cs2 = p / Sigma * gamma (cbdgam_2d.c:231-236)
+        sm.z[Q_SQ][a][b] = sqrt(T);
+        // strain (cbdgam_2d.c:278-294): (4/3 gx_vx) / dx - (2/3 gy_vy) / dy, ...
+        sm.z[Q_SXX][a][b] = div_by(4.0 / 3.0 * gx[1], k.dx, k.inv_dx) - div_by(2.0 / 3.0 * gy[2], k.dy, k.inv_dy);
+        sm.z[Q_SXY][a][b] = div_by(gx[2], k.dx, k.inv_dx) + div_by(gy[1], k.dy, k.inv_dy);
+        sm.z[Q_SYY][a][b] = div_by(-2.0 / 3.0 * gx[1], k.dx, k.inv_dx) + div_by(4.0 / 3.0 * gy[2], k.dy, k.inv_dy);
+    }
+    if (k.alpha > 0.0 && !st.massless) {
+        for (int s = tid; s < (TI + 1) * TJ; s += TI * TJ) {
+            const int a = s / TJ, b = s % TJ;
+            const int i = i0 + a, j = j0 + b;
+            sm.fx[a][b] = root_w2(st.m, k.xl + (i + 0.0) * k.dx, k.yl + (j + 0.5) * k.dy);
+        }
+        for (int s = tid; s < TI * (TJ + 1); s += TI * TJ) {
+            const int a = s / (TJ + 1), b = s % (TJ + 1);
+            const int i = i0 + a, j = j0 + b;
+            sm.fy[a][b] = root_w2(st.m, k.xl + (i + 0.5) * k.dx, k.yl + (j + 0.0) * k.dy);
+        }
+    }
 }
 
-// cbdgam_2d.c:364-434: HLLE flux across a face with normal DIR
-template <int DIR>
-__device__ __forceinline__ void hlle(const double *pl, const double *pr, double cs2, double gamma, double *f)
+// Phase 2: zone (i, j) = (i0 + ty, j0 + tx); returns its new primitives.
+__device__ __forceinline__ void stage_phase2(const Consts &k, const Stage &st, const StageSmem &sm, int ty, int tx,
+                                             const double *un, double *out)
 {
-    double ul[NF], ur[NF];
-    prim_to_cons(pl, ul, gamma);
-    prim_to_cons(pr, ur, gamma);
-    const double vl = DIR == 0 ? pl[1] : pl[2], vr = DIR == 0 ? pr[1] : pr[2];
-    const double fl[NF] = {vl * ul[0], vl * ul[1] + pl[3] * (double)(DIR == 0), vl * ul[2] + pl[3] * (double)(DIR == 1),
-                           vl * (ul[3] + pl[3])};
-    const double fr[NF] = {vr * ur[0], vr * ur[1] + pr[3] * (double)(DIR == 0), vr * ur[2] + pr[3] * (double)(DIR == 1),
-                           vr * (ur[3] + pr[3])};
-    const double cs = sqrt(cs2);
-    const double am = lesser(0.0, lesser(vl - cs, vr - cs));
-    const double ap = greater(0.0, greater(vl + cs, vr + cs));
+    const int i = blockIdx.y * TI + ty, j = blockIdx.x * TJ + tx;
+    const double dt = st.dt;
+    const double xc = k.xl + (i + 0.5) * k.dx, yc = k.yl + (j + 0.5) * k.dy;
+    // primitives and per-zone quantities of the zone and its four neighbours
+    auto P = [&](int di, int dj, int q) { return sm.prim[q][ty + NG + di][tx + NG + dj]; };
+    auto Z = [&](int di, int dj, int q) { return sm.z[q][ty + 1 + di][tx + 1 + dj]; };
+    double c[NF];
 #pragma unroll
     for (int q = 0; q < NF; ++q)
-        f[q] = (fl[q] * ap - fr[q] * am - (ul[q] - ur[q]) * ap * am) / (ap - am);
-}
-
-// cbdgam_2d.c:401-409
-template <class V>
-__device__ __forceinline__ double max_wavespeed(const V &p, double cs2)
-{
-    const double cs = sqrt(cs2);
-    const double ax = greater(fabs(p[1] - cs), fabs(p[1] + cs));
-    const double ay = greater(fabs(p[2] - cs), fabs(p[2] + cs));
-    return greater(ax, ay);
-}
-
-// One zone's stage update (cbdgam_2d.c:499-682); P(di, dj) gives the input
-// primitives of the zone (i + di, j + dj), indexed by field.
-template <class Load>
-__device__ void zone_update(const Consts &k, const Stage &st, int i, int j, const Load &P, const double *un,
-                            double *out)
-{
-    const double dx = k.dx, dy = k.dy, theta = k.theta, gamma = k.gamma;
-    const double xl = k.xl + (i + 0.0) * dx, xc = k.xl + (i + 0.5) * dx, xr = k.xl + (i + 1.0) * dx;
-    const double yl = k.yl + (j + 0.0) * dy, yc = k.yl + (j + 0.5) * dy, yr = k.yl + (j + 1.0) * dy;
-    const auto c = P(0, 0), w1 = P(-1, 0), e1 = P(1, 0), s1 = P(0, -1), n1 = P(0, 1);
-
-    double gxw[NF], gxc[NF], gxe[NF], gys[NF], gyc[NF], gyn[NF];
-    slopes(P(-2, 0), w1, c, theta, gxw);
-    slopes(w1, c, e1, theta, gxc);
-    slopes(c, e1, P(2, 0), theta, gxe);
-    slopes(P(0, -2), s1, c, theta, gys);
-    slopes(s1, c, n1, theta, gyc);
-    slopes(c, n1, P(0, 2), theta, gyn);
-
-    const double cs2w = cs2_of(gamma, w1), cs2e = cs2_of(gamma, e1);
-    const double cs2s = cs2_of(gamma, s1), cs2n = cs2_of(gamma, n1);
-    const double hc = scale_height(st.m, xc, yc, c);
+        c[q] = P(0, 0, q);
 
     double fw[NF], fe[NF], fs[NF], fn[NF];
     {
         double lo[NF], hi[NF];
 #pragma unroll
         for (int q = 0; q < NF; ++q) {
-            lo[q] = w1[q] + 0.5 * gxw[q];
-            hi[q] = c[q] - 0.5 * gxc[q];
+            lo[q] = P(-1, 0, q) + 0.5 * Z(-1, 0, Q_GX + q);
+            hi[q] = c[q] - 0.5 * Z(0, 0, Q_GX + q);
         }
-        hlle<0>(lo, hi, cs2w, gamma, fw);
+        hlle_fast<0>(k, lo, hi, Z(-1, 0, Q_CS), fw);
 #pragma unroll
         for (int q = 0; q < NF; ++q) {
-            lo[q] = c[q] + 0.5 * gxc[q];
-            hi[q] = e1[q] - 0.5 * gxe[q];
+            lo[q] = c[q] + 0.5 * Z(0, 0, Q_GX + q);
+            hi[q] = P(1, 0, q) - 0.5 * Z(1, 0, Q_GX + q);
         }
-        hlle<0>(lo, hi, cs2e, gamma, fe);
+        hlle_fast<0>(k, lo, hi, Z(1, 0, Q_CS), fe);
 #pragma unroll
         for (int q = 0; q < NF; ++q) {
-            lo[q] = s1[q] + 0.5 * gys[q];
-            hi[q] = c[q] - 0.5 * gyc[q];
+            lo[q] = P(0, -1, q) + 0.5 * Z(0, -1, Q_GY + q);
+            hi[q] = c[q] - 0.5 * Z(0, 0, Q_GY + q);
         }
-        hlle<1>(lo, hi, cs2s, gamma, fs);
+        hlle_fast<1>(k, lo, hi, Z(0, -1, Q_CS), fs);
 #pragma unroll
         for (int q = 0; q < NF; ++q) {
-            lo[q] = c[q] + 0.5 * gyc[q];
-            hi[q] = n1[q] - 0.5 * gyn[q];
+            lo[q] = c[q] + 0.5 * Z(0, 0, Q_GY + q);
+            hi[q] = P(0, 1, q) - 0.5 * Z(0, 1, Q_GY + q);
         }
-        hlle<1>(lo, hi, cs2n, gamma, fn);
+        hlle_fast<1>(k, lo, hi, Z(0, 1, Q_CS), fn);
     }
+
+    const double hc = st.massless ? 1.0 : Z(0, 0, Q_SQ) / root_w2(st.m, xc, yc);
 
     if (k.alpha > 0.0) {
-        double gyw[NF], gye[NF], gxs[NF], gxn[NF];
-        slopes(P(-1, -1), w1, P(-1, 1), theta, gyw);
-        slopes(P(1, -1), e1, P(1, 1), theta, gye);
-        slopes(P(-1, -1), s1, P(1, -1), theta, gxs);
-        slopes(P(-1, 1), n1, P(1, 1), theta, gxn);
-        double tw[4], te[4], ts[4], tn[4], tc[4];
-        strain(gxw, gyw, dx, dy, tw);
-        strain(gxe, gye, dx, dy, te);
-        strain(gxs, gys, dx, dy, ts);
-        strain(gxn, gyn, dx, dy, tn);
-        strain(gxc, gyc, dx, dy, tc);
-        const double cs2c = cs2_of(gamma, c);
-        const double hw = scale_height(st.m, xl, yc, w1), he = scale_height(st.m, xr, yc, e1);
-        const double hs = scale_height(st.m, xc, yl, s1), hn = scale_height(st.m, xc, yr, n1);
-        const double nuc = k.alpha * hc * sqrt(cs2c);
-        const double nuw = k.alpha * hw * sqrt(cs2w), nue = k.alpha * he * sqrt(cs2e);
-        const double nus = k.alpha * hs * sqrt(cs2s), nun = k.alpha * hn * sqrt(cs2n);
+        const double hw = st.massless ? 1.0 : Z(-1, 0, Q_SQ) / sm.fx[ty][tx];
+        const double he = st.massless ? 1.0 : Z(1, 0, Q_SQ) / sm.fx[ty + 1][tx];
+        const double hs = st.massless ? 1.0 : Z(0, -1, Q_SQ) / sm.fy[ty][tx];
+        const double hn = st.massless ? 1.0 : Z(0, 1, Q_SQ) / sm.fy[ty][tx + 1];
+        const double nuc = k.alpha * hc * Z(0, 0, Q_CS);
+        const double nuw = k.alpha * hw * Z(-1, 0, Q_CS), nue = k.alpha * he * Z(1, 0, Q_CS);
+        const double nus = k.alpha * hs * Z(0, -1, Q_CS), nun = k.alpha * hn * Z(0, 1, Q_CS);
+        const double w0 = P(-1, 0, 0), e0 = P(1, 0, 0), s0 = P(0, -1, 0), n0 = P(0, 1, 0);
+        // strain tensors (xx, xy, yx = xy, yy) of the zone and its neighbours
+        const double tc0 = Z(0, 0, Q_SXX), tc1 = Z(0, 0, Q_SXY), tc3 = Z(0, 0, Q_SYY);
+        const double tw0 = Z(-1, 0, Q_SXX), tw1 = Z(-1, 0, Q_SXY);
+        const double te0 = Z(1, 0, Q_SXX), te1 = Z(1, 0, Q_SXY);
+        const double ts2 = Z(0, -1, Q_SXY), ts3 = Z(0, -1, Q_SYY);
+        const double tn2 = Z(0, 1, Q_SXY), tn3 = Z(0, 1, Q_SYY);
+        const double tc2 = tc1;
 
-        fw[1] -= 0.5 * (nuw * w1[0] * tw[0] + nuc * c[0] * tc[0]);
-        fw[2] -= 0.5 * (nuw * w1[0] * tw[1] + nuc * c[0] * tc[1]);
-        fe[1] -= 0.5 * (nuc * c[0] * tc[0] + nue * e1[0] * te[0]);
-        fe[2] -= 0.5 * (nuc * c[0] * tc[1] + nue * e1[0] * te[1]);
-        fs[1] -= 0.5 * (nus * s1[0] * ts[2] + nuc * c[0] * tc[2]);
-        fs[2] -= 0.5 * (nus * s1[0] * ts[3] + nuc * c[0] * tc[3]);
-        fn[1] -= 0.5 * (nuc * c[0] * tc[2] + nun * n1[0] * tn[2]);
-        fn[2] -= 0.5 * (nuc * c[0] * tc[3] + nun * n1[0] * tn[3]);
+        fw[1] -= 0.5 * (nuw * w0 * tw0 + nuc * c[0] * tc0);
+        fw[2] -= 0.5 * (nuw * w0 * tw1 + nuc * c[0] * tc1);
+        fe[1] -= 0.5 * (nuc * c[0] * tc0 + nue * e0 * te0);
+        fe[2] -= 0.5 * (nuc * c[0] * tc1 + nue * e0 * te1);
+        fs[1] -= 0.5 * (nus * s0 * ts2 + nuc * c[0] * tc2);
+        fs[2] -= 0.5 * (nus * s0 * ts3 + nuc * c[0] * tc3);
+        fn[1] -= 0.5 * (nuc * c[0] * tc2 + nun * n0 * tn2);
+        fn[2] -= 0.5 * (nuc * c[0] * tc3 + nun * n0 * tn3);
 
-        fw[3] -= 0.5 * (nuw * w1[0] * tw[0] * w1[1] + nuc * c[0] * tc[0] * c[1]);
-        fe[3] -= 0.5 * (nuc * c[0] * tc[0] * c[1] + nue * e1[0] * te[0] * e1[1]);
-        fw[3] -= 0.5 * (nuw * w1[0] * tw[1] * w1[2] + nuc * c[0] * tc[1] * c[2]);
-        fe[3] -= 0.5 * (nuc * c[0] * tc[1] * c[2] + nue * e1[0] * te[1] * e1[2]);
-        fs[3] -= 0.5 * (nus * s1[0] * ts[2] * s1[1] + nuc * c[0] * tc[2] * c[1]);
-        fn[3] -= 0.5 * (nuc * c[0] * tc[2] * c[1] + nun * n1[0] * tn[2] * n1[1]);
-        fs[3] -= 0.5 * (nus * s1[0] * ts[3] * s1[2] + nuc * c[0] * tc[3] * c[2]);
-        fn[3] -= 0.5 * (nuc * c[0] * tc[3] * c[2] + nun * n1[0] * tn[3] * n1[2]);
+        fw[3] -= 0.5 * (nuw * w0 * tw0 * P(-1, 0, 1) + nuc * c[0] * tc0 * c[1]);
+        fe[3] -= 0.5 * (nuc * c[0] * tc0 * c[1] + nue * e0 * te0 * P(1, 0, 1));
+        fw[3] -= 0.5 * (nuw * w0 * tw1 * P(-1, 0, 2) + nuc * c[0] * tc1 * c[2]);
+        fe[3] -= 0.5 * (nuc * c[0] * tc1 * c[2] + nue * e0 * te1 * P(1, 0, 2));
+        fs[3] -= 0.5 * (nus * s0 * ts2 * P(0, -1, 1) + nuc * c[0] * tc2 * c[1]);
+        fn[3] -= 0.5 * (nuc * c[0] * tc2 * c[1] + nun * n0 * tn2 * P(0, 1, 1));
+        fs[3] -= 0.5 * (nus * s0 * ts3 * P(0, -1, 2) + nuc * c[0] * tc3 * c[2]);
+        fn[3] -= 0.5 * (nuc * c[0] * tc3 * c[2] + nun * n0 * tn3 * P(0, 1, 2));
     }
 
+    const double T = Z(0, 0, Q_T);
     double u[NF];
-    prim_to_cons(c, u, gamma);
-    buffer_source(k, st.buf_mass, xc, yc, st.dt, u);
+    p2c_fast(k, c, u);
+    buffer_source(k, st.buf_mass, xc, yc, dt, u);
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
         double du[NF];
-        mass_source(st.m[m], xc, yc, st.dt, c, hc, k.constant_softening, gamma, du);
+        mass_source_fast(k, st.m[m], xc, yc, dt, c, T, hc, du);
 #pragma unroll
         for (int q = 0; q < NF; ++q)
             u[q] += du[q];
     }
-    cooling(k, st.dt, c, u);
+    cooling_fast(k, dt, c, T, u);
 #pragma unroll
     for (int q = 0; q < NF; ++q) {
-        u[q] -= ((fe[q] - fw[q]) / dx + (fn[q] - fs[q]) / dy) * st.dt;
+        u[q] -= (div_by(fe[q] - fw[q], k.dx, k.inv_dx) + div_by(fn[q] - fs[q], k.dy, k.inv_dy)) * dt;
         u[q] = (1.0 - st.a) * u[q] + st.a * un[q];
     }
-    cons_to_prim(k, u, out);
+    c2p_fast(k, u, out);
 }
-
-// a maximum that keeps a NaN operand, so that a NaN wavespeed reaches the host
-__device__ __forceinline__ double max_nan(double a, double b) { return (a > b || a != a) ? a : b; }
-
-// The primitives of one zone in the field-major shared tile.
-struct TileZone {
-    const double *p;
-    __device__ double operator[](int q) const { return p[q * (HI * HJ)]; }
-};
 
 // One RK stage. primitive_n supplies u_n (cons of it, rebuilt in the kernel)
 // or un_all does (the reference's conserved_rk array). With ws_max set, the
 // largest wavespeed of the written zones is max-ed into it (non-negative
 // doubles order as their bit patterns do).
-__global__ void __launch_bounds__(TI * TJ) stage_kernel(Consts k, Stage st, const double *__restrict__ prd,
-                                                         const double *pn,
-                                                         const double *__restrict__ un_all, double *pwr,
-                                                         unsigned long long *ws_max)
+__global__ void __launch_bounds__(TI * TJ, STAGE_MIN_BLOCKS) stage_kernel(Consts k, Stage st,
+                                                                          const double *__restrict__ prd,
+                                                                          const double *pn,
+                                                                          const double *__restrict__ un_all,
+                                                                          double *pwr, unsigned long long *ws_max)
 {
-    __shared__ double tile[NF][HI][HJ];
-    __shared__ double warp_max[TI * TJ / 32];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StageSmem &sm = *reinterpret_cast<StageSmem *>(smem_raw);
     const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
     const int ni = k.ni, nj = k.nj;
     const int tid = threadIdx.y * TJ + threadIdx.x;
@@ -518,14 +645,15 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(Consts k, Stage st, cons
             const double *src = prd + at(ii, jj, nj);
 #pragma unroll
             for (int q = 0; q < NF; ++q)
-                tile[q][s / HJ][s % HJ] = src[q];
+                sm.prim[q][s / HJ][s % HJ] = src[q];
         }
     }
+    __syncthreads();
+    stage_phase1(k, st, sm, i0, j0, tid);
     __syncthreads();
     const int i = i0 + threadIdx.y, j = j0 + threadIdx.x;
     double ws = 0.0;
     if (i < ni && j < nj) {
-        auto P = [&](int di, int dj) { return TileZone{&tile[0][threadIdx.y + NG + di][threadIdx.x + NG + dj]}; };
         // u_n enters as (1 - a) u + a u_n even when a = 0, as in the reference
         double un[NF];
         if (st.un_from_primitive) {
@@ -533,14 +661,14 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(Consts k, Stage st, cons
 #pragma unroll
             for (int q = 0; q < NF; ++q)
                 pn_z[q] = pn[at(i, j, nj) + q];
-            prim_to_cons(pn_z, un, k.gamma);
+            p2c_fast(k, pn_z, un);
         } else {
 #pragma unroll
             for (int q = 0; q < NF; ++q)
                 un[q] = un_all[at(i, j, nj) + q];
         }
         double out[NF];
-        zone_update(k, st, i, j, P, un, out);
+        stage_phase2(k, st, sm, threadIdx.y, threadIdx.x, un, out);
         // the zone and, on the edges, its zero-gradient guard images
         const int ilo = (st.write_guards && i == 0) ? -NG : i, ihi = (st.write_guards && i == ni - 1) ? ni + 1 : i;
         const int jlo = (st.write_guards && j == 0) ? -NG : j, jhi = (st.write_guards && j == nj - 1) ? nj + 1 : j;
@@ -559,12 +687,12 @@ __global__ void __launch_bounds__(TI * TJ) stage_kernel(Consts k, Stage st, cons
         for (int o = 16; o > 0; o >>= 1)
             ws = max_nan(ws, __shfl_xor_sync(0xffffffffu, ws, o));
         if ((tid & 31) == 0)
-            warp_max[tid >> 5] = ws;
+            sm.warp_max[tid >> 5] = ws;
         __syncthreads();
         if (tid == 0) {
-            double m = warp_max[0];
+            double m = sm.warp_max[0];
             for (int w = 1; w < TI * TJ / 32; ++w)
-                m = max_nan(m, warp_max[w]);
+                m = max_nan(m, sm.warp_max[w]);
             atomicMax(ws_max, (unsigned long long)__double_as_longlong(m));
         }
     }
@@ -792,6 +920,11 @@ Consts consts_of(const cbdgam_grid_t *g)
     k.buf_width = g->buffer_onset_width;
     k.buf_onset_m3 = std::pow(g->buffer_outer_radius - g->buffer_onset_width, -3.0);
     k.mach_m2 = std::pow(g->mach_ceiling, -2.0);
+    k.inv_dx = 1.0 / k.dx;
+    k.inv_dy = 1.0 / k.dy;
+    k.gm1 = k.gamma - 1.0;
+    k.inv_gm1 = 1.0 / k.gm1;
+    k.inv_gamma = 1.0 / k.gamma;
     return k;
 }
 
@@ -811,8 +944,22 @@ int status_of(cudaError_t e) { return e == cudaSuccess ? CBD_OK : CBD_ERR_CUDA; 
 int launch_stage(const Consts &k, const Stage &st, const double *prd, const double *pn, const double *un,
                  double *pwr, double *ws_max, cudaStream_t s)
 {
+    // the dynamic shared memory limit is a per-device attribute of the kernel
+    static bool ready[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return CBD_ERR_CUDA;
+    if (!ready[dev]) {
+        if (cudaFuncSetAttribute(stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(StageSmem)) != cudaSuccess)
+            return CBD_ERR_CUDA;
+        ready[dev] = true;
+    }
+    Stage s2 = st;
+    s2.massless = st.m[0].mass == 0.0 && st.m[1].mass == 0.0;
     const dim3 grid((k.nj + TJ - 1) / TJ, (k.ni + TI - 1) / TI), block(TJ, TI);
-    stage_kernel<<<grid, block, 0, s>>>(k, st, prd, pn, un, pwr, reinterpret_cast<unsigned long long *>(ws_max));
+    stage_kernel<<<grid, block, sizeof(StageSmem), s>>>(k, s2, prd, pn, un, pwr,
+                                                        reinterpret_cast<unsigned long long *>(ws_max));
     return status_of(cudaGetLastError());
 }
 
