@@ -314,3 +314,39 @@ class Solver(SolverBase):
             k += 1
             out.append(complex(re, im) * da if d.quantity in COMPLEX_QUANTITIES else float(re) * da)
         return out
+
+
+def main(argv=None):
+    """A gamma-law circumbinary disk driven as the reference's driver does
+    (dt = CFL min(dx, dy) / max wavespeed every step; a profiling and smoke
+    case): python -m sailfish_b200.cbdgam_2d --resolution 2048 --steps 10"""
+    import argparse
+    import time
+
+    import torch
+
+    from .setups import CircumbinaryDisk
+
+    p = argparse.ArgumentParser(description=main.__doc__)
+    p.add_argument("--resolution", type=int, default=1024)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--cfl", type=float, default=0.1)
+    p.add_argument("--alpha", type=float, default=0.1)
+    p.add_argument("--cooling", type=float, default=0.0)
+    a = p.parse_args(argv)
+    setup = CircumbinaryDisk(eos="gamma-law", alpha=a.alpha, cooling_coefficient=a.cooling)
+    mesh = setup.mesh(a.resolution)
+    s = Solver(setup=setup, mesh=mesh, physics=setup.physics)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        s.advance(mesh.min_spacing() / s.maximum_wavespeed() * a.cfl)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    print(f"{a.steps} steps at {a.resolution}^2: {el / a.steps * 1e3:.3f} ms/step, "
+          f"{a.resolution ** 2 * a.steps / el:.3e} zone-updates/s, t = {s.time:.6f}, "
+          f"max wavespeed {s.maximum_wavespeed():.6f}")
+
+
+if __name__ == "__main__":
+    main()

@@ -178,10 +178,13 @@ class _Pickler(pickle._Pickler):
         super().save_global(obj, name)
 
 
-# the reference's solver options (cbdiso_2d.py:23-30); the others this
-# package's Solver takes are stored under their own key, which the
-# reference's restart does not read
-REFERENCE_OPTIONS = ("velocity_ceiling", "density_floor", "rk_order")
+# the reference's solver options per solver (cbdiso_2d.py:23-30,
+# cbdgam_2d.py:23-27); the others this package's solvers take are stored
+# under their own key, which the reference's restart does not read
+REFERENCE_OPTIONS = {
+    "cbdiso_2d": ("velocity_ceiling", "density_floor", "rk_order"),
+    "cbdgam_2d": ("pressure_floor", "density_floor", "velocity_ceiling", "mach_ceiling"),
+}
 EXTRA_OPTIONS_KEY = "b200_solver_options"
 
 
@@ -190,7 +193,8 @@ def checkpoint_dict(solver, setup, mesh, iteration, timestep_dt, cfl_number, tim
     """The dict the reference's write_checkpoint stores (driver.py:159-175),
     plus this package's own solver options under EXTRA_OPTIONS_KEY."""
     options = dict(solver.options)
-    extra = {k: v for k, v in options.items() if k not in REFERENCE_OPTIONS}
+    ref_keys = REFERENCE_OPTIONS[setup.solver]
+    extra = {k: v for k, v in options.items() if k not in ref_keys}
     out = dict(
         iteration=iteration,
         time=solver.time,
@@ -200,7 +204,7 @@ def checkpoint_dict(solver, setup, mesh, iteration, timestep_dt, cfl_number, tim
         primitive=solver.primitive,
         timeseries=list(timeseries),
         solver=setup.solver,
-        solver_options={k: v for k, v in options.items() if k in REFERENCE_OPTIONS},
+        solver_options={k: v for k, v in options.items() if k in ref_keys},
         event_states=dict(event_states or {}),
         driver=driver if driver is not None else DriverArgs(),
         model_parameters=setup.model_parameter_dict(),

@@ -112,3 +112,90 @@ def test_restart_continues_like_the_reference_driver():
         solver.advance(dt)
     assert solver.time == float(ref["time"])
     np.testing.assert_array_equal(solver.solution, ref["solution"])
+
+
+# ---------------------------------------------------------------------------
+# the gamma-law solver's checkpoints (chkpt_gam_n24.pk, written by the
+# reference driver running cbdgam_2d with alpha viscosity and cooling)
+# ---------------------------------------------------------------------------
+
+GAM_CHKPT = os.path.join(GOLDEN, "chkpt_gam_n24.pk")
+
+
+def _gam_continued():
+    return np.load(os.path.join(GOLDEN, "chkpt_gam_n24_continued.npz"))
+
+
+def test_reference_gamma_checkpoint_loads():
+    c = load_checkpoint(GAM_CHKPT)
+    assert c["solver"] == "cbdgam_2d" and c["solution"].shape == (24, 24, 4)
+    assert set(c["solver_options"]) == {"pressure_floor", "density_floor", "velocity_ceiling", "mach_ceiling"}
+    setup = find_setup_class(c["setup_name"])(**c["model_parameters"])
+    assert setup.solver == "cbdgam_2d" and setup.model_parameter_dict() == c["model_parameters"]
+    assert list(setup.point_masses(c["time"])) == list(c["point_masses"])
+
+
+def _gam_oracle_from_checkpoint(c):
+    from oracle import host_gam as og
+
+    p = c["model_parameters"]
+    m = c["mesh"]
+    setup = CircumbinaryDisk(**p)
+    onset = [0.0] * 4
+    setup.primitive(c["time"], [m.x1 - 0.1, 0.0], onset)
+    o = c["solver_options"]
+    cfg = og.GamConfig(m.x0, m.x1, m.y0, m.y1, m.ni, m.nj, gamma_law_index=p["gamma_law_index"], alpha=p["alpha"],
+                       cooling_coefficient=p["cooling_coefficient"], constant_softening=p["constant_softening"],
+                       buffer_is_enabled=p["buffer_is_enabled"], buffer_surface_density=onset[0],
+                       buffer_surface_pressure=onset[3], pressure_floor=o["pressure_floor"],
+                       density_floor=o["density_floor"], velocity_ceiling=o["velocity_ceiling"],
+                       mach_ceiling=o["mach_ceiling"],
+                       masses=oh.binary_masses(1.0, 1.0, p["mass_ratio"], p["eccentricity"], p["softening_length"],
+                                               p["sink_model"], p["sink_rate"], p["sink_radius"]))
+    return og.GamOracleSolver(cfg, np.array(c["solution"]), time=c["time"])
+
+
+def test_restarted_gamma_oracle_continues_like_the_reference_driver():
+    c = load_checkpoint(GAM_CHKPT)
+    ref = _gam_continued()
+    s = _gam_oracle_from_checkpoint(c)
+    for n in range(6):
+        dt = c["mesh"].min_spacing() / s.maximum_wavespeed() * c["cfl_number"]
+        assert dt == ref["dts"][n]
+        s.advance(dt)
+    assert s.time == float(ref["time"])
+    np.testing.assert_array_equal(s.solution, ref["solution"])
+
+
+def test_written_gamma_checkpoint_keeps_the_gamma_options_apart(tmp_path):
+    c = load_checkpoint(GAM_CHKPT)
+    setup = CircumbinaryDisk(**c["model_parameters"])
+    solver = types.SimpleNamespace(time=c["time"], solution=c["solution"], primitive=None,
+                                   options=dict(c["solver_options"], plm_theta=1.5))
+    name = write_checkpoint(3, str(tmp_path), solver, setup, c["mesh"], c["iteration"], c["timestep_dt"],
+                            c["cfl_number"], c["timeseries"], c["event_states"], c["driver"])
+    back = load_checkpoint(name)
+    assert back["solver"] == "cbdgam_2d"
+    assert back["solver_options"] == c["solver_options"]
+    assert back["b200_solver_options"] == dict(plm_theta=1.5)
+    np.testing.assert_array_equal(back["solution"], c["solution"])
+
+
+@pytest.mark.gpu
+def test_gamma_restart_continues_like_the_reference_driver():
+    """restart() builds the gamma-law B200 solver from the reference's
+    checkpoint; six more iterations with the driver's dt rule match the
+    reference's own continuation."""
+    from sailfish_b200.checkpoint import restart
+
+    ref = _gam_continued()
+    solver, state = restart(GAM_CHKPT)
+    assert type(solver).__module__ == "sailfish_b200.cbdgam_2d"
+    for n in range(6):
+        dt = state.mesh.min_spacing() / solver.maximum_wavespeed() * state.cfl_number
+        assert dt == pytest.approx(ref["dts"][n], rel=1e-14)
+        solver.advance(dt)
+    assert solver.time == pytest.approx(float(ref["time"]), rel=1e-15)
+    got, want = solver.solution, ref["solution"]
+    for q in range(4):
+        assert np.abs(got[..., q] - want[..., q]).max() <= 1e-13 * np.abs(want[..., q]).max()
