@@ -24,7 +24,7 @@ from typing import List, NamedTuple, Optional, Sequence
 
 import numpy as np
 
-from . import _capi
+from . import _capi, _hostio
 from ._graphs import capture
 from .cbdiso_2d import COMPLEX_QUANTITIES, NG, NQ, RK_WEIGHTS, Options, Solver, _diag_struct
 from .physics import Diagnostic, Physics, enum_value
@@ -271,7 +271,7 @@ class BatchedSolver:
         """Primitive state (ni, nj, 3) of disk i, on the host."""
         ni, nj = self.solvers[i].mesh.shape
         a = self._buf[0][self.offsets[i]:self.offsets[i] + (ni + 2 * NG) * (nj + 2 * NG) * NQ]
-        return a.reshape(ni + 2 * NG, nj + 2 * NG, NQ)[NG:-NG, NG:-NG].cpu().numpy()
+        return _hostio.download(a.reshape(ni + 2 * NG, nj + 2 * NG, NQ)[NG:-NG, NG:-NG])
 
 
 def config2_disks(num=64, seed=2024, sizes=(128, 192, 256, 384, 512, 768, 1024)):

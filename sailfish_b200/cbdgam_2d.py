@@ -31,7 +31,7 @@ from typing import NamedTuple
 
 import numpy as np
 
-from . import _capi
+from . import _capi, _hostio
 from .cbdiso_2d import _as_diagnostic, _diag_struct, _mass_struct
 from .mesh import is_planar_cartesian_2d
 from .physics import Physics, enum_value
@@ -157,7 +157,7 @@ class Solver(SolverBase):
 
         f64 = dict(dtype=torch.float64, device=self.device)
         self._buf = [torch.empty((ni + 2 * NG, nj + 2 * NG, NQ), **f64) for _ in range(2)]
-        self._buf[0][NG:-NG, NG:-NG] = torch.from_numpy(primitive).to(self.device)
+        _hostio.upload(primitive, self._buf[0][NG:-NG, NG:-NG])
         self._check(self._lib.cbdgam_b200_fill_guards(ctypes.byref(g), self._ptr(self._buf[0]), self._stream()),
                     "fill_guards")
         nscratch = int(self._lib.cbdgam_b200_scratch_bytes(ctypes.byref(g)))
@@ -225,7 +225,7 @@ class Solver(SolverBase):
 
     @property
     def solution(self):
-        return self._buf[0][NG:-NG, NG:-NG].cpu().numpy()
+        return _hostio.download(self._buf[0][NG:-NG, NG:-NG])
 
     @property
     def primitive(self):

