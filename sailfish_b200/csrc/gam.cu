@@ -10,11 +10,11 @@
 // the reference only where glibc's pow / exp are not (about one call in a
 // thousand for the non-integer exponents).
 //
-// One thread per zone over a CTA tile of 8 x 32 zones. The tile's primitives
-// (with a two-zone halo) are staged in shared memory; a first phase computes
-// the per-zone quantities every neighbouring update needs (slopes, p / Sigma,
-// sound speed, strain) and the scale heights' face geometry, a second the
-// zone updates. The reference's face fluxes are not shareable between the two
+// A CTA of 256 threads over a tile of 16 x 32 zones (two rows of zones per
+// thread). The tile's primitives (with a two-zone halo) are staged in shared
+// memory; a first phase computes the per-zone quantities every neighbouring
+// update needs (slopes, p / Sigma, sound speed, strain) and the scale
+// heights' face geometry, a second the zone updates. The reference's face fluxes are not shareable between the two
 // zones of a face (each zone takes the sound speed of the neighbour across
 // the face, cbdgam_2d.c:608-611, and the viscous flux the neighbour's scale
 // height), so each zone computes its four faces, as the reference does.
@@ -33,7 +33,9 @@ namespace gam {
 
 constexpr int NF = 4;
 constexpr int NG = 2;
-constexpr int TI = 8, TJ = 32;  // CTA tile (rows i, columns j)
+constexpr int TI = 16, TJ = 32;  // CTA tile (rows i, columns j)
+constexpr int RPT = 2;            // tile rows per thread: zone rows ty and ty + TI / RPT
+constexpr int NT = TI * TJ / RPT; // threads per CTA, a (TJ, TI / RPT) block
 constexpr int HI = TI + 2 * NG, HJ = TJ + 2 * NG;
 constexpr int STAGE_MIN_BLOCKS = 2;  // resident CTAs per SM the stage kernel is built for
 
@@ -193,14 +195,21 @@ __device__ __forceinline__ double greater(double a, double b) { return a > b ? a
 __device__ __forceinline__ double sign_of(double x) { return copysign(1.0, x); }
 __device__ __forceinline__ size_t at(int i, int j, int nj) { return ((size_t)(i + NG) * (nj + 2 * NG) + (j + NG)) * NF; }
 
-// cbdgam_2d.c:27-33
+// cbdgam_2d.c:27-33: 0.25 |sgn a + sgn b| (sgn a + sgn c) min(|a|, |b|, |c|),
+// returned exactly (signed zeros included) with the sign logic done on the
+// sign bits: it is m, -m, +0 or -0.
 __device__ __forceinline__ double slope(double yl, double y0, double yr, double theta)
 {
     const double a = (y0 - yl) * theta;
     const double b = (yr - yl) * 0.5;
     const double c = (yr - y0) * theta;
     const double m = lesser(fabs(a), lesser(fabs(b), fabs(c)));
-    return 0.25 * fabs(sign_of(a) + sign_of(b)) * (sign_of(a) + sign_of(c)) * m;
+    const unsigned sa = (unsigned)__double2hiint(a) >> 31;
+    const unsigned sb = (unsigned)__double2hiint(b) >> 31;
+    const unsigned sc = (unsigned)__double2hiint(c) >> 31;
+    if ((sa == sb) & (sa == sc))
+        return sa ? -m : m;
+    return (sa & sc & (sa ^ sb)) ? -0.0 : 0.0;
 }
 
 // cbdgam_2d.c:75-106
@@ -347,7 +356,7 @@ struct StageSmem {
     double z[NZQ][ZI][ZJ];
     double fx[TI + 1][TJ];  // sqrt(sum_m M_m r^-3) at the x-faces (x_l of zone i0 + a, y_c of zone j0 + b)
     double fy[TI][TJ + 1];  // the same at the y-faces (x_c of zone i0 + a, y_l of zone j0 + b)
-    double warp_max[TI * TJ / 32];
+    double warp_max[NT / 32];
 };
 
 // sqrt(w2) of the scale height (cbdgam_2d.c:75-106) at (x, y)
@@ -486,7 +495,7 @@ __device__ __forceinline__ double max_nan(double a, double b) { return (a > b ||
 __device__ __forceinline__ void stage_phase1(const Consts &k, const Stage &st, StageSmem &sm, int i0, int j0, int tid)
 {
     const double theta = k.theta;
-    for (int s = tid; s < ZI * ZJ; s += TI * TJ) {
+    for (int s = tid; s < ZI * ZJ; s += NT) {
         const int a = s / ZJ, b = s % ZJ;
         if (i0 - 1 + a > k.ni || j0 - 1 + b > k.nj)
             continue;  // beyond the guard zones of the last tile: never read
@@ -508,12 +517,12 @@ __device__ __forceinline__ void stage_phase1(const Consts &k, const Stage &st, S
         sm.z[Q_SYY][a][b] = div_by(-2.0 / 3.0 * gx[1], k.dx, k.inv_dx) + div_by(4.0 / 3.0 * gy[2], k.dy, k.inv_dy);
     }
     if (k.alpha > 0.0 && !st.massless) {
-        for (int s = tid; s < (TI + 1) * TJ; s += TI * TJ) {
+        for (int s = tid; s < (TI + 1) * TJ; s += NT) {
             const int a = s / TJ, b = s % TJ;
             const int i = i0 + a, j = j0 + b;
             sm.fx[a][b] = root_w2(st.m, k.xl + (i + 0.0) * k.dx, k.yl + (j + 0.5) * k.dy);
         }
-        for (int s = tid; s < TI * (TJ + 1); s += TI * TJ) {
+        for (int s = tid; s < TI * (TJ + 1); s += NT) {
             const int a = s / (TJ + 1), b = s % (TJ + 1);
             const int i = i0 + a, j = j0 + b;
             sm.fy[a][b] = root_w2(st.m, k.xl + (i + 0.5) * k.dx, k.yl + (j + 0.0) * k.dy);
@@ -536,31 +545,34 @@ __device__ __forceinline__ void stage_phase2(const Consts &k, const Stage &st, c
     for (int q = 0; q < NF; ++q)
         c[q] = P(0, 0, q);
 
+    // p +- g / 2 and f - S / 2 below are single FMAs: halving a normal number
+    // is exact, so the fused operation rounds as the reference's multiply
+    // then add
     double fw[NF], fe[NF], fs[NF], fn[NF];
     {
         double lo[NF], hi[NF];
 #pragma unroll
         for (int q = 0; q < NF; ++q) {
-            lo[q] = P(-1, 0, q) + 0.5 * Z(-1, 0, Q_GX + q);
-            hi[q] = c[q] - 0.5 * Z(0, 0, Q_GX + q);
+            lo[q] = fma(0.5, Z(-1, 0, Q_GX + q), P(-1, 0, q));
+            hi[q] = fma(-0.5, Z(0, 0, Q_GX + q), c[q]);
         }
         hlle_fast<0>(k, lo, hi, Z(-1, 0, Q_CS), fw);
 #pragma unroll
         for (int q = 0; q < NF; ++q) {
-            lo[q] = c[q] + 0.5 * Z(0, 0, Q_GX + q);
-            hi[q] = P(1, 0, q) - 0.5 * Z(1, 0, Q_GX + q);
+            lo[q] = fma(0.5, Z(0, 0, Q_GX + q), c[q]);
+            hi[q] = fma(-0.5, Z(1, 0, Q_GX + q), P(1, 0, q));
         }
         hlle_fast<0>(k, lo, hi, Z(1, 0, Q_CS), fe);
 #pragma unroll
         for (int q = 0; q < NF; ++q) {
-            lo[q] = P(0, -1, q) + 0.5 * Z(0, -1, Q_GY + q);
-            hi[q] = c[q] - 0.5 * Z(0, 0, Q_GY + q);
+            lo[q] = fma(0.5, Z(0, -1, Q_GY + q), P(0, -1, q));
+            hi[q] = fma(-0.5, Z(0, 0, Q_GY + q), c[q]);
         }
         hlle_fast<1>(k, lo, hi, Z(0, -1, Q_CS), fs);
 #pragma unroll
         for (int q = 0; q < NF; ++q) {
-            lo[q] = c[q] + 0.5 * Z(0, 0, Q_GY + q);
-            hi[q] = P(0, 1, q) - 0.5 * Z(0, 1, Q_GY + q);
+            lo[q] = fma(0.5, Z(0, 0, Q_GY + q), c[q]);
+            hi[q] = fma(-0.5, Z(0, 1, Q_GY + q), P(0, 1, q));
         }
         hlle_fast<1>(k, lo, hi, Z(0, 1, Q_CS), fn);
     }
@@ -584,23 +596,23 @@ __device__ __forceinline__ void stage_phase2(const Consts &k, const Stage &st, c
         const double tn2 = Z(0, 1, Q_SXY), tn3 = Z(0, 1, Q_SYY);
         const double tc2 = tc1;
 
-        fw[1] -= 0.5 * (nuw * w0 * tw0 + nuc * c[0] * tc0);
-        fw[2] -= 0.5 * (nuw * w0 * tw1 + nuc * c[0] * tc1);
-        fe[1] -= 0.5 * (nuc * c[0] * tc0 + nue * e0 * te0);
-        fe[2] -= 0.5 * (nuc * c[0] * tc1 + nue * e0 * te1);
-        fs[1] -= 0.5 * (nus * s0 * ts2 + nuc * c[0] * tc2);
-        fs[2] -= 0.5 * (nus * s0 * ts3 + nuc * c[0] * tc3);
-        fn[1] -= 0.5 * (nuc * c[0] * tc2 + nun * n0 * tn2);
-        fn[2] -= 0.5 * (nuc * c[0] * tc3 + nun * n0 * tn3);
+        fw[1] = fma(-0.5, nuw * w0 * tw0 + nuc * c[0] * tc0, fw[1]);
+        fw[2] = fma(-0.5, nuw * w0 * tw1 + nuc * c[0] * tc1, fw[2]);
+        fe[1] = fma(-0.5, nuc * c[0] * tc0 + nue * e0 * te0, fe[1]);
+        fe[2] = fma(-0.5, nuc * c[0] * tc1 + nue * e0 * te1, fe[2]);
+        fs[1] = fma(-0.5, nus * s0 * ts2 + nuc * c[0] * tc2, fs[1]);
+        fs[2] = fma(-0.5, nus * s0 * ts3 + nuc * c[0] * tc3, fs[2]);
+        fn[1] = fma(-0.5, nuc * c[0] * tc2 + nun * n0 * tn2, fn[1]);
+        fn[2] = fma(-0.5, nuc * c[0] * tc3 + nun * n0 * tn3, fn[2]);
 
-        fw[3] -= 0.5 * (nuw * w0 * tw0 * P(-1, 0, 1) + nuc * c[0] * tc0 * c[1]);
-        fe[3] -= 0.5 * (nuc * c[0] * tc0 * c[1] + nue * e0 * te0 * P(1, 0, 1));
-        fw[3] -= 0.5 * (nuw * w0 * tw1 * P(-1, 0, 2) + nuc * c[0] * tc1 * c[2]);
-        fe[3] -= 0.5 * (nuc * c[0] * tc1 * c[2] + nue * e0 * te1 * P(1, 0, 2));
-        fs[3] -= 0.5 * (nus * s0 * ts2 * P(0, -1, 1) + nuc * c[0] * tc2 * c[1]);
-        fn[3] -= 0.5 * (nuc * c[0] * tc2 * c[1] + nun * n0 * tn2 * P(0, 1, 1));
-        fs[3] -= 0.5 * (nus * s0 * ts3 * P(0, -1, 2) + nuc * c[0] * tc3 * c[2]);
-        fn[3] -= 0.5 * (nuc * c[0] * tc3 * c[2] + nun * n0 * tn3 * P(0, 1, 2));
+        fw[3] = fma(-0.5, nuw * w0 * tw0 * P(-1, 0, 1) + nuc * c[0] * tc0 * c[1], fw[3]);
+        fe[3] = fma(-0.5, nuc * c[0] * tc0 * c[1] + nue * e0 * te0 * P(1, 0, 1), fe[3]);
+        fw[3] = fma(-0.5, nuw * w0 * tw1 * P(-1, 0, 2) + nuc * c[0] * tc1 * c[2], fw[3]);
+        fe[3] = fma(-0.5, nuc * c[0] * tc1 * c[2] + nue * e0 * te1 * P(1, 0, 2), fe[3]);
+        fs[3] = fma(-0.5, nus * s0 * ts2 * P(0, -1, 1) + nuc * c[0] * tc2 * c[1], fs[3]);
+        fn[3] = fma(-0.5, nuc * c[0] * tc2 * c[1] + nun * n0 * tn2 * P(0, 1, 1), fn[3]);
+        fs[3] = fma(-0.5, nus * s0 * ts3 * P(0, -1, 2) + nuc * c[0] * tc3 * c[2], fs[3]);
+        fn[3] = fma(-0.5, nuc * c[0] * tc3 * c[2] + nun * n0 * tn3 * P(0, 1, 2), fn[3]);
     }
 
     const double T = Z(0, 0, Q_T);
@@ -628,7 +640,7 @@ __device__ __forceinline__ void stage_phase2(const Consts &k, const Stage &st, c
 // or un_all does (the reference's conserved_rk array). With ws_max set, the
 // largest wavespeed of the written zones is max-ed into it (non-negative
 // doubles order as their bit patterns do).
-__global__ void __launch_bounds__(TI * TJ, STAGE_MIN_BLOCKS) stage_kernel(Consts k, Stage st,
+__global__ void __launch_bounds__(NT, STAGE_MIN_BLOCKS) stage_kernel(Consts k, Stage st,
                                                                           const double *__restrict__ prd,
                                                                           const double *pn,
                                                                           const double *__restrict__ un_all,
@@ -639,7 +651,7 @@ __global__ void __launch_bounds__(TI * TJ, STAGE_MIN_BLOCKS) stage_kernel(Consts
     const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
     const int ni = k.ni, nj = k.nj;
     const int tid = threadIdx.y * TJ + threadIdx.x;
-    for (int s = tid; s < HI * HJ; s += TI * TJ) {
+    for (int s = tid; s < HI * HJ; s += NT) {
         const int ii = i0 - NG + s / HJ, jj = j0 - NG + s % HJ;
         if (ii <= ni + 1 && jj <= nj + 1) {
             const double *src = prd + at(ii, jj, nj);
@@ -651,9 +663,13 @@ __global__ void __launch_bounds__(TI * TJ, STAGE_MIN_BLOCKS) stage_kernel(Consts
     __syncthreads();
     stage_phase1(k, st, sm, i0, j0, tid);
     __syncthreads();
-    const int i = i0 + threadIdx.y, j = j0 + threadIdx.x;
     double ws = 0.0;
-    if (i < ni && j < nj) {
+#pragma unroll 1
+    for (int h = 0; h < RPT; ++h) {
+        const int ty = threadIdx.y + h * (TI / RPT);
+        const int i = i0 + ty, j = j0 + threadIdx.x;
+        if (i >= ni || j >= nj)
+            continue;
         // u_n enters as (1 - a) u + a u_n even when a = 0, as in the reference
         double un[NF];
         if (st.un_from_primitive) {
@@ -668,7 +684,7 @@ __global__ void __launch_bounds__(TI * TJ, STAGE_MIN_BLOCKS) stage_kernel(Consts
                 un[q] = un_all[at(i, j, nj) + q];
         }
         double out[NF];
-        stage_phase2(k, st, sm, threadIdx.y, threadIdx.x, un, out);
+        stage_phase2(k, st, sm, ty, threadIdx.x, un, out);
         // the zone and, on the edges, its zero-gradient guard images
         const int ilo = (st.write_guards && i == 0) ? -NG : i, ihi = (st.write_guards && i == ni - 1) ? ni + 1 : i;
         const int jlo = (st.write_guards && j == 0) ? -NG : j, jhi = (st.write_guards && j == nj - 1) ? nj + 1 : j;
@@ -680,7 +696,7 @@ __global__ void __launch_bounds__(TI * TJ, STAGE_MIN_BLOCKS) stage_kernel(Consts
                     dst[q] = out[q];
             }
         if (ws_max)
-            ws = max_wavespeed(out, cs2_of(k.gamma, out));
+            ws = max_nan(ws, max_wavespeed(out, cs2_of(k.gamma, out)));
     }
     if (ws_max) {  // uniform over the block
 #pragma unroll
@@ -691,7 +707,7 @@ __global__ void __launch_bounds__(TI * TJ, STAGE_MIN_BLOCKS) stage_kernel(Consts
         __syncthreads();
         if (tid == 0) {
             double m = sm.warp_max[0];
-            for (int w = 1; w < TI * TJ / 32; ++w)
+            for (int w = 1; w < NT / 32; ++w)
                 m = max_nan(m, sm.warp_max[w]);
             atomicMax(ws_max, (unsigned long long)__double_as_longlong(m));
         }
@@ -957,7 +973,7 @@ int launch_stage(const Consts &k, const Stage &st, const double *prd, const doub
     }
     Stage s2 = st;
     s2.massless = st.m[0].mass == 0.0 && st.m[1].mass == 0.0;
-    const dim3 grid((k.nj + TJ - 1) / TJ, (k.ni + TI - 1) / TI), block(TJ, TI);
+    const dim3 grid((k.nj + TJ - 1) / TJ, (k.ni + TI - 1) / TI), block(TJ, TI / RPT);
     stage_kernel<<<grid, block, sizeof(StageSmem), s>>>(k, s2, prd, pn, un, pwr,
                                                         reinterpret_cast<unsigned long long *>(ws_max));
     return status_of(cudaGetLastError());
