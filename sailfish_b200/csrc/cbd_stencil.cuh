@@ -723,8 +723,10 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
             double pl[NQ], pr[NQ];
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
-                pl[q] = sp[s0][q][kk] + 0.5 * gx0[q];
-                pr[q] = sp[s1][q][kk] - 0.5 * gx1[q];
+                // one FMA each: halving a normal number is exact, so this rounds
+                // as the reference's multiply then add
+                pl[q] = fma(0.5, gx0[q], sp[s0][q][kk]);
+                pr[q] = fma(-0.5, gx1[q], sp[s1][q][kk]);
             }
             const double xf = k.xl + (double)(r + 1) * k.dx;
             const double yc = k.yl + ((double)j + 0.5) * k.dy;
@@ -752,8 +754,8 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 double pl[NQ], pr[NQ], g[NQ];
 #pragma unroll
                 for (int q = 0; q < NQ; ++q) {
-                    pl[q] = sp[s0][q][fidx + 1] + 0.5 * sgy[g0][q][fidx];
-                    pr[q] = sp[s0][q][fidx + 2] - 0.5 * sgy[g0][q][fidx + 1];
+                    pl[q] = fma(0.5, sgy[g0][q][fidx], sp[s0][q][fidx + 1]);
+                    pr[q] = fma(-0.5, sgy[g0][q][fidx + 1], sp[s0][q][fidx + 2]);
                 }
                 const double xc = k.xl + ((double)r + 0.5) * k.dx;
                 const double yf = k.yl + (double)(c0 + fidx) * k.dy;
