@@ -79,8 +79,8 @@ def download(tensor):
     out = np.empty(tuple(src.shape), dtype=np.float64)
     with _lock:
         stage = _staging_view(nbytes, tuple(src.shape))
-        stage.copy_(src, non_blocking=True)
-        torch.cuda.current_stream().synchronize()
+        stage.copy_(src, non_blocking=True)  # on the source device's current stream
+        torch.cuda.current_stream(src.device).synchronize()
         _parallel_copy(out, stage.numpy())
     return out
 
@@ -100,5 +100,5 @@ def upload(array, target):
     with _lock:
         stage = _staging_view(nbytes, tuple(array.shape))
         _parallel_copy(stage.numpy(), array)
-        target.copy_(stage, non_blocking=True)
-        torch.cuda.current_stream().synchronize()
+        target.copy_(stage, non_blocking=True)  # on the target device's current stream
+        torch.cuda.current_stream(target.device).synchronize()
