@@ -33,6 +33,12 @@ BYTES_PER_ZONE_UPDATE = 120.0  # RK2 x FP64 x 3 fields: 48 B stage 1 + 72 B stag
 # dram__bytes_write.sum, mean of an RK2 stage 1 and stage 2 launch at 2048^2,
 # profiles/stage_kernel_2048_exact_full.md); scaled by the zone count.
 NCU_TRAFFIC_PER_ZONE_LAUNCH = (108.9e6 + 74.2e6 + 213.7e6 + 69.8e6) / 2 / 2048 ** 2
+# FP64 thread-instructions (DADD + DMUL + DFMA) per zone and stage launch, mean
+# of an RK2 stage 1 and stage 2 launch at 2048^2 (ncu, the sum of
+# smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum over zones;
+# profiles/stage_kernels_2048_fp64.md)
+FP64_INST_PER_ZONE_LAUNCH = (537.2 + 710.8) / 2
+GAM_FP64_INST_PER_ZONE_LAUNCH = (1321.8 + 1346.8) / 2
 DIAGNOSTICS = [dict(quantity="time"), dict(quantity="mdot", which_mass=1, accretion=True),
                dict(quantity="mdot", which_mass=2, accretion=True),
                dict(quantity="torque", which_mass="both", gravity=True)]
@@ -59,6 +65,46 @@ def parse():
     p.add_argument("--no-extras", action="store_true",
                    help="skip the batched-disk and adjoint measurements added to the line at N=1")
     return p.parse_args()
+
+
+def fp64_peak():
+    """FP64 issue rate of this GPU (thread-FMAs per second), measured with
+    the library's probe: 8 CTAs of 256 threads per SM, eight independent FMA
+    chains per thread, best of three launches timed with CUDA events."""
+    import ctypes
+
+    import torch
+
+    from sailfish_b200 import _capi
+
+    lib = _capi.lib()
+    blocks = 8 * torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    iterations = 200000
+    out = torch.zeros(blocks, dtype=torch.float64, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = float("inf")
+    for rep in range(4):
+        start.record()
+        _capi.check(lib.cbdiso_b200_fp64_probe(iterations, blocks, ctypes.c_void_p(out.data_ptr()), stream), "probe")
+        stop.record()
+        torch.cuda.synchronize()
+        if rep:
+            best = min(best, start.elapsed_time(stop) * 1e-3)
+    return lib.cbdiso_b200_fp64_probe_fmas(iterations, blocks) / best
+
+
+def fp64_roofline(inst_per_launch, kernel_s):
+    """The stage kernel against the FP64 pipe: its FP64 thread-instructions
+    per launch (ncu counts) over its CUDA-event launch time, against this
+    GPU's measured FMA issue rate."""
+    peak = fp64_peak()
+    achieved = inst_per_launch / kernel_s
+    return {"bound": "fp64", "achieved": round(achieved / 1e12, 3), "peak": round(peak / 1e12, 3),
+            "unit": "T FP64 thread-instructions/s", "frac": round(achieved / peak, 4),
+            "inst_per_launch": inst_per_launch,
+            "inst_source": "ncu DADD + DMUL + DFMA thread-instructions per zone at 2048^2 scaled by zones",
+            "peak_source": "measured: cbdiso_b200_fp64_probe, independent DFMA chains at full occupancy"}
 
 
 def measured_peaks():
@@ -323,6 +369,8 @@ def run_ours(args, rank, world):
                 "kernel": "stage_kernel (one fused RK stage)", "kernel_ms": round(kernel_s * 1e3, 4),
                 "bytes_per_launch": BYTES_PER_ZONE_UPDATE / 2 * zones}
 
+    fp64 = fp64_roofline(FP64_INST_PER_ZONE_LAUNCH * zones, kernel_s)
+
     line = {
         "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
@@ -339,6 +387,7 @@ def run_ours(args, rank, world):
                     "note": "value loop: stepper record in, time series out, per step"},
         "gpu_launches": 3 * args.steps + 1,
         "roofline": roofline,
+        "roofline_fp64": fp64,
         "clocks": clocks.summary(),
     }
     return line
@@ -512,7 +561,8 @@ def gamma_law_extra(steps=50, warmup=5):
             "roofline": {"bound": "fp64 issue (HBM shown for reference)", "kernel": "gam::stage_kernel (RK stage 2)",
                          "kernel_ms": round(kernel_s * 1e3, 4), "bytes_per_launch": 96 * zones,
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "peak_source": peak_kind}}
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind},
+            "roofline_fp64": fp64_roofline(GAM_FP64_INST_PER_ZONE_LAUNCH * zones, kernel_s)}
     del s, out
     try:
         line["cpu_baseline"] = gamma_cpu_baseline()

@@ -494,6 +494,15 @@ size_t cbdgam_b200_scratch_bytes(const cbdgam_grid_t *grid);
 int cbdgam_b200_reduce(const cbdgam_grid_t *grid, const cbd_mass_t *masses, const cbd_diag_t *diags, int num_diags,
                        const double *primitive, double *scratch, double *result, void *stream);
 
+/* Measurement hook (no counterpart in the reference): the FP64 issue-rate
+ * probe behind the stencil kernels' FP64 roofline. `blocks` CTAs of 256
+ * threads each run eight independent FMA chains of `iterations` steps;
+ * cbdiso_b200_fp64_probe_fmas gives the thread-FMA count of one launch, to be
+ * divided by its device time. `out` (device, `blocks` doubles) is written
+ * only to keep the chains live. */
+int cbdiso_b200_fp64_probe(long iterations, int blocks, double *out, void *stream);
+long cbdiso_b200_fp64_probe_fmas(long iterations, int blocks);
+
 /* sizeof of cbdgam_grid_t and cbdgam_stage_t, for bindings to check. */
 void cbdgam_b200_abi_sizes(size_t out[2]);
 

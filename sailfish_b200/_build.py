@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "--expt-relaxed-constexpr"]
 NO_FMA = {"stage_exact.cu", "elementwise.cu", "stepper.cu", "batched_exact.cu", "adjoint.cu", "gam.cu"}
 SOURCES = ["capi.cu", "elementwise.cu", "stage_exact.cu", "stage_fma.cu", "stage_fast.cu", "noalloc.cu",
-           "stepper.cu", "batched_exact.cu", "batched.cu", "adjoint.cu", "gam.cu"]
+           "stepper.cu", "batched_exact.cu", "batched.cu", "adjoint.cu", "gam.cu", "fp64_peak.cu"]
 
 
 def nvcc():

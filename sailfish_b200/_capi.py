@@ -186,6 +186,10 @@ def _declare(lib):
         f = getattr(lib, name)
         f.argtypes = args
         f.restype = c_int
+    lib.cbdiso_b200_fp64_probe.argtypes = [ctypes.c_long, c_int, c_void_p, c_void_p]
+    lib.cbdiso_b200_fp64_probe.restype = c_int
+    lib.cbdiso_b200_fp64_probe_fmas.argtypes = [ctypes.c_long, c_int]
+    lib.cbdiso_b200_fp64_probe_fmas.restype = ctypes.c_long
     lib.cbdgam_b200_scratch_bytes.argtypes = [POINTER(GamGrid)]
     lib.cbdgam_b200_scratch_bytes.restype = c_size_t
     lib.cbdgam_b200_abi_sizes.argtypes = [POINTER(c_size_t)]
@@ -233,7 +237,7 @@ def exported_symbols():
         "cbdgam_2d_advance_rk", "cbdgam_2d_wavespeed", "cbdgam_2d_primitive_to_conserved",
         "cbdgam_2d_point_mass_source_term", "cbdgam_b200_set_plm_theta", "cbdgam_b200_advance_stage",
         "cbdgam_b200_fill_guards", "cbdgam_b200_scratch_bytes", "cbdgam_b200_reduce", "cbdgam_b200_abi_sizes",
-        "cbdgam_b200_eval_powers",
+        "cbdgam_b200_eval_powers", "cbdiso_b200_fp64_probe", "cbdiso_b200_fp64_probe_fmas",
     ]
 
 
