@@ -1,7 +1,7 @@
 """
 Benchmark: zone-updates/s of the plain cbdiso_2d drop-in on one B200.
 
-Workload (the north-star throughput configuration): circumbinary disk on
+Workload (the headline throughput configuration): circumbinary disk on
 [-8, 8]^2 at 4096^2 zones, FP64, equal-mass circular binary (softening 0.05,
 sink radius 0.05, sink rate 10, torque-free sinks), Mach 10 locally
 isothermal, nu = 1e-3, PLM theta 1.5, RK2, CFL 0.3, Keplerian buffer beyond

@@ -361,7 +361,7 @@ class OracleSolver:
         reproduces the reference's summation order for a run split into that
         many slabs along i (subdivide.py:35-60): per-slab sums of per-slab
         fields, then their sum. With `absolute`, sums |f| instead of f: the
-        scale against which a cancelling sum's rounding error is judged.
+        scale against which a cancelling sum's rounding error is measured.
         """
         c = self.cfg
         acc = [self.source_rates(1, accretion=True), self.source_rates(2, accretion=True)]

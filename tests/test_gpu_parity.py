@@ -1,7 +1,7 @@
 """
 Parity of the CUDA path with the CPU oracle and the reference fixtures.
 
-Tolerances (north-star: 1e-12 relative per step, 1e-10 after 1000 steps):
+Tolerances (the parity bar: 1e-12 relative per step, 1e-10 after 1000 steps):
   * EXACT precision runs the reference's arithmetic operation by operation;
     it differs from the CPU build only where CUDA's pow / exp round
     differently from glibc's (about one ulp), so its states agree to 1e-14 of
@@ -89,7 +89,7 @@ def test_solver_matches_reference_fixtures_exact(name):
     np.testing.assert_allclose(dts, d["dts"], rtol=1e-13, atol=0)
     got = np.array(series, dtype=complex)
     want = d["series"]
-    # sums such as torque and sigma_m1 cancel: judge them against sum |f| dA
+    # sums such as torque and sigma_m1 cancel: measure their error against sum |f| dA
     cfg = oracle_config(meta)
     o = oh.OracleSolver(cfg, d["last"], float(d["time"]), oh.Kernels("oracle", cfg.plm_theta))
     scale = np.abs(np.array(o.reductions(diagnostics(meta), absolute=True), dtype=complex))
