@@ -79,7 +79,7 @@ def fp64_peak():
 
     lib = _capi.lib()
     blocks = 8 * torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-    iterations = 200000
+    iterations = 40000
     out = torch.zeros(blocks, dtype=torch.float64, device="cuda")
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
