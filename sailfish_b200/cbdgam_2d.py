@@ -55,22 +55,24 @@ class Options(NamedTuple):
     plm_theta: float = 1.5
 
 
-def initial_condition(setup, mesh, time):
-    """Primitive data (ni, nj, 4) from a setup (cbdgam_2d.py:30-43); setups
-    with a vectorised `primitive_array(t, x, y)` are evaluated at once."""
+def initial_condition(setup, mesh, time, rows=None):
+    """Primitive data (ni, nj, 4) from a setup (cbdgam_2d.py:30-43), or only
+    the rows a <= i < b of it for rows=(a, b); setups with a vectorised
+    `primitive_array(t, x, y)` are evaluated at once."""
     ni, nj = mesh.shape
+    a, b = rows if rows is not None else (0, ni)
     if hasattr(setup, "primitive_array"):
-        i = np.arange(ni, dtype=np.float64)[:, None]
+        i = np.arange(a, b, dtype=np.float64)[:, None]
         j = np.arange(nj, dtype=np.float64)[None, :]
-        x = np.broadcast_to(mesh.x0 + (i + 0.5) * mesh.dx, (ni, nj))
-        y = np.broadcast_to(mesh.y0 + (j + 0.5) * mesh.dy, (ni, nj))
+        x = np.broadcast_to(mesh.x0 + (i + 0.5) * mesh.dx, (b - a, nj))
+        y = np.broadcast_to(mesh.y0 + (j + 0.5) * mesh.dy, (b - a, nj))
         out = np.ascontiguousarray(setup.primitive_array(time, x, y), dtype=np.float64)
-        if out.shape == (ni, nj, NQ):
+        if out.shape == (b - a, nj, NQ):
             return out
-    primitive = np.zeros([ni, nj, NQ])
-    for i in range(ni):
+    primitive = np.zeros([b - a, nj, NQ])
+    for i in range(a, b):
         for j in range(nj):
-            setup.primitive(time, mesh.cell_coordinates(i, j), primitive[i, j])
+            setup.primitive(time, mesh.cell_coordinates(i, j), primitive[i - a, j])
     return primitive
 
 
@@ -78,7 +80,14 @@ class Solver(SolverBase):
     """Adapter driving the gamma-law sm_100a kernels of libcbdiso_b200.so."""
 
     def __init__(self, setup=None, mesh=None, time=0.0, solution=None, num_patches=1, mode="gpu",
-                 physics=dict(), options=dict()):
+                 physics=dict(), options=dict(), index_range=None):
+        """
+        `index_range` (a, b) makes this solver one patch of the mesh: rows
+        a <= i < b, with the patch's own edge coordinates as the reference's
+        Patch has them (cbdgam_2d.py:66-78); `solution` is then the whole
+        mesh's or the patch's. The multi-GPU solver (distributed.py) runs one
+        patch per rank and exchanges the guard rows between stages.
+        """
         import torch
 
         physics = dict(physics)
@@ -107,16 +116,27 @@ class Solver(SolverBase):
         self.num_cons = NQ
         self.num_patches = num_patches
         self.device = torch.device("cuda", torch.cuda.current_device())
-        ni, nj = mesh.shape
+        ni_mesh, nj = mesh.shape
+        a, b = index_range if index_range is not None else (0, ni_mesh)
+        if not 0 <= a < b <= ni_mesh:
+            raise ValueError(f"index_range {index_range} is outside the mesh's {ni_mesh} rows")
+        self.index_range = (a, b)
+        ni = b - a
+        # called after each RK stage with (stage, output buffer) and after each
+        # step, on the launching stream (the multi-GPU solver's exchanges)
+        self._stage_hook = None
+        self._step_hook = None
 
         logger.info(f"initiate with time={time:0.4f}")
         logger.info(f"mesh is {mesh}")
         logger.info("boundary condition is outflow")
 
         if solution is None:
-            primitive = initial_condition(setup, mesh, time)
+            primitive = initial_condition(setup, mesh, time, rows=(a, b))
         else:
             primitive = np.asarray(solution, dtype=np.float64)
+        if primitive.shape == (ni_mesh, nj, NQ) and ni != ni_mesh:
+            primitive = primitive[a:b]
         if primitive.shape != (ni, nj, NQ):
             raise ValueError(f"solution has shape {primitive.shape}, expected {(ni, nj, NQ)}")
 
@@ -136,8 +156,8 @@ class Solver(SolverBase):
 
         g = _capi.GamGrid()
         g.ni, g.nj = ni, nj
-        g.xl, g.yl = mesh.vertex_coordinates(0, 0)
-        g.xr, g.yr = mesh.vertex_coordinates(ni, nj)
+        g.xl, g.yl = mesh.vertex_coordinates(a, 0)
+        g.xr, g.yr = mesh.vertex_coordinates(b, nj)
         g.plm_theta = options.plm_theta
         g.gamma_law_index = physics.gamma_law_index
         g.alpha = physics.alpha
@@ -274,20 +294,42 @@ class Solver(SolverBase):
         self._result[:1].zero_()
         self._check(lib.cbdgam_b200_advance_stage(ctypes.byref(g), ctypes.byref(s1), self._ptr(a_buf), None,
                                                   self._ptr(b_buf), None, stream), "advance_stage")
+        if self._stage_hook is not None:
+            self._stage_hook(0, b_buf)
         self._check(lib.cbdgam_b200_advance_stage(ctypes.byref(g), ctypes.byref(s2), self._ptr(b_buf),
                                                   self._ptr(a_buf), self._ptr(a_buf), self._ptr(self._result),
                                                   stream), "advance_stage")
+        if self._stage_hook is not None:
+            self._stage_hook(1, a_buf)
         self._time = t2
         self._ws_valid = True
+        if self._step_hook is not None:
+            self._step_hook()
 
-    def reductions(self):
-        """
-        Time series row in the order of physics.diagnostics
-        (cbdgam_2d.py:341-447): time in units of the setup's reference time
-        scale, then each sum times dx dy; sigma_m1 and eccentricity_vector
-        are complex. mdot and torque take the accretion rates when the
-        diagnostic asks for accretion, else the gravity rates.
-        """
+    # hooks of the multi-GPU solver (distributed.py)
+
+    def state_buffer(self):
+        """The padded device state (its guard rows are exchanged in place)."""
+        return self._buf[0]
+
+    def wavespeed_buffer(self):
+        """One-element device view holding the wavespeed maximum of the
+        current state once ensure_wavespeed() has run."""
+        return self._result[0:1]
+
+    def ensure_wavespeed(self):
+        """Compute the wavespeed maximum of the current state if it is not
+        already known; True if it was computed now."""
+        if self._ws_valid:
+            return False
+        self._reduce([])
+        return True
+
+    def wavespeed_changed(self):
+        """The wavespeed buffer was rewritten on the device (all-reduced);
+        nothing of it is cached on the host."""
+
+    def _device_sums(self):
         diagnostics = self._physics.diagnostics
         device = [d for d in diagnostics if d.quantity != "time"]
         for d in device:
@@ -304,6 +346,25 @@ class Solver(SolverBase):
             self._reduce(chunk)
             res = self._read(1 + 2 * len(chunk))
             sums += [(res[1 + 2 * k], res[2 + 2 * k]) for k in range(len(chunk))]
+        return device, sums
+
+    def reduction_sums(self):
+        """The diagnostic sums over this solver's zones before the dx dy
+        factor (float or complex per non-time diagnostic)."""
+        device, sums = self._device_sums()
+        return [complex(re, im) if d.quantity in COMPLEX_QUANTITIES else float(re)
+                for d, (re, im) in zip(device, sums)]
+
+    def reductions(self):
+        """
+        Time series row in the order of physics.diagnostics
+        (cbdgam_2d.py:341-447): time in units of the setup's reference time
+        scale, then each sum times dx dy; sigma_m1 and eccentricity_vector
+        are complex. mdot and torque take the accretion rates when the
+        diagnostic asks for accretion, else the gravity rates.
+        """
+        diagnostics = self._physics.diagnostics
+        _, sums = self._device_sums()
         da = self.mesh.dx * self.mesh.dy
         out, k = [], 0
         for d in diagnostics:

@@ -461,7 +461,11 @@ __device__ __forceinline__ void cooling_fast(const Consts &k, double dt, const V
 {
     const double sigma = p[0];
     const double eps = div_by(T, k.gm1, k.inv_gm1);
-    double cooled = eps * pow_m13_rn(1.0 + 3.0 * k.cooling * inv_square_rn(sigma) * cube_rn(eps) * dt);
+    // without cooling the power's argument is exactly 1 and so is the power
+    // (for finite Sigma^-2 eps^3, which the floors keep)
+    double cooled = k.cooling == 0.0
+                        ? eps
+                        : eps * pow_m13_rn(1.0 + 3.0 * k.cooling * inv_square_rn(sigma) * cube_rn(eps) * dt);
     const double ek = 0.5 * (p[1] * p[1] + p[2] * p[2]);
     cooled = greater(cooled, div_by(div_by(2.0 * ek, k.gamma, k.inv_gamma), k.gm1, k.inv_gm1) * k.mach_m2);
     u[3] += sigma * (cooled - eps);

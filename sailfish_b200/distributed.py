@@ -8,7 +8,8 @@ Per RK stage each rank runs the fused stage kernel on its slab (which writes
 zero-gradient guards on all four sides), then replaces the guard rows that
 face a neighbouring patch with the neighbour's two edge rows, as the
 reference's set_bc copies them between patches (cbdiso_2d.py:553-586): one
-contiguous block of 2 (nj + 4) 3 doubles each way, exchanged with
+contiguous block of 2 (nj + 4) 3 doubles each way (4 fields for the
+gamma-law solver), exchanged with
 torch.distributed point-to-point operations (NCCL over NVLink between GPUs,
 gloo between CPU processes). After each step the wavespeed maximum is
 all-reduced (MAX, exact), so every rank's next dt is the same; the
@@ -41,10 +42,11 @@ def subdivide(n, parts):
 
 class DistributedSolver(SolverBase):
     """
-    cbdiso_2d over the ranks of a torch.distributed process group, one patch
-    per rank. Same interface as cbdiso_2d.Solver; `solution` gathers the
-    whole mesh on every rank. `engine` builds the per-rank patch solver
-    (default cbdiso_2d.Solver) from the same arguments plus index_range.
+    cbdiso_2d (or cbdgam_2d) over the ranks of a torch.distributed process
+    group, one patch per rank. Same interface as the single-GPU Solver;
+    `solution` gathers the whole mesh on every rank. `engine` builds the
+    per-rank patch solver from the same arguments plus index_range (default:
+    cbdgam_2d.Solver for a gamma-law physics dict, else cbdiso_2d.Solver).
     """
 
     def __init__(self, setup=None, mesh=None, time=0.0, solution=None, physics=dict(), options=dict(), group=None,
@@ -66,7 +68,14 @@ class DistributedSolver(SolverBase):
         self.ranges = list(subdivide(ni, self.world))
         self.mesh = mesh
         self.setup = setup
-        make = engine or Solver
+        if engine is None:
+            from .physics import enum_value
+
+            if enum_value(dict(physics).get("eos_type", 1)) == 3:
+                from .cbdgam_2d import Solver as engine  # the gamma-law solver's patches
+            else:
+                engine = Solver
+        make = engine
         self.local = make(setup=setup, mesh=mesh, time=time, solution=solution, physics=physics, options=options,
                           index_range=self.ranges[self.rank])
         self.local._stage_hook = self._exchange

@@ -161,3 +161,74 @@ class SerialPatches:
     @property
     def solution(self):
         return np.concatenate([p.o.solution for p in self.p], axis=0)
+
+
+class GamOraclePatch:
+    """The gamma-law solver's patch (cbdgam_2d.py:46-223) on the gamma-law
+    oracle's kernels, with the same hooks as cbdgam_2d.Solver."""
+
+    def __init__(self, setup, mesh, time, solution, physics, options, index_range):
+        from oracle import host_gam as og
+        from sailfish_b200.cbdiso_2d import _as_diagnostic
+
+        a, b = index_range
+        ni, nj = mesh.shape
+        self.setup, self.mesh = setup, mesh
+        self.options = dict(options)
+        self.physics = dict(physics, diagnostics=[_as_diagnostic(d) for d in physics.get("diagnostics", [])])
+        self.diagnostics = [d for d in physics.get("diagnostics", []) if d["quantity"] != "time"]
+        onset = physics["buffer_onset_width"]
+        prim = [0.0] * 4
+        setup.primitive(time, [mesh.x1 - onset, 0.0], prim)
+        on = physics["buffer_is_enabled"]
+        xl, yl = mesh.vertex_coordinates(a, 0)
+        xr, yr = mesh.vertex_coordinates(b, nj)
+        cfg = og.GamConfig(xl, xr, yl, yr, b - a, nj, gamma_law_index=physics["gamma_law_index"],
+                           alpha=physics["alpha"], cooling_coefficient=physics["cooling_coefficient"],
+                           constant_softening=physics["constant_softening"], buffer_is_enabled=on,
+                           buffer_driving_rate=physics["buffer_driving_rate"], buffer_onset_width=onset,
+                           buffer_surface_density=prim[0] if on else 0.0,
+                           buffer_surface_pressure=prim[3] if on else 0.0,
+                           masses=oh.binary_masses(1.0, 1.0, setup.mass_ratio, setup.eccentricity,
+                                                   setup.softening_length, setup.sink_model, setup.sink_rate,
+                                                   setup.sink_radius),
+                           plm_theta=options.get("plm_theta", 1.5))
+        sol = np.asarray(solution)
+        self.o = og.GamOracleSolver(cfg, sol[a:b] if sol.shape[0] == ni else sol, time)
+        self.o.xl, self.o.xr, self.o.yl, self.o.yr = xl, xr, yl, yr
+        self.o.buffer_outer_radius = mesh.x1 if on else 0.0
+        zero_gradient(self.o.p1)
+        self._stage_hook = None
+        self._step_hook = None
+        self._ws = torch.zeros(1, dtype=torch.float64)
+        self._valid = False
+
+    time = OraclePatch.time
+    solution = OraclePatch.solution
+    recommended_cfl = 0.1
+    maximum_cfl = 0.4
+    state_buffer = OraclePatch.state_buffer
+    wavespeed_buffer = OraclePatch.wavespeed_buffer
+    ensure_wavespeed = OraclePatch.ensure_wavespeed
+    wavespeed_changed = OraclePatch.wavespeed_changed
+    maximum_wavespeed = OraclePatch.maximum_wavespeed
+    reduction_sums = OraclePatch.reduction_sums
+
+    def advance(self, dt):
+        o, c = self.o, self.o.cfg
+        o.time0 = o.time
+        o.k.primitive_to_conserved(c.ni, c.nj, o.p1, o.u0, c.gamma_law_index)
+        for s, a in enumerate((0.0, 0.5)):
+            m1, m2 = c.point_masses(o.time)
+            buf = (c.buffer_surface_density, c.buffer_surface_pressure, m1.mass + m2.mass, c.buffer_driving_rate,
+                   o.buffer_outer_radius, c.buffer_onset_width, int(c.buffer_is_enabled))
+            o.k.advance_rk(c, o.xl, o.xr, o.yl, o.yr, o.u0, o.p1, o.p2, buf, m1, m2, a, dt)
+            o.time = o.time0 * a + (o.time + dt) * (1.0 - a)
+            o.p1, o.p2 = o.p2, o.p1
+            zero_gradient(o.p1)
+            if self._stage_hook is not None:
+                self._stage_hook(s, torch.from_numpy(o.p1))
+        self._valid = False
+        self.ensure_wavespeed()
+        if self._step_hook is not None:
+            self._step_hook()

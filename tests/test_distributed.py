@@ -133,3 +133,92 @@ def test_thread_ranks_match_gloo_ranks():
     for sol, red in out:
         np.testing.assert_array_equal(sol, serial.solution)
         assert red == out[0][1]
+
+
+# ---------------------------------------------------------------------------
+# the gamma-law solver's patches, against the reference's own two-patch run
+# (tests/golden/gam_n48_cool_p2.npz: 48^2, cooling, eccentric q = 0.5 binary)
+# ---------------------------------------------------------------------------
+
+
+def _gam_problem():
+    from cases import diagnostics, gam_initial_state, load
+    from sailfish_b200.mesh import PlanarCartesian2DMesh
+    from sailfish_b200.setups import CircumbinaryDisk
+
+    d = load("gam_n48_cool_p2")
+    meta = d["meta"]
+    x0, y0, x1, y1, ni, nj = meta["mesh"]
+    setup = CircumbinaryDisk(**meta["params"])
+    mesh = PlanarCartesian2DMesh(x0, y0, x1, y1, int(ni), int(nj))
+    physics = setup.physics
+    physics["diagnostics"] = diagnostics(meta)
+    return d, setup, mesh, gam_initial_state(d), physics
+
+
+def _gam_rank(rank, world, port, out_dir):
+    import torch.distributed as dist
+
+    from patch_engine import GamOraclePatch
+    from sailfish_b200.distributed import DistributedSolver
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        d, setup, mesh, prim, physics = _gam_problem()
+        s = DistributedSolver(setup=setup, mesh=mesh, solution=prim, physics=physics, engine=GamOraclePatch)
+        dts, series = [], []
+        for _ in range(d["meta"]["steps"]):
+            dt = mesh.min_spacing() / s.maximum_wavespeed() * d["meta"]["cfl"]
+            s.advance(dt)
+            dts.append(dt)
+            series.append(s.reductions())
+        sol = s.solution
+        if rank == 0:
+            np.savez(os.path.join(out_dir, "out.npz"), solution=sol, dts=np.array(dts),
+                     series=np.array(series, dtype=complex), time=s.time)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gamma_patch_ranks_reproduce_the_reference_two_patch_run():
+    """Two gloo ranks, one gamma-law patch each (oracle kernels), against
+    the reference solver run with num_patches=2: dts and states bit for
+    bit, the time series to rounding (the sums are regrouped per patch)."""
+    with tempfile.TemporaryDirectory() as out:
+        mp.spawn(_gam_rank, args=(2, _free_port(), out), nprocs=2, join=True)
+        got = dict(np.load(os.path.join(out, "out.npz")))
+    d = _gam_problem()[0]
+    assert d["meta"]["patches"] == 2
+    np.testing.assert_array_equal(got["dts"], d["dts"])
+    np.testing.assert_array_equal(got["solution"], d["last"])
+    assert float(got["time"]) == float(d["time"])
+    want = d["series"]
+    scale = np.maximum(np.abs(want).max(axis=0), 1e-300)
+    assert (np.abs(got["series"] - want).max(axis=0) / scale).max() <= 1e-12
+
+
+def test_default_engine_follows_the_equation_of_state():
+    """A gamma-law physics dict makes the distributed solver's patches
+    cbdgam_2d patches; it is checked by the engine it picks, without a GPU."""
+    from sailfish_b200.distributed import DistributedSolver
+    from thread_comm import ThreadComm
+
+    d, setup, mesh, prim, physics = _gam_problem()
+    picked = []
+
+    class Probe:
+        def __init__(self, **kwargs):
+            raise RuntimeError("stop")
+
+    import sailfish_b200.cbdgam_2d as gam
+
+    real = gam.Solver
+    try:
+        gam.Solver = lambda **kw: picked.append("cbdgam_2d") or Probe(**kw)
+        comm = ThreadComm(1)
+        with pytest.raises(RuntimeError, match="stop"):
+            comm.run(lambda r: DistributedSolver(setup=setup, mesh=mesh, solution=prim, physics=physics,
+                                                 comm=comm))
+    finally:
+        gam.Solver = real
+    assert picked == ["cbdgam_2d"]

@@ -111,3 +111,39 @@ def test_one_nccl_rank():
         assert err.max() <= 1e-13, err
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gamma_patch_kernels_against_the_reference_two_patch_run(world):
+    """The gamma-law solver as thread ranks with its real stage kernels on
+    the reference's two-patch fixture (48^2, cooling): with two ranks the
+    patches are the reference's own, with three they differ only in the
+    patches' edge rounding; dts to 1e-13, states to 1e-12 of each field's
+    maximum, every rank's view identical."""
+    from test_distributed import _gam_problem
+
+    d, setup, mesh, prim, physics = _gam_problem()
+    comm = ThreadComm(world)
+    meta = d["meta"]
+
+    def rank(r):
+        torch.cuda.set_device(0)
+        s = DistributedSolver(setup=setup, mesh=mesh, solution=prim, physics=physics, comm=comm)
+        dts, series = [], []
+        for _ in range(meta["steps"]):
+            dt = mesh.min_spacing() / s.maximum_wavespeed() * meta["cfl"]
+            s.advance(dt)
+            dts.append(dt)
+            series.append(s.reductions())
+        return s.solution, dts, series, type(s.local).__module__
+
+    out = comm.run(rank)
+    for sol, dts, series, module in out:
+        assert module == "sailfish_b200.cbdgam_2d"
+        np.testing.assert_array_equal(sol, out[0][0])
+        assert dts == out[0][1] and series == out[0][2]
+    sol, dts = out[0][0], np.array(out[0][1])
+    np.testing.assert_allclose(dts, d["dts"], rtol=1e-13, atol=0)
+    want = d["last"]
+    err = np.abs(sol - want).max(axis=(0, 1)) / np.abs(want).max(axis=(0, 1))
+    assert err.max() <= 1e-12, err
