@@ -182,7 +182,10 @@ class Solver(SolverBase):
                     "fill_guards")
         nscratch = int(self._lib.cbdgam_b200_scratch_bytes(ctypes.byref(g)))
         self._scratch = torch.zeros(nscratch // 8 + 8, **f64)
+        # the wavespeed maximum of the current state (slot 0; the multi-GPU
+        # solver all-reduces it in place) and, apart, the diagnostic sums
         self._result = torch.zeros(1 + 2 * _capi.GAM_MAX_DIAG, **f64)
+        self._sums = torch.zeros(1 + 2 * _capi.GAM_MAX_DIAG, **f64)
         self._result_host = torch.zeros(1 + 2 * _capi.GAM_MAX_DIAG, dtype=torch.float64).pin_memory()
         self._ws_valid = False
         self._time = float(time)
@@ -216,17 +219,19 @@ class Solver(SolverBase):
         st.a, st.dt = a, dt
         return st
 
-    def _read(self, n):
+    def _read(self, n, source=None):
         import torch
 
-        self._result_host[:n].copy_(self._result[:n], non_blocking=True)
+        source = self._result if source is None else source
+        self._result_host[:n].copy_(source[:n], non_blocking=True)
         torch.cuda.current_stream().synchronize()
         self.d2h_bytes += 8 * n
         return self._result_host[:n].numpy().copy()
 
     def _reduce(self, diags):
-        """Wavespeed maximum and the sums of `diags` (at most 4) on the
-        current state, into self._result."""
+        """The sums of `diags` (at most 4) on the current state into
+        self._sums; with no diagnostics, the wavespeed maximum into
+        self._result."""
         masses = (_capi.Mass * 2)()
         m1, m2 = self._physics.point_masses(self._time)
         _mass_struct(m1, masses[0])
@@ -234,10 +239,12 @@ class Solver(SolverBase):
         structs = (_capi.Diag * max(1, len(diags)))()
         for k, d in enumerate(diags):
             _diag_struct(d, structs[k])
+        out = self._sums if diags else self._result
         self._check(self._lib.cbdgam_b200_reduce(ctypes.byref(self._grid), masses, structs, len(diags),
                                                  self._ptr(self._buf[0]), self._ptr(self._scratch),
-                                                 self._ptr(self._result), self._stream()), "reduce")
-        self._ws_valid = True
+                                                 self._ptr(out), self._stream()), "reduce")
+        if not diags:
+            self._ws_valid = True
 
     # ------------------------------------------------------------------
     # SolverBase
@@ -344,7 +351,7 @@ class Solver(SolverBase):
         for first in range(0, len(device), _capi.GAM_MAX_DIAG):
             chunk = device[first:first + _capi.GAM_MAX_DIAG]
             self._reduce(chunk)
-            res = self._read(1 + 2 * len(chunk))
+            res = self._read(1 + 2 * len(chunk), self._sums)
             sums += [(res[1 + 2 * k], res[2 + 2 * k]) for k in range(len(chunk))]
         return device, sums
 
