@@ -377,3 +377,34 @@ def test_powers_are_correctly_rounded():
         glibc_agree += list(g[:7]) == glibc
     # the C library's pow / exp are correctly rounded in nearly every case
     assert glibc_agree >= 0.99 * len(x)
+
+
+def test_one_full_size_step_against_oracle():
+    """One RK2 step of the 1024^2 gamma-law disk with cooling (the oracle
+    takes a few seconds on the host): states within 1e-13 of each field's
+    maximum, the driver dt bit for bit."""
+    from cases import GAM_DEFAULTS
+    from sailfish_b200.setups import CircumbinaryDisk as Disk
+
+    n = 1024
+    setup = Disk(eos="gamma-law", domain_radius=8.0, cooling_coefficient=2.0, mass_ratio=0.7, eccentricity=0.1)
+    mesh = setup.mesh(n)
+    s = make_solver("cbdgam_2d", setup.physics, {}, setup=setup, mesh=mesh)
+    prim0 = s.solution
+    onset = [0.0] * 4
+    setup.primitive(0.0, [mesh.x1 - 0.1, 0.0], onset)
+    p = dict(GAM_DEFAULTS, domain_radius=8.0, cooling_coefficient=2.0, mass_ratio=0.7, eccentricity=0.1)
+    from oracle import host as oh
+
+    cfg = og.GamConfig(mesh.x0, mesh.x1, mesh.y0, mesh.y1, n, n, alpha=p["alpha"],
+                       cooling_coefficient=p["cooling_coefficient"], buffer_is_enabled=True,
+                       buffer_surface_density=onset[0], buffer_surface_pressure=onset[3],
+                       masses=oh.binary_masses(1.0, 1.0, p["mass_ratio"], p["eccentricity"], p["softening_length"],
+                                               p["sink_model"], p["sink_rate"], p["sink_radius"]))
+    o = og.GamOracleSolver(cfg, prim0, 0.0)
+    dt = mesh.min_spacing() / s.maximum_wavespeed() * 0.1
+    assert dt == og.driver_dt(o, 0.1)
+    s.advance(dt)
+    o.advance(dt)
+    assert field_error(s.solution, o.solution) <= 1e-13
+    assert s.maximum_wavespeed() == pytest.approx(o.maximum_wavespeed(), rel=1e-14)

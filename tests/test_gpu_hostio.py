@@ -1,8 +1,8 @@
 """
 Whole-state host <-> device copies through the pinned staging buffer
 (sailfish_b200/_hostio.py): bit-exact round trips for strided device views
-above and below the staging threshold, concurrent callers, and the solvers'
-`solution` / constructor using them.
+above and below the staging threshold, and concurrent callers. Also the
+FP64 issue-rate probe the benchmark's FP64 roofline divides by.
 """
 
 import threading
@@ -65,3 +65,26 @@ def test_concurrent_callers_and_release():
     assert not errors
     _hostio.release_staging()
     np.testing.assert_array_equal(_hostio.download(bufs[1]), arrays[1])
+
+
+def test_fp64_probe_measures_a_plausible_rate():
+    """The FP64 issue-rate probe behind the bench's FP64 roofline runs and
+    reports a rate between 1 and 100 T thread-FMAs/s."""
+    import ctypes
+
+    from sailfish_b200 import _capi
+
+    lib = _capi.lib()
+    blocks = 8 * torch.cuda.get_device_properties(0).multi_processor_count
+    out = torch.zeros(blocks, dtype=torch.float64, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    assert lib.cbdiso_b200_fp64_probe(1000, blocks, ctypes.c_void_p(out.data_ptr()), stream) == 0
+    start.record()
+    assert lib.cbdiso_b200_fp64_probe(20000, blocks, ctypes.c_void_p(out.data_ptr()), stream) == 0
+    stop.record()
+    torch.cuda.synchronize()
+    rate = lib.cbdiso_b200_fp64_probe_fmas(20000, blocks) / (start.elapsed_time(stop) * 1e-3)
+    assert 1e12 < rate < 1e14
+    assert not out.any()  # the guard store never fires
+    assert lib.cbdiso_b200_fp64_probe(0, blocks, ctypes.c_void_p(out.data_ptr()), stream) == 1
