@@ -8,8 +8,9 @@ touched (faulted in and zeroed) by the single copying thread. These helpers
 instead go through one pinned staging buffer kept for the process (the
 device copy then runs at PCIe speed) and copy between it and the numpy array
 with several host threads (numpy releases the GIL while copying), so the
-page faults and the memcpy run in parallel. Measured on the B200 host at
-4096^2: download 186 -> 21 ms, upload 37 -> 13 ms.
+page faults and the memcpy run in parallel, block by block behind the device
+copies. Measured on the B200 host at 4096^2 before the pipelining: download
+186 -> 21 ms, upload 37 -> 13 ms.
 
 The staging buffer is allocated on first use (pinning is itself slow: about
 0.2 s for 403 MB) and grows to the largest state copied; `release_staging()`
@@ -53,14 +54,6 @@ def _staging_view(nbytes, shape):
     return _staging[:nbytes].view(torch.float64).view(shape)
 
 
-def _parallel_copy(dst, src):
-    """np.copyto(dst, src) over row blocks on the thread pool."""
-    n = dst.shape[0]
-    k = min(_threads(), n)
-    blocks = [(a * n // k, (a + 1) * n // k) for a in range(k)]
-    list(_get_pool().map(lambda ab: np.copyto(dst[ab[0]:ab[1]], src[ab[0]:ab[1]]), blocks))
-
-
 def release_staging():
     """Free the pinned staging buffer (it is allocated again when needed)."""
     global _staging
@@ -68,8 +61,17 @@ def release_staging():
         _staging = None
 
 
+def _blocks(n, k):
+    k = max(1, min(k, n))
+    return [(a * n // k, (a + 1) * n // k) for a in range(k)]
+
+
 def download(tensor):
-    """A new numpy array equal to a float64 device tensor (any strides)."""
+    """A new numpy array equal to a float64 device tensor (any strides).
+
+    Pipelined in row blocks: each block's device-to-pinned copy is followed,
+    as soon as it has landed, by its copy into the numpy array on a pool
+    thread, while the next blocks are still in flight."""
     import torch
 
     nbytes = tensor.numel() * 8
@@ -79,15 +81,30 @@ def download(tensor):
     out = np.empty(tuple(src.shape), dtype=np.float64)
     with _lock:
         stage = _staging_view(nbytes, tuple(src.shape))
-        stage.copy_(src, non_blocking=True)  # on the source device's current stream
-        torch.cuda.current_stream(src.device).synchronize()
-        _parallel_copy(out, stage.numpy())
+        host = stage.numpy()
+        stream = torch.cuda.current_stream(src.device)
+        events = []
+        for a, b in _blocks(src.shape[0], 2 * _threads()):
+            stage[a:b].copy_(src[a:b], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            events.append((a, b, ev))
+        pool = _get_pool()
+        jobs = []
+        for a, b, ev in events:
+            ev.synchronize()
+            jobs.append(pool.submit(np.copyto, out[a:b], host[a:b]))
+        for j in jobs:
+            j.result()
     return out
 
 
 def upload(array, target):
     """Copy a float64 numpy array into a device tensor view of its shape
-    (any strides); returns after the copy has completed."""
+    (any strides); returns after the copy has completed.
+
+    Pipelined in row blocks: pool threads copy the blocks into pinned memory
+    and each block goes to the device as soon as it is staged."""
     import torch
 
     array = np.asarray(array, dtype=np.float64)
@@ -99,6 +116,11 @@ def upload(array, target):
         return
     with _lock:
         stage = _staging_view(nbytes, tuple(array.shape))
-        _parallel_copy(stage.numpy(), array)
-        target.copy_(stage, non_blocking=True)  # on the target device's current stream
+        host = stage.numpy()
+        pool = _get_pool()
+        blocks = _blocks(array.shape[0], 2 * _threads())
+        jobs = [pool.submit(np.copyto, host[a:b], array[a:b]) for a, b in blocks]
+        for (a, b), j in zip(blocks, jobs):
+            j.result()
+            target[a:b].copy_(stage[a:b], non_blocking=True)  # on the target device's current stream
         torch.cuda.current_stream(target.device).synchronize()
