@@ -34,6 +34,7 @@
 #include <stdint.h>
 
 #include "../../include/cbdiso_b200.h"
+#include "cr_math.cuh"
 
 namespace cbd {
 
@@ -112,30 +113,9 @@ __device__ __forceinline__ double div_rn(double a, double b)
     return div_by<FAST>(a, b, __drcp_rn(b));
 }
 
-// RN(x^-1.5) for positive normal x. 1/x and then its square root are carried
-// as double-double pairs (error-free products via FMA, one Newton correction
-// of the square root), and their product is rounded once; the result equals
-// the correctly rounded power except within ~2^-100 of a rounding midpoint.
-__device__ __forceinline__ double pow_m15_rn(double x)
-{
-    const double u = __drcp_rn(x);
-    const double u_lo = u * fma(-u, x, 1.0);
-    const double w = sqrt(u);
-    const double w_lo = (fma(-w, w, u) + u_lo) * (0.5 * w * x);
-    const double h = u * w;
-    const double h_lo = fma(u, w, -h) + (u * w_lo + u_lo * w);
-    return h + h_lo;
-}
-
-// RN(q^4): q^2 as an exact double-double pair, squared, rounded once.
-__device__ __forceinline__ double pow4_rn(double q)
-{
-    const double h = q * q;
-    const double h_lo = fma(q, q, -h);
-    const double r = h * h;
-    const double r_lo = fma(h, h, -r) + 2.0 * h * h_lo;
-    return r + r_lo;
-}
+// correctly rounded powers (cr_math.cuh)
+using crm::pow4_rn;
+using crm::pow_m15_rn;
 
 // s^-1.5 for the gravity term
 template <bool FAST>
