@@ -408,3 +408,14 @@ def test_one_full_size_step_against_oracle():
     o.advance(dt)
     assert field_error(s.solution, o.solution) <= 1e-13
     assert s.maximum_wavespeed() == pytest.approx(o.maximum_wavespeed(), rel=1e-14)
+
+
+@pytest.mark.parametrize("name", [n for n in gam_names() if "first" in load(n)])
+def test_gamma_first_step_is_bit_identical_to_the_reference(name):
+    """The gamma-law stage reproduces the reference's first step bit for bit
+    (correctly rounded powers, exponential, divisions and square roots in the
+    reference's operation order)."""
+    d = load(name)
+    s = gam_solver(d)
+    s.advance(float(d["dts"][0]))
+    np.testing.assert_array_equal(s.solution, d["first"])
