@@ -56,11 +56,10 @@ __device__ __forceinline__ Dual g_sqrt(Dual x)
     const double s = sqrt(x.v);
     return {s, x.d / (2.0 * s)};
 }
-// the value as the forward stage computes it (correctly rounded)
-__device__ __forceinline__ double g_exp(double x) { return crm::exp_rn(x); }
+__device__ __forceinline__ double g_exp(double x) { return exp(x); }
 __device__ __forceinline__ Dual g_exp(Dual x)
 {
-    const double e = crm::exp_rn(x.v);
+    const double e = exp(x.v);
     return {e, e * x.d};
 }
 __device__ __forceinline__ double g_pow15(double x) { return inv_pow15<false>(x); }
