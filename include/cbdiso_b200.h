@@ -503,6 +503,13 @@ int cbdgam_b200_reduce(const cbdgam_grid_t *grid, const cbd_mass_t *masses, cons
 int cbdiso_b200_fp64_probe(long iterations, int blocks, double *out, void *stream);
 long cbdiso_b200_fp64_probe_fmas(long iterations, int blocks);
 
+/* Host function (no device work): the gamma-law circumbinary disk's initial
+ * primitives (sailfish/setups/circumbinary_disk.py:95-110) at n points, with
+ * the C library's sqrt / pow / exp in the setup's operation order, which is
+ * what Python's float arithmetic computes; primitive holds 4 n doubles. */
+void cbdgam_b200_disk_primitive(long n, const double *x, const double *y, double softening_length,
+                                double initial_sigma, double initial_pressure, double *primitive);
+
 /* sizeof of cbdgam_grid_t and cbdgam_stage_t, for bindings to check. */
 void cbdgam_b200_abi_sizes(size_t out[2]);
 

@@ -190,6 +190,9 @@ def _declare(lib):
     lib.cbdiso_b200_fp64_probe.restype = c_int
     lib.cbdiso_b200_fp64_probe_fmas.argtypes = [ctypes.c_long, c_int]
     lib.cbdiso_b200_fp64_probe_fmas.restype = ctypes.c_long
+    lib.cbdgam_b200_disk_primitive.argtypes = [ctypes.c_long, c_void_p, c_void_p, c_double, c_double, c_double,
+                                               c_void_p]
+    lib.cbdgam_b200_disk_primitive.restype = None
     lib.cbdgam_b200_scratch_bytes.argtypes = [POINTER(GamGrid)]
     lib.cbdgam_b200_scratch_bytes.restype = c_size_t
     lib.cbdgam_b200_abi_sizes.argtypes = [POINTER(c_size_t)]
@@ -238,6 +241,7 @@ def exported_symbols():
         "cbdgam_2d_point_mass_source_term", "cbdgam_b200_set_plm_theta", "cbdgam_b200_advance_stage",
         "cbdgam_b200_fill_guards", "cbdgam_b200_scratch_bytes", "cbdgam_b200_reduce", "cbdgam_b200_abi_sizes",
         "cbdgam_b200_eval_powers", "cbdiso_b200_fp64_probe", "cbdiso_b200_fp64_probe_fmas",
+        "cbdgam_b200_disk_primitive",
     ]
 
 

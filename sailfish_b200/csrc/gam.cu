@@ -892,6 +892,26 @@ int cbdgam_b200_eval_powers(long n, const double *x, double *out, void *stream)
     return status_of(cudaGetLastError());
 }
 
+void cbdgam_b200_disk_primitive(long n, const double *x, const double *y, double softening_length,
+                                double initial_sigma, double initial_pressure, double *primitive)
+{
+    // host code: the C library's sqrt / pow / exp, as Python's math and float
+    // power call them, in the setup's operation order
+    for (long k = 0; k < n; ++k) {
+        const double xk = x[k], yk = y[k];
+        const double r = std::sqrt(xk * xk + yk * yk);
+        const double rs = std::sqrt(xk * xk + yk * yk + softening_length * softening_length);
+        const double rmax = 1e-12 > r ? 1e-12 : r;
+        const double phx = -yk / rmax, phy = +xk / rmax;
+        const double taper = 0.0001 + 0.9999 * std::exp(-std::pow(1.0 / rs, 30.0));
+        double *p = primitive + 4 * k;
+        p[0] = initial_sigma * std::pow(rs, -3.0 / 5.0) * taper;
+        p[1] = std::sqrt(1.0 / rs) * phx;
+        p[2] = std::sqrt(1.0 / rs) * phy;
+        p[3] = initial_pressure * std::pow(rs, -3.0 / 2.0) * taper;
+    }
+}
+
 void cbdgam_b200_abi_sizes(size_t out[2])
 {
     out[0] = sizeof(cbdgam_grid_t);

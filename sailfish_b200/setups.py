@@ -162,23 +162,31 @@ class CircumbinaryDisk(SetupBase):
             primitive[3] = self.initial_pressure * r_softened ** (-3.0 / 2.0) * taper
 
     def primitive_array(self, t, x, y):
-        """primitive() on whole arrays of zone centres. The isothermal fields
-        match primitive() bit for bit; the gamma-law power laws and taper go
-        through numpy's pow / exp, which may differ from Python's math in
-        the last place."""
+        """primitive() on whole arrays of zone centres, bit for bit. The
+        isothermal fields need only IEEE operations, which numpy performs
+        exactly; the gamma-law power laws and taper call the C library's pow /
+        exp as Python's float arithmetic does (numpy's own vectorised pow /
+        exp can differ from those in the last place)."""
         GM = 1.0
+        x, y = np.broadcast_arrays(np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64))
+        if self.is_gamma_law:
+            import ctypes
+
+            from . import _capi
+
+            xc, yc = np.ascontiguousarray(x), np.ascontiguousarray(y)
+            out = np.empty(x.shape + (4,))
+            _capi.lib().cbdgam_b200_disk_primitive(xc.size, ctypes.c_void_p(xc.ctypes.data),
+                                                   ctypes.c_void_p(yc.ctypes.data), float(self.softening_length),
+                                                   float(self.initial_sigma), float(self.initial_pressure),
+                                                   ctypes.c_void_p(out.ctypes.data))
+            return out
         r = np.sqrt(x * x + y * y)
         r_softened = np.sqrt(x * x + y * y + self.softening_length * self.softening_length)
-        nq = 4 if self.is_gamma_law else 3
-        out = np.empty(np.broadcast(x, y).shape + (nq,))
+        out = np.empty(x.shape + (3,))
+        out[..., 0] = self.initial_sigma
         out[..., 1] = np.sqrt(GM / r_softened) * (-y / np.maximum(r, 1e-12))
         out[..., 2] = np.sqrt(GM / r_softened) * (+x / np.maximum(r, 1e-12))
-        if self.is_gamma_law:
-            taper = 0.0001 + 0.9999 * np.exp(-((1.0 / r_softened) ** 30))
-            out[..., 0] = self.initial_sigma * r_softened ** (-3.0 / 5.0) * taper
-            out[..., 3] = self.initial_pressure * r_softened ** (-3.0 / 2.0) * taper
-        else:
-            out[..., 0] = self.initial_sigma
         return out
 
     def mesh(self, resolution):

@@ -26,17 +26,29 @@ def test_gamma_setup_primitive_matches_restatement():
         assert tuple(out) == og.gamma_disk_primitive(x, y)
 
 
-def test_gamma_setup_primitive_array_close_to_zone_wise():
+def test_gamma_setup_primitive_array_equals_zone_wise():
+    """The vectorised initial data equals the per-zone setup formula (the
+    reference's initial_condition loop) bit for bit, on random points, the
+    origin and a 96^2 mesh."""
     setup = CircumbinaryDisk(eos="gamma-law", initial_pressure=3e-3, softening_length=0.1)
     rng = np.random.default_rng(5)
-    x, y = rng.uniform(-8, 8, (2, 50, 7))
+    x, y = rng.uniform(-8, 8, (2, 400, 7))
+    x[0, 0] = y[0, 0] = 0.0
     arr = setup.primitive_array(0.0, x, y)
-    assert arr.shape == (50, 7, 4)
+    assert arr.shape == (400, 7, 4)
     out = [0.0] * 4
-    for i in range(50):
+    for i in range(400):
         for j in range(7):
             setup.primitive(0.0, (x[i, j], y[i, j]), out)
-            np.testing.assert_allclose(arr[i, j], out, rtol=1e-14, atol=0)
+            assert tuple(arr[i, j]) == tuple(out), (i, j)
+    from sailfish_b200.cbdgam_2d import initial_condition
+
+    mesh = setup.mesh(96)
+    fast = initial_condition(setup, mesh, 0.0)
+    for i in (0, 17, 47, 48, 95):
+        for j in (0, 5, 48, 95):
+            setup.primitive(0.0, mesh.cell_coordinates(i, j), out)
+            assert tuple(fast[i, j]) == tuple(out)
 
 
 def test_gamma_setup_physics_and_solver():
