@@ -99,73 +99,6 @@ __device__ __forceinline__ double slope(double yl, double y0, double yr, double 
     return (sa & sc & (sa ^ sb)) ? -0.0 : 0.0;
 }
 
-// cbdgam_2d.c:75-106
-template <class V>
-__device__ __forceinline__ double scale_height(const Mass *m, double x, double y, const V &p)
-{
-    if (m[0].mass == 0.0 && m[1].mass == 0.0)
-        return 1.0;
-    double w2 = 0.0;
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        if (m[k].mass > 0.0) {
-            const double dx = x - m[k].x, dy = y - m[k].y;
-            const double r = sqrt(dx * dx + dy * dy + 1e-12);
-            w2 += m[k].mass * inv_cube_rn(r);
-        }
-    }
-    return sqrt(p[3] / p[0]) / sqrt(w2);
-}
-
-// cbdgam_2d.c:108-203
-template <class V>
-__device__ __forceinline__ void mass_source(const Mass &m, double x, double y, double dt, const V &p, double h,
-                                            int constant_softening, double gamma, double *du)
-{
-    const double sigma = p[0];
-    const double eps = p[3] / sigma / (gamma - 1.0);
-    const double dx = x - m.x, dy = y - m.y;
-    const double r2 = dx * dx + dy * dy;
-    const double dr = sqrt(r2);
-    const double rs = m.radius;
-    double soft;
-    if (constant_softening) {
-        soft = m.soft;
-    } else if (dr > rs) {
-        soft = 0.5 * h;
-    } else {
-        const double q = dr / rs;
-        const double w = (1.0 - q * q) * (1.0 - q * q);  // pow(., 2.0) is the correctly rounded square
-        soft = w * rs + (1.0 - w) * 0.5 * h;
-    }
-    const double rate = (dr < 4.0 * rs) ? m.rate * exp_rn(-fourth_rn(dr / rs)) : 0.0;
-    const double fnum = sigma * m.mass * inv_pow15_rn(r2 + soft * soft);
-    const double fx = -fnum * dx, fy = -fnum * dy;
-    const double mdot = sigma * rate * -1.0;
-    const double vx = p[1], vy = p[2];
-    if (m.model == 1) {
-        du[0] = dt * mdot;
-        du[1] = dt * mdot * p[1] + dt * fx;
-        du[2] = dt * mdot * p[2] + dt * fy;
-        du[3] = dt * (mdot * eps + 0.5 * mdot * (vx * vx + vy * vy)) + dt * (fx * vx + fy * vy);
-    } else if (m.model == 2) {
-        const double ex = dx / (dr + 1e-12), ey = dy / (dr + 1e-12);
-        const double dvr = (vx - m.vx) * ex + (vy - m.vy) * ey;
-        const double wx = dvr * ex + m.vx, wy = dvr * ey + m.vy;
-        du[0] = dt * mdot;
-        du[1] = dt * mdot * wx + dt * fx;
-        du[2] = dt * mdot * wy + dt * fy;
-        du[3] = dt * (mdot * eps + 0.5 * mdot * (wx * wx + wy * wy)) + dt * (fx * vx + fy * vy);
-    } else if (m.model == 3) {
-        du[0] = dt * mdot;
-        du[1] = dt * fx;
-        du[2] = dt * fy;
-        du[3] = dt * (fx * vx + fy * vy);
-    } else {
-        du[0] = du[1] = du[2] = du[3] = 0.0;
-    }
-}
-
 template <class V>
 __device__ __forceinline__ double cs2_of(double gamma, const V &p) { return p[3] / p[0] * gamma; }
 
@@ -292,19 +225,20 @@ __device__ __forceinline__ void hlle_fast(const Consts &k, const double *pl, con
         f[q] = div_by(fl[q] * ap - fr[q] * am - (ul[q] - ur[q]) * ap * am, den, y);
 }
 
-// cbdgam_2d.c:108-203 for the stage kernel: T = p / Sigma and h given
+// cbdgam_2d.c:108-203: gravity, sink and their work on the gas for one mass,
+// given T = p / Sigma, the disk height h and gamma - 1 with its reciprocal
 template <class V>
-__device__ __forceinline__ void mass_source_fast(const Consts &k, const Mass &m, double x, double y, double dt,
-                                                 const V &p, double T, double h, double *du)
+__device__ __forceinline__ void mass_source(const Mass &m, double x, double y, double dt, const V &p, double T,
+                                            double h, int constant_softening, double gm1, double inv_gm1, double *du)
 {
     const double sigma = p[0];
-    const double eps = div_by(T, k.gm1, k.inv_gm1);
+    const double eps = div_by(T, gm1, inv_gm1);
     const double dx = x - m.x, dy = y - m.y;
     const double r2 = dx * dx + dy * dy;
     const double dr = sqrt(r2);
     const double rs = m.radius;
     double soft;
-    if (k.constant_softening) {
+    if (constant_softening) {
         soft = m.soft;
     } else if (dr > rs) {
         soft = 0.5 * h;
@@ -513,7 +447,7 @@ __device__ __forceinline__ void stage_phase2(const Consts &k, const Stage &st, c
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
         double du[NF];
-        mass_source_fast(k, st.m[m], xc, yc, dt, c, T, hc, du);
+        mass_source(st.m[m], xc, yc, dt, c, T, hc, k.constant_softening, k.gm1, k.inv_gm1, du);
 #pragma unroll
         for (int q = 0; q < NF; ++q)
             u[q] += du[q];
@@ -625,16 +559,19 @@ __global__ void wavespeed_kernel(int ni, int nj, double gamma, const double *pri
 }
 
 __global__ void source_kernel(int ni, int nj, double xl, double yl, double dx, double dy, Mass m1, Mass m2,
-                              int which, int constant_softening, double gamma, const double *prim, double *rate)
+                              int which, int constant_softening, double gm1, double inv_gm1, const double *prim,
+                              double *rate)
 {
     const Mass ms[2] = {m1, m2};
+    const bool massless = m1.mass == 0.0 && m2.mass == 0.0;
     const long n = (long)ni * nj;
     for (long z = blockIdx.x * (long)blockDim.x + threadIdx.x; z < n; z += (long)gridDim.x * blockDim.x) {
         const int i = (int)(z / nj), j = (int)(z % nj);
         const double xc = xl + (i + 0.5) * dx, yc = yl + (j + 0.5) * dy;
         const double *p = prim + at(i, j, nj);
-        const double h = scale_height(ms, xc, yc, p);
-        mass_source(ms[which - 1], xc, yc, 1.0, p, h, constant_softening, gamma, rate + at(i, j, nj));
+        const double T = p[3] / p[0];
+        const double h = massless ? 1.0 : sqrt(T) / root_w2(ms, xc, yc);  // cbdgam_2d.c:75-106
+        mass_source(ms[which - 1], xc, yc, 1.0, p, T, h, constant_softening, gm1, inv_gm1, rate + at(i, j, nj));
     }
 }
 
@@ -687,8 +624,10 @@ __device__ __forceinline__ void diag_rates(const RedArgs &r, const Diag &d, int 
         ms[k].mass = ms[k].mass * gravity;
         ms[k].rate = ms[k].rate * accretion;
     }
-    const double h = scale_height(ms, xc, yc, p);
-    mass_source(ms[which - 1], xc, yc, 1.0, p, h, r.k.constant_softening, r.k.gamma, rate);
+    const double T = p[3] / p[0];
+    const bool massless = ms[0].mass == 0.0 && ms[1].mass == 0.0;
+    const double h = massless ? 1.0 : sqrt(T) / root_w2(ms, xc, yc);  // cbdgam_2d.c:75-106
+    mass_source(ms[which - 1], xc, yc, 1.0, p, T, h, r.k.constant_softening, r.k.gm1, r.k.inv_gm1, rate);
 }
 
 __device__ __forceinline__ void diag_value(const RedArgs &r, const Diag &d, double x, double y, const double *p,
@@ -1008,8 +947,8 @@ int cbdgam_2d_point_mass_source_term(int ni, int nj, double xl, double xr, doubl
     const Mass m2 = mass_args(x2, y2, vx2, vy2, mass2, softening_length2, sink_rate2, sink_radius2, sink_model2);
     source_kernel<<<blocks_for((long)ni * nj, 256), 256, 0,
                     cbd::drop_in_stream()>>>(
-        ni, nj, xl, yl, (xr - xl) / ni, (yr - yl) / nj, m1, m2, which_mass, constant_softening, gamma_law_index,
-        primitive, cons_rate);
+        ni, nj, xl, yl, (xr - xl) / ni, (yr - yl) / nj, m1, m2, which_mass, constant_softening, gamma_law_index - 1.0,
+        1.0 / (gamma_law_index - 1.0), primitive, cons_rate);
     return status_of(cudaGetLastError());
 }
 
