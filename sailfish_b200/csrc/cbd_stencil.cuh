@@ -361,9 +361,12 @@ __device__ __forceinline__ void end_rates(const MassDev *e, int need, double x, 
         rg[q][0] = rg[q][1] = rg[q][2] = 0.0;
         ra[q][0] = ra[q][1] = ra[q][2] = 0.0;
         if (need & (1 << q)) {
+            // the gravity rates only enter sums whose own rounding (their
+            // summation order) is far above an ulp per zone: rsqrt-based
+            // arithmetic, not the correctly rounded power
             MassDev m = e[q];
             m.sink_rate = 0.0;
-            mass_source<FAST>(m, x, y, 1.0, p, rg[q]);
+            mass_source<true>(m, x, y, 1.0, p, rg[q]);
         }
         if (need & (4 << q)) {
             MassDev m = e[q];
