@@ -37,7 +37,7 @@ NCU_TRAFFIC_PER_ZONE_LAUNCH = (108.9e6 + 74.2e6 + 213.7e6 + 69.8e6) / 2 / 2048 *
 # of an RK2 stage 1 and stage 2 launch at 2048^2 (ncu, the sum of
 # smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum over zones;
 # profiles/stage_kernels_2048_fp64.md)
-FP64_INST_PER_ZONE_LAUNCH = (537.2 + 710.8) / 2
+FP64_INST_PER_ZONE_LAUNCH = (537.2 + 670.8) / 2
 GAM_FP64_INST_PER_ZONE_LAUNCH = (1224.8 + 1249.8) / 2
 DIAGNOSTICS = [dict(quantity="time"), dict(quantity="mdot", which_mass=1, accretion=True),
                dict(quantity="mdot", which_mass=2, accretion=True),
