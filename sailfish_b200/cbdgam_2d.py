@@ -212,12 +212,25 @@ class Solver(SolverBase):
 
     def _stage(self, time, a, dt):
         st = _capi.GamStage()
-        m1, m2 = self._physics.point_masses(time)
+        m1, m2 = self._point_masses(time)
         _mass_struct(m1, st.mass[0])
         _mass_struct(m2, st.mass[1])
         st.buffer_central_mass = m1.mass + m2.mass
         st.a, st.dt = a, dt
         return st
+
+    def _point_masses(self, t):
+        """physics.point_masses(t), remembering the last few times (a step
+        starts at the previous step's end)."""
+        cache = self.__dict__.setdefault("_mass_cache", [])
+        for tc, masses in cache:
+            if tc == t:
+                return masses
+        masses = self._physics.point_masses(t)
+        cache.append((t, masses))
+        if len(cache) > 4:
+            cache.pop(0)
+        return masses
 
     def _read(self, n, source=None):
         import torch
@@ -233,7 +246,7 @@ class Solver(SolverBase):
         self._sums; with no diagnostics, the wavespeed maximum into
         self._result."""
         masses = (_capi.Mass * 2)()
-        m1, m2 = self._physics.point_masses(self._time)
+        m1, m2 = self._point_masses(self._time)
         _mass_struct(m1, masses[0])
         _mass_struct(m2, masses[1])
         structs = (_capi.Diag * max(1, len(diags)))()
@@ -297,12 +310,13 @@ class Solver(SolverBase):
         t2 = t0 * 0.5 + (t1 + dt) * (1.0 - 0.5)
         a_buf, b_buf = self._buf
         s1 = self._stage(t0, 0.0, dt)
-        s2 = self._stage(t1, 0.5, dt)
         self._result[:1].zero_()
         self._check(lib.cbdgam_b200_advance_stage(ctypes.byref(g), ctypes.byref(s1), self._ptr(a_buf), None,
                                                   self._ptr(b_buf), None, stream), "advance_stage")
         if self._stage_hook is not None:
             self._stage_hook(0, b_buf)
+        # the second stage's orbit is solved while the first stage runs
+        s2 = self._stage(t1, 0.5, dt)
         self._check(lib.cbdgam_b200_advance_stage(ctypes.byref(g), ctypes.byref(s2), self._ptr(b_buf),
                                                   self._ptr(a_buf), self._ptr(a_buf), self._ptr(self._result),
                                                   stream), "advance_stage")

@@ -268,7 +268,7 @@ class Solver(SolverBase):
 
     def _epilogue(self, time, want_ws, diags):
         ep = _capi.Epilogue()
-        m1, m2 = self._physics.point_masses(time)
+        m1, m2 = self._point_masses(time)
         _mass_struct(m1, ep.mass[0])
         _mass_struct(m2, ep.mass[1])
         ep.want_wavespeed = int(want_ws)
@@ -336,6 +336,10 @@ class Solver(SolverBase):
         return float(self._read_result()[0])
 
     def advance(self, dt):
+        """One step of the configured RK order. The first stage is launched
+        as soon as its record (point masses at the step's start, whose orbit
+        is usually known from the previous step's end) is staged; the later
+        stages' orbits and records are built on the host while it runs."""
         import torch
 
         dt = float(dt)
@@ -352,33 +356,61 @@ class Solver(SolverBase):
             t = time0 * a + (t + dt) * (1.0 - a)
         time_end = t
 
-        epilogue = self._epilogue(time_end, True, self._device_diags if self._fused else [])
         slot = self._ring_next
         self._ring_next = (slot + 1) % len(self._ring)
         if self._ring_events[slot] is not None:
             self._ring_events[slot].synchronize()
         host = self._ring[slot]
-        for s, (a, ts) in enumerate(zip(weights, times)):
+        rb = self._rec_bytes
+        plan = self._stage_plan(len(weights))
+        diags = self._device_diags if self._fused else []
+
+        def record(s, epilogue):
             st = _capi.Stage()
-            m1, m2 = self._physics.point_masses(ts)
+            m1, m2 = self._point_masses(times[s])
             _mass_struct(m1, st.mass[0])
             _mass_struct(m2, st.mass[1])
-            st.a = a
+            st.a = weights[s]
             st.dt = dt
             st.buffer_central_mass = m1.mass + m2.mass
             self._check(lib.cbdiso_b200_stage_record(ctypes.byref(g), ctypes.byref(st), ctypes.byref(epilogue),
-                                                     ctypes.c_void_p(host.data_ptr() + s * self._rec_bytes)),
-                        "stage_record")
-        self._records.copy_(host, non_blocking=True)
+                                                     ctypes.c_void_p(host.data_ptr() + s * rb)), "stage_record")
+
+        first = 0
+        if len(weights) > 1:
+            # the first stage has no epilogue: its record's end-of-step masses
+            # are never read, so any epilogue serves to build it
+            record(0, self._epilogue(times[0], False, []))
+            self._records[:rb].copy_(host[:rb], non_blocking=True)
+            self._launch_stage(0, plan, weights, None, stream)
+            first = 1
+        epilogue = self._epilogue(time_end, True, diags)
+        for s in range(first, len(weights)):
+            record(s, epilogue)
+        self._records[first * rb:].copy_(host[first * rb:], non_blocking=True)
         ev = torch.cuda.Event()
         ev.record()
         self._ring_events[slot] = ev
         self.h2d_bytes += host.numel()
-
-        self._launch_stages(weights, epilogue, stream)
+        for s in range(first, len(weights)):
+            self._launch_stage(s, plan, weights, epilogue if s == len(weights) - 1 else None, stream)
+        self._finish_stages(len(weights), None)
         self._time = time_end
         self._cached = None
         self._result_valid = True
+
+    def _point_masses(self, t):
+        """physics.point_masses(t), remembering the last few times (a step
+        starts at the previous step's end)."""
+        cache = self.__dict__.setdefault("_mass_cache", [])
+        for tc, masses in cache:
+            if tc == t:
+                return masses
+        masses = self._physics.point_masses(t)
+        cache.append((t, masses))
+        if len(cache) > 4:
+            cache.pop(0)
+        return masses
 
     # ------------------------------------------------------------------
     # device-resident stepping
@@ -594,41 +626,51 @@ class Solver(SolverBase):
             out.append(vals + [dt])
         return out
 
-    def _launch_stages(self, weights, epilogue, stream, rk2_buffers=None):
-        """The RK stages of one step, reading the stage records in
-        self._records; the last stage carries the epilogue. Buffers: RK1
-        A -> B (then swapped), RK2 A -> B, B (+A) -> A, RK3 A -> B,
-        B (+A) -> C, C (+A) -> A; or, for RK2, the given (u_n, stage 1
-        output, result)."""
-        lib, g = self._lib, self._grid
+    def _stage_plan(self, nstages, rk2_buffers=None):
+        """(read, u_n source, write) buffers of each RK stage: RK1 A -> B
+        (then swapped), RK2 A -> B, B (+A) -> A, RK3 A -> B, B (+A) -> C,
+        C (+A) -> A; or, for RK2, the given (u_n, stage 1 output, result)."""
         A = self._buf[0]
         B = self._buf[1]
         if rk2_buffers is not None:
             un, mid, out = rk2_buffers
-            plan = [(un, None, mid, None), (mid, un, out, epilogue)]
-        elif len(weights) == 1:
-            plan = [(A, None, B, epilogue)]
-        elif len(weights) == 2:
-            plan = [(A, None, B, None), (B, A, A, epilogue)]
-        else:
-            C = self._buf[2]
-            plan = [(A, None, B, None), (B, A, C, None), (C, A, A, epilogue)]
+            return [(un, None, mid), (mid, un, out)]
+        if nstages == 1:
+            return [(A, None, B)]
+        if nstages == 2:
+            return [(A, None, B), (B, A, A)]
+        C = self._buf[2]
+        return [(A, None, B), (B, A, C), (C, A, A)]
+
+    def _launch_stage(self, s, plan, weights, epilogue, stream):
+        """Stage s of one step, reading its record in self._records; the last
+        stage carries the epilogue."""
+        rd, pn, wr = plan[s]
         dummy = _capi.Stage()
-        for s, (rd, pn, wr, ep) in enumerate(plan):
-            dummy.a = weights[s]
-            rec = ctypes.c_void_p(self._records.data_ptr() + s * self._rec_bytes)
-            status = lib.cbdiso_b200_advance_stage(
-                ctypes.byref(g), ctypes.byref(dummy), rec, self._ptr(rd),
-                self._ptr(pn) if pn is not None else None, self._ptr(wr),
-                ctypes.byref(ep) if ep is not None else None, self._ptr(self._scratch), self._ptr(self._result),
-                stream)
-            self._check(status, "advance_stage")
-            if self._stage_hook is not None:
-                self._stage_hook(s, wr)
-        if len(weights) == 1 and rk2_buffers is None:
-            self._buf[0], self._buf[1] = B, A
+        dummy.a = weights[s]
+        rec = ctypes.c_void_p(self._records.data_ptr() + s * self._rec_bytes)
+        status = self._lib.cbdiso_b200_advance_stage(
+            ctypes.byref(self._grid), ctypes.byref(dummy), rec, self._ptr(rd),
+            self._ptr(pn) if pn is not None else None, self._ptr(wr),
+            ctypes.byref(epilogue) if epilogue is not None else None, self._ptr(self._scratch),
+            self._ptr(self._result), stream)
+        self._check(status, "advance_stage")
+        if self._stage_hook is not None:
+            self._stage_hook(s, wr)
+
+    def _finish_stages(self, nstages, rk2_buffers):
+        if nstages == 1 and rk2_buffers is None:
+            self._buf[0], self._buf[1] = self._buf[1], self._buf[0]
         if self._step_hook is not None:
             self._step_hook()
+
+    def _launch_stages(self, weights, epilogue, stream, rk2_buffers=None):
+        """The RK stages of one step, reading the stage records in
+        self._records; the last stage carries the epilogue."""
+        plan = self._stage_plan(len(weights), rk2_buffers)
+        for s in range(len(weights)):
+            self._launch_stage(s, plan, weights, epilogue if s == len(weights) - 1 else None, stream)
+        self._finish_stages(len(weights), rk2_buffers)
 
     def reset(self, solution, time=0.0):
         """Start again from `solution` (host (ni, nj, 3)) at `time`, keeping
