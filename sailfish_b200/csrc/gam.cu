@@ -319,8 +319,26 @@ __device__ __forceinline__ double max_nan(double a, double b) { return (a > b ||
 // face geometry of the tile.
 __device__ __forceinline__ void stage_phase1(const Consts &k, const Stage &st, StageSmem &sm, int i0, int j0, int tid)
 {
+    // one pool of work items for the whole CTA: the zones of the tile and its
+    // ring, then (with viscosity) the x-faces and the y-faces, so that the
+    // last pass over the pool is the only partly idle one
+    constexpr int NZI = ZI * ZJ, NFX = (TI + 1) * TJ, NFY = TI * (TJ + 1);
+    const bool faces = k.alpha > 0.0 && !st.massless;
+    const int total = NZI + (faces ? NFX + NFY : 0);
     const double theta = k.theta;
-    for (int s = tid; s < ZI * ZJ; s += NT) {
+    for (int s = tid; s < total; s += NT) {
+        if (s >= NZI + NFX) {
+            const int f = s - NZI - NFX, a = f / (TJ + 1), b = f % (TJ + 1);
+            const int i = i0 + a, j = j0 + b;
+            sm.fy[a][b] = root_w2(st.m, k.xl + (i + 0.5) * k.dx, k.yl + (j + 0.0) * k.dy);
+            continue;
+        }
+        if (s >= NZI) {
+            const int f = s - NZI, a = f / TJ, b = f % TJ;
+            const int i = i0 + a, j = j0 + b;
+            sm.fx[a][b] = root_w2(st.m, k.xl + (i + 0.0) * k.dx, k.yl + (j + 0.5) * k.dy);
+            continue;
+        }
         const int a = s / ZJ, b = s % ZJ;
         if (i0 - 1 + a > k.ni || j0 - 1 + b > k.nj)
             continue;  // beyond the guard zones of the last tile: never read
@@ -340,18 +358,6 @@ __device__ __forceinline__ void stage_phase1(const Consts &k, const Stage &st, S
         sm.z[Q_SXX][a][b] = div_by(4.0 / 3.0 * gx[1], k.dx, k.inv_dx) - div_by(2.0 / 3.0 * gy[2], k.dy, k.inv_dy);
         sm.z[Q_SXY][a][b] = div_by(gx[2], k.dx, k.inv_dx) + div_by(gy[1], k.dy, k.inv_dy);
         sm.z[Q_SYY][a][b] = div_by(-2.0 / 3.0 * gx[1], k.dx, k.inv_dx) + div_by(4.0 / 3.0 * gy[2], k.dy, k.inv_dy);
-    }
-    if (k.alpha > 0.0 && !st.massless) {
-        for (int s = tid; s < (TI + 1) * TJ; s += NT) {
-            const int a = s / TJ, b = s % TJ;
-            const int i = i0 + a, j = j0 + b;
-            sm.fx[a][b] = root_w2(st.m, k.xl + (i + 0.0) * k.dx, k.yl + (j + 0.5) * k.dy);
-        }
-        for (int s = tid; s < TI * (TJ + 1); s += NT) {
-            const int a = s / (TJ + 1), b = s % (TJ + 1);
-            const int i = i0 + a, j = j0 + b;
-            sm.fy[a][b] = root_w2(st.m, k.xl + (i + 0.5) * k.dx, k.yl + (j + 0.0) * k.dy);
-        }
     }
 }
 
