@@ -37,7 +37,7 @@ import numpy as np
 from . import _capi, _hostio
 from ._graphs import capture
 from .mesh import is_planar_cartesian_2d
-from .physics import Diagnostic, Physics, enum_value
+from .physics import Diagnostic, MassCache, Physics, enum_value
 from .solver_base import SolverBase
 
 logger = getLogger(__name__)
@@ -400,12 +400,10 @@ class Solver(SolverBase):
         self._result_valid = True
 
     def _point_masses(self, t):
-        """physics.point_masses(t), remembering the last few times (a step
-        starts at the previous step's end)."""
-        cache = self.__dict__.setdefault("_mass_cache", [])
-        for tc, masses in cache:
-            if tc == t:
-                return masses
+        masses = self.__dict__.get("_mass_cache")
+        if masses is None or masses.physics is not self._physics:
+            masses = self._mass_cache = MassCache(self._physics)
+        return masses(t)
         masses = self._physics.point_masses(t)
         cache.append((t, masses))
         if len(cache) > 4:

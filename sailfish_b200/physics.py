@@ -98,3 +98,24 @@ class Physics(NamedTuple):
             if len(masses) == 2:
                 return masses
         raise ValueError("point_mass_function returned an unsupported description of point masses")
+
+
+class MassCache:
+    """physics.point_masses(t) remembered for the last few times t: a solver
+    asks for the same time several times (a step starts at the previous
+    step's end, and the end-of-step reductions use it too)."""
+
+    def __init__(self, physics, size=4):
+        self.physics = physics
+        self.size = size
+        self.entries = []
+
+    def __call__(self, t):
+        for tc, masses in self.entries:
+            if tc == t:
+                return masses
+        masses = self.physics.point_masses(t)
+        self.entries.append((t, masses))
+        if len(self.entries) > self.size:
+            self.entries.pop(0)
+        return masses

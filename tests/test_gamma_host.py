@@ -143,3 +143,22 @@ def test_gamma_capi_argument_checks():
     m9 = [0.0] * 8 + [0]
     assert lib.cbdgam_2d_point_mass_source_term(8, 8, -1.0, 1.0, -1.0, 1.0, *m9, *m9, 3, a, b, 1,
                                                 5.0 / 3.0) == 1
+
+
+def test_mass_cache_calls_the_physics_once_per_time():
+    from sailfish_b200.physics import MassCache, Physics
+
+    calls = []
+
+    def masses(t):
+        calls.append(t)
+        return CircumbinaryDisk().point_masses(t)
+
+    cache = MassCache(Physics(point_mass_function=masses), size=2)
+    a = cache(0.5)
+    assert cache(0.5) is a and calls == [0.5]
+    cache(0.75)
+    cache(1.0)  # 0.5 drops out
+    cache(0.5)
+    assert calls == [0.5, 0.75, 1.0, 0.5]
+    assert tuple(a) == tuple(CircumbinaryDisk().point_masses(0.5))
