@@ -14,10 +14,11 @@
 // thread). The tile's primitives (with a two-zone halo) are staged in shared
 // memory; a first phase computes the per-zone quantities every neighbouring
 // update needs (slopes, p / Sigma, sound speed, strain) and the scale
-// heights' face geometry, a second the zone updates. The reference's face fluxes are not shareable between the two
-// zones of a face (each zone takes the sound speed of the neighbour across
-// the face, cbdgam_2d.c:608-611, and the viscous flux the neighbour's scale
-// height), so each zone computes its four faces, as the reference does.
+// heights' face geometry, a second the zone updates. The reference's face
+// fluxes are not shareable between the two zones of a face (each zone takes
+// the sound speed of the neighbour across the face, cbdgam_2d.c:608-611, and
+// the viscous flux the neighbour's scale height), so each zone computes its
+// four faces, as the reference does.
 #include <cuda_runtime.h>
 
 #include <cmath>
