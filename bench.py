@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--tile", default=None, help="columns,rows,occupancy of the stage kernel (default: library)")
+    p.add_argument("--no-face-cache", action="store_true",
+                   help="recompute the face sound speeds and gravity factors in every stage")
     p.add_argument("--mode", default="auto", choices=["auto", "slab", "replicas"],
                    help="slab: one mesh split into N row slabs (guard rows exchanged over NCCL); replicas: N "
                         "independent runs; auto: slab for N > 1")
@@ -305,7 +307,8 @@ def run_ours(args, rank, world):
     def fresh():
         tile = tuple(int(v) for v in args.tile.split(",")) if args.tile else None
         return make_solver("cbdiso_2d", physics,
-                           dict(rk_order=2, plm_theta=THETA, precision=args.precision, tile=tile),
+                           dict(rk_order=2, plm_theta=THETA, precision=args.precision, tile=tile,
+                                face_cache=not args.no_face_cache),
                            setup=setup, mesh=mesh, solution=prim)
 
     solver = fresh()

@@ -209,6 +209,29 @@ size_t cbdiso_b200_stage_record_bytes(void);
 int cbdiso_b200_stage_record(const cbd_grid_t *grid, const cbd_stage_t *stage, const cbd_epilogue_t *epilogue,
                              void *record);
 
+/* cbdiso_b200_advance_stage with a face cache (no counterpart in the
+ * reference, which recomputes these values in every stage,
+ * cbdiso_2d.c:555-558 and :97-175).
+ *
+ * The face sound speeds and the zones' gravity factors depend only on the mesh,
+ * the EOS constants and the point masses' positions, masses and softenings. A
+ * stage with a != 0 whose masses equal its record's end-of-step masses (the
+ * last RK2 stage, RK3's second; the epilogue's masses on the host path) stores
+ * them in `face_cache`, tagged with a key of everything they depend on; a
+ * stage with a == 0 (the next step's first) whose masses and constants match
+ * that key loads them instead of recomputing them. In EXACT precision the
+ * results are bit-identical to cbdiso_b200_advance_stage (in FMA and FAST the
+ * compiler may contract the two code paths differently: equal to rounding).
+ * `face_cache` is a caller-owned, 16-byte aligned device buffer of
+ * cbdiso_b200_face_cache_bytes(grid) bytes for this grid only; zero its first
+ * 256 bytes before its first use. Calls on one cache must be ordered on one
+ * stream. */
+size_t cbdiso_b200_face_cache_bytes(const cbd_grid_t *grid);
+int cbdiso_b200_advance_stage_cached(
+    const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
+    const double *primitive_rd, const double *primitive_n, double *primitive_wr,
+    const cbd_epilogue_t *epilogue, double *scratch, double *result, double *face_cache, void *stream);
+
 /* cbdiso_b200_advance_stage without a scratch argument (no counterpart in the
  * reference, whose kernels take only the solver's own arrays).
  *

@@ -113,6 +113,8 @@ def _declare(lib):
         "cbdiso_b200_fill_guards": [POINTER(Grid), P, V],
         "cbdiso_b200_advance_stage": [POINTER(Grid), POINTER(Stage), P, P, P, P, POINTER(Epilogue), P, P, V],
         "cbdiso_b200_advance_stage_noalloc": [POINTER(Grid), POINTER(Stage), P, P, P, P, POINTER(Epilogue), P, V],
+        "cbdiso_b200_advance_stage_cached": [POINTER(Grid), POINTER(Stage), P, P, P, P, POINTER(Epilogue), P, P, P,
+                                             V],
         "cbdiso_b200_reduce": [POINTER(Grid), POINTER(Epilogue), P, P, P, V],
     }
     for name, args in sig.items():
@@ -121,6 +123,8 @@ def _declare(lib):
         f.restype = c_int
     lib.cbdiso_b200_scratch_bytes.argtypes = [POINTER(Grid)]
     lib.cbdiso_b200_scratch_bytes.restype = c_size_t
+    lib.cbdiso_b200_face_cache_bytes.argtypes = [POINTER(Grid)]
+    lib.cbdiso_b200_face_cache_bytes.restype = c_size_t
     lib.cbdiso_b200_stage_record_bytes.argtypes = []
     lib.cbdiso_b200_stage_record_bytes.restype = c_size_t
     lib.cbdiso_b200_stage_record.argtypes = [POINTER(Grid), POINTER(Stage), POINTER(Epilogue), c_void_p]
@@ -229,7 +233,8 @@ def exported_symbols():
         "cbdiso_b200_status_string", "cbdiso_b200_version", "cbdiso_b200_scratch_bytes", "cbdiso_b200_fill_guards",
         "cbdiso_b200_advance_stage", "cbdiso_b200_reduce", "cbdiso_b200_abi_sizes",
         "cbdiso_b200_stage_record_bytes", "cbdiso_b200_stage_record", "cbdiso_b200_eval_primitives",
-        "cbdiso_b200_advance_stage_noalloc", "cbdiso_b200_stepper_bytes", "cbdiso_b200_stepper_init",
+        "cbdiso_b200_advance_stage_noalloc", "cbdiso_b200_face_cache_bytes", "cbdiso_b200_advance_stage_cached",
+        "cbdiso_b200_stepper_bytes", "cbdiso_b200_stepper_init",
         "cbdiso_b200_step_prologue", "cbdiso_b200_batch_disk_bytes", "cbdiso_b200_batch_disk_record",
         "cbdiso_b200_batched_stage", "cbdiso_b200_batched_finalize", "cbdiso_b200_batched_prologue",
         "cbdiso_b200_adjoint_workspace_bytes", "cbdiso_b200_stage_record_branches", "cbdiso_b200_stage_tangent",

@@ -20,9 +20,12 @@ only its reduction summation order depends on it.
 
 Extra solver options beyond the reference's (velocity_ceiling, density_floor,
 rk_order): `plm_theta` (default 1.8, the reference's compile-time
-PLM_THETA), `precision` ("exact" | "fma" | "fast"), `fuse_reductions`, and
+PLM_THETA), `precision` ("exact" | "fma" | "fast"), `fuse_reductions`,
 `tile` ((columns, rows[, occupancy]) of the stage kernel's CTA tile, or
-None for the library default).
+None for the library default), and `face_cache` (default True: a step's
+first stage loads the face sound speeds and gravity factors that the previous
+step's last stage computed for the same point masses, instead of recomputing
+them; bit-identical results in EXACT precision).
 """
 
 from __future__ import annotations
@@ -58,6 +61,7 @@ class Options(NamedTuple):
     precision: str = "exact"
     fuse_reductions: bool = True
     tile: Optional[tuple] = None
+    face_cache: bool = True
 
 
 def initial_condition(setup, mesh, time, rows=None):
@@ -230,6 +234,12 @@ class Solver(SolverBase):
                     "fill_guards")
         nscratch = int(self._lib.cbdiso_b200_scratch_bytes(ctypes.byref(g)))
         self._scratch = torch.zeros(nscratch // 8 + 8, **f64)
+        # face sound speeds and gravity factors carried from a step's last
+        # stage to the next step's first (same bits as recomputing them)
+        self._fcache = None
+        if options.face_cache:
+            self._fcache = torch.empty(int(self._lib.cbdiso_b200_face_cache_bytes(ctypes.byref(g))) // 8, **f64)
+            self._fcache[:32].zero_()
         self._result = torch.zeros(1 + 2 * _capi.MAX_DIAG, **f64)
         self._result_host = torch.zeros(1 + 2 * _capi.MAX_DIAG, dtype=torch.float64).pin_memory()
 
@@ -647,11 +657,14 @@ class Solver(SolverBase):
         dummy = _capi.Stage()
         dummy.a = weights[s]
         rec = ctypes.c_void_p(self._records.data_ptr() + s * self._rec_bytes)
-        status = self._lib.cbdiso_b200_advance_stage(
-            ctypes.byref(self._grid), ctypes.byref(dummy), rec, self._ptr(rd),
-            self._ptr(pn) if pn is not None else None, self._ptr(wr),
-            ctypes.byref(epilogue) if epilogue is not None else None, self._ptr(self._scratch),
-            self._ptr(self._result), stream)
+        common = (ctypes.byref(self._grid), ctypes.byref(dummy), rec, self._ptr(rd),
+                  self._ptr(pn) if pn is not None else None, self._ptr(wr),
+                  ctypes.byref(epilogue) if epilogue is not None else None, self._ptr(self._scratch),
+                  self._ptr(self._result))
+        if self._fcache is not None:
+            status = self._lib.cbdiso_b200_advance_stage_cached(*common, self._ptr(self._fcache), stream)
+        else:
+            status = self._lib.cbdiso_b200_advance_stage(*common, stream)
         self._check(status, "advance_stage")
         if self._stage_hook is not None:
             self._stage_hook(s, wr)

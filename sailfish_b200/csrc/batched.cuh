@@ -97,6 +97,7 @@ __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs
         sa.stage_dev = nullptr;
         sa.scratch = nullptr;
         sa.result = nullptr;
+        sa.fcache = nullptr;
         double acc[PARTIAL_STRIDE];
 #pragma unroll
         for (int v = 0; v < PARTIAL_STRIDE; ++v)

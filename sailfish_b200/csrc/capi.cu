@@ -291,7 +291,7 @@ int cbdiso_2d_advance_rk(
 
     const LaunchShape s = stage_shape(ni, nj, 0, 0);
     k.rows_per_cta = s.rows;
-    StageArgs args = {primitive_rd, conserved_rk, primitive_wr, nullptr, nullptr, nullptr};
+    StageArgs args = {primitive_rd, conserved_rk, primitive_wr, nullptr, nullptr, nullptr, nullptr};
     return status_of(dispatch_stage(g_precision, s, k, st, args, g_stream));
 }
 
@@ -390,10 +390,14 @@ int cbdiso_b200_stage_record(const cbd_grid_t *grid, const cbd_stage_t *stage, c
     return CBD_OK;
 }
 
-int cbdiso_b200_advance_stage(
-    const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
-    const double *primitive_rd, const double *primitive_n, double *primitive_wr,
-    const cbd_epilogue_t *epilogue, double *scratch, double *result, void *stream)
+}  // extern "C"
+
+namespace {
+
+int advance_stage(const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
+                  const double *primitive_rd, const double *primitive_n, double *primitive_wr,
+                  const cbd_epilogue_t *epilogue, double *scratch, double *result, double *face_cache,
+                  void *stream)
 {
     if (!valid_grid(grid) || !stage || !primitive_rd || !primitive_wr || primitive_rd == primitive_wr)
         return CBD_ERR_ARGUMENT;
@@ -417,8 +421,40 @@ int cbdiso_b200_advance_stage(
     const LaunchShape s = stage_shape(grid->ni, grid->nj, grid->tile_columns, grid->tile_rows, grid->tile_occupancy);
     k.rows_per_cta = s.rows;
     StageArgs args = {primitive_rd, primitive_n, primitive_wr, static_cast<const StageDev *>(stage_dev), scratch,
-                      result};
+                      result, face_cache};
     return status_of(dispatch_stage(grid->precision, s, k, st, args, static_cast<cudaStream_t>(stream)));
+}
+
+}  // namespace
+
+extern "C" {
+
+int cbdiso_b200_advance_stage(
+    const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
+    const double *primitive_rd, const double *primitive_n, double *primitive_wr,
+    const cbd_epilogue_t *epilogue, double *scratch, double *result, void *stream)
+{
+    return advance_stage(grid, stage, stage_dev, primitive_rd, primitive_n, primitive_wr, epilogue, scratch,
+                         result, nullptr, stream);
+}
+
+size_t cbdiso_b200_face_cache_bytes(const cbd_grid_t *grid)
+{
+    if (!valid_grid(grid))
+        return 0;
+    return face_cache_doubles(grid->ni, grid->nj) * sizeof(double);
+}
+
+int cbdiso_b200_advance_stage_cached(
+    const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
+    const double *primitive_rd, const double *primitive_n, double *primitive_wr,
+    const cbd_epilogue_t *epilogue, double *scratch, double *result, double *face_cache, void *stream)
+{
+    // the cache's pairs are loaded and stored as 16-byte vectors
+    if (!face_cache || (reinterpret_cast<uintptr_t>(face_cache) & 15) != 0)
+        return CBD_ERR_ARGUMENT;
+    return advance_stage(grid, stage, stage_dev, primitive_rd, primitive_n, primitive_wr, epilogue, scratch,
+                         result, face_cache, stream);
 }
 
 int cbdiso_b200_reduce(

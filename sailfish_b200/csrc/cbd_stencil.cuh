@@ -179,8 +179,10 @@ __device__ __forceinline__ double sound_speed2(const Consts &k, const MassDev *m
 }
 
 // HLLE flux across a face with normal DIR (0: x, 1: y), cbdiso_2d.c:352-380
+// cs = sqrt(cs2), passed in so that a face's sound speed can come from the
+// face cache.
 template <bool FAST, int DIR>
-__device__ __forceinline__ void hlle(const double *pl, const double *pr, double cs2, double *f)
+__device__ __forceinline__ void hlle(const double *pl, const double *pr, double cs2, double cs, double *f)
 {
     const double ul0 = pl[0], ul1 = pl[1] * pl[0], ul2 = pl[2] * pl[0];
     const double ur0 = pr[0], ur1 = pr[1] * pr[0], ur2 = pr[2] * pr[0];
@@ -195,7 +197,6 @@ __device__ __forceinline__ void hlle(const double *pl, const double *pr, double 
     const double fl2 = DIR == 1 ? vl * ul2 + gl : vl * ul2;
     const double fr1 = DIR == 0 ? vr * ur1 + gr : vr * ur1;
     const double fr2 = DIR == 1 ? vr * ur2 + gr : vr * ur2;
-    const double cs = sqrt(cs2);
     const double am = lesser(0.0, lesser(vl - cs, vr - cs));
     const double ap = greater(0.0, greater(vl + cs, vr + cs));
     const double den = ap - am;
@@ -249,17 +250,22 @@ __device__ __forceinline__ double fourth_power(double q)
 
 // Gravity and sink terms of one mass, added into du (cbdiso_2d.c:97-175).
 // Terms that are exactly zero (no mass, or a zone outside 4 sink radii) are
-// skipped: adding them changes no value.
+// skipped: adding them changes no value. The gravity factor
+// (r^2 + s^2)^-1.5 is taken from *g_in when given (a face-cache value), and
+// stored to *g_out when given.
 template <bool FAST>
 __device__ __forceinline__ void mass_source(const MassDev &m, double x, double y, double dt, const double *p,
-                                            double *du)
+                                            double *du, const double *g_in = nullptr, double *g_out = nullptr)
 {
     const double sigma = p[0];
     const double dx = x - m.x;
     const double dy = y - m.y;
     const double r2 = dx * dx + dy * dy;
     if (m.mass != 0.0) {
-        const double fnum = sigma * m.mass * inv_pow15<FAST>(r2 + m.soft2);
+        const double g = g_in ? *g_in : inv_pow15<FAST>(r2 + m.soft2);
+        if (g_out)
+            *g_out = g;
+        const double fnum = sigma * m.mass * g;
         const double fx = -fnum * dx;
         const double fy = -fnum * dy;
         du[1] += fx * dt;
@@ -585,22 +591,147 @@ struct StageArgs {
     const StageDev *stage_dev;  // optional device copy of the stage parameters
     double *scratch;     // reductions scratch (epilogue only)
     double *result;      // reductions result (epilogue only)
+    double *fcache;      // optional face cache (face_cache_doubles), null: none
 };
+
+// ---------------------------------------------------------------------------
+// face cache
+//
+// The face sound speeds (cs^2, cs) at every x- and y-face centre and the
+// gravity factors (r^2 + s^2)^-1.5 of both masses at every zone centre depend
+// only on the mesh, the EOS constants and the point masses' positions, masses
+// and softenings, not on the fluid state. The last RK stage of a step usually
+// runs with the masses of the step's end time, which are the next step's
+// first-stage masses: RK2's second stage at t0 + dt, the next step at
+// t0 / 2 + (t0 + 2 dt) / 2, equal in all but about 1 step in 5000. So a
+// stage with a != 0 whose masses equal its record's end-of-step masses
+// computes these values and writes them (with a key of everything they depend
+// on), and a first stage (a == 0) whose key matches reads them instead of
+// recomputing them. The values are the same bits either way. A launch either
+// writes (never reading the key) or may read (never writing anything), so no
+// launch reads what it writes; launches on one cache must be stream-ordered.
+//
+// Layout (doubles): a 32-double header holding the key, then
+//   x-faces (ni + 1) x nj pairs (cs^2, cs): pair [i][j] is the face between
+//     rows i - 1 and i in column j;
+//   y-faces ni x (nj + 1) pairs: [i][j] is the face between columns j - 1 and
+//     j in row i;
+//   zones ni x nj pairs (g_1, g_2).
+// ---------------------------------------------------------------------------
+
+enum { CACHE_NONE = 0, CACHE_WRITE = 1, CACHE_READ = 2 };
+constexpr int CACHE_HEADER = 32;  // doubles
+constexpr int CACHE_KEY = 20;     // doubles of the header in use
+
+__host__ __device__ inline size_t face_cache_doubles(int ni, int nj)
+{
+    return CACHE_HEADER + 2 * ((size_t)(ni + 1) * nj + (size_t)ni * (nj + 1) + (size_t)ni * nj);
+}
+
+// The key: a format tag, the precision, then every input of the cached values.
+template <int PREC>
+__device__ __forceinline__ double cache_key_value(const Consts &k, const MassDev *m, int v)
+{
+    switch (v) {
+    case 0: return 20260101.5;
+    case 1: return (double)PREC;
+    case 2: return (double)k.eos;
+    case 3: return (double)k.ni;
+    case 4: return (double)k.nj;
+    case 5: return k.xl;
+    case 6: return k.yl;
+    case 7: return k.dx;
+    case 8: return k.dy;
+    case 9: return k.cs2;
+    case 10: return k.mach2;
+    case 11: return k.inv_mach2;
+    default: {
+        const MassDev &q = m[(v - 12) >> 2];
+        switch ((v - 12) & 3) {
+        case 0: return q.x;
+        case 1: return q.y;
+        case 2: return q.mass;
+        default: return q.soft2;
+        }
+    }
+    }
+}
+
+__device__ __forceinline__ bool same_bits(double a, double b)
+{
+    return __double_as_longlong(a) == __double_as_longlong(b);
+}
+
+// What this launch does with the cache (the same answer in every thread of
+// every CTA). In a writing launch, `key_writer` (one thread) writes the key.
+template <int PREC>
+__device__ int cache_op(const Consts &k, const StageDev &st, double *fc, bool key_writer)
+{
+    if (!fc)
+        return CACHE_NONE;
+    if (st.a != 0.0) {
+        bool end_masses = true;
+#pragma unroll
+        for (int p = 0; p < 2; ++p)
+            end_masses = end_masses && same_bits(st.m[p].x, st.e[p].x) && same_bits(st.m[p].y, st.e[p].y) &&
+                         same_bits(st.m[p].mass, st.e[p].mass) && same_bits(st.m[p].soft2, st.e[p].soft2);
+        if (!end_masses)
+            return CACHE_NONE;
+        if (key_writer)
+            for (int v = 0; v < CACHE_KEY; ++v)
+                fc[v] = cache_key_value<PREC>(k, st.m, v);
+        return CACHE_WRITE;
+    }
+    for (int v = 0; v < CACHE_KEY; ++v)
+        if (!same_bits(fc[v], cache_key_value<PREC>(k, st.m, v)))
+            return CACHE_NONE;
+    return CACHE_READ;
+}
+
+__device__ __forceinline__ double2 cache_load(const double *p)
+{
+    return __ldcs(reinterpret_cast<const double2 *>(p));
+}
+
+__device__ __forceinline__ void cache_store(double *p, double a, double b)
+{
+    __stcs(reinterpret_cast<double2 *>(p), make_double2(a, b));
+}
+
+// Shared memory of the march, one instance per kernel whichever copies of
+// march_tile it holds.
+template <int BJ>
+struct StageSmem {
+    double sp[4][NQ][BJ + 4];   // primitive rows ring, columns c0-2 .. c0+BJ+1
+    double sgy[2][NQ][BJ + 2];  // y-slopes ring, columns c0-1 .. c0+BJ
+    double srs[2][NQ][BJ + 2];  // rho * strain ring, same columns
+    double sg[NQ][BJ + 1];      // y-face fluxes of the current row
+    double sun[2][NQ][BJ];      // u_n source zones, fetched one row ahead
+};
+
+template <int BJ>
+__device__ __forceinline__ StageSmem<BJ> &stage_smem()
+{
+    __shared__ StageSmem<BJ> m;
+    return m;
+}
 
 // One tile of the march: columns c0 .. c0 + width - 1 (width <= BJ) and rows
 // r0 .. r0 + k.rows_per_cta - 1 of one grid. `st` must live in shared memory
 // and be visible after the first barrier; epilogue values of the updated
-// zones are accumulated into `acc`. All threads of the block must call it.
-template <int BJ, bool FAST>
+// zones are accumulated into `acc`. `COP` (CACHE_*) says what the tile does
+// with args.fcache. All threads of the block must call it.
+template <int BJ, bool FAST, int COP = CACHE_NONE>
 __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, const StageArgs &args, int c0,
                                            int width, int r0, double (&acc)[PARTIAL_STRIDE])
 {
-    constexpr int W4 = BJ + 4;
-    __shared__ double sp[4][NQ][W4];       // primitive rows ring, columns c0-2 .. c0+BJ+1
-    __shared__ double sgy[2][NQ][BJ + 2];  // y-slopes ring, columns c0-1 .. c0+BJ
-    __shared__ double srs[2][NQ][BJ + 2];  // rho * strain ring, same columns
-    __shared__ double sg[NQ][BJ + 1];      // y-face fluxes of the current row
-    __shared__ double sun[2][NQ][BJ];      // u_n source zones, fetched one row ahead
+    constexpr int cop = COP;
+    StageSmem<BJ> &sm = stage_smem<BJ>();
+    auto &sp = sm.sp;
+    auto &sgy = sm.sgy;
+    auto &srs = sm.srs;
+    auto &sg = sm.sg;
+    auto &sun = sm.sun;
 
     const int t = threadIdx.x;
     const int ni = k.ni, nj = k.nj;
@@ -610,6 +741,11 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
     const int j = c0 + t;
     const size_t row_stride = (size_t)(nj + 2 * NG) * NQ;
     const bool viscous = k.nu > 0.0;
+
+    // face-cache arrays (pairs of doubles), used when cop != CACHE_NONE
+    double *const cfx = cop != CACHE_NONE ? args.fcache + CACHE_HEADER : nullptr;
+    double *const cfy = cop != CACHE_NONE ? cfx + 2 * (size_t)(ni + 1) * nj : nullptr;
+    double *const cfz = cop != CACHE_NONE ? cfy + 2 * (size_t)ni * (nj + 1) : nullptr;
 
     auto zone = [&](const double *base, int i, int jj) -> const double * {
         return base + (size_t)(i + NG) * row_stride + (size_t)(jj + NG) * NQ;
@@ -663,6 +799,22 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
         const int s0 = r & 3, s1 = (r + 1) & 3, s2 = (r + 2) & 3;
         const int g1 = (r + 1) & 1, g0 = r & 1;
 
+        // cached face sound speeds and gravity factors of this row, loaded
+        // ahead of the slopes so that their latency overlaps them
+        double2 c_xf = make_double2(0.0, 0.0), c_yf = c_xf, c_ye = c_xf, c_z = c_xf;
+        if (cop == CACHE_READ) {
+            if (r >= r0 - 1 && active)
+                c_xf = cache_load(cfx + 2 * ((size_t)(r + 1) * nj + j));
+            if (r >= r0) {
+                if (active) {
+                    c_yf = cache_load(cfy + 2 * ((size_t)r * (nj + 1) + j));
+                    c_z = cache_load(cfz + 2 * ((size_t)r * nj + j));
+                }
+                if (t == FACE_LANE)
+                    c_ye = cache_load(cfy + 2 * ((size_t)r * (nj + 1) + c0 + W));
+            }
+        }
+
         // (1) slopes and rho * strain at row r + 1: own column, plus the two
         //     halo columns (c0 - 1 and c0 + W) handled by two lanes of one warp.
         double gx1[NQ] = {0.0, 0.0, 0.0}, rs1[NQ] = {0.0, 0.0, 0.0};
@@ -713,10 +865,20 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 pl[q] = fma(0.5, gx0[q], sp[s0][q][kk]);
                 pr[q] = fma(-0.5, gx1[q], sp[s1][q][kk]);
             }
-            const double xf = k.xl + (double)(r + 1) * k.dx;
-            const double yc = k.yl + ((double)j + 0.5) * k.dy;
-            const double cs2 = sound_speed2<FAST>(k, st.m, xf, yc);
-            hlle<FAST, 0>(pl, pr, cs2, f1);
+            double cs2, cs;
+            if (cop == CACHE_READ) {
+                cs2 = c_xf.x;
+                cs = c_xf.y;
+            } else {
+                const double xf = k.xl + (double)(r + 1) * k.dx;
+                const double yc = k.yl + ((double)j + 0.5) * k.dy;
+                cs2 = sound_speed2<FAST>(k, st.m, xf, yc);
+                cs = sqrt(cs2);
+                // face r + 1/2 is stored by the tile below it, except the first
+                if (cop == CACHE_WRITE && (r >= r0 || r0 == 0))
+                    cache_store(cfx + 2 * ((size_t)(r + 1) * nj + j), cs2, cs);
+            }
+            hlle<FAST, 0>(pl, pr, cs2, cs, f1);
             if (viscous) {
                 f1[1] -= k.half_nu * (rs0[0] + rs1[0]);
                 f1[2] -= k.half_nu * (rs0[1] + rs1[1]);
@@ -742,10 +904,20 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                     pl[q] = fma(0.5, sgy[g0][q][fidx], sp[s0][q][fidx + 1]);
                     pr[q] = fma(-0.5, sgy[g0][q][fidx + 1], sp[s0][q][fidx + 2]);
                 }
-                const double xc = k.xl + ((double)r + 0.5) * k.dx;
-                const double yf = k.yl + (double)(c0 + fidx) * k.dy;
-                const double cs2 = sound_speed2<FAST>(k, st.m, xc, yf);
-                hlle<FAST, 1>(pl, pr, cs2, g);
+                double cs2, cs;
+                if (cop == CACHE_READ) {
+                    cs2 = pass == 0 ? c_yf.x : c_ye.x;
+                    cs = pass == 0 ? c_yf.y : c_ye.y;
+                } else {
+                    const double xc = k.xl + ((double)r + 0.5) * k.dx;
+                    const double yf = k.yl + (double)(c0 + fidx) * k.dy;
+                    cs2 = sound_speed2<FAST>(k, st.m, xc, yf);
+                    cs = sqrt(cs2);
+                    // the strip's last face is stored by the next strip, except the last
+                    if (cop == CACHE_WRITE && (pass == 0 || c0 + W == nj))
+                        cache_store(cfy + 2 * ((size_t)r * (nj + 1) + c0 + fidx), cs2, cs);
+                }
+                hlle<FAST, 1>(pl, pr, cs2, cs, g);
                 if (viscous) {
                     g[1] -= k.half_nu * (srs[g0][1][fidx] + srs[g0][1][fidx + 1]);
                     g[2] -= k.half_nu * (srs[g0][2][fidx] + srs[g0][2][fidx + 1]);
@@ -787,8 +959,18 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
             }
             const double dt = st.dt;
             buffer_source<FAST>(k, st, xc, yc, dt, u, du);
-            mass_source<FAST>(st.m[0], xc, yc, dt, pc, du);
-            mass_source<FAST>(st.m[1], xc, yc, dt, pc, du);
+            if (cop == CACHE_READ) {
+                mass_source<FAST>(st.m[0], xc, yc, dt, pc, du, &c_z.x);
+                mass_source<FAST>(st.m[1], xc, yc, dt, pc, du, &c_z.y);
+            } else if (cop == CACHE_WRITE) {
+                double grav1 = 0.0, grav2 = 0.0;
+                mass_source<FAST>(st.m[0], xc, yc, dt, pc, du, nullptr, &grav1);
+                mass_source<FAST>(st.m[1], xc, yc, dt, pc, du, nullptr, &grav2);
+                cache_store(cfz + 2 * ((size_t)r * nj + j), grav1, grav2);
+            } else {
+                mass_source<FAST>(st.m[0], xc, yc, dt, pc, du);
+                mass_source<FAST>(st.m[1], xc, yc, dt, pc, du);
+            }
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
                 const double gn = sg[q][t + 1], gs = sg[q][t];
@@ -844,7 +1026,17 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
 #pragma unroll
     for (int v = 0; v < PARTIAL_STRIDE; ++v)
         acc[v] = 0.0;
-    march_tile<BJ, FAST>(k, st, args, blockIdx.x * BJ, BJ, blockIdx.y * k.rows_per_cta, acc);
+    __syncthreads();
+    // every thread finds the same answer
+    const int cop = cache_op<PREC>(k, st, args.fcache, threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0);
+    // one copy of the march per cache use, each with its own register allocation
+    const int c0 = blockIdx.x * BJ, r0 = blockIdx.y * k.rows_per_cta;
+    if (cop == CACHE_READ)
+        march_tile<BJ, FAST, CACHE_READ>(k, st, args, c0, BJ, r0, acc);
+    else if (cop == CACHE_WRITE)
+        march_tile<BJ, FAST, CACHE_WRITE>(k, st, args, c0, BJ, r0, acc);
+    else
+        march_tile<BJ, FAST, CACHE_NONE>(k, st, args, c0, BJ, r0, acc);
     if (k.want_ws || k.num_diag > 0) {
         double red[PARTIAL_STRIDE];
         block_reduce<BJ>(acc, sred, red);

@@ -1,0 +1,138 @@
+"""
+The face cache (cbdiso_b200_advance_stage_cached): a step's last stage stores
+the face sound speeds and zone gravity factors for its point masses, and the
+next step's first stage loads them when its masses match. In EXACT precision
+states, dts and reductions must be bit-identical to recomputing them in every
+stage.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from cases import load
+from test_gpu_parity import field_error, product_solver
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+CASES = ["cbd_t15_n64", "cbd_t18_48x40_ecc", "kitp_t15_n56_rk1_forcefree", "kitp_t18_n64_rk3_p2",
+         "bondi_t18_64x32", "explosion_t15_n40", "cbd_t18_n48_inactive"]
+
+
+def _host_loop(s, steps):
+    dts, red = [], []
+    for _ in range(steps):
+        dt = s.mesh.min_spacing() / s.maximum_wavespeed() * 0.3
+        s.advance(dt)
+        dts.append(dt)
+        red.append(s.reductions())
+    return dts, red
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_host_loop_bit_identical_with_and_without_cache(name):
+    d = load(name)
+    on = product_solver(d, "exact", face_cache=True)
+    off = product_solver(d, "exact", face_cache=False)
+    assert on._fcache is not None and off._fcache is None
+    a = _host_loop(on, 12)
+    b = _host_loop(off, 12)
+    assert a[0] == b[0]
+    assert a[1] == b[1]
+    assert np.array_equal(on.solution, off.solution)
+
+
+@pytest.mark.parametrize("name", ["cbd_t15_n64", "kitp_t18_n64_rk3_p2", "bondi_t18_64x32"])
+@pytest.mark.parametrize("precision", ["fma", "fast"])
+def test_host_loop_with_and_without_cache_contracted(name, precision):
+    """The FMA and FAST builds let the compiler contract a * b + c freely,
+    and it may contract the kernel's cached and uncached code paths
+    differently: the two agree to rounding, not bit for bit."""
+    d = load(name)
+    on = product_solver(d, precision, face_cache=True)
+    off = product_solver(d, precision, face_cache=False)
+    a = _host_loop(on, 12)
+    b = _host_loop(off, 12)
+    np.testing.assert_allclose(a[0], b[0], rtol=1e-13, atol=0)
+    assert field_error(on.solution, off.solution) <= 1e-13
+
+
+@pytest.mark.parametrize("name", ["cbd_t15_n64", "kitp_t18_n64_rk3_p2", "kitp_t15_n56_rk1_forcefree"])
+def test_device_loop_bit_identical_with_and_without_cache(name):
+    d = load(name)
+    on = product_solver(d, "exact", face_cache=True)
+    off = product_solver(d, "exact", face_cache=False)
+    ra = on.run(20, cfl=0.3, graph=True, steps_per_graph=5)
+    rb = off.run(20, cfl=0.3, graph=True, steps_per_graph=5)
+    assert ra == rb
+    assert np.array_equal(on.solution, off.solution)
+
+
+def _face_values(s, time):
+    """cs^2 at the x-faces (numpy, the reference's operation order) for the
+    locally isothermal EOS, with the point masses at `time`."""
+    g = s._grid
+    ni, nj = g.ni, g.nj
+    dx, dy = (g.xr - g.xl) / ni, (g.yr - g.yl) / nj
+    i = np.arange(ni + 1, dtype=np.float64)[:, None]
+    j = np.arange(nj, dtype=np.float64)[None, :]
+    x = g.xl + i * dx
+    y = g.yl + (j + 0.5) * dy
+    phi = np.zeros((ni + 1, nj))
+    for m in s._point_masses(time):
+        if m.mass > 0.0:
+            dxm, dym = x - m.position_x, y - m.position_y
+            r2 = dxm * dxm + dym * dym
+            phi -= m.mass / np.sqrt(r2 + m.softening_length * m.softening_length)
+    return -phi / g.mach2
+
+
+def test_cache_holds_the_end_of_step_face_sound_speeds():
+    d = load("cbd_t15_n64")
+    s = product_solver(d, "exact", face_cache=True)
+    s.advance(s.mesh.min_spacing() / s.maximum_wavespeed() * 0.3)
+    torch.cuda.synchronize()
+    c = s._fcache.cpu().numpy()
+    assert c[0] == 20260101.5  # the key's format tag: the last stage stored its values
+    g = s._grid
+    ni, nj = g.ni, g.nj
+    pairs = c[32:32 + 2 * (ni + 1) * nj].reshape(ni + 1, nj, 2)
+    want = _face_values(s, s.time)
+    assert np.array_equal(pairs[..., 0], want)
+    assert np.array_equal(pairs[..., 1], np.sqrt(want))
+
+
+def test_cache_after_reset():
+    d = load("cbd_t18_48x40_ecc")
+    on = product_solver(d, "exact", face_cache=True)
+    off = product_solver(d, "exact", face_cache=False)
+    start, t0 = on.solution.copy(), on.time
+    # back to an earlier time: the cached key no longer matches
+    _host_loop(on, 5)
+    on.reset(start, t0)
+    assert _host_loop(on, 6) == _host_loop(off, 6)
+    assert np.array_equal(on.solution, off.solution)
+    # another state at the cached time: the key matches, the values still apply
+    t1 = on.time
+    on.reset(start, t1)
+    off.reset(start, t1)
+    assert _host_loop(on, 4) == _host_loop(off, 4)
+    assert np.array_equal(on.solution, off.solution)
+
+
+def test_cached_entry_rejects_a_misaligned_cache():
+    from sailfish_b200 import _capi
+
+    d = load("cbd_t15_n64")
+    s = product_solver(d, "exact", face_cache=True)
+    st = _capi.Stage()
+    status = s._lib.cbdiso_b200_advance_stage_cached(
+        ctypes.byref(s._grid), ctypes.byref(st), None, s._ptr(s._buf[0]), None, s._ptr(s._buf[1]), None,
+        None, None, ctypes.c_void_p(s._fcache.data_ptr() + 8), s._stream())
+    assert status == 1  # invalid argument
+    assert int(s._lib.cbdiso_b200_face_cache_bytes(ctypes.byref(s._grid))) == \
+        8 * (32 + 2 * (65 * 64 + 64 * 65 + 64 * 64))
