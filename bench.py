@@ -30,14 +30,15 @@ sys.path.insert(0, ROOT)
 
 BYTES_PER_ZONE_UPDATE = 120.0  # RK2 x FP64 x 3 fields: 48 B stage 1 + 72 B stage 2
 # DRAM bytes per zone and stage launch measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum, mean of an RK2 stage 1 and stage 2 launch at 2048^2,
-# profiles/stage_kernel_2048_exact_full.md); scaled by the zone count.
-NCU_TRAFFIC_PER_ZONE_LAUNCH = (108.9e6 + 74.2e6 + 213.7e6 + 69.8e6) / 2 / 2048 ** 2
+# dram__bytes_write.sum, mean of an RK2 stage 1 launch reading the face cache
+# and a stage 2 launch writing it, at 2048^2,
+# profiles/stage_kernels_2048_face_cache.md); scaled by the zone count. It is
+# above the algorithmic 60 B because of the cache's 48 B per zone and step.
+NCU_TRAFFIC_PER_ZONE_LAUNCH = (313.02e6 + 75.39e6 + 224.86e6 + 273.31e6) / 2 / 2048 ** 2
 # FP64 thread-instructions (DADD + DMUL + DFMA) per zone and stage launch, mean
-# of an RK2 stage 1 and stage 2 launch at 2048^2 (ncu, the sum of
-# smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum over zones;
-# profiles/stage_kernels_2048_fp64.md)
-FP64_INST_PER_ZONE_LAUNCH = (537.2 + 670.8) / 2
+# of the same two launches (ncu, the sum of
+# smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum over zones)
+FP64_INST_PER_ZONE_LAUNCH = (346.9 + 673.0) / 2
 GAM_FP64_INST_PER_ZONE_LAUNCH = (1224.8 + 1249.8) / 2
 DIAGNOSTICS = [dict(quantity="time"), dict(quantity="mdot", which_mass=1, accretion=True),
                dict(quantity="mdot", which_mass=2, accretion=True),
@@ -382,6 +383,7 @@ def run_ours(args, rank, world):
                                "per-step mdot/torque reductions", "zones": zones, "precision": args.precision,
                    "timed": "Solver.run: device-side dt / Kepler, CUDA graph of 16-step groups",
                    "l2": "state arrays (403 MB each at 4096^2) exceed L2; no flush",
+                   "face_cache": not args.no_face_cache,
                    "parallelism": "replicas" if world > 1 else "single"},
         "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": int(e2e_h2d),
                 "d2h_bytes_per_step": int(e2e_d2h), "steps": e2e_steps,
