@@ -214,23 +214,27 @@ int cbdiso_b200_stage_record(const cbd_grid_t *grid, const cbd_stage_t *stage, c
  * cbdiso_2d.c:555-558 and :97-175).
  *
  * The face sound speeds and the zones' gravity factors depend only on the mesh,
- * the EOS constants and the point masses' positions, masses and softenings. A
- * stage with a != 0 whose masses equal its record's end-of-step masses (the
- * last RK2 stage, RK3's second; the epilogue's masses on the host path) stores
- * them in `face_cache`, tagged with a key of everything they depend on; a
- * stage with a == 0 (the next step's first) whose masses and constants match
- * that key loads them instead of recomputing them. In EXACT precision the
- * results are bit-identical to cbdiso_b200_advance_stage (in FMA and FAST the
- * compiler may contract the two code paths differently: equal to rounding).
- * `face_cache` is a caller-owned, 16-byte aligned device buffer of
- * cbdiso_b200_face_cache_bytes(grid) bytes for this grid only; zero its first
- * 256 bytes before its first use. Calls on one cache must be ordered on one
- * stream. */
+ * the EOS constants and the point masses' positions, masses and softenings, so
+ * a step's first stage can reuse what the previous step's last stage computed
+ * for the same masses. `role`:
+ *   0  no cache use (as cbdiso_b200_advance_stage);
+ *   1  writer (RK2's second stage, RK3's second): when the stage's masses equal
+ *      its record's end-of-step masses, also stores the values in `face_cache`
+ *      with a key of everything they depend on;
+ *   2  reader (a step's first stage): loads the values; a fill pass before the
+ *      stage recomputes them when the key does not match the stage's masses.
+ * In EXACT precision the results are bit-identical to
+ * cbdiso_b200_advance_stage (in FMA and FAST the compiler may contract the code
+ * paths differently: equal to rounding). `face_cache` is a caller-owned,
+ * 16-byte aligned device buffer of cbdiso_b200_face_cache_bytes(grid) bytes for
+ * this grid only; zero its first 256 bytes before its first use. Calls on one
+ * cache must be ordered on one stream. */
 size_t cbdiso_b200_face_cache_bytes(const cbd_grid_t *grid);
 int cbdiso_b200_advance_stage_cached(
     const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
     const double *primitive_rd, const double *primitive_n, double *primitive_wr,
-    const cbd_epilogue_t *epilogue, double *scratch, double *result, double *face_cache, void *stream);
+    const cbd_epilogue_t *epilogue, double *scratch, double *result, double *face_cache, int role,
+    void *stream);
 
 /* cbdiso_b200_advance_stage without a scratch argument (no counterpart in the
  * reference, whose kernels take only the solver's own arrays).
@@ -321,20 +325,6 @@ int cbdiso_b200_batched_stage(const void *disks, int num_disks, int total_units,
                               const double *primitive_n, double *primitive_wr, const void *records, int num_stages,
                               int stage, int epilogue, double *partials, unsigned int *counters, int precision,
                               void *stream);
-
-/* cbdiso_b200_batched_stage with face caches (see
- * cbdiso_b200_advance_stage_cached): disk d's cache lies at
- * face_cache + its record's cache offset, set by
- * cbdiso_b200_batch_disk_set_face_cache (an even number of doubles; records
- * without one run uncached). Each disk's cache holds
- * cbdiso_b200_face_cache_bytes(its grid) bytes with its first 256 bytes
- * zeroed before the first use; `face_cache` is 16-byte aligned. No
- * counterpart in the reference. */
-int cbdiso_b200_batch_disk_set_face_cache(void *record, long long cache_offset);
-int cbdiso_b200_batched_stage_cached(const void *disks, int num_disks, int total_units, const double *primitive_rd,
-                                     const double *primitive_n, double *primitive_wr, const void *records,
-                                     int num_stages, int stage, int epilogue, double *partials,
-                                     unsigned int *counters, int precision, double *face_cache, void *stream);
 
 /* Per-disk reduction of the tile partials, in tile order: results[d * stride]
  * = max wavespeed, then the diagnostic sums. */

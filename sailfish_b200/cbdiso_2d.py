@@ -661,13 +661,24 @@ class Solver(SolverBase):
                   self._ptr(pn) if pn is not None else None, self._ptr(wr),
                   ctypes.byref(epilogue) if epilogue is not None else None, self._ptr(self._scratch),
                   self._ptr(self._result))
-        if self._fcache is not None:
-            status = self._lib.cbdiso_b200_advance_stage_cached(*common, self._ptr(self._fcache), stream)
+        role = self._cache_role(s, len(weights))
+        if role:
+            status = self._lib.cbdiso_b200_advance_stage_cached(*common, self._ptr(self._fcache), role, stream)
         else:
             status = self._lib.cbdiso_b200_advance_stage(*common, stream)
         self._check(status, "advance_stage")
         if self._stage_hook is not None:
             self._stage_hook(s, wr)
+
+    def _cache_role(self, s, nstages):
+        """Face-cache role of stage s of a step (0 none, 1 writer, 2 reader):
+        the stage at t0 + dt (RK2's and RK3's second) writes, the next step's
+        first stage reads; RK1 has no stage at t0 + dt."""
+        if self._fcache is None or nstages == 1:
+            return 0
+        if s == 0:
+            return 2
+        return 1 if s == 1 else 0
 
     def _finish_stages(self, nstages, rk2_buffers):
         if nstages == 1 and rk2_buffers is None:

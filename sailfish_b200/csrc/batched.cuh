@@ -18,7 +18,6 @@ struct DiskDev {
     int strips;
     int segments;
     int unit_begin;      // index of the disk's first tile in the batch's tile list
-    long long cache_offset;  // offset of the disk's face cache in BatchArgs::fcache, in doubles; -1: none
 };
 
 struct BatchArgs {
@@ -35,7 +34,6 @@ struct BatchArgs {
     int _pad;
     double *partials;    // [total_units][PARTIAL_STRIDE]
     unsigned int *counters;  // [0] next tile, [1] CTAs finished; both return to zero at the end
-    double *fcache;      // face-cache arena (disk d's cache at disks[d].cache_offset), or null
 };
 
 template <int BJ, int MINB, int PREC>
@@ -99,20 +97,12 @@ __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs
         sa.stage_dev = nullptr;
         sa.scratch = nullptr;
         sa.result = nullptr;
-        sa.fcache = (a.fcache && D.cache_offset >= 0) ? a.fcache + D.cache_offset : nullptr;
-        // the same answer in every thread; the disk's first tile writes the key
-        const int cop = cache_op<PREC>(k, st, sa.fcache, t == 0 && u == D.unit_begin);
+        sa.fcache = nullptr;
         double acc[PARTIAL_STRIDE];
 #pragma unroll
         for (int v = 0; v < PARTIAL_STRIDE; ++v)
             acc[v] = 0.0;
-        const int c0 = strip * D.strip_width, r0 = seg * k.rows_per_cta;
-        if (cop == CACHE_READ)
-            march_tile<BJ, FAST, CACHE_READ>(k, st, sa, c0, D.strip_width, r0, acc);
-        else if (cop == CACHE_WRITE)
-            march_tile<BJ, FAST, CACHE_WRITE>(k, st, sa, c0, D.strip_width, r0, acc);
-        else
-            march_tile<BJ, FAST, CACHE_NONE>(k, st, sa, c0, D.strip_width, r0, acc);
+        march_tile<BJ, FAST>(k, st, sa, strip * D.strip_width, D.strip_width, seg * k.rows_per_cta, acc);
         if (a.epilogue) {
             double red[PARTIAL_STRIDE];
             block_reduce<BJ>(acc, sred, red);

@@ -128,15 +128,15 @@ LaunchShape stage_shape(int ni, int nj, int bj, int rows, int occupancy = 0)
 }
 
 cudaError_t dispatch_stage(int precision, const LaunchShape &s, const Consts &k, const StageDev &st,
-                           const StageArgs &a, cudaStream_t stream)
+                           const StageArgs &a, cudaStream_t stream, int role = ROLE_NONE)
 {
     switch (precision) {
     case CBD_PRECISION_EXACT:
-        return launch_stage_exact(s, k, st, a, stream);
+        return launch_stage_exact(s, k, st, a, role, stream);
     case CBD_PRECISION_FMA:
-        return launch_stage_fma(s, k, st, a, stream);
+        return launch_stage_fma(s, k, st, a, role, stream);
     default:
-        return launch_stage_fast(s, k, st, a, stream);
+        return launch_stage_fast(s, k, st, a, role, stream);
     }
 }
 
@@ -397,7 +397,7 @@ namespace {
 int advance_stage(const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
                   const double *primitive_rd, const double *primitive_n, double *primitive_wr,
                   const cbd_epilogue_t *epilogue, double *scratch, double *result, double *face_cache,
-                  void *stream)
+                  int role, void *stream)
 {
     if (!valid_grid(grid) || !stage || !primitive_rd || !primitive_wr || primitive_rd == primitive_wr)
         return CBD_ERR_ARGUMENT;
@@ -422,7 +422,7 @@ int advance_stage(const cbd_grid_t *grid, const cbd_stage_t *stage, const void *
     k.rows_per_cta = s.rows;
     StageArgs args = {primitive_rd, primitive_n, primitive_wr, static_cast<const StageDev *>(stage_dev), scratch,
                       result, face_cache};
-    return status_of(dispatch_stage(grid->precision, s, k, st, args, static_cast<cudaStream_t>(stream)));
+    return status_of(dispatch_stage(grid->precision, s, k, st, args, static_cast<cudaStream_t>(stream), role));
 }
 
 }  // namespace
@@ -435,7 +435,7 @@ int cbdiso_b200_advance_stage(
     const cbd_epilogue_t *epilogue, double *scratch, double *result, void *stream)
 {
     return advance_stage(grid, stage, stage_dev, primitive_rd, primitive_n, primitive_wr, epilogue, scratch,
-                         result, nullptr, stream);
+                         result, nullptr, ROLE_NONE, stream);
 }
 
 size_t cbdiso_b200_face_cache_bytes(const cbd_grid_t *grid)
@@ -448,13 +448,14 @@ size_t cbdiso_b200_face_cache_bytes(const cbd_grid_t *grid)
 int cbdiso_b200_advance_stage_cached(
     const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
     const double *primitive_rd, const double *primitive_n, double *primitive_wr,
-    const cbd_epilogue_t *epilogue, double *scratch, double *result, double *face_cache, void *stream)
+    const cbd_epilogue_t *epilogue, double *scratch, double *result, double *face_cache, int role, void *stream)
 {
     // the cache's pairs are loaded and stored as 16-byte vectors
-    if (!face_cache || (reinterpret_cast<uintptr_t>(face_cache) & 15) != 0)
+    if (!face_cache || (reinterpret_cast<uintptr_t>(face_cache) & 15) != 0 || role < ROLE_NONE ||
+        role > ROLE_READER)
         return CBD_ERR_ARGUMENT;
     return advance_stage(grid, stage, stage_dev, primitive_rd, primitive_n, primitive_wr, epilogue, scratch,
-                         result, face_cache, stream);
+                         result, face_cache, role, stream);
 }
 
 int cbdiso_b200_reduce(

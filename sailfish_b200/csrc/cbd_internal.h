@@ -14,11 +14,11 @@ struct LaunchShape {
 };
 
 cudaError_t launch_stage_exact(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a,
-                               cudaStream_t stream);
+                               int role, cudaStream_t stream);
 cudaError_t launch_stage_fma(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a,
-                             cudaStream_t stream);
+                             int role, cudaStream_t stream);
 cudaError_t launch_stage_fast(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a,
-                              cudaStream_t stream);
+                              int role, cudaStream_t stream);
 
 // Kernel constants of a grid (mesh, EOS, options, buffer), with host-side
 // reciprocals of the constant divisors; and the diagnostics of an epilogue

@@ -179,10 +179,10 @@ __device__ __forceinline__ double sound_speed2(const Consts &k, const MassDev *m
 }
 
 // HLLE flux across a face with normal DIR (0: x, 1: y), cbdiso_2d.c:352-380
-// cs = sqrt(cs2), passed in so that a face's sound speed can come from the
-// face cache.
-template <bool FAST, int DIR>
-__device__ __forceinline__ void hlle(const double *pl, const double *pr, double cs2, double cs, double *f)
+// cs = sqrt(cs2): computed here, or with CS_GIVEN taken from the caller (a
+// face-cache value); the caller receives it either way.
+template <bool FAST, int DIR, bool CS_GIVEN = false>
+__device__ __forceinline__ void hlle(const double *pl, const double *pr, double cs2, double &cs, double *f)
 {
     const double ul0 = pl[0], ul1 = pl[1] * pl[0], ul2 = pl[2] * pl[0];
     const double ur0 = pr[0], ur1 = pr[1] * pr[0], ur2 = pr[2] * pr[0];
@@ -197,6 +197,8 @@ __device__ __forceinline__ void hlle(const double *pl, const double *pr, double 
     const double fl2 = DIR == 1 ? vl * ul2 + gl : vl * ul2;
     const double fr1 = DIR == 0 ? vr * ur1 + gr : vr * ur1;
     const double fr2 = DIR == 1 ? vr * ur2 + gr : vr * ur2;
+    if (!CS_GIVEN)
+        cs = sqrt(cs2);
     const double am = lesser(0.0, lesser(vl - cs, vr - cs));
     const double ap = greater(0.0, greater(vl + cs, vr + cs));
     const double den = ap - am;
@@ -603,13 +605,18 @@ struct StageArgs {
 // and softenings, not on the fluid state. The last RK stage of a step usually
 // runs with the masses of the step's end time, which are the next step's
 // first-stage masses: RK2's second stage at t0 + dt, the next step at
-// t0 / 2 + (t0 + 2 dt) / 2, equal in all but about 1 step in 5000. So a
-// stage with a != 0 whose masses equal its record's end-of-step masses
-// computes these values and writes them (with a key of everything they depend
-// on), and a first stage (a == 0) whose key matches reads them instead of
-// recomputing them. The values are the same bits either way. A launch either
-// writes (never reading the key) or may read (never writing anything), so no
-// launch reads what it writes; launches on one cache must be stream-ordered.
+// t0 / 2 + (t0 + 2 dt) / 2, equal in all but about 1 step in 5000. The host
+// gives each stage launch a role:
+//  * ROLE_WRITER (RK2's second stage, RK3's second): computes the values as
+//    usual and, when its masses equal its record's end-of-step masses, also
+//    stores them with a key of everything they depend on;
+//  * ROLE_READER (a step's first stage): loads them. A fill kernel runs
+//    before it: when the key does not match the reader's masses it marks the
+//    key invalid and computes the values for those masses.
+//  * ROLE_NONE: neither.
+// The values are the same bits as recomputing them. Each role is its own
+// kernel, so that each keeps its own register allocation. Launches on one
+// cache must be stream-ordered.
 //
 // Layout (doubles): a 32-double header holding the key, then
 //   x-faces (ni + 1) x nj pairs (cs^2, cs): pair [i][j] is the face between
@@ -619,6 +626,7 @@ struct StageArgs {
 //   zones ni x nj pairs (g_1, g_2).
 // ---------------------------------------------------------------------------
 
+enum { ROLE_NONE = 0, ROLE_WRITER = 1, ROLE_READER = 2 };
 enum { CACHE_NONE = 0, CACHE_WRITE = 1, CACHE_READ = 2 };
 constexpr int CACHE_HEADER = 32;  // doubles
 constexpr int CACHE_KEY = 20;     // doubles of the header in use
@@ -662,30 +670,29 @@ __device__ __forceinline__ bool same_bits(double a, double b)
     return __double_as_longlong(a) == __double_as_longlong(b);
 }
 
-// What this launch does with the cache (the same answer in every thread of
-// every CTA). In a writing launch, `key_writer` (one thread) writes the key.
 template <int PREC>
-__device__ int cache_op(const Consts &k, const StageDev &st, double *fc, bool key_writer)
+__device__ bool cache_key_matches(const Consts &k, const StageDev &st, const double *fc)
 {
-    if (!fc)
-        return CACHE_NONE;
-    if (st.a != 0.0) {
-        bool end_masses = true;
-#pragma unroll
-        for (int p = 0; p < 2; ++p)
-            end_masses = end_masses && same_bits(st.m[p].x, st.e[p].x) && same_bits(st.m[p].y, st.e[p].y) &&
-                         same_bits(st.m[p].mass, st.e[p].mass) && same_bits(st.m[p].soft2, st.e[p].soft2);
-        if (!end_masses)
-            return CACHE_NONE;
-        if (key_writer)
-            for (int v = 0; v < CACHE_KEY; ++v)
-                fc[v] = cache_key_value<PREC>(k, st.m, v);
-        return CACHE_WRITE;
-    }
     for (int v = 0; v < CACHE_KEY; ++v)
         if (!same_bits(fc[v], cache_key_value<PREC>(k, st.m, v)))
-            return CACHE_NONE;
-    return CACHE_READ;
+            return false;
+    return true;
+}
+
+// A writer stores the values when its masses are the end-of-step masses (the
+// same answer in every thread); `key_writer` (one thread) then writes the key.
+template <int PREC>
+__device__ bool cache_write_check(const Consts &k, const StageDev &st, double *fc, bool key_writer)
+{
+    bool end_masses = true;
+#pragma unroll
+    for (int p = 0; p < 2; ++p)
+        end_masses = end_masses && same_bits(st.m[p].x, st.e[p].x) && same_bits(st.m[p].y, st.e[p].y) &&
+                     same_bits(st.m[p].mass, st.e[p].mass) && same_bits(st.m[p].soft2, st.e[p].soft2);
+    if (end_masses && key_writer)
+        for (int v = 0; v < CACHE_KEY; ++v)
+            fc[v] = cache_key_value<PREC>(k, st.m, v);
+    return end_masses;
 }
 
 __device__ __forceinline__ double2 cache_load(const double *p)
@@ -720,10 +727,11 @@ __device__ __forceinline__ StageSmem<BJ> &stage_smem()
 // r0 .. r0 + k.rows_per_cta - 1 of one grid. `st` must live in shared memory
 // and be visible after the first barrier; epilogue values of the updated
 // zones are accumulated into `acc`. `COP` (CACHE_*) says what the tile does
-// with args.fcache. All threads of the block must call it.
+// with args.fcache; with CACHE_WRITE it stores only if `store`. All threads of
+// the block must call it.
 template <int BJ, bool FAST, int COP = CACHE_NONE>
 __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, const StageArgs &args, int c0,
-                                           int width, int r0, double (&acc)[PARTIAL_STRIDE])
+                                           int width, int r0, double (&acc)[PARTIAL_STRIDE], bool store = false)
 {
     constexpr int cop = COP;
     StageSmem<BJ> &sm = stage_smem<BJ>();
@@ -865,20 +873,19 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 pl[q] = fma(0.5, gx0[q], sp[s0][q][kk]);
                 pr[q] = fma(-0.5, gx1[q], sp[s1][q][kk]);
             }
-            double cs2, cs;
             if (cop == CACHE_READ) {
-                cs2 = c_xf.x;
-                cs = c_xf.y;
+                double cs = c_xf.y;
+                hlle<FAST, 0, true>(pl, pr, c_xf.x, cs, f1);
             } else {
                 const double xf = k.xl + (double)(r + 1) * k.dx;
                 const double yc = k.yl + ((double)j + 0.5) * k.dy;
-                cs2 = sound_speed2<FAST>(k, st.m, xf, yc);
-                cs = sqrt(cs2);
+                const double cs2 = sound_speed2<FAST>(k, st.m, xf, yc);
+                double cs;
+                hlle<FAST, 0>(pl, pr, cs2, cs, f1);
                 // face r + 1/2 is stored by the tile below it, except the first
-                if (cop == CACHE_WRITE && (r >= r0 || r0 == 0))
+                if (cop == CACHE_WRITE && store && (r >= r0 || r0 == 0))
                     cache_store(cfx + 2 * ((size_t)(r + 1) * nj + j), cs2, cs);
             }
-            hlle<FAST, 0>(pl, pr, cs2, cs, f1);
             if (viscous) {
                 f1[1] -= k.half_nu * (rs0[0] + rs1[0]);
                 f1[2] -= k.half_nu * (rs0[1] + rs1[1]);
@@ -904,20 +911,19 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                     pl[q] = fma(0.5, sgy[g0][q][fidx], sp[s0][q][fidx + 1]);
                     pr[q] = fma(-0.5, sgy[g0][q][fidx + 1], sp[s0][q][fidx + 2]);
                 }
-                double cs2, cs;
                 if (cop == CACHE_READ) {
-                    cs2 = pass == 0 ? c_yf.x : c_ye.x;
-                    cs = pass == 0 ? c_yf.y : c_ye.y;
+                    double cs = pass == 0 ? c_yf.y : c_ye.y;
+                    hlle<FAST, 1, true>(pl, pr, pass == 0 ? c_yf.x : c_ye.x, cs, g);
                 } else {
                     const double xc = k.xl + ((double)r + 0.5) * k.dx;
                     const double yf = k.yl + (double)(c0 + fidx) * k.dy;
-                    cs2 = sound_speed2<FAST>(k, st.m, xc, yf);
-                    cs = sqrt(cs2);
+                    const double cs2 = sound_speed2<FAST>(k, st.m, xc, yf);
+                    double cs;
+                    hlle<FAST, 1>(pl, pr, cs2, cs, g);
                     // the strip's last face is stored by the next strip, except the last
-                    if (cop == CACHE_WRITE && (pass == 0 || c0 + W == nj))
+                    if (cop == CACHE_WRITE && store && (pass == 0 || c0 + W == nj))
                         cache_store(cfy + 2 * ((size_t)r * (nj + 1) + c0 + fidx), cs2, cs);
                 }
-                hlle<FAST, 1>(pl, pr, cs2, cs, g);
                 if (viscous) {
                     g[1] -= k.half_nu * (srs[g0][1][fidx] + srs[g0][1][fidx + 1]);
                     g[2] -= k.half_nu * (srs[g0][2][fidx] + srs[g0][2][fidx + 1]);
@@ -966,7 +972,8 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 double grav1 = 0.0, grav2 = 0.0;
                 mass_source<FAST>(st.m[0], xc, yc, dt, pc, du, nullptr, &grav1);
                 mass_source<FAST>(st.m[1], xc, yc, dt, pc, du, nullptr, &grav2);
-                cache_store(cfz + 2 * ((size_t)r * nj + j), grav1, grav2);
+                if (store)
+                    cache_store(cfz + 2 * ((size_t)r * nj + j), grav1, grav2);
             } else {
                 mass_source<FAST>(st.m[0], xc, yc, dt, pc, du);
                 mass_source<FAST>(st.m[1], xc, yc, dt, pc, du);
@@ -1013,8 +1020,9 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
     __syncthreads();
 }
 
-// One RK stage on one grid: CTA (x, y) marches strip x, segment y.
-template <int BJ, int MINB, int PREC>
+// One RK stage on one grid: CTA (x, y) marches strip x, segment y. ROLE
+// (ROLE_*) is what the launch does with args.fcache.
+template <int BJ, int MINB, int PREC, int ROLE = ROLE_NONE>
 __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const StageDev st_param, StageArgs args)
 {
     constexpr bool FAST = PREC == CBD_PRECISION_FAST;
@@ -1026,22 +1034,80 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
 #pragma unroll
     for (int v = 0; v < PARTIAL_STRIDE; ++v)
         acc[v] = 0.0;
-    __syncthreads();
-    // every thread finds the same answer
-    const int cop = cache_op<PREC>(k, st, args.fcache, threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0);
-    // one copy of the march per cache use, each with its own register allocation
     const int c0 = blockIdx.x * BJ, r0 = blockIdx.y * k.rows_per_cta;
-    if (cop == CACHE_READ)
+    if (ROLE == ROLE_WRITER) {
+        __syncthreads();
+        const bool store = cache_write_check<PREC>(k, st, args.fcache,
+                                                   threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0);
+        march_tile<BJ, FAST, CACHE_WRITE>(k, st, args, c0, BJ, r0, acc, store);
+    } else if (ROLE == ROLE_READER) {
         march_tile<BJ, FAST, CACHE_READ>(k, st, args, c0, BJ, r0, acc);
-    else if (cop == CACHE_WRITE)
-        march_tile<BJ, FAST, CACHE_WRITE>(k, st, args, c0, BJ, r0, acc);
-    else
+    } else {
         march_tile<BJ, FAST, CACHE_NONE>(k, st, args, c0, BJ, r0, acc);
+    }
     if (k.want_ws || k.num_diag > 0) {
         double red[PARTIAL_STRIDE];
         block_reduce<BJ>(acc, sred, red);
         grid_finish<BJ>(red, 1 + 2 * k.num_diag, args.scratch, k.want_ws ? args.result : nullptr, args.result + 1,
                         sred);
+    }
+}
+
+// Makes the face cache valid for a reader stage: when the key does not match
+// the stage's masses, marks it invalid (no later key check passes on what
+// follows) and computes every face's (cs^2, cs) and every zone's gravity
+// factors for those masses, with the stage kernel's own expressions. Grid:
+// any number of 128-thread CTAs, each taking rows i = blockIdx.x, ... .
+template <int PREC>
+__global__ void __launch_bounds__(128) face_cache_fill_kernel(const Consts k, const StageDev st_param,
+                                                              const StageDev *stage_dev, double *fc)
+{
+    constexpr bool FAST = PREC == CBD_PRECISION_FAST;
+    __shared__ StageDev st;
+    __shared__ int fill;
+    if (threadIdx.x == 0) {
+        st = stage_dev ? *stage_dev : st_param;
+        fill = cache_key_matches<PREC>(k, st, fc) ? 0 : 1;
+        if (fill)
+            fc[0] = 0.0;
+    }
+    __syncthreads();
+    if (!fill)
+        return;
+    const int ni = k.ni, nj = k.nj;
+    double *const cfx = fc + CACHE_HEADER;
+    double *const cfy = cfx + 2 * (size_t)(ni + 1) * nj;
+    double *const cfz = cfy + 2 * (size_t)ni * (nj + 1);
+    for (int i = blockIdx.x; i <= ni; i += gridDim.x) {
+        for (int j = threadIdx.x; j <= nj; j += blockDim.x) {
+            if (j < nj) {
+                const double xf = k.xl + (double)i * k.dx;
+                const double yc = k.yl + ((double)j + 0.5) * k.dy;
+                const double cs2 = sound_speed2<FAST>(k, st.m, xf, yc);
+                cache_store(cfx + 2 * ((size_t)i * nj + j), cs2, sqrt(cs2));
+            }
+            if (i < ni) {
+                const double xc = k.xl + ((double)i + 0.5) * k.dx;
+                const double yf = k.yl + (double)j * k.dy;
+                const double cs2 = sound_speed2<FAST>(k, st.m, xc, yf);
+                cache_store(cfy + 2 * ((size_t)i * (nj + 1) + j), cs2, sqrt(cs2));
+            }
+            if (i < ni && j < nj) {
+                const double xc = k.xl + ((double)i + 0.5) * k.dx;
+                const double yc = k.yl + ((double)j + 0.5) * k.dy;
+                double g[2] = {0.0, 0.0};
+#pragma unroll
+                for (int p = 0; p < 2; ++p) {
+                    const MassDev &m = st.m[p];
+                    if (m.mass != 0.0) {
+                        const double dx = xc - m.x;
+                        const double dy = yc - m.y;
+                        g[p] = inv_pow15<FAST>(dx * dx + dy * dy + m.soft2);
+                    }
+                }
+                cache_store(cfz + 2 * ((size_t)i * nj + j), g[0], g[1]);
+            }
+        }
     }
 }
 

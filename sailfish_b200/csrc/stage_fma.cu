@@ -4,9 +4,9 @@
 namespace cbd {
 
 cudaError_t launch_stage_fma(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a,
-                              cudaStream_t stream)
+                              int role, cudaStream_t stream)
 {
-    return launch_stage<CBD_PRECISION_FMA>(s, k, st, a, stream);
+    return launch_stage<CBD_PRECISION_FMA>(s, k, st, a, role, stream);
 }
 
 }  // namespace cbd

@@ -1,5 +1,5 @@
-// Instantiates the stage kernel for the supported strip widths and occupancy
-// targets at precision PREC.
+// Instantiates the stage kernel for the supported strip widths, occupancy
+// targets and face-cache roles at precision PREC.
 #pragma once
 
 #include "cbd_internal.h"
@@ -7,36 +7,50 @@
 namespace cbd {
 
 template <int BJ, int MINB, int PREC>
-cudaError_t launch_one(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a,
+cudaError_t launch_one(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a, int role,
                        cudaStream_t stream)
 {
-    stage_kernel<BJ, MINB, PREC><<<s.grid, BJ, 0, stream>>>(k, st, a);
+    switch (role) {
+    case ROLE_WRITER:
+        stage_kernel<BJ, MINB, PREC, ROLE_WRITER><<<s.grid, BJ, 0, stream>>>(k, st, a);
+        break;
+    case ROLE_READER: {
+        // at most four CTAs per SM, each over rows i, i + grid, ...
+        const int rows = k.ni + 1 < 148 * 4 ? k.ni + 1 : 148 * 4;
+        face_cache_fill_kernel<PREC><<<rows, 128, 0, stream>>>(k, st, a.stage_dev, a.fcache);
+        stage_kernel<BJ, MINB, PREC, ROLE_READER><<<s.grid, BJ, 0, stream>>>(k, st, a);
+        break;
+    }
+    default:
+        stage_kernel<BJ, MINB, PREC, ROLE_NONE><<<s.grid, BJ, 0, stream>>>(k, st, a);
+        break;
+    }
     return cudaGetLastError();
 }
 
 template <int PREC>
-cudaError_t launch_stage(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a,
+cudaError_t launch_stage(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a, int role,
                          cudaStream_t stream)
 {
     // minb = target resident CTAs per SM, which caps registers per thread
     if (s.bj == 128) {
         switch (s.minb) {
         case 5:
-            return launch_one<128, 5, PREC>(s, k, st, a, stream);
+            return launch_one<128, 5, PREC>(s, k, st, a, role, stream);
         case 6:
-            return launch_one<128, 6, PREC>(s, k, st, a, stream);
+            return launch_one<128, 6, PREC>(s, k, st, a, role, stream);
         default:
-            return launch_one<128, 1, PREC>(s, k, st, a, stream);
+            return launch_one<128, 1, PREC>(s, k, st, a, role, stream);
         }
     }
     if (s.bj == 64) {
         switch (s.minb) {
         case 10:
-            return launch_one<64, 10, PREC>(s, k, st, a, stream);
+            return launch_one<64, 10, PREC>(s, k, st, a, role, stream);
         case 12:
-            return launch_one<64, 12, PREC>(s, k, st, a, stream);
+            return launch_one<64, 12, PREC>(s, k, st, a, role, stream);
         default:
-            return launch_one<64, 1, PREC>(s, k, st, a, stream);
+            return launch_one<64, 1, PREC>(s, k, st, a, role, stream);
         }
     }
     return cudaErrorInvalidValue;

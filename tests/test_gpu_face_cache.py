@@ -1,9 +1,9 @@
 """
-The face cache (cbdiso_b200_advance_stage_cached): a step's last stage stores
+The face cache (cbdiso_b200_advance_stage_cached): the stage at t0 + dt stores
 the face sound speeds and zone gravity factors for its point masses, and the
-next step's first stage loads them when its masses match. In EXACT precision
-states, dts and reductions must be bit-identical to recomputing them in every
-stage.
+next step's first stage loads them (after a fill pass when the key does not
+match its masses). In EXACT precision states, dts and reductions must be
+bit-identical to recomputing them in every stage.
 """
 
 import ctypes
@@ -130,9 +130,11 @@ def test_cached_entry_rejects_a_misaligned_cache():
     d = load("cbd_t15_n64")
     s = product_solver(d, "exact", face_cache=True)
     st = _capi.Stage()
-    status = s._lib.cbdiso_b200_advance_stage_cached(
-        ctypes.byref(s._grid), ctypes.byref(st), None, s._ptr(s._buf[0]), None, s._ptr(s._buf[1]), None,
-        None, None, ctypes.c_void_p(s._fcache.data_ptr() + 8), s._stream())
-    assert status == 1  # invalid argument
+    args = (ctypes.byref(s._grid), ctypes.byref(st), None, s._ptr(s._buf[0]), None, s._ptr(s._buf[1]), None,
+            None, None)
+    lib = s._lib
+    assert lib.cbdiso_b200_advance_stage_cached(*args, ctypes.c_void_p(s._fcache.data_ptr() + 8), 2,
+                                                s._stream()) == 1  # invalid argument
+    assert lib.cbdiso_b200_advance_stage_cached(*args, s._ptr(s._fcache), 3, s._stream()) == 1
     assert int(s._lib.cbdiso_b200_face_cache_bytes(ctypes.byref(s._grid))) == \
         8 * (32 + 2 * (65 * 64 + 64 * 65 + 64 * 64))
