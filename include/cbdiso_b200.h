@@ -326,6 +326,21 @@ int cbdiso_b200_batched_stage(const void *disks, int num_disks, int total_units,
                               int stage, int epilogue, double *partials, unsigned int *counters, int precision,
                               void *stream);
 
+/* cbdiso_b200_batched_stage with face caches and a role (as in
+ * cbdiso_b200_advance_stage_cached: 0 none, 1 writer, 2 reader, the reader
+ * preceded by a fill pass per disk). Disk d's cache lies at face_cache + its
+ * record's cache offset, set by cbdiso_b200_batch_disk_set_face_cache (an even
+ * number of doubles); it holds cbdiso_b200_face_cache_bytes(its grid) bytes
+ * with its first 256 bytes zeroed before the first use, and `face_cache` is
+ * 16-byte aligned. A reader needs a cache for every disk: it leaves the tiles
+ * of a disk without one unwritten. No counterpart in the reference. */
+int cbdiso_b200_batch_disk_set_face_cache(void *record, long long cache_offset);
+int cbdiso_b200_batched_stage_cached(const void *disks, int num_disks, int total_units, const double *primitive_rd,
+                                     const double *primitive_n, double *primitive_wr, const void *records,
+                                     int num_stages, int stage, int epilogue, double *partials,
+                                     unsigned int *counters, int precision, double *face_cache, int role,
+                                     void *stream);
+
 /* Per-disk reduction of the tile partials, in tile order: results[d * stride]
  * = max wavespeed, then the diagnostic sums. */
 int cbdiso_b200_batched_finalize(const void *disks, int num_disks, const double *partials, double *results,

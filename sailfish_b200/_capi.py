@@ -148,6 +148,12 @@ def _declare(lib):
     lib.cbdiso_b200_batched_stage.argtypes = [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                               c_int, c_int, c_int, c_void_p, c_void_p, c_int, c_void_p]
     lib.cbdiso_b200_batched_stage.restype = c_int
+    lib.cbdiso_b200_batched_stage_cached.argtypes = [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p,
+                                                     c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_int,
+                                                     c_void_p, c_int, c_void_p]
+    lib.cbdiso_b200_batched_stage_cached.restype = c_int
+    lib.cbdiso_b200_batch_disk_set_face_cache.argtypes = [c_void_p, ctypes.c_longlong]
+    lib.cbdiso_b200_batch_disk_set_face_cache.restype = c_int
     lib.cbdiso_b200_batched_finalize.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p]
     lib.cbdiso_b200_batched_finalize.restype = c_int
     lib.cbdiso_b200_batched_prologue.argtypes = [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int,
@@ -237,6 +243,7 @@ def exported_symbols():
         "cbdiso_b200_stepper_bytes", "cbdiso_b200_stepper_init",
         "cbdiso_b200_step_prologue", "cbdiso_b200_batch_disk_bytes", "cbdiso_b200_batch_disk_record",
         "cbdiso_b200_batched_stage", "cbdiso_b200_batched_finalize", "cbdiso_b200_batched_prologue",
+        "cbdiso_b200_batched_stage_cached", "cbdiso_b200_batch_disk_set_face_cache",
         "cbdiso_b200_adjoint_workspace_bytes", "cbdiso_b200_stage_record_branches", "cbdiso_b200_stage_tangent",
         "cbdiso_b200_stage_adjoint", "cbdiso_b200_objective_tangent", "cbdiso_b200_objective_adjoint",
         "cbdiso_b200_stepper_attach", "cbdiso_b200_stage_adjoint_chained", "cbdiso_b200_objective_adjoint_chained",

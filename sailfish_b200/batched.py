@@ -75,6 +75,9 @@ class BatchedSolver:
         if len(self._device_diags) > _capi.MAX_FUSED:
             raise ValueError(f"at most {_capi.MAX_FUSED} diagnostics besides time")
         opts = dict(options or {})
+        # the batch keeps one face-cache arena for all disks (option
+        # face_cache, default on); the per-disk solvers need none
+        face_cache = bool(opts.pop("face_cache", True))
         opts.update(rk_order=rk_order, plm_theta=plm_theta, precision=precision, face_cache=False)
 
         # One single-disk Solver per disk builds the grid record, the initial
@@ -110,6 +113,8 @@ class BatchedSolver:
         records = bytearray(rec_bytes * n)
         offset = 0
         unit = 0
+        cache_offset = 0
+        cache_offsets = []
         self.offsets = [0] * n
         for slot, i in enumerate(self.order):
             s = self.solvers[i]
@@ -122,6 +127,10 @@ class BatchedSolver:
             _capi.check(lib.cbdiso_b200_batch_disk_record(ctypes.byref(s._grid), ctypes.byref(ep), width, rows,
                                                           offset, unit, ctypes.byref(units), buf),
                         "batch_disk_record")
+            if face_cache:
+                _capi.check(lib.cbdiso_b200_batch_disk_set_face_cache(buf, cache_offset), "batch_disk_set_face_cache")
+                cache_offsets.append(cache_offset)
+                cache_offset += int(lib.cbdiso_b200_face_cache_bytes(ctypes.byref(s._grid))) // 8
             records[slot * rec_bytes:(slot + 1) * rec_bytes] = bytes(buf)
             self.offsets[i] = offset
             offset += (ni + 2 * NG) * (nj + 2 * NG) * NQ
@@ -131,6 +140,13 @@ class BatchedSolver:
         f64 = dict(dtype=torch.float64, device=self.device)
         nbuf = 3 if rk_order == 3 else 2
         self._buf = [torch.empty(offset, **f64) for _ in range(nbuf)]
+        # per-disk face caches (carried from the stage at t0 + dt to the next
+        # step's first stage), each with its key header zeroed
+        self._fcache = None
+        if face_cache:
+            self._fcache = torch.empty(cache_offset, **f64)
+            for c in cache_offsets:
+                self._fcache[c:c + 32].zero_()
         for i, s in enumerate(self.solvers):
             self._buf[0][self.offsets[i]:self.offsets[i] + s._buf[0].numel()] = s._buf[0].reshape(-1)
         self._disks_dev = torch.frombuffer(records, dtype=torch.uint8).to(self.device)
@@ -182,11 +198,16 @@ class BatchedSolver:
             plan = [(A, None, B), (B, A, C), (C, A, A)]
         for stage, (rd, pn, wr) in enumerate(plan):
             last = stage == len(plan) - 1
-            _capi.check(lib.cbdiso_b200_batched_stage(
-                self._ptr(self._disks_dev), n, self.total_units, self._ptr(rd),
-                self._ptr(pn) if pn is not None else None, self._ptr(wr), self._ptr(self._records), self.rk_order,
-                stage, int(last), self._ptr(self._partials), self._ptr(self._counters), prec, stream),
-                "batched_stage")
+            common = (self._ptr(self._disks_dev), n, self.total_units, self._ptr(rd),
+                      self._ptr(pn) if pn is not None else None, self._ptr(wr), self._ptr(self._records),
+                      self.rk_order, stage, int(last), self._ptr(self._partials), self._ptr(self._counters), prec)
+            # face-cache role: the stage at t0 + dt writes, the next step's first reads
+            role = 0 if self._fcache is None else (2 if stage == 0 else (1 if stage == 1 else 0))
+            if role:
+                status = lib.cbdiso_b200_batched_stage_cached(*common, self._ptr(self._fcache), role, stream)
+            else:
+                status = lib.cbdiso_b200_batched_stage(*common, stream)
+            _capi.check(status, "batched_stage")
         _capi.check(lib.cbdiso_b200_batched_finalize(self._ptr(self._disks_dev), n, self._ptr(self._partials),
                                                      self._ptr(self._results), RESULT_STRIDE, stream),
                     "batched_finalize")

@@ -9,16 +9,14 @@
 
 namespace cbd {
 
-cudaError_t launch_batched_fma(const BatchArgs &a, int ctas, cudaStream_t s)
+cudaError_t launch_batched_fma(const BatchArgs &a, int ctas, int role, cudaStream_t s)
 {
-    batched_stage_kernel<128, 6, CBD_PRECISION_FMA><<<ctas, 128, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_batched<CBD_PRECISION_FMA>(a, ctas, role, s);
 }
 
-cudaError_t launch_batched_fast(const BatchArgs &a, int ctas, cudaStream_t s)
+cudaError_t launch_batched_fast(const BatchArgs &a, int ctas, int role, cudaStream_t s)
 {
-    batched_stage_kernel<128, 6, CBD_PRECISION_FAST><<<ctas, 128, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_batched<CBD_PRECISION_FAST>(a, ctas, role, s);
 }
 
 namespace {
@@ -87,15 +85,32 @@ int cbdiso_b200_batch_disk_record(const cbd_grid_t *grid, const cbd_epilogue_t *
     d.strips = (grid->nj + strip_width - 1) / strip_width;
     d.segments = (grid->ni + rows - 1) / rows;
     d.unit_begin = unit_begin;
+    d.cache_offset = -1;
     *units = d.strips * d.segments;
     std::memcpy(record, &d, sizeof(d));
     return CBD_OK;
 }
 
-int cbdiso_b200_batched_stage(const void *disks, int num_disks, int total_units, const double *primitive_rd,
-                              const double *primitive_n, double *primitive_wr, const void *records, int num_stages,
-                              int stage, int epilogue, double *partials, unsigned int *counters, int precision,
-                              void *stream)
+int cbdiso_b200_batch_disk_set_face_cache(void *record, long long cache_offset)
+{
+    // pairs are moved as 16-byte vectors: an even offset in an aligned arena
+    if (!record || cache_offset < 0 || (cache_offset & 1))
+        return CBD_ERR_ARGUMENT;
+    DiskDev d;
+    std::memcpy(&d, record, sizeof(d));
+    d.cache_offset = cache_offset;
+    std::memcpy(record, &d, sizeof(d));
+    return CBD_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int batched_stage(const void *disks, int num_disks, int total_units, const double *primitive_rd,
+                  const double *primitive_n, double *primitive_wr, const void *records, int num_stages, int stage,
+                  int epilogue, double *partials, unsigned int *counters, int precision, double *face_cache,
+                  int role, void *stream)
 {
     if (!disks || num_disks <= 0 || total_units <= 0 || !primitive_rd || !primitive_wr || !records ||
         num_stages < 1 || num_stages > 3 || stage < 0 || stage >= num_stages || !counters ||
@@ -115,6 +130,7 @@ int cbdiso_b200_batched_stage(const void *disks, int num_disks, int total_units,
     a.epilogue = epilogue ? 1 : 0;
     a.partials = partials;
     a.counters = counters;
+    a.fcache = face_cache;
     int ctas = 148 * 6;
     if (total_units < ctas)
         ctas = total_units;
@@ -122,16 +138,42 @@ int cbdiso_b200_batched_stage(const void *disks, int num_disks, int total_units,
     cudaError_t e;
     switch (precision) {
     case CBD_PRECISION_EXACT:
-        e = launch_batched_exact(a, ctas, s);
+        e = launch_batched_exact(a, ctas, role, s);
         break;
     case CBD_PRECISION_FMA:
-        e = launch_batched_fma(a, ctas, s);
+        e = launch_batched_fma(a, ctas, role, s);
         break;
     default:
-        e = launch_batched_fast(a, ctas, s);
+        e = launch_batched_fast(a, ctas, role, s);
         break;
     }
     return e == cudaSuccess ? CBD_OK : CBD_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cbdiso_b200_batched_stage(const void *disks, int num_disks, int total_units, const double *primitive_rd,
+                              const double *primitive_n, double *primitive_wr, const void *records, int num_stages,
+                              int stage, int epilogue, double *partials, unsigned int *counters, int precision,
+                              void *stream)
+{
+    return batched_stage(disks, num_disks, total_units, primitive_rd, primitive_n, primitive_wr, records,
+                         num_stages, stage, epilogue, partials, counters, precision, nullptr, ROLE_NONE, stream);
+}
+
+int cbdiso_b200_batched_stage_cached(const void *disks, int num_disks, int total_units, const double *primitive_rd,
+                                     const double *primitive_n, double *primitive_wr, const void *records,
+                                     int num_stages, int stage, int epilogue, double *partials,
+                                     unsigned int *counters, int precision, double *face_cache, int role,
+                                     void *stream)
+{
+    if (!face_cache || (reinterpret_cast<uintptr_t>(face_cache) & 15) != 0 || role < ROLE_NONE ||
+        role > ROLE_READER)
+        return CBD_ERR_ARGUMENT;
+    return batched_stage(disks, num_disks, total_units, primitive_rd, primitive_n, primitive_wr, records,
+                         num_stages, stage, epilogue, partials, counters, precision, face_cache, role, stream);
 }
 
 int cbdiso_b200_batched_finalize(const void *disks, int num_disks, const double *partials, double *results,

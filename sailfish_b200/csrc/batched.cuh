@@ -18,6 +18,7 @@ struct DiskDev {
     int strips;
     int segments;
     int unit_begin;      // index of the disk's first tile in the batch's tile list
+    long long cache_offset;  // offset of the disk's face cache in BatchArgs::fcache, in doubles; -1: none
 };
 
 struct BatchArgs {
@@ -34,9 +35,14 @@ struct BatchArgs {
     int _pad;
     double *partials;    // [total_units][PARTIAL_STRIDE]
     unsigned int *counters;  // [0] next tile, [1] CTAs finished; both return to zero at the end
+    double *fcache;      // face-cache arena (disk d's cache at disks[d].cache_offset), or null
 };
 
-template <int BJ, int MINB, int PREC>
+// ROLE (ROLE_*) is what the launch does with each disk's face cache: a writer
+// stores into the caches of the disks that have one; a reader requires one
+// for every disk (the batch's fill kernel ran before it) and skips the tiles
+// of a disk without one.
+template <int BJ, int MINB, int PREC, int ROLE = ROLE_NONE>
 __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs a)
 {
     constexpr bool FAST = PREC == CBD_PRECISION_FAST;
@@ -97,12 +103,23 @@ __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs
         sa.stage_dev = nullptr;
         sa.scratch = nullptr;
         sa.result = nullptr;
-        sa.fcache = nullptr;
+        const bool cached = ROLE != ROLE_NONE && a.fcache && D.cache_offset >= 0;
+        sa.fcache = cached ? a.fcache + D.cache_offset : nullptr;
         double acc[PARTIAL_STRIDE];
 #pragma unroll
         for (int v = 0; v < PARTIAL_STRIDE; ++v)
             acc[v] = 0.0;
-        march_tile<BJ, FAST>(k, st, sa, strip * D.strip_width, D.strip_width, seg * k.rows_per_cta, acc);
+        const int c0 = strip * D.strip_width, r0 = seg * k.rows_per_cta;
+        if (ROLE == ROLE_WRITER) {
+            // the same answer in every thread; the disk's first tile writes the key
+            const bool store = cached && cache_write_check<PREC>(k, st, sa.fcache, t == 0 && u == D.unit_begin);
+            march_tile<BJ, FAST, CACHE_WRITE>(k, st, sa, c0, D.strip_width, r0, acc, store);
+        } else if (ROLE == ROLE_READER) {
+            if (cached)
+                march_tile<BJ, FAST, CACHE_READ>(k, st, sa, c0, D.strip_width, r0, acc);
+        } else {
+            march_tile<BJ, FAST, CACHE_NONE>(k, st, sa, c0, D.strip_width, r0, acc);
+        }
         if (a.epilogue) {
             double red[PARTIAL_STRIDE];
             block_reduce<BJ>(acc, sred, red);
@@ -125,8 +142,55 @@ __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs
     }
 }
 
-cudaError_t launch_batched_exact(const BatchArgs &a, int ctas, cudaStream_t s);
-cudaError_t launch_batched_fma(const BatchArgs &a, int ctas, cudaStream_t s);
-cudaError_t launch_batched_fast(const BatchArgs &a, int ctas, cudaStream_t s);
+// The face caches of every disk valid for a reader stage (see
+// face_cache_fill_kernel): CTA (y, d) checks disk d's key and, when it does not
+// match, marks it invalid and fills rows y, y + gridDim.x, ... of its cache.
+template <int PREC>
+__global__ void __launch_bounds__(128) batched_fill_kernel(const BatchArgs a)
+{
+    constexpr bool FAST = PREC == CBD_PRECISION_FAST;
+    __shared__ StageDev st;
+    __shared__ int fill;
+    const DiskDev &D = a.disks[blockIdx.y];
+    const Consts &k = D.k;
+    if (threadIdx.x == 0) {
+        st = a.records[(size_t)blockIdx.y * a.num_stages + a.stage];
+        fill = 0;
+        if (D.cache_offset >= 0) {
+            double *fc = a.fcache + D.cache_offset;
+            fill = cache_key_matches<PREC>(k, st, fc) ? 0 : 1;
+            if (fill)
+                fc[0] = 0.0;
+        }
+    }
+    __syncthreads();
+    if (!fill)
+        return;
+    face_cache_fill_rows<FAST>(k, st, a.fcache + D.cache_offset, blockIdx.x, gridDim.x);
+}
+
+cudaError_t launch_batched_exact(const BatchArgs &a, int ctas, int role, cudaStream_t s);
+cudaError_t launch_batched_fma(const BatchArgs &a, int ctas, int role, cudaStream_t s);
+cudaError_t launch_batched_fast(const BatchArgs &a, int ctas, int role, cudaStream_t s);
+
+// One batched stage launch at precision PREC with a face-cache role; the
+// reader is preceded by the fill kernel.
+template <int PREC>
+cudaError_t launch_batched(const BatchArgs &a, int ctas, int role, cudaStream_t s)
+{
+    switch (role) {
+    case ROLE_WRITER:
+        batched_stage_kernel<128, 6, PREC, ROLE_WRITER><<<ctas, 128, 0, s>>>(a);
+        break;
+    case ROLE_READER:
+        batched_fill_kernel<PREC><<<dim3(8, a.num_disks), 128, 0, s>>>(a);
+        batched_stage_kernel<128, 6, PREC, ROLE_READER><<<ctas, 128, 0, s>>>(a);
+        break;
+    default:
+        batched_stage_kernel<128, 6, PREC, ROLE_NONE><<<ctas, 128, 0, s>>>(a);
+        break;
+    }
+    return cudaGetLastError();
+}
 
 }  // namespace cbd

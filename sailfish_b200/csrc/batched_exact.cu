@@ -3,10 +3,9 @@
 
 namespace cbd {
 
-cudaError_t launch_batched_exact(const BatchArgs &a, int ctas, cudaStream_t s)
+cudaError_t launch_batched_exact(const BatchArgs &a, int ctas, int role, cudaStream_t s)
 {
-    batched_stage_kernel<128, 6, CBD_PRECISION_EXACT><<<ctas, 128, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_batched<CBD_PRECISION_EXACT>(a, ctas, role, s);
 }
 
 }  // namespace cbd

@@ -1053,32 +1053,17 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
     }
 }
 
-// Makes the face cache valid for a reader stage: when the key does not match
-// the stage's masses, marks it invalid (no later key check passes on what
-// follows) and computes every face's (cs^2, cs) and every zone's gravity
-// factors for those masses, with the stage kernel's own expressions. Grid:
-// any number of 128-thread CTAs, each taking rows i = blockIdx.x, ... .
-template <int PREC>
-__global__ void __launch_bounds__(128) face_cache_fill_kernel(const Consts k, const StageDev st_param,
-                                                              const StageDev *stage_dev, double *fc)
+// Rows i = first, first + stride, ... (0 <= i <= ni) of a face cache for the
+// masses of `st`: every face's (cs^2, cs) and every zone's gravity factors,
+// with the stage kernel's own expressions. One CTA of any width.
+template <bool FAST>
+__device__ void face_cache_fill_rows(const Consts &k, const StageDev &st, double *fc, int first, int stride)
 {
-    constexpr bool FAST = PREC == CBD_PRECISION_FAST;
-    __shared__ StageDev st;
-    __shared__ int fill;
-    if (threadIdx.x == 0) {
-        st = stage_dev ? *stage_dev : st_param;
-        fill = cache_key_matches<PREC>(k, st, fc) ? 0 : 1;
-        if (fill)
-            fc[0] = 0.0;
-    }
-    __syncthreads();
-    if (!fill)
-        return;
     const int ni = k.ni, nj = k.nj;
     double *const cfx = fc + CACHE_HEADER;
     double *const cfy = cfx + 2 * (size_t)(ni + 1) * nj;
     double *const cfz = cfy + 2 * (size_t)ni * (nj + 1);
-    for (int i = blockIdx.x; i <= ni; i += gridDim.x) {
+    for (int i = first; i <= ni; i += stride) {
         for (int j = threadIdx.x; j <= nj; j += blockDim.x) {
             if (j < nj) {
                 const double xf = k.xl + (double)i * k.dx;
@@ -1109,6 +1094,28 @@ __global__ void __launch_bounds__(128) face_cache_fill_kernel(const Consts k, co
             }
         }
     }
+}
+
+// Makes the face cache valid for a reader stage: when the key does not match
+// the stage's masses, marks it invalid (no later key check passes on what
+// follows) and fills it for those masses. Grid: any number of 128-thread
+// CTAs, each taking rows i = blockIdx.x, blockIdx.x + gridDim.x, ... .
+template <int PREC>
+__global__ void __launch_bounds__(128) face_cache_fill_kernel(const Consts k, const StageDev st_param,
+                                                              const StageDev *stage_dev, double *fc)
+{
+    __shared__ StageDev st;
+    __shared__ int fill;
+    if (threadIdx.x == 0) {
+        st = stage_dev ? *stage_dev : st_param;
+        fill = cache_key_matches<PREC>(k, st, fc) ? 0 : 1;
+        if (fill)
+            fc[0] = 0.0;
+    }
+    __syncthreads();
+    if (!fill)
+        return;
+    face_cache_fill_rows<PREC == CBD_PRECISION_FAST>(k, st, fc, blockIdx.x, gridDim.x);
 }
 
 }  // namespace cbd

@@ -60,3 +60,17 @@ def test_batched_tiles_from_autotuner(tmp_path, monkeypatch):
     assert (96, 96) in t and t[(96, 96)][0] in (64, 128)
     assert (tmp_path / "tiles.json").exists()
     assert tuned_tiles([(96, 96)], "exact") == t  # served from the cache
+
+
+def test_batched_face_cache_is_bit_identical():
+    disks = config2_disks(num=5, seed=7, sizes=(64, 96, 128))
+    on = BatchedSolver(disks, diagnostics=DIAGS)
+    off = BatchedSolver(disks, diagnostics=DIAGS, options=dict(face_cache=False))
+    assert on._fcache is not None and off._fcache is None
+    a = on.run(12, cfl=0.3, graph=True, steps_per_graph=4)
+    b = off.run(12, cfl=0.3, graph=True, steps_per_graph=4)
+    assert a == b
+    for i in range(len(disks)):
+        assert np.array_equal(on.solution(i), off.solution(i))
+    torch.cuda.synchronize()
+    assert float(on._fcache[0]) == 20260101.5  # the first disk's key was written
