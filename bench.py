@@ -34,11 +34,11 @@ BYTES_PER_ZONE_UPDATE = 120.0  # RK2 x FP64 x 3 fields: 48 B stage 1 + 72 B stag
 # and a stage 2 launch writing it, at 2048^2,
 # profiles/stage_kernels_2048_face_cache.md); scaled by the zone count. It is
 # above the algorithmic 60 B because of the cache's 48 B per zone and step.
-NCU_TRAFFIC_PER_ZONE_LAUNCH = (313.02e6 + 75.39e6 + 224.86e6 + 273.31e6) / 2 / 2048 ** 2
+NCU_TRAFFIC_PER_ZONE_LAUNCH = (314.69e6 + 75.12e6 + 223.57e6 + 260.25e6) / 2 / 2048 ** 2
 # FP64 thread-instructions (DADD + DMUL + DFMA) per zone and stage launch, mean
 # of the same two launches (ncu, the sum of
 # smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum over zones)
-FP64_INST_PER_ZONE_LAUNCH = (346.9 + 673.0) / 2
+FP64_INST_PER_ZONE_LAUNCH = (346.9 + 670.9) / 2
 GAM_FP64_INST_PER_ZONE_LAUNCH = (1224.8 + 1249.8) / 2
 DIAGNOSTICS = [dict(quantity="time"), dict(quantity="mdot", which_mass=1, accretion=True),
                dict(quantity="mdot", which_mass=2, accretion=True),
