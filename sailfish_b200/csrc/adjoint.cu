@@ -1338,12 +1338,15 @@ AdjArgs adj_args(const cbd_grid_t *grid, const void *stage_dev, void *workspace,
 // Blocks of the adjoint passes: one item (zone or face) per thread; the face
 // pass is the widest. Rows of the chained accumulator and of the per-block
 // partials.
+// shortest segment of the fused kernel's march
+constexpr int AM_MIN_ROWS = 4;
+
 int adj_rows(const cbd_grid_t *grid)
 {
     const long faces = 2L * (grid->ni + 2) * (grid->nj + 2);
     const long pass = (faces + ADJ_THREADS - 1) / ADJ_THREADS;
-    // the fused kernel's CTAs at its shortest (8-row) segments
-    const long march = (long)((grid->nj + AM_BJ - 1) / AM_BJ) * ((grid->ni + 7) / 8);
+    // the fused kernel's CTAs at its shortest segments
+    const long march = (long)((grid->nj + AM_BJ - 1) / AM_BJ) * ((grid->ni + AM_MIN_ROWS - 1) / AM_MIN_ROWS);
     return (int)(pass > march ? pass : march);
 }
 
@@ -1356,8 +1359,10 @@ constexpr int SINK_PASS_BLOCKS = 148;
 // the fused row-marching stage adjoint (default) or the separate passes
 int g_fused_adjoint = 1;
 
-// Strips of AM_BJ columns x segments of rows: 32-row segments, halved down to
-// 8 while the grid is under two waves of three CTAs per SM.
+// Strips of AM_BJ columns x segments of rows. A CTA marches its rows plus six
+// (the pipeline's lead rows), and CTAs run in waves of three per SM: the
+// segment length (4 .. 32 rows) minimises waves x (rows + 6), the longer
+// segment on a tie.
 dim3 march_grid(int ni, int nj)
 {
     int sms = 148, dev = 0;
@@ -1365,10 +1370,18 @@ dim3 march_grid(int ni, int nj)
                                                    cudaSuccess)
         cudaGetLastError();
     const int strips = (nj + AM_BJ - 1) / AM_BJ;
-    int rows = 32;
-    while (rows > 8 && (long)strips * ((ni + rows - 1) / rows) < 2L * 3 * sms)
-        rows /= 2;
-    return dim3(strips, (ni + rows - 1) / rows, 1);
+    const long slots = 3L * sms;
+    int best = 32;
+    long best_cost = -1;
+    for (int rows = 32; rows >= AM_MIN_ROWS; --rows) {
+        const long ctas = (long)strips * ((ni + rows - 1) / rows);
+        const long cost = (ctas + slots - 1) / slots * (rows + 6);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = rows;
+        }
+    }
+    return dim3(strips, (ni + best - 1) / best, 1);
 }
 
 template <bool CHAIN>
