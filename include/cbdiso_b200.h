@@ -423,6 +423,14 @@ size_t cbdiso_b200_adjoint_chain_blocks(const cbd_grid_t *grid);
  * zones and faces; lambda_rd and lambda_n agree bit for bit, the parameter
  * sums to rounding. Process-wide. */
 int cbdiso_b200_set_adjoint_variant(int fused);
+
+/* Rows per CTA segment of the fused stage adjoint (no counterpart in the
+ * reference). 0 (default): chosen per grid to finish a lone sweep soonest
+ * (whole waves of CTAs; short segments on small grids); 4 .. 32: fixed, for
+ * sweeps that share the GPU with others (several disks over streams), where
+ * the total work of the longer segments counts. Process-wide; read when a
+ * stage adjoint is launched or captured into a CUDA graph. */
+int cbdiso_b200_set_adjoint_segment_rows(int rows);
 int cbdiso_b200_adjoint_chain_finish(const double *chain_acc, int num_blocks, double *out4, void *stream);
 
 /* The epilogue quantities alone, on a given state (guards not needed). */

@@ -163,6 +163,8 @@ def _declare(lib):
     lib.cbdiso_b200_adjoint_workspace_bytes.restype = c_size_t
     lib.cbdiso_b200_set_adjoint_variant.argtypes = [c_int]
     lib.cbdiso_b200_set_adjoint_variant.restype = c_int
+    lib.cbdiso_b200_set_adjoint_segment_rows.argtypes = [c_int]
+    lib.cbdiso_b200_set_adjoint_segment_rows.restype = c_int
     lib.cbdiso_b200_adjoint_chain_blocks.argtypes = [POINTER(Grid)]
     lib.cbdiso_b200_adjoint_chain_blocks.restype = c_size_t
     V = c_void_p
@@ -248,7 +250,7 @@ def exported_symbols():
         "cbdiso_b200_stage_adjoint", "cbdiso_b200_objective_tangent", "cbdiso_b200_objective_adjoint",
         "cbdiso_b200_stepper_attach", "cbdiso_b200_stage_adjoint_chained", "cbdiso_b200_objective_adjoint_chained",
         "cbdiso_b200_adjoint_chain_finish", "cbdiso_b200_adjoint_chain_blocks",
-        "cbdiso_b200_set_adjoint_variant",
+        "cbdiso_b200_set_adjoint_variant", "cbdiso_b200_set_adjoint_segment_rows",
         "cbdgam_2d_advance_rk", "cbdgam_2d_wavespeed", "cbdgam_2d_primitive_to_conserved",
         "cbdgam_2d_point_mass_source_term", "cbdgam_b200_set_plm_theta", "cbdgam_b200_advance_stage",
         "cbdgam_b200_fill_guards", "cbdgam_b200_scratch_bytes", "cbdgam_b200_reduce", "cbdgam_b200_abi_sizes",

@@ -113,6 +113,10 @@ def _kepler_complex_many(t, a, m, q, e):
     return np.stack([x1, y1, vx1, vy1, m1 * ones, -x1 / q, -y1 / q, -vx1 / q, -vy1 / q, m2 * ones])
 
 
+# segment rows of the stage adjoints when many sweeps share the GPU
+SHARED_SWEEP_ROWS = 32
+
+
 def mass_jacobians(times, q, e, a=1.0, m=1.0, h=1e-30):
     """mass_jacobian at every time of `times`: len(times) x 10 x 2."""
     jq = _kepler_complex_many(times, a, m, complex(q, h), complex(e, 0.0)).imag / h
@@ -616,8 +620,15 @@ class BatchedAdjoint:
 
     def gradient(self, weights=(1.0, 0.0)):
         """(dJ/dprim0, dJ/d(q, e, nu, sink_rate)) of every disk, after
-        forward(keep=True)."""
-        return self._each(lambda i: self.runs[i].gradient(weights))
+        forward(keep=True). The sweeps share the GPU, so the stage adjoints
+        run in the longest segments (least total work); the library's default
+        segment choice is restored afterwards."""
+        lib = _capi.lib()
+        _capi.check(lib.cbdiso_b200_set_adjoint_segment_rows(SHARED_SWEEP_ROWS), "set_adjoint_segment_rows")
+        try:
+            return self._each(lambda i: self.runs[i].gradient(weights))
+        finally:
+            lib.cbdiso_b200_set_adjoint_segment_rows(0)
 
 
 def config4_disks(num=32, seed=4096, sizes=(256, 512)):

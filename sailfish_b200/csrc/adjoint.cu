@@ -1358,6 +1358,8 @@ constexpr int SINK_PASS_BLOCKS = 148;
 
 // the fused row-marching stage adjoint (default) or the separate passes
 int g_fused_adjoint = 1;
+// the fused kernel's segment length: 0 = by the wave rule of march_grid
+int g_march_rows = 0;
 
 // Strips of AM_BJ columns x segments of rows. A CTA marches its rows plus six
 // (the pipeline's lead rows), and CTAs run in waves of three per SM: the
@@ -1370,6 +1372,8 @@ dim3 march_grid(int ni, int nj)
                                                    cudaSuccess)
         cudaGetLastError();
     const int strips = (nj + AM_BJ - 1) / AM_BJ;
+    if (g_march_rows > 0)
+        return dim3(strips, (ni + g_march_rows - 1) / g_march_rows, 1);
     const long slots = 3L * sms;
     int best = 32;
     long best_cost = -1;
@@ -1572,6 +1576,14 @@ int cbdiso_b200_set_adjoint_variant(int fused)
     if (fused != 0 && fused != 1)
         return CBD_ERR_ARGUMENT;
     g_fused_adjoint = fused;
+    return CBD_OK;
+}
+
+int cbdiso_b200_set_adjoint_segment_rows(int rows)
+{
+    if (rows != 0 && (rows < AM_MIN_ROWS || rows > 32))
+        return CBD_ERR_ARGUMENT;
+    g_march_rows = rows;
     return CBD_OK;
 }
 
