@@ -528,6 +528,24 @@ typedef struct cbdgam_stage {
 int cbdgam_b200_advance_stage(const cbdgam_grid_t *grid, const cbdgam_stage_t *stage, const double *primitive_rd,
                               const double *primitive_n, double *primitive_wr, double *wavespeed_max, void *stream);
 
+/* cbdgam_b200_advance_stage with a face cache (no counterpart in the
+ * reference, which recomputes these values in every stage,
+ * cbdgam_2d.c:75-106 and :108-203). The scale heights' geometry at every face
+ * and zone centre and, with constant softening, the zones' gravity factors
+ * depend only on the mesh and the point masses. `role` 1 (writer; the caller
+ * gives it to the stage at t0 + dt when its masses equal the end-of-step
+ * masses) stores them with a key of their inputs; role 2 (reader; a step's
+ * first stage) loads them after a fill pass that recomputes them when the key
+ * does not match the stage's masses; role 0 neither. Bit-identical to
+ * cbdgam_b200_advance_stage. `face_cache`: a caller-owned, 16-byte aligned
+ * device buffer of cbdgam_b200_face_cache_bytes(grid) bytes for this grid
+ * only, its first 256 bytes zeroed before the first use; calls on one cache
+ * ordered on one stream. */
+size_t cbdgam_b200_face_cache_bytes(const cbdgam_grid_t *grid);
+int cbdgam_b200_advance_stage_cached(const cbdgam_grid_t *grid, const cbdgam_stage_t *stage,
+                                     const double *primitive_rd, const double *primitive_n, double *primitive_wr,
+                                     double *wavespeed_max, double *face_cache, int role, void *stream);
+
 /* Writes the zero-gradient guard zones of a state from its edge zones
  * (cbdgam_2d.py:491-520 on one patch). */
 int cbdgam_b200_fill_guards(const cbdgam_grid_t *grid, double *primitive, void *stream);

@@ -191,6 +191,7 @@ def _declare(lib):
         "cbdgam_2d_point_mass_source_term": [I, I, D, D, D, D] + m9 + m9 + [I, V, V, I, D],
         "cbdgam_b200_set_plm_theta": [D],
         "cbdgam_b200_advance_stage": [POINTER(GamGrid), POINTER(GamStage), V, V, V, V, V],
+        "cbdgam_b200_advance_stage_cached": [POINTER(GamGrid), POINTER(GamStage), V, V, V, V, V, I, V],
         "cbdgam_b200_fill_guards": [POINTER(GamGrid), V, V],
         "cbdgam_b200_reduce": [POINTER(GamGrid), POINTER(Mass), POINTER(Diag), c_int, V, V, V, V],
         "cbdgam_b200_eval_powers": [ctypes.c_long, V, V, V],
@@ -207,6 +208,8 @@ def _declare(lib):
     lib.cbdgam_b200_disk_primitive.restype = None
     lib.cbdgam_b200_scratch_bytes.argtypes = [POINTER(GamGrid)]
     lib.cbdgam_b200_scratch_bytes.restype = c_size_t
+    lib.cbdgam_b200_face_cache_bytes.argtypes = [POINTER(GamGrid)]
+    lib.cbdgam_b200_face_cache_bytes.restype = c_size_t
     lib.cbdgam_b200_abi_sizes.argtypes = [POINTER(c_size_t)]
     lib.cbdgam_b200_abi_sizes.restype = None
     lib.cbdiso_b200_abi_sizes.argtypes = [POINTER(c_size_t)]
@@ -253,6 +256,7 @@ def exported_symbols():
         "cbdiso_b200_set_adjoint_variant", "cbdiso_b200_set_adjoint_segment_rows",
         "cbdgam_2d_advance_rk", "cbdgam_2d_wavespeed", "cbdgam_2d_primitive_to_conserved",
         "cbdgam_2d_point_mass_source_term", "cbdgam_b200_set_plm_theta", "cbdgam_b200_advance_stage",
+        "cbdgam_b200_face_cache_bytes", "cbdgam_b200_advance_stage_cached",
         "cbdgam_b200_fill_guards", "cbdgam_b200_scratch_bytes", "cbdgam_b200_reduce", "cbdgam_b200_abi_sizes",
         "cbdgam_b200_eval_powers", "cbdiso_b200_fp64_probe", "cbdiso_b200_fp64_probe_fmas",
         "cbdgam_b200_disk_primitive",

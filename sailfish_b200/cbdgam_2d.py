@@ -46,13 +46,17 @@ COMPLEX_QUANTITIES = ("sigma_m1", "eccentricity_vector")
 
 
 class Options(NamedTuple):
-    """Solver options (cbdgam_2d.py:23-27, plus the PLM parameter)."""
+    """Solver options (cbdgam_2d.py:23-27, plus the PLM parameter and
+    `face_cache`: a step's first stage loads the scale-height geometry and
+    gravity factors that the previous step's second stage computed for the
+    same point masses; the same bits either way)."""
 
     pressure_floor: float = 1e-12
     density_floor: float = 1e-10
     velocity_ceiling: float = 1e16
     mach_ceiling: float = 1e5
     plm_theta: float = 1.5
+    face_cache: bool = True
 
 
 def initial_condition(setup, mesh, time, rows=None):
@@ -182,6 +186,10 @@ class Solver(SolverBase):
                     "fill_guards")
         nscratch = int(self._lib.cbdgam_b200_scratch_bytes(ctypes.byref(g)))
         self._scratch = torch.zeros(nscratch // 8 + 8, **f64)
+        self._fcache = None
+        if self._options.face_cache:
+            self._fcache = torch.empty(int(self._lib.cbdgam_b200_face_cache_bytes(ctypes.byref(g))) // 8, **f64)
+            self._fcache[:32].zero_()
         # the wavespeed maximum of the current state (slot 0; the multi-GPU
         # solver all-reduces it in place) and, apart, the diagnostic sums
         self._result = torch.zeros(1 + 2 * _capi.GAM_MAX_DIAG, **f64)
@@ -218,6 +226,25 @@ class Solver(SolverBase):
         st.buffer_central_mass = m1.mass + m2.mass
         st.a, st.dt = a, dt
         return st
+
+    def _launch(self, st, rd, pn, wr, ws, role, stream):
+        """One product stage; `role` (1 writer, 2 reader) is used when the
+        solver keeps a face cache."""
+        lib, g = self._lib, self._grid
+        args = (ctypes.byref(g), ctypes.byref(st), self._ptr(rd), self._ptr(pn) if pn is not None else None,
+                self._ptr(wr), self._ptr(ws) if ws is not None else None)
+        if self._fcache is not None and role:
+            status = lib.cbdgam_b200_advance_stage_cached(*args, self._ptr(self._fcache), role, stream)
+        else:
+            status = lib.cbdgam_b200_advance_stage(*args, stream)
+        self._check(status, "advance_stage")
+
+    @staticmethod
+    def _same_masses(a, b):
+        """Whether two stages' masses agree in every input of the cached
+        values (position, mass, softening)."""
+        return all(x.x == y.x and x.y == y.y and x.mass == y.mass and x.softening_length == y.softening_length
+                   for x, y in zip(a.mass, b.mass))
 
     def _point_masses(self, t):
         masses = self.__dict__.get("_mass_cache")
@@ -309,15 +336,14 @@ class Solver(SolverBase):
         a_buf, b_buf = self._buf
         s1 = self._stage(t0, 0.0, dt)
         self._result[:1].zero_()
-        self._check(lib.cbdgam_b200_advance_stage(ctypes.byref(g), ctypes.byref(s1), self._ptr(a_buf), None,
-                                                  self._ptr(b_buf), None, stream), "advance_stage")
+        self._launch(s1, a_buf, None, b_buf, None, 2, stream)
         if self._stage_hook is not None:
             self._stage_hook(0, b_buf)
-        # the second stage's orbit is solved while the first stage runs
+        # the second stage's orbit is solved while the first stage runs; it
+        # fills the face cache when its masses are the step's end masses
         s2 = self._stage(t1, 0.5, dt)
-        self._check(lib.cbdgam_b200_advance_stage(ctypes.byref(g), ctypes.byref(s2), self._ptr(b_buf),
-                                                  self._ptr(a_buf), self._ptr(a_buf), self._ptr(self._result),
-                                                  stream), "advance_stage")
+        writer = self._same_masses(s2, self._stage(t2, 0.5, dt))
+        self._launch(s2, b_buf, a_buf, a_buf, self._result, 1 if writer else 0, stream)
         if self._stage_hook is not None:
             self._stage_hook(1, a_buf)
         self._time = t2

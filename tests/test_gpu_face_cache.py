@@ -138,3 +138,27 @@ def test_cached_entry_rejects_a_misaligned_cache():
     assert lib.cbdiso_b200_advance_stage_cached(*args, s._ptr(s._fcache), 3, s._stream()) == 1
     assert int(s._lib.cbdiso_b200_face_cache_bytes(ctypes.byref(s._grid))) == \
         8 * (32 + 2 * (65 * 64 + 64 * 65 + 64 * 64))
+
+
+@pytest.mark.parametrize("name", ["gam_n64", "gam_n40_soft_inviscid", "gam_n48_cool_p2", "gam_n256"])
+def test_gamma_law_bit_identical_with_and_without_cache(name):
+    """The gamma-law solver's cache (scale-height geometry at faces and
+    centres, gravity factors with constant softening) changes no bit."""
+    from cases import gam_names
+    from test_gpu_gamma import gam_solver
+
+    assert name in gam_names()
+    d = load(name)
+    on, off = gam_solver(d, face_cache=True), gam_solver(d, face_cache=False)
+    assert on._fcache is not None and off._fcache is None
+    cfl = d["meta"]["cfl"]
+    for _ in range(10):
+        dt = on.mesh.min_spacing() / on.maximum_wavespeed() * cfl
+        assert dt == off.mesh.min_spacing() / off.maximum_wavespeed() * cfl
+        on.advance(dt)
+        off.advance(dt)
+        assert on.reductions() == off.reductions()
+    assert np.array_equal(on.solution, off.solution)
+    torch.cuda.synchronize()
+    assert float(on._fcache[0]) == 20260102.5  # the second stages wrote their values
+
