@@ -414,11 +414,6 @@ class Solver(SolverBase):
         if masses is None or masses.physics is not self._physics:
             masses = self._mass_cache = MassCache(self._physics)
         return masses(t)
-        masses = self._physics.point_masses(t)
-        cache.append((t, masses))
-        if len(cache) > 4:
-            cache.pop(0)
-        return masses
 
     # ------------------------------------------------------------------
     # device-resident stepping
