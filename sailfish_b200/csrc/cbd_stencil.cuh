@@ -627,6 +627,7 @@ struct StageArgs {
 // ---------------------------------------------------------------------------
 
 enum { ROLE_NONE = 0, ROLE_WRITER = 1, ROLE_READER = 2 };
+// what one march (march_tile's COP) does with the cache, by role
 enum { CACHE_NONE = 0, CACHE_WRITE = 1, CACHE_READ = 2 };
 constexpr int CACHE_HEADER = 32;  // doubles
 constexpr int CACHE_KEY = 20;     // doubles of the header in use
