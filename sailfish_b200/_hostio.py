@@ -32,7 +32,9 @@ _pool = None
 
 
 def _threads():
-    return max(1, min(8, os.cpu_count() or 1))
+    # the copies into a new array are bound by its page faults, which scale
+    # with the threads taking them
+    return max(1, min(16, os.cpu_count() or 1))
 
 
 def _get_pool():
