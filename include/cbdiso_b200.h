@@ -225,13 +225,10 @@ int cbdiso_b200_stage_record(const cbd_grid_t *grid, const cbd_stage_t *stage, c
  *      stage recomputes them when the key does not match the stage's masses.
  * In EXACT precision the results are bit-identical to
  * cbdiso_b200_advance_stage (in FMA and FAST the compiler may contract the code
- * paths differently: equal to rounding). Both roles also take the Keplerian
- * buffer's per-zone terms, which depend on the mesh alone, from a table in the
- * same buffer (filled by the same pass when its own key does not match).
- * `face_cache` is a caller-owned, 16-byte aligned device buffer of
- * cbdiso_b200_face_cache_bytes(grid) bytes for this grid only; zero its first
- * 512 bytes before its first use. Calls on one cache must be ordered on one
- * stream. */
+ * paths differently: equal to rounding). `face_cache` is a caller-owned,
+ * 16-byte aligned device buffer of cbdiso_b200_face_cache_bytes(grid) bytes for
+ * this grid only; zero its first 256 bytes before its first use. Calls on one
+ * cache must be ordered on one stream. */
 size_t cbdiso_b200_face_cache_bytes(const cbd_grid_t *grid);
 int cbdiso_b200_advance_stage_cached(
     const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
@@ -334,7 +331,7 @@ int cbdiso_b200_batched_stage(const void *disks, int num_disks, int total_units,
  * preceded by a fill pass per disk). Disk d's cache lies at face_cache + its
  * record's cache offset, set by cbdiso_b200_batch_disk_set_face_cache (an even
  * number of doubles); it holds cbdiso_b200_face_cache_bytes(its grid) bytes
- * with its first 512 bytes zeroed before the first use, and `face_cache` is
+ * with its first 256 bytes zeroed before the first use, and `face_cache` is
  * 16-byte aligned. A reader needs a cache for every disk: it leaves the tiles
  * of a disk without one unwritten. No counterpart in the reference. */
 int cbdiso_b200_batch_disk_set_face_cache(void *record, long long cache_offset);

@@ -146,7 +146,7 @@ class BatchedSolver:
         if face_cache:
             self._fcache = torch.empty(cache_offset, **f64)
             for c in cache_offsets:
-                self._fcache[c:c + 64].zero_()
+                self._fcache[c:c + 32].zero_()
         for i, s in enumerate(self.solvers):
             self._buf[0][self.offsets[i]:self.offsets[i] + s._buf[0].numel()] = s._buf[0].reshape(-1)
         self._disks_dev = torch.frombuffer(records, dtype=torch.uint8).to(self.device)

@@ -239,7 +239,7 @@ class Solver(SolverBase):
         self._fcache = None
         if options.face_cache:
             self._fcache = torch.empty(int(self._lib.cbdiso_b200_face_cache_bytes(ctypes.byref(g))) // 8, **f64)
-            self._fcache[:64].zero_()
+            self._fcache[:32].zero_()
         self._result = torch.zeros(1 + 2 * _capi.MAX_DIAG, **f64)
         self._result_host = torch.zeros(1 + 2 * _capi.MAX_DIAG, dtype=torch.float64).pin_memory()
 

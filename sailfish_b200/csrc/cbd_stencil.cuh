@@ -336,30 +336,6 @@ __device__ __forceinline__ void buffer_source(const Consts &k, const StageDev &s
     du[2] -= (u[2] - t2) * rate * dt;
 }
 
-// The terms of buffer_source that depend on the zone alone: the Keplerian
-// target momenta t_1, t_2 and the relaxation rate, with the same operations;
-// rate = -1 where buffer_source adds nothing.
-template <bool FAST>
-__device__ __forceinline__ void buffer_terms(const Consts &k, const StageDev &st, double x, double y, double &t1,
-                                             double &t2, double &rate)
-{
-    t1 = t2 = 0.0;
-    rate = -1.0;
-    if (!k.buffer_on)
-        return;
-    const double r2 = x * x + y * y;
-    if (!(r2 > k.buf_lo2))
-        return;
-    const double rc = sqrt(r2);
-    if (!(rc > k.buf_onset))
-        return;
-    const double yr = FAST ? 1.0 / rc : __drcp_rn(rc);
-    const double vk = sqrt(div_by<FAST>(st.buffer_mass, rc, yr));
-    t1 = k.buf_sigma * div_by<FAST>(-y, rc, yr) * vk;
-    t2 = k.buf_sigma * div_by<FAST>(+x, rc, yr) * vk;
-    rate = div_by<FAST>(st.buffer_k * (rc - k.buf_onset), k.buf_span, k.inv_buf_span);
-}
-
 // cbdiso_2d.c:268-283
 template <bool FAST>
 __device__ __forceinline__ void cons_to_prim(const double *u, double *p, const Consts &k)
@@ -653,23 +629,12 @@ struct StageArgs {
 enum { ROLE_NONE = 0, ROLE_WRITER = 1, ROLE_READER = 2 };
 // what one march (march_tile's COP) does with the cache, by role
 enum { CACHE_NONE = 0, CACHE_WRITE = 1, CACHE_READ = 2 };
-constexpr int CACHE_HEADER = 64;  // doubles
-constexpr int CACHE_KEY = 20;     // doubles of the header in use by the face key
-constexpr int STATIC_KEY_AT = 32; // the buffer table's key
-constexpr int STATIC_KEY = 16;
-constexpr int FILL_COUNTER_AT = 56;  // the fill kernel's CTA counter (one 32-bit word, zero between launches)
+constexpr int CACHE_HEADER = 32;  // doubles
+constexpr int CACHE_KEY = 20;     // doubles of the header in use
 
 __host__ __device__ inline size_t face_cache_doubles(int ni, int nj)
 {
-    return CACHE_HEADER + 2 * ((size_t)(ni + 1) * nj + (size_t)ni * (nj + 1) + (size_t)ni * nj) +
-           3 * (size_t)ni * nj;
-}
-
-// The buffer table after the face arrays: (t_1, t_2) pairs ni x nj, then the
-// rates ni x nj (negative outside the buffer).
-__device__ __forceinline__ double *buffer_pairs(double *fc, int ni, int nj)
-{
-    return fc + CACHE_HEADER + 2 * ((size_t)(ni + 1) * nj + (size_t)ni * (nj + 1) + (size_t)ni * nj);
+    return CACHE_HEADER + 2 * ((size_t)(ni + 1) * nj + (size_t)ni * (nj + 1) + (size_t)ni * nj);
 }
 
 // The key: a format tag, the precision, then every input of the cached values.
@@ -704,41 +669,6 @@ __device__ __forceinline__ double cache_key_value(const Consts &k, const MassDev
 __device__ __forceinline__ bool same_bits(double a, double b)
 {
     return __double_as_longlong(a) == __double_as_longlong(b);
-}
-
-// The buffer table's key: a format tag, the precision, then every input of
-// the buffer terms (mesh, buffer constants, the stage's central mass and
-// driving factor, constant over a run).
-template <int PREC>
-__device__ __forceinline__ double static_key_value(const Consts &k, const StageDev &st, int v)
-{
-    switch (v) {
-    case 0: return 20260104.5;
-    case 1: return (double)PREC;
-    case 2: return (double)k.ni;
-    case 3: return (double)k.nj;
-    case 4: return k.xl;
-    case 5: return k.yl;
-    case 6: return k.dx;
-    case 7: return k.dy;
-    case 8: return (double)k.buffer_on;
-    case 9: return k.buf_sigma;
-    case 10: return k.buf_onset;
-    case 11: return k.buf_lo2;
-    case 12: return k.buf_span;
-    case 13: return k.inv_buf_span;
-    case 14: return st.buffer_mass;
-    default: return st.buffer_k;
-    }
-}
-
-template <int PREC>
-__device__ bool static_key_matches(const Consts &k, const StageDev &st, const double *fc)
-{
-    for (int v = 0; v < STATIC_KEY; ++v)
-        if (!same_bits(fc[STATIC_KEY_AT + v], static_key_value<PREC>(k, st, v)))
-            return false;
-    return true;
 }
 
 template <int PREC>
@@ -800,7 +730,7 @@ __device__ __forceinline__ StageSmem<BJ> &stage_smem()
 // zones are accumulated into `acc`. `COP` (CACHE_*) says what the tile does
 // with args.fcache; with CACHE_WRITE it stores only if `store`. All threads of
 // the block must call it.
-template <int BJ, bool FAST, int COP = CACHE_NONE, bool BT = false>
+template <int BJ, bool FAST, int COP = CACHE_NONE>
 __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, const StageArgs &args, int c0,
                                            int width, int r0, double (&acc)[PARTIAL_STRIDE], bool store = false)
 {
@@ -1035,22 +965,7 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 }
             }
             const double dt = st.dt;
-            if (BT) {
-                // the buffer terms from the table (filled before the launch)
-                if (k.buffer_on && xc * xc + yc * yc > k.buf_lo2) {
-                    const double *bp = buffer_pairs(args.fcache, ni, nj);
-                    const size_t z = (size_t)r * nj + j;
-                    const double rate = bp[2 * (size_t)ni * nj + z];
-                    const double2 t = cache_load(bp + 2 * z);
-                    if (rate >= 0.0) {
-                        du[0] -= (u[0] - k.buf_sigma) * rate * dt;
-                        du[1] -= (u[1] - t.x) * rate * dt;
-                        du[2] -= (u[2] - t.y) * rate * dt;
-                    }
-                }
-            } else {
-                buffer_source<FAST>(k, st, xc, yc, dt, u, du);
-            }
+            buffer_source<FAST>(k, st, xc, yc, dt, u, du);
             if (cop == CACHE_READ) {
                 mass_source<FAST>(st.m[0], xc, yc, dt, pc, du, &c_z.x);
                 mass_source<FAST>(st.m[1], xc, yc, dt, pc, du, &c_z.y);
@@ -1125,9 +1040,9 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
         __syncthreads();
         const bool store = cache_write_check<PREC>(k, st, args.fcache,
                                                    threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0);
-        march_tile<BJ, FAST, CACHE_WRITE, true>(k, st, args, c0, BJ, r0, acc, store);
+        march_tile<BJ, FAST, CACHE_WRITE>(k, st, args, c0, BJ, r0, acc, store);
     } else if (ROLE == ROLE_READER) {
-        march_tile<BJ, FAST, CACHE_READ, true>(k, st, args, c0, BJ, r0, acc);
+        march_tile<BJ, FAST, CACHE_READ>(k, st, args, c0, BJ, r0, acc);
     } else {
         march_tile<BJ, FAST, CACHE_NONE>(k, st, args, c0, BJ, r0, acc);
     }
@@ -1182,66 +1097,26 @@ __device__ void face_cache_fill_rows(const Consts &k, const StageDev &st, double
     }
 }
 
-// Rows i = first, first + stride, ... (0 <= i < ni) of the buffer table:
-// every zone's buffer_terms.
-template <bool FAST>
-__device__ void buffer_table_fill_rows(const Consts &k, const StageDev &st, double *fc, int first, int stride)
-{
-    const int ni = k.ni, nj = k.nj;
-    double *const bp = buffer_pairs(fc, ni, nj);
-    double *const br = bp + 2 * (size_t)ni * nj;
-    for (int i = first; i < ni; i += stride) {
-        for (int j = threadIdx.x; j < nj; j += blockDim.x) {
-            const double xc = k.xl + ((double)i + 0.5) * k.dx;
-            const double yc = k.yl + ((double)j + 0.5) * k.dy;
-            double t1, t2, rate;
-            buffer_terms<FAST>(k, st, xc, yc, t1, t2, rate);
-            const size_t z = (size_t)i * nj + j;
-            cache_store(bp + 2 * z, t1, t2);
-            br[z] = rate;
-        }
-    }
-}
-
-// Makes the cache valid for a stage launch: the buffer table (for readers
-// and writers) and, with `faces` (readers), the face values. Each part whose
-// key does not match the stage is marked invalid (no later key check passes
-// on what follows) and filled for it. Grid: any number of 128-thread CTAs,
-// each taking rows i = blockIdx.x, blockIdx.x + gridDim.x, ... .
+// Makes the face cache valid for a reader stage: when the key does not match
+// the stage's masses, marks it invalid (no later key check passes on what
+// follows) and fills it for those masses. Grid: any number of 128-thread
+// CTAs, each taking rows i = blockIdx.x, blockIdx.x + gridDim.x, ... .
 template <int PREC>
 __global__ void __launch_bounds__(128) face_cache_fill_kernel(const Consts k, const StageDev st_param,
-                                                              const StageDev *stage_dev, double *fc, int faces)
+                                                              const StageDev *stage_dev, double *fc)
 {
     __shared__ StageDev st;
-    __shared__ int fill_faces, fill_table;
+    __shared__ int fill;
     if (threadIdx.x == 0) {
         st = stage_dev ? *stage_dev : st_param;
-        fill_faces = faces && !cache_key_matches<PREC>(k, st, fc);
-        fill_table = k.buffer_on && !static_key_matches<PREC>(k, st, fc);
-        if (fill_faces)
+        fill = cache_key_matches<PREC>(k, st, fc) ? 0 : 1;
+        if (fill)
             fc[0] = 0.0;
-        if (fill_table)
-            fc[STATIC_KEY_AT] = 0.0;
     }
     __syncthreads();
-    if (fill_faces)
-        face_cache_fill_rows<PREC == CBD_PRECISION_FAST>(k, st, fc, blockIdx.x, gridDim.x);
-    if (!fill_table)
+    if (!fill)
         return;
-    buffer_table_fill_rows<PREC == CBD_PRECISION_FAST>(k, st, fc, blockIdx.x, gridDim.x);
-    // every CTA fills (the key matched for none of them, or for all): the
-    // last one to finish writes the table's key and re-arms the counter
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned int *counter = reinterpret_cast<unsigned int *>(fc + FILL_COUNTER_AT);
-        __threadfence();
-        if (atomicAdd(counter, 1u) == gridDim.x - 1) {
-            __threadfence();
-            for (int v = 0; v < STATIC_KEY; ++v)
-                fc[STATIC_KEY_AT + v] = static_key_value<PREC>(k, st, v);
-            *counter = 0u;
-        }
-    }
+    face_cache_fill_rows<PREC == CBD_PRECISION_FAST>(k, st, fc, blockIdx.x, gridDim.x);
 }
 
 }  // namespace cbd

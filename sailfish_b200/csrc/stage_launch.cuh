@@ -10,19 +10,17 @@ template <int BJ, int MINB, int PREC>
 cudaError_t launch_one(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a, int role,
                        cudaStream_t stream)
 {
-    if (role == ROLE_WRITER || role == ROLE_READER) {
-        // the buffer table for both roles, the face values for a reader; at
-        // most four CTAs per SM, each over rows i, i + grid, ...
-        const int rows = k.ni + 1 < 148 * 4 ? k.ni + 1 : 148 * 4;
-        face_cache_fill_kernel<PREC><<<rows, 128, 0, stream>>>(k, st, a.stage_dev, a.fcache, role == ROLE_READER);
-    }
     switch (role) {
     case ROLE_WRITER:
         stage_kernel<BJ, MINB, PREC, ROLE_WRITER><<<s.grid, BJ, 0, stream>>>(k, st, a);
         break;
-    case ROLE_READER:
+    case ROLE_READER: {
+        // at most four CTAs per SM, each over rows i, i + grid, ...
+        const int rows = k.ni + 1 < 148 * 4 ? k.ni + 1 : 148 * 4;
+        face_cache_fill_kernel<PREC><<<rows, 128, 0, stream>>>(k, st, a.stage_dev, a.fcache);
         stage_kernel<BJ, MINB, PREC, ROLE_READER><<<s.grid, BJ, 0, stream>>>(k, st, a);
         break;
+    }
     default:
         stage_kernel<BJ, MINB, PREC, ROLE_NONE><<<s.grid, BJ, 0, stream>>>(k, st, a);
         break;

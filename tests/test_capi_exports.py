@@ -54,9 +54,8 @@ def test_face_cache_and_adjoint_settings_host_checks():
     (nothing is launched)."""
     lib = _capi.lib()
     g = _capi.Grid(ni=8, nj=6, xl=-1.0, xr=1.0, yl=-1.0, yr=1.0, eos_type=2, mach2=100.0, plm_theta=1.5)
-    # header, (cs^2, cs) pairs of every x- and y-face and (g_1, g_2) of every
-    # zone, the buffer table's (t_1, t_2) and rate of every zone
-    assert lib.cbdiso_b200_face_cache_bytes(ctypes.byref(g)) == 8 * (64 + 2 * (9 * 6 + 8 * 7 + 8 * 6) + 3 * 48)
+    # header, (cs^2, cs) pairs of every x- and y-face and (g_1, g_2) of every zone
+    assert lib.cbdiso_b200_face_cache_bytes(ctypes.byref(g)) == 8 * (32 + 2 * (9 * 6 + 8 * 7 + 8 * 6))
     assert lib.cbdiso_b200_face_cache_bytes(ctypes.byref(_capi.Grid(ni=0, nj=6))) == 0
     st = _capi.Stage()
     a, b = ctypes.c_void_p(0x1000), ctypes.c_void_p(0x2000)
