@@ -31,9 +31,9 @@ sys.path.insert(0, ROOT)
 BYTES_PER_ZONE_UPDATE = 120.0  # RK2 x FP64 x 3 fields: 48 B stage 1 + 72 B stage 2
 # DRAM bytes per zone and stage launch measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum, mean of an RK2 stage 1 launch reading the face cache
-# and a stage 2 launch writing it, at 2048^2,
-# profiles/stage_kernels_2048_face_cache.md); scaled by the zone count. It is
-# above the algorithmic 60 B because of the cache's 48 B per zone and step.
+# and a stage 2 launch writing it, one capture of each at 2048^2); scaled by
+# the zone count. It is above the algorithmic 60 B because of the cache's 48 B
+# per zone and step.
 NCU_TRAFFIC_PER_ZONE_LAUNCH = (314.69e6 + 75.12e6 + 223.57e6 + 260.25e6) / 2 / 2048 ** 2
 # FP64 thread-instructions (DADD + DMUL + DFMA) per zone and stage launch, mean
 # of the same two launches (ncu, the sum of
@@ -144,15 +144,18 @@ class ClockSampler:
     def __init__(self, device_index):
         self.device_index = device_index
         self.proc = None
+        self.error = None
+        self.lines = []
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device_index), f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except (OSError, FileNotFoundError):
+                stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+        except (OSError, FileNotFoundError) as e:
             self.proc = None
+            self.error = f"nvidia-smi could not be started: {e}"
         return self
 
     def __exit__(self, *exc):
@@ -160,11 +163,14 @@ class ClockSampler:
         if self.proc is not None:
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                out, err = self.proc.communicate(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
+                out, err = self.proc.communicate()
             self.lines = [l for l in out.splitlines() if l.strip()]
+            if not self.lines:
+                self.error = ("nvidia-smi returned no samples (exit code "
+                              f"{self.proc.returncode}): {err.strip()[:200] or 'no message'}")
 
     def summary(self):
         sm, smax, reasons = [], None, set()
@@ -182,7 +188,9 @@ class ClockSampler:
                 if flag.lower() == "active":
                     reasons.add(name)
         if not sm:
-            return None
+            # never a silent null: say why there is no clock record
+            why = self.error or f"no parsable samples among {len(self.lines)} lines"
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "unavailable": why}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
                 "samples": len(sm)}
 
@@ -345,18 +353,25 @@ def run_ours(args, rank, world):
     # end-to-end through the public API, from host data: upload the initial
     # state, run the steps, download the final state (amortised per step)
     # the same number of steps as the device-timed loop: a run's fixed costs
-    # (state upload, solver set-up, state download) are spread as in `value`
+    # (state upload, solver set-up, state download) are spread as in `value`.
+    # The phases are timed separately too (synchronised at their
+    # boundaries), so that the fixed cost and the per-step cost are known
+    # whatever the step count.
     e2e_steps = max(1, args.steps)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s2 = fresh()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
     for _ in range(e2e_steps):
         dt = mesh.min_spacing() / s2.maximum_wavespeed() * CFL
         s2.advance(dt)
         s2.reductions()
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
     final = s2.solution
-    t1 = time.perf_counter()
-    e2e_elapsed = t1 - t0
+    t3 = time.perf_counter()
+    e2e_elapsed = t3 - t0
     if dist:
         t = torch.tensor([e2e_elapsed], device="cuda", dtype=torch.float64)
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
@@ -364,6 +379,10 @@ def run_ours(args, rank, world):
     e2e_value = zones * e2e_steps * world / e2e_elapsed  # host-driven loop: one dt round trip per step
     e2e_h2d = (s2.h2d_bytes + prim.nbytes) / e2e_steps
     e2e_d2h = (s2.d2h_bytes + final.nbytes) / e2e_steps
+    e2e_phases = {"setup_and_upload_ms": (t1 - t0) * 1e3, "steps_ms": (t2 - t1) * 1e3,
+                  "download_ms": (t3 - t2) * 1e3, "fixed_ms": (t1 - t0 + t3 - t2) * 1e3,
+                  "per_step_ms": (t2 - t1) * 1e3 / e2e_steps}
+    e2e_phases.update(transfer_floor(prim.nbytes))
     del s2
 
     kernel_s = stage_kernel_time(solver)
@@ -387,9 +406,10 @@ def run_ours(args, rank, world):
                    "l2": "state arrays (403 MB each at 4096^2) exceed L2; no flush",
                    "face_cache": not args.no_face_cache,
                    "parallelism": "replicas" if world > 1 else "single"},
-        "e2e": {"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": int(e2e_h2d),
-                "d2h_bytes_per_step": int(e2e_d2h), "steps": e2e_steps,
-                "includes": "initial-state upload, public-API driver loop, final-state download"},
+        "e2e": dict({"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": int(e2e_h2d),
+                     "d2h_bytes_per_step": int(e2e_d2h), "steps": e2e_steps,
+                     "includes": "solver set-up and initial-state upload, public-API driver loop, final-state "
+                                 "download"}, **e2e_phases),
         "step_io": {"h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "note": "value loop: stepper record in, time series out, per step"},
         # per step: prologue, first stage (with its face-cache fill pass when
@@ -400,6 +420,66 @@ def run_ours(args, rank, world):
         "clocks": clocks.summary(),
     }
     return line
+
+
+def transfer_floor(nbytes, repeats=3):
+    """Pinned host <-> device copy times of one state's bytes on this box
+    (best of `repeats`, CUDA events): the least that an upload plus a download
+    of the state can cost."""
+    import torch
+
+    host = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    dev = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = {}
+    for name, (dst, src) in (("h2d", (dev, host)), ("d2h", (host, dev))):
+        ms = float("inf")
+        for _ in range(repeats):
+            start.record()
+            dst.copy_(src, non_blocking=True)
+            stop.record()
+            torch.cuda.synchronize()
+            ms = min(ms, start.elapsed_time(stop))
+        best[name] = ms
+    del host, dev
+    return {"pinned_h2d_ms": best["h2d"], "pinned_d2h_ms": best["d2h"],
+            "pinned_h2d_gbs": nbytes / best["h2d"] / 1e6, "pinned_d2h_gbs": nbytes / best["d2h"] / 1e6,
+            "transfer_floor_ms": best["h2d"] + best["d2h"]}
+
+
+def sizes_extra(args, sizes=(1024, 2048), steps=100):
+    """The other two grid sizes of the plain-solver throughput configuration:
+    the same device-resident loop as `value` (face cache on, EXACT), and the
+    stage kernel's launch time against the HBM copy bandwidth."""
+    import torch
+
+    from sailfish_b200 import make_solver
+
+    out = {}
+    peak, peak_kind = measured_peaks()
+    for n in sizes:
+        setup, mesh, prim = initial_state(n, args.seed)
+        physics = setup.physics
+        physics["diagnostics"] = DIAGNOSTICS
+        s = make_solver("cbdiso_2d", physics, dict(rk_order=2, plm_theta=THETA, precision=args.precision),
+                        setup=setup, mesh=mesh, solution=prim)
+        s.run(16, cfl=CFL)
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        s.run(steps, cfl=CFL)
+        stop.record()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(stop) / steps
+        kernel_s = stage_kernel_time(s)
+        achieved = BYTES_PER_ZONE_UPDATE / 2 * n * n / kernel_s / 1e9
+        out[str(n)] = {"value": n * n / (ms * 1e-3), "unit": "zone-updates/s", "ms_per_step": ms,
+                       "steps": steps, "kernel_ms": round(kernel_s * 1e3, 4),
+                       "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                                    "frac": round(achieved / peak, 4), "peak_source": peak_kind}}
+        del s
+    out["note"] = "same workload and loop as `value` at the configuration's other grid sizes"
+    return out
 
 
 def precision_extra(args, steps=50):
@@ -457,43 +537,60 @@ def batched_extra(plain_value):
             "vs_single_disk_value": value / plain_value}
 
 
-def adjoint_extra():
-    """Forward + gradient of the time-averaged accretion rate at 512^2 over
-    400 RK2 steps (dt frozen), per step, against a plain device step."""
+def _event_ms(fn):
+    """Device time of fn() on the current stream, CUDA events around it."""
+    import torch
+
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    fn()
+    stop.record()
+    torch.cuda.synchronize()
+    return start.elapsed_time(stop)
+
+
+def adjoint_extra(cases=((512, 400), (2048, 100))):
+    """Forward + gradient of the time-averaged accretion rate over RK2 steps
+    (dt frozen), per step, against a plain device step of the same grid, in
+    both sweep forms: `checkpointed` keeps one state every 20 steps and
+    recomputes each segment in the reverse sweep (the configured form), and
+    `stored` keeps every stage state of the forward run. 512^2 x 400 steps is
+    the configured size; 2048^2 (100 steps) is where the plain step is
+    throughput-bound. Timed with CUDA events on the launching stream."""
     import torch
 
     from sailfish_b200.adjoint import AdjointRun, Params
 
-    run = AdjointRun(resolution=512, steps=400, checkpoint_every=20)
     params = Params(0.5, 0.1, 1e-3, 10.0)
-    prim = run.initial_state(seed=0)
-    run.forward(prim, params, freeze=True, keep=True)
-    run.gradient((1.0, 0.0))
-    # warm-up with the frozen dt sequence (records this form's CUDA graphs)
-    run.forward(prim, params, keep=True)
-    run.gradient((1.0, 0.0))
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    run.forward(prim, params, keep=True)
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    run.gradient((1.0, 0.0))
-    torch.cuda.synchronize()
-    t2 = time.perf_counter()
-    solver = run._solver(params, prim)
-    solver.run(16, cfl=run.cfl)
-    torch.cuda.synchronize()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record()
-    solver.run(run.steps, cfl=run.cfl)
-    stop.record()
-    torch.cuda.synchronize()
-    plain = start.elapsed_time(stop) / run.steps
-    fwd, adj = (t1 - t0) * 1e3 / run.steps, (t2 - t1) * 1e3 / run.steps
-    return {"workload": "512^2, q 0.5, e 0.1, 400 RK2 steps, d(mean accretion)/d(Sigma_0, q, e, nu, sink rate)",
-            "forward_ms_per_step": fwd, "gradient_ms_per_step": adj, "plain_ms_per_step": plain,
-            "forward_plus_gradient_vs_plain": (fwd + adj) / plain,
-            "stored_states": run._fwd["trajectory"] is not None, "timing": "host wall clock around each call"}
+    out = {"workload": "q 0.5, e 0.1, RK2, d(mean accretion)/d(Sigma_0, q, e, nu, sink rate), checkpoint every 20",
+           "timing": "CUDA events on the launching stream"}
+    for n, steps in cases:
+        block = {"steps": steps}
+        plain = None
+        for form, store in (("checkpointed", False), ("stored", True)):
+            run = AdjointRun(resolution=n, steps=steps, checkpoint_every=20, store_states=store)
+            prim = run.initial_state(seed=0)
+            run.forward(prim, params, freeze=True, keep=True)
+            run.gradient((1.0, 0.0))
+            # warm-up with the frozen dt sequence (records this form's CUDA graphs)
+            run.forward(prim, params, keep=True)
+            run.gradient((1.0, 0.0))
+            fwd = _event_ms(lambda: run.forward(prim, params, keep=True)) / steps
+            adj = _event_ms(lambda: run.gradient((1.0, 0.0))) / steps
+            if plain is None:
+                solver = run._solver(params, prim)
+                solver.run(16, cfl=run.cfl)
+                plain = _event_ms(lambda: solver.run(steps, cfl=run.cfl)) / steps
+                del solver
+            block[form] = {"forward_ms_per_step": fwd, "gradient_ms_per_step": adj,
+                           "forward_plus_gradient_vs_plain": (fwd + adj) / plain,
+                           "stored_states": run._fwd["trajectory"] is not None}
+            del run
+            torch.cuda.empty_cache()
+        block["plain_ms_per_step"] = plain
+        out[str(n)] = block
+    return out
 
 
 def batched_adjoint_extra():
@@ -739,6 +836,7 @@ def main():
     else:
         line = run_ours(args, rank, world)
         if world == 1 and not args.no_extras:
+            line["sizes"] = sizes_extra(args)
             line["precision_modes"] = precision_extra(args)
             line["batched"] = batched_extra(line["value"])
             line["adjoint"] = adjoint_extra()

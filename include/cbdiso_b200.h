@@ -248,13 +248,17 @@ int cbdiso_b200_advance_stage_cached(
  * device memory (each GPU that loads the library holds it until the process
  * exits); the caller still passes the state arrays and `result`.
  *
- * Limit: grids whose cbdiso_b200_scratch_bytes() exceeds 5 MiB are rejected
- * with CBD_ERR_CAPACITY before anything is launched; 4096 x 4096 fits.
+ * Limit: a call with an epilogue on a grid whose cbdiso_b200_scratch_bytes()
+ * exceeds 5 MiB is rejected with CBD_ERR_CAPACITY before anything is
+ * launched; 4096 x 4096 fits. A call without an epilogue uses no scratch and
+ * has no such limit.
  * The first call with an epilogue on a device looks up the array's device
- * address for that device, so make that first call before any stream
- * capture. All calls on a device share the array, which keeps the last
- * call's contents (each call clears the counter it needs zeroed): calls that
- * overlap on the GPU, from different streams or threads, race on it. */
+ * address for that device and keeps it for the life of the process, so make
+ * that first call before any stream capture, and make no call after
+ * cudaDeviceReset (the kept address would be stale). All calls on a device
+ * share the array, which keeps the last call's contents (each call clears the
+ * counter it needs zeroed): calls that overlap on the GPU, from different
+ * streams or threads, race on it. */
 int cbdiso_b200_advance_stage_noalloc(
     const cbd_grid_t *grid, const cbd_stage_t *stage, const void *stage_dev,
     const double *primitive_rd, const double *primitive_n, double *primitive_wr,
@@ -297,7 +301,13 @@ int cbdiso_b200_stepper_attach(void *stepper, const double *dt_sequence, int dt_
  * dt = min_spacing / max wavespeed * cfl, solves the Kepler orbit at every
  * stage time and at the end of the step, and writes the stage records that
  * cbdiso_b200_advance_stage reads as `stage_dev`. A Kepler solve that does
- * not converge sets the stepper's status to CBD_ERR_KEPLER and stops it. */
+ * not converge sets the stepper's status to CBD_ERR_KEPLER and stops it. A
+ * dt that is not finite and positive (a NaN, infinite or zero wavespeed, or
+ * such an entry of a frozen dt sequence) sets CBD_ERR_NONFINITE, stops the
+ * stepper and marks the step's stage records halted: stage launches that
+ * read them return without touching any array, so a captured sequence of
+ * steps leaves the state as it was before the failing step. (The reference's
+ * driver has no such check, sailfish/driver.py:508-510.) */
 int cbdiso_b200_step_prologue(void *stepper_dev, const double *result, void *records_dev, double *series,
                               int num_values, int finalize, void *stream);
 

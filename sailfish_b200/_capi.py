@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcbdiso_b200.so")
 
 CBD_OK = 0
+NONFINITE = 3  # CBD_ERR_NONFINITE
 STATUS = {
     0: "success",
     1: "invalid argument",

@@ -26,6 +26,7 @@ compile-time PLM_THETA, cbdgam_2d.c:15).
 from __future__ import annotations
 
 import ctypes
+import math
 from logging import getLogger
 from typing import NamedTuple
 
@@ -313,16 +314,23 @@ class Solver(SolverBase):
         return 0.4
 
     def maximum_wavespeed(self):
-        """Largest |v +- cs| over the grid (cbdgam_2d.c:685-708)."""
+        """Largest |v +- cs| over the grid (cbdgam_2d.c:685-708). Raises
+        CbdError (CBD_ERR_NONFINITE) when it is not finite (a NaN or infinity
+        in the state), where the reference returns it and runs on."""
         if not self._ws_valid:
             self._reduce([])
-        return float(self._read(1)[0])
+        value = float(self._read(1)[0])
+        if not math.isfinite(value):
+            raise _capi.CbdError(_capi.NONFINITE, "maximum_wavespeed")
+        return value
 
     def advance(self, dt):
         """One RK2 step (cbdgam_2d.py:473-489): two stage kernels, masses at
         each stage's start time, the stage times as the reference updates
         them."""
         dt = float(dt)
+        if not math.isfinite(dt):
+            raise _capi.CbdError(_capi.NONFINITE, "advance: time step")
         lib, g = self._lib, self._grid
         stream = self._stream()
         t0 = self._time

@@ -340,10 +340,16 @@ class Solver(SolverBase):
         return 0.4
 
     def maximum_wavespeed(self):
-        """Largest |v +- cs| over the grid, with point masses at the current time."""
+        """Largest |v +- cs| over the grid, with point masses at the current
+        time. Raises CbdError (CBD_ERR_NONFINITE) when it is not finite: the
+        state holds a NaN or infinity, from which the driver's CFL rule would
+        take a NaN time step (the reference returns the value and runs on)."""
         if not self._result_valid:
             self._reduce_now(True, self._device_diags if self._fused else [])
-        return float(self._read_result()[0])
+        value = float(self._read_result()[0])
+        if not math.isfinite(value):
+            raise _capi.CbdError(_capi.NONFINITE, "maximum_wavespeed")
+        return value
 
     def advance(self, dt):
         """One step of the configured RK order. The first stage is launched
@@ -353,6 +359,8 @@ class Solver(SolverBase):
         import torch
 
         dt = float(dt)
+        if not math.isfinite(dt):
+            raise _capi.CbdError(_capi.NONFINITE, "advance: time step")
         weights = RK_WEIGHTS[self._options.rk_order]
         time0 = self._time
         lib, g = self._lib, self._grid

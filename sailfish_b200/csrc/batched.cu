@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(128) batched_finalize_kernel(const DiskDev *di
         const double *p = partials + (size_t)(D.unit_begin + u) * PARTIAL_STRIDE;
 #pragma unroll
         for (int v = 0; v < PARTIAL_STRIDE; ++v)
-            acc[v] = v == 0 ? greater(acc[v], p[v]) : acc[v] + p[v];
+            acc[v] = v == 0 ? max_nan(acc[v], p[v]) : acc[v] + p[v];
     }
     double red[PARTIAL_STRIDE];
     block_reduce<128>(acc, sred, red);

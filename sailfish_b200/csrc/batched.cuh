@@ -110,7 +110,9 @@ __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs
         for (int v = 0; v < PARTIAL_STRIDE; ++v)
             acc[v] = 0.0;
         const int c0 = strip * D.strip_width, r0 = seg * k.rows_per_cta;
-        if (ROLE == ROLE_WRITER) {
+        if (st.halt) {
+            // the disk's stepper stopped: no march, zero partials
+        } else if (ROLE == ROLE_WRITER) {
             // the same answer in every thread; the disk's first tile writes the key
             const bool store = cached && cache_write_check<PREC>(k, st, sa.fcache, t == 0 && u == D.unit_begin);
             march_tile<BJ, FAST, CACHE_WRITE>(k, st, sa, c0, D.strip_width, r0, acc, store);

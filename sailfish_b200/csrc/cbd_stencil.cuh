@@ -86,6 +86,8 @@ struct StageDev {
     MassDev e[2];       // masses at the end-of-step time (epilogue)
     double a, one_minus_a, dt;
     double buffer_mass, buffer_k;  // central mass, driving_rate * omega_outer
+    int halt;           // set by a device stepper that stopped: the stage leaves every array untouched
+    int _pad;
 };
 
 // ---------------------------------------------------------------------------
@@ -94,6 +96,9 @@ struct StageDev {
 
 __device__ __forceinline__ double lesser(double a, double b) { return a < b ? a : b; }
 __device__ __forceinline__ double greater(double a, double b) { return a > b ? a : b; }
+// the maximum of the wavespeed reductions: keeps a NaN operand, as numpy's
+// max over the reference's wavespeed array does (cbdiso_2d.py:174)
+__device__ __forceinline__ double max_nan(double a, double b) { return (a > b || a != a) ? a : b; }
 
 // a / b rounded to nearest, given y = RN(1/b): the remainder a - q b of
 // q = RN(a y) is exact under FMA, and one correction q + (a - q b) y rounds
@@ -463,7 +468,7 @@ __device__ __forceinline__ void accumulate_zone(const Consts &k, const MassDev *
                                                 const double *p, double (&acc)[PARTIAL_STRIDE])
 {
     if (k.want_ws)
-        acc[0] = greater(acc[0], max_wavespeed(p, sound_speed2<FAST>(k, e, x, y)));
+        acc[0] = max_nan(acc[0], max_wavespeed(p, sound_speed2<FAST>(k, e, x, y)));
     if (k.num_diag > 0) {
         double rg[2][3], ra[2][3];
         end_rates<FAST>(e, k.need_rates, x, y, p, rg, ra);
@@ -498,7 +503,7 @@ __device__ __forceinline__ void block_reduce(const double (&vals)[PARTIAL_STRIDE
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const double y = __shfl_down_sync(0xffffffffu, x, o);
-            x = v == 0 ? greater(x, y) : x + y;
+            x = v == 0 ? max_nan(x, y) : x + y;
         }
         if (lane == 0)
             smem[v * NW + warp] = x;
@@ -509,7 +514,7 @@ __device__ __forceinline__ void block_reduce(const double (&vals)[PARTIAL_STRIDE
         for (int v = 0; v < PARTIAL_STRIDE; ++v) {
             double x = smem[v * NW];
             for (int w = 1; w < NW; ++w)
-                x = v == 0 ? greater(x, smem[v * NW + w]) : x + smem[v * NW + w];
+                x = v == 0 ? max_nan(x, smem[v * NW + w]) : x + smem[v * NW + w];
             out[v] = x;
         }
     }
@@ -550,7 +555,7 @@ __device__ void grid_finish(const double (&mine)[PARTIAL_STRIDE], int n, double 
 #pragma unroll
         for (int v = 0; v < PARTIAL_STRIDE; ++v) {
             const double x = src[v];
-            acc[v] = v == 0 ? greater(acc[v], x) : acc[v] + x;
+            acc[v] = v == 0 ? max_nan(acc[v], x) : acc[v] + x;
         }
     }
     double red[PARTIAL_STRIDE];
@@ -1036,8 +1041,10 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
     for (int v = 0; v < PARTIAL_STRIDE; ++v)
         acc[v] = 0.0;
     const int c0 = blockIdx.x * BJ, r0 = blockIdx.y * k.rows_per_cta;
+    __syncthreads();
+    if (st.halt)
+        return;
     if (ROLE == ROLE_WRITER) {
-        __syncthreads();
         const bool store = cache_write_check<PREC>(k, st, args.fcache,
                                                    threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0);
         march_tile<BJ, FAST, CACHE_WRITE>(k, st, args, c0, BJ, r0, acc, store);

@@ -852,7 +852,7 @@ __global__ void __launch_bounds__(RED_THREADS) reduce_kernel(RedArgs r, const do
     for (long z = blockIdx.x * (long)RED_THREADS + threadIdx.x; z < n; z += (long)gridDim.x * RED_THREADS) {
         const int i = (int)(z / k.nj), j = (int)(z % k.nj);
         const double *p = prim + at(i, j, k.nj);
-        v[0] = greater(v[0], max_wavespeed(p, cs2_of(k.gamma, p)));
+        v[0] = max_nan(v[0], max_wavespeed(p, cs2_of(k.gamma, p)));
         const double x = k.xl + (i + 0.5) * k.dx, y = k.yl + (j + 0.5) * k.dy;
         for (int d = 0; d < r.nd; ++d) {
             double re, im;
@@ -866,7 +866,7 @@ __global__ void __launch_bounds__(RED_THREADS) reduce_kernel(RedArgs r, const do
     __syncthreads();
     for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
         if ((int)threadIdx.x < w) {
-            sm[0][threadIdx.x] = greater(sm[0][threadIdx.x], sm[0][threadIdx.x + w]);
+            sm[0][threadIdx.x] = max_nan(sm[0][threadIdx.x], sm[0][threadIdx.x + w]);
             for (int q = 1; q < RED_VALUES; ++q)
                 sm[q][threadIdx.x] += sm[q][threadIdx.x + w];
         }
@@ -884,7 +884,7 @@ __global__ void finish_kernel(const double *partials, int nblocks, double *resul
     double s = 0.0;
     for (int b = 0; b < nblocks; ++b) {
         const double x = partials[(size_t)b * RED_VALUES + q];
-        s = q == 0 ? greater(s, x) : s + x;
+        s = q == 0 ? max_nan(s, x) : s + x;
     }
     result[q] = s;
 }

@@ -21,7 +21,9 @@ double *g_scratch_address[kMaxDevices] = {};
 
 // The array's name is a host-side stand-in in host code, not a device
 // address; its device address is looked up once per device, with that device
-// current, and handed to the kernel.
+// current, and handed to the kernel. The address is kept for the life of the
+// process: after cudaDeviceReset (which unloads the library's device code)
+// it would be stale, so calls after a reset are not supported.
 int static_scratch(double **out)
 {
     int dev = 0;
@@ -50,10 +52,11 @@ extern "C" int cbdiso_b200_advance_stage_noalloc(
     const size_t need = cbdiso_b200_scratch_bytes(grid);
     if (need == 0)
         return CBD_ERR_ARGUMENT;
-    if (need > kStaticScratchBytes)
-        return CBD_ERR_CAPACITY;
     double *scratch = nullptr;
     if (epilogue) {
+        // only the epilogue uses scratch: a stage without one has no size limit here
+        if (need > kStaticScratchBytes)
+            return CBD_ERR_CAPACITY;
         const int rc = static_scratch(&scratch);
         if (rc != CBD_OK)
             return rc;

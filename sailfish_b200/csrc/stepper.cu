@@ -45,6 +45,16 @@ __global__ void step_prologue_kernel(StepperDev *steppers, int n, const double *
     }
     const double dt = s->dt_sequence ? s->dt_sequence[s->step]
                                      : (s->fixed_dt > 0.0 ? s->fixed_dt : s->min_spacing / result[0] * s->cfl);
+    StageDev *rec = records + (size_t)d * s->num_stages;
+    if (!(isfinite(dt) && dt > 0.0)) {
+        // a NaN, infinite or zero wavespeed (or a bad dt sequence entry):
+        // stop here, and make the stages of this and every later step of a
+        // captured sequence leave the state as it is
+        s->status = CBD_ERR_NONFINITE;
+        for (int k = 0; k < s->num_stages; ++k)
+            rec[k].halt = 1;
+        return;
+    }
     const double time0 = s->time;
     double t = time0;
     double times[3];
@@ -57,7 +67,6 @@ __global__ void step_prologue_kernel(StepperDev *steppers, int n, const double *
         s->status = CBD_ERR_KEPLER;
         return;
     }
-    StageDev *rec = records + (size_t)d * s->num_stages;
     for (int k = 0; k < s->num_stages; ++k) {
         StageDev &r = rec[k];
         if (!orbit_masses(s->orbit, times[k], r.m)) {
@@ -71,6 +80,7 @@ __global__ void step_prologue_kernel(StepperDev *steppers, int n, const double *
         r.dt = dt;
         r.buffer_mass = r.m[0].mass + r.m[1].mass;
         r.buffer_k = s->buffer_k;
+        r.halt = 0;
         if (s->history && s->step < s->history_capacity)
             s->history[(size_t)s->step * s->num_stages + k] = r;
     }

@@ -16,7 +16,8 @@ struct StepperDev {
     cbd_orbit_t orbit;
     int num_stages;
     int step;            // steps taken
-    int status;          // CBD_OK, or CBD_ERR_KEPLER once a solve failed (then no further steps)
+    int status;          // CBD_OK; CBD_ERR_KEPLER once an orbit solve failed, CBD_ERR_NONFINITE once a
+                         // step's dt was not finite and positive (then no further steps)
     int series_capacity; // rows available in the time-series buffer
     const double *dt_sequence;  // if set: dt of step n is dt_sequence[n] (n < dt_count)
     StageDev *history;          // if set: stage records of step n also go to history[n * num_stages ...]

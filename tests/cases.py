@@ -19,10 +19,17 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 def golden_names():
     """The isothermal solver-run fixtures (make_golden.py); the gamma-law ones
-    (gam_*) and the checkpoint fixtures (chkpt_*, make_checkpoint.py) have
+    (gam_*), the checkpoint fixtures (chkpt_*, make_checkpoint.py) and the
+    1000-step throughput-configuration ones (config1_*, `long_names`) have
     their own tests."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith(("chkpt_", "gam_")))
+                  if not os.path.basename(p).startswith(("chkpt_", "gam_", "config1_")))
+
+
+def long_names():
+    """The 1000-step fixtures of the plain-solver throughput configuration
+    (1024^2, 2048^2, 4096^2; make_golden.py LONG_CASES)."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "config1_*.npz")))
 
 
 def gam_names():

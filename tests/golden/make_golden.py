@@ -20,6 +20,17 @@ seeded noise), the noise seed, the time step sequence chosen by the driver's
 CFL rule (driver.py:508-510), the state after the first and after the last
 step, the wavespeed maximum after the last step, and the reductions time
 series (cbdiso_2d.py:370-503) after every step.
+
+The long cases (`LONG_CASES`: the plain-solver throughput configuration at
+1024^2, 2048^2 and 4096^2, 1000 RK2 steps each) run the reference's kernels
+in its OpenMP mode (`mode="omp"`, one zone per loop iteration, so the results
+are the serial build's bit for bit) and store, instead of whole states, the
+full dt and reductions series, a 1-in-16 subsample of the states after the
+first and the last step, and per-row (fixed i) maximum magnitudes and sums of
+each field of the last state. They take about 5 min, 15 min and an hour on
+8 cores, and run only when named:
+
+    python tests/golden/make_golden.py config1_t15_n1024 config1_t15_n2048 config1_t15_n4096
 """
 
 import json
@@ -146,6 +157,17 @@ CASES = {
         diagnostics=CBD_DIAG, store="subsample8"),
 }
 
+# the plain-solver throughput configuration: config-0 physics, 1000 steps (see the module docstring)
+CONFIG1_PARAMS = dict(domain_radius=8.0, mach_number=10.0, mass_ratio=1.0, eccentricity=0.0, sink_rate=10.0,
+                      sink_radius=0.05, softening_length=0.05, nu=0.001)
+LONG_CASES = {
+    f"config1_t15_n{n}": dict(
+        setup="circumbinary-disk", theta=1.5, resolution=n, steps=1000, seed=0, patches=1, rk=2,
+        params=CONFIG1_PARAMS, diagnostics=CBD_DIAG, store="long16", mode="omp")
+    for n in (1024, 2048, 4096)
+}
+CASES.update(LONG_CASES)
+
 
 def run_case(name, out_path):
     import numpy as np
@@ -162,6 +184,13 @@ def run_case(name, out_path):
         open(src, "w").write(text)
         sys.path.insert(0, tmp)
         os.environ.setdefault("CC", "/usr/bin/gcc")
+        # the system compiler links OpenMP (the interpreter's default LDSHARED may not)
+        os.environ.setdefault("LDSHARED", "/usr/bin/gcc -shared")
+        mode = case.get("mode", "cpu")
+        if mode == "omp":
+            from sailfish.kernel.system import configure_build
+
+            configure_build(enable_openmp=True, execution_mode="omp")
         from sailfish.setup_base import SetupBase
         import sailfish.setups  # noqa: F401  (registers the setup classes)
         from sailfish.mesh import PlanarCartesian2DMesh
@@ -193,7 +222,7 @@ def run_case(name, out_path):
         options = dict(rk_order=case["rk"]) if solver_name == "cbdiso_2d" else dict()
         solver = make_solver(
             solver_name, physics, options, setup=setup, mesh=mesh, time=0.0, solution=prim,
-            num_patches=case["patches"], mode="cpu")
+            num_patches=case["patches"], mode=mode)
         cfl = case.get("cfl", 0.3)
         dts, series, first = [], [], None
         for n in range(case["steps"]):
@@ -203,6 +232,8 @@ def run_case(name, out_path):
             series.append([complex(v) for v in solver.reductions()])
             if n == 0:
                 first = solver.solution
+            if case.get("store") == "long16" and (n + 1) % 50 == 0:
+                print(f"{name}: step {n + 1} t={solver.time:.6f} dt={dt:.6e}", file=sys.stderr, flush=True)
         last = solver.solution
         ws = solver.maximum_wavespeed()
         meta = dict(case, name=name, mesh=list(mesh), cfl=cfl, rk=case.get("rk", 2))
@@ -212,6 +243,12 @@ def run_case(name, out_path):
             out.update(first_sub=first[::8, ::8], last_sub=last[::8, ::8],
                        last_sums=np.array([last[..., q].sum() for q in range(nq)]),
                        ic=ic[::8, ::8])
+        elif case.get("store") == "long16":
+            out.update(first_sub=first[::16, ::16], last_sub=last[::16, ::16],
+                       last_row_max=np.abs(last).max(axis=1), last_row_sum=last.sum(axis=1),
+                       last_row_abs=np.abs(last).sum(axis=1),
+                       last_sums=np.array([last[..., q].sum() for q in range(nq)]),
+                       ic=ic[::16, ::16])
         else:
             out.update(first=first, last=last)
         np.savez_compressed(out_path, **out)
@@ -223,7 +260,7 @@ def main(argv):
     if len(argv) >= 2 and argv[0] == "--one":
         run_case(argv[1], argv[2])
         return
-    names = argv or list(CASES)
+    names = argv or [n for n in CASES if n not in LONG_CASES]
     for name in names:
         out = os.path.join(HERE, f"{name}.npz")
         subprocess.run([sys.executable, __file__, "--one", name, out], check=True)

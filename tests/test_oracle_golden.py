@@ -9,7 +9,7 @@ import os
 import numpy as np
 import pytest
 
-from cases import diagnostics, golden_names, initial_state, load, oracle_config
+from cases import diagnostics, golden_names, initial_state, load, long_names, oracle_config
 from oracle import host as oh
 
 NAMES = golden_names()
@@ -71,3 +71,24 @@ def test_oracle_theta_is_a_runtime_parameter():
 def test_kepler_newton_rejects_nonconvergence():
     with pytest.raises(ValueError):
         oh.kepler_eccentric_anomaly(1.0, 1.0, 1.0, 1.5)  # e > 1: no bound orbit
+
+
+@pytest.mark.parametrize("name", [n for n in long_names() if n.endswith("_n1024")])
+def test_oracle_reproduces_first_step_of_long_fixture(name):
+    """The 1000-step fixtures were written by the reference's solver in its
+    OpenMP mode; the oracle reproduces their first step (state subsample,
+    driver dt, wavespeed-derived time and reductions) bit for bit. (The
+    larger fixtures hold the same data at 2048^2 and 4096^2; one CPU step of
+    those takes too long for this suite.)"""
+    d = load(name)
+    meta = d["meta"]
+    cfg = oracle_config(meta)
+    x, y = oh.cell_centres(cfg)
+    prim = oh.circumbinary_disk_primitive(x, y, 0.05, 1.0)
+    assert np.array_equal(prim[::16, ::16], d["ic"])
+    prim[..., 0] += oh.seeded_noise(cfg.ni, cfg.nj, meta["seed"])
+    solver = oh.OracleSolver(cfg, prim, 0.0, oh.Kernels("oracle", cfg.plm_theta, threads="omp"))
+    dts, series = oh.run(solver, 1, 0.3, diagnostics(meta))
+    assert dts[0] == d["dts"][0]
+    assert np.array_equal(np.array(series[0], dtype=complex), d["series"][0])
+    assert np.array_equal(solver.solution[::16, ::16], d["first_sub"])

@@ -115,3 +115,28 @@ def test_noalloc_rejects_grids_beyond_its_capacity():
                                                    ctypes.byref(ep), None, None)
     assert status == CAPACITY_ERROR
     assert lib.cbdiso_b200_status_string(status) == b"request exceeds library capacity"
+
+
+def test_noalloc_stage_without_epilogue_has_no_size_limit():
+    """A stage with no epilogue uses no scratch: an 8192^2 grid, beyond the
+    array's capacity with an epilogue, runs and equals the allocating entry
+    point's result bit for bit (the same kernel on the same inputs)."""
+    lib = _capi.lib()
+    g, st, _, small = _problem(16, 16)
+    n = 8192
+    g.ni = g.nj = n
+    g.xl, g.xr, g.yl, g.yr = -8.0, 8.0, -8.0, 8.0
+    cfg = oh.Config(g.xl, g.xr, g.yl, g.yr, n, n)
+    x, y = oh.cell_centres(cfg)
+    p = torch.zeros((n + 4, n + 4, 3), dtype=torch.float64, device="cuda")
+    p[2:-2, 2:-2] = torch.from_numpy(oh.circumbinary_disk_primitive(x, y)).cuda()
+    del x, y
+    assert lib.cbdiso_b200_fill_guards(ctypes.byref(g), _ptr(p), _stream()) == 0
+    got = torch.zeros_like(p)
+    status = lib.cbdiso_b200_advance_stage_noalloc(ctypes.byref(g), ctypes.byref(st), None, _ptr(p), None,
+                                                   _ptr(got), None, None, _stream())
+    assert status == 0
+    want = torch.zeros_like(p)
+    assert lib.cbdiso_b200_advance_stage(ctypes.byref(g), ctypes.byref(st), None, _ptr(p), None, _ptr(want),
+                                         None, None, None, _stream()) == 0
+    assert torch.equal(got, want)
