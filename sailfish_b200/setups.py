@@ -109,30 +109,30 @@ class CircumbinaryDisk(SetupBase):
     (cbdgam_2d).
     """
 
-    eos = param("isothermal", "EOS type: either isothermal or gamma-law")
-    domain_radius = param(12.0, "half side length of the square computational domain")
-    mach_number = param(10.0, "orbital Mach number (isothermal)", mutable=True)
-    eccentricity = param(0.0, "orbital eccentricity of the binary", mutable=True)
-    mass_ratio = param(1.0, "component mass ratio m2 / m1 <= 1", mutable=True)
-    sink_rate = param(10.0, "component sink rate", mutable=True)
-    sink_radius = param(0.05, "component sink radius", mutable=True)
-    softening_length = param(0.05, "gravitational softening length", mutable=True)
-    buffer_is_enabled = param(True, "whether the buffer zone is enabled", mutable=True)
-    sink_model = param("torque_free", "sink [acceleration_free|force_free|torque_free]", mutable=True)
-    initial_sigma = param(1.0, "initial disk surface density at r=a (gamma-law)")
-    initial_pressure = param(1e-2, "initial disk surface pressure at r=a (gamma-law)")
-    cooling_coefficient = param(0.0, "strength of the cooling term (gamma-law)")
-    alpha = param(0.1, "alpha-viscosity parameter (gamma-law)")
-    nu = param(0.001, "kinematic viscosity parameter (isothermal)")
-    constant_softening = param(True, "whether to use constant softening (gamma-law)")
-    gamma_law_index = param(5.0 / 3.0, "adiabatic index (gamma-law)")
-    which_diagnostics = param("none", "diagnostics set to get from solver [none|mdots]")
+    eos = param("isothermal", "equation of state, isothermal or gamma-law (picks cbdiso_2d or cbdgam_2d)")
+    domain_radius = param(12.0, "the mesh spans [-R, R] in x and y; this is R")
+    mach_number = param(10.0, "ratio of orbital speed to sound speed (isothermal disk)", mutable=True)
+    eccentricity = param(0.0, "eccentricity e of the binary orbit", mutable=True)
+    mass_ratio = param(1.0, "q = m2 / m1, at most 1", mutable=True)
+    sink_rate = param(10.0, "accretion rate coefficient of each sink", mutable=True)
+    sink_radius = param(0.05, "radius of each sink", mutable=True)
+    softening_length = param(0.05, "softening of each mass's gravity", mutable=True)
+    buffer_is_enabled = param(True, "relax the outer ring of the mesh toward the initial disk", mutable=True)
+    sink_model = param("torque_free", "how a sink removes mass: acceleration_free, force_free or torque_free", mutable=True)
+    initial_sigma = param(1.0, "surface density of the gamma-law disk at radius 1")
+    initial_pressure = param(1e-2, "vertically integrated pressure of the gamma-law disk at radius 1")
+    cooling_coefficient = param(0.0, "coefficient of the gamma-law disk's cooling term (0: no cooling)")
+    alpha = param(0.1, "alpha of the gamma-law disk's viscosity (0: inviscid)")
+    nu = param(0.001, "constant kinematic viscosity nu of the isothermal disk (0: inviscid)")
+    constant_softening = param(True, "gamma-law disk: fixed softening length rather than one following the disk height")
+    gamma_law_index = param(5.0 / 3.0, "ratio of specific heats of the gamma-law gas")
+    which_diagnostics = param("none", "time series the solver reduces each step: none, or mdots (both accretion rates)")
 
     def validate(self):
         if not self.is_isothermal and not self.is_gamma_law:
-            raise SetupError(f"eos must be isothermal or gamma-law, got {self.eos}")
+            raise SetupError(f"unknown eos {self.eos!r}: use isothermal or gamma-law")
         if self.which_diagnostics not in ["none", "mdots"]:
-            raise SetupError(f"which_diagnostics must be none or mdots, got {self.which_diagnostics}")
+            raise SetupError(f"unknown which_diagnostics {self.which_diagnostics!r}: use none or mdots")
 
     @property
     def is_isothermal(self):
@@ -268,23 +268,23 @@ class KitpCodeComparison(SetupBase):
     radius 2.5, a sub-Keplerian profile and a small radial kick.
     """
 
-    mach_number = param(10.0, "nominal orbital Mach number", mutable=True)
-    eccentricity = param(0.0, "orbital eccentricity")
-    mass_ratio = param(1.0, "binary mass ratio M2 / M1")
-    sink_radius = param(0.05, "sink radius", mutable=True)
-    softening_length = param(0.05, "softening length", mutable=True)
-    nu = param(0.001, "kinematic viscosity coefficient", mutable=True)
-    single_point_mass = param(False, "put one point mass at the origin (no binary)")
-    sink_model = param("acceleration_free", "sink [acceleration_free|force_free|torque_free]", mutable=True)
-    domain_radius = param(8.0, "half side length of the square computational domain")
-    sink_rate = param(10.0, "component sink rate", mutable=True)
-    buffer_is_enabled = param(True, "whether the buffer zone is enabled", mutable=True)
-    disk_kick = param(1e-4, "kick velocity to seed eccentric cavity growth")
-    which_diagnostics = param("kitp", "output diagnostics option [kitp|forces]")
+    mach_number = param(10.0, "ratio of orbital speed to sound speed", mutable=True)
+    eccentricity = param(0.0, "eccentricity e of the binary orbit")
+    mass_ratio = param(1.0, "q = M2 / M1")
+    sink_radius = param(0.05, "radius of each sink", mutable=True)
+    softening_length = param(0.05, "softening of each mass's gravity", mutable=True)
+    nu = param(0.001, "constant kinematic viscosity nu", mutable=True)
+    single_point_mass = param(False, "one unit mass fixed at the origin instead of the binary")
+    sink_model = param("acceleration_free", "how a sink removes mass: acceleration_free, force_free or torque_free", mutable=True)
+    domain_radius = param(8.0, "the mesh spans [-R, R] in x and y; this is R")
+    sink_rate = param(10.0, "accretion rate coefficient of each sink", mutable=True)
+    buffer_is_enabled = param(True, "relax the outer ring of the mesh toward the initial disk", mutable=True)
+    disk_kick = param(1e-4, "amplitude of the small radial velocity that breaks the cavity's symmetry")
+    which_diagnostics = param("kitp", "time series the solver reduces each step: kitp or forces")
 
     def validate(self):
         if self.which_diagnostics not in ["kitp", "forces"]:
-            raise SetupError("Unknown option for diagnostics.")
+            raise SetupError(f"unknown which_diagnostics {self.which_diagnostics!r}: use kitp or forces")
 
     def primitive(self, t, coords, primitive):
         x, y = coords
@@ -382,19 +382,19 @@ class KitpCodeComparison(SetupBase):
 class BinaryBondi(SetupBase):
     """A binary in a uniform wind, globally isothermal (sailfish/setups/binary_bondi.py:19-102)."""
 
-    aspect = param(1, "aspect ratio of the domain, width / height")
-    height = param(1.0, "domain height in units of the binary separation")
-    x_bin = param(0.0, "horizontal offset of binary COM from domain center")
-    sound_speed = param(1.0, "speed of sound (uniform)")
-    wind_vel = param(1.0, "horizontal speed of the background flow")
-    bh_sep = param(0.25, "black hole semi-major axis")
-    bh_mass = param(1.0, "mass of the primary")
-    sink_radius = param(0.05, "black hole sink radius")
-    sink_model = param("acceleration_free", "sink prescription")
-    sink_rate = param(1e2, "sink rate")
-    mass_ratio = param(1.0, "system mass ratio: [0.0-1.0]")
-    eccentricity = param(0.0, "eccentricity")
-    softening_length = param(0.05, "gravitational softening length", mutable=True)
+    aspect = param(1, "mesh width divided by mesh height (an integer)")
+    height = param(1.0, "mesh height, in units of the binary separation")
+    x_bin = param(0.0, "x offset of the binary's centre of mass from the mesh centre")
+    sound_speed = param(1.0, "the gas's uniform sound speed")
+    wind_vel = param(1.0, "x velocity of the incoming wind")
+    bh_sep = param(0.25, "semi-major axis of the binary")
+    bh_mass = param(1.0, "mass of the heavier component")
+    sink_radius = param(0.05, "radius of each sink")
+    sink_model = param("acceleration_free", "how a sink removes mass: acceleration_free, force_free or torque_free")
+    sink_rate = param(1e2, "accretion rate coefficient of each sink")
+    mass_ratio = param(1.0, "q = m2 / m1, between 0 and 1")
+    eccentricity = param(0.0, "eccentricity e of the binary orbit")
+    softening_length = param(0.05, "softening of each mass's gravity", mutable=True)
 
     def primitive(self, t, coords, primitive):
         primitive[0] = 1.0
