@@ -38,10 +38,9 @@ struct BatchArgs {
     double *fcache;      // face-cache arena (disk d's cache at disks[d].cache_offset), or null
 };
 
-// ROLE (ROLE_*) is what the launch does with each disk's face cache: a writer
-// stores into the caches of the disks that have one; a reader requires one
-// for every disk (the batch's fill kernel ran before it) and skips the tiles
-// of a disk without one.
+// ROLE (ROLE_*) is what the launch does with each disk's face cache: a reader
+// requires one for every disk (the batch's fill kernel ran before it), skips
+// the tiles of a disk without one, and the disk's first tile records the key.
 template <int BJ, int MINB, int PREC, int ROLE = ROLE_NONE>
 __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs a)
 {
@@ -112,13 +111,13 @@ __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs
         const int c0 = strip * D.strip_width, r0 = seg * k.rows_per_cta;
         if (st.halt) {
             // the disk's stepper stopped: no march, zero partials
-        } else if (ROLE == ROLE_WRITER) {
-            // the same answer in every thread; the disk's first tile writes the key
-            const bool store = cached && cache_write_check<PREC>(k, st, sa.fcache, t == 0 && u == D.unit_begin);
-            march_tile<BJ, FAST, CACHE_WRITE>(k, st, sa, c0, D.strip_width, r0, acc, store);
         } else if (ROLE == ROLE_READER) {
-            if (cached)
+            if (cached) {
                 march_tile<BJ, FAST, CACHE_READ>(k, st, sa, c0, D.strip_width, r0, acc);
+                // the fill kernel ran before this launch; no tile reads the key
+                if (t == 0 && u == D.unit_begin)
+                    cache_write_key<PREC>(k, st, sa.fcache);
+            }
         } else {
             march_tile<BJ, FAST, CACHE_NONE>(k, st, sa, c0, D.strip_width, r0, acc);
         }
@@ -145,30 +144,39 @@ __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs
 }
 
 // The face caches of every disk valid for a reader stage (see
-// face_cache_fill_kernel): CTA (y, d) checks disk d's key and, when it does not
-// match, marks it invalid and fills rows y, y + gridDim.x, ... of its cache.
-template <int PREC>
-__global__ void __launch_bounds__(128) batched_fill_kernel(const BatchArgs a)
+// face_cache_fill_kernel): CTA u fills tile u of the batch's tile list (the
+// same tiles as the stage) when its disk has a cache whose key does not match
+// the disk's stage masses. Grid: total_units CTAs of BJ threads.
+template <int BJ, int PREC>
+__global__ void __launch_bounds__(BJ) batched_fill_kernel(const BatchArgs a)
 {
     constexpr bool FAST = PREC == CBD_PRECISION_FAST;
     __shared__ StageDev st;
-    __shared__ int fill;
-    const DiskDev &D = a.disks[blockIdx.y];
-    const Consts &k = D.k;
+    __shared__ int s_disk, fill;
+    const int u = blockIdx.x;
     if (threadIdx.x == 0) {
-        st = a.records[(size_t)blockIdx.y * a.num_stages + a.stage];
-        fill = 0;
-        if (D.cache_offset >= 0) {
-            double *fc = a.fcache + D.cache_offset;
-            fill = cache_key_matches<PREC>(k, st, fc) ? 0 : 1;
-            if (fill)
-                fc[0] = 0.0;
+        int lo = 0, hi = a.num_disks - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (a.disks[mid].unit_begin <= u)
+                lo = mid;
+            else
+                hi = mid - 1;
         }
+        s_disk = lo;
+        const DiskDev &D = a.disks[lo];
+        st = a.records[(size_t)lo * a.num_stages + a.stage];
+        fill = D.cache_offset >= 0 && !st.halt && !cache_key_matches<PREC>(D.k, st, a.fcache + D.cache_offset);
     }
     __syncthreads();
     if (!fill)
         return;
-    face_cache_fill_rows<FAST>(k, st, a.fcache + D.cache_offset, blockIdx.x, gridDim.x);
+    const DiskDev &D = a.disks[s_disk];
+    const int local = u - D.unit_begin;
+    const int strip = local % D.strips;
+    const int seg = local / D.strips;
+    face_cache_fill_tile<BJ, FAST>(D.k, st.m, a.fcache + D.cache_offset, strip * D.strip_width, D.strip_width,
+                                   seg * D.k.rows_per_cta, D.k.rows_per_cta);
 }
 
 cudaError_t launch_batched_exact(const BatchArgs &a, int ctas, int role, cudaStream_t s);
@@ -181,11 +189,8 @@ template <int PREC>
 cudaError_t launch_batched(const BatchArgs &a, int ctas, int role, cudaStream_t s)
 {
     switch (role) {
-    case ROLE_WRITER:
-        batched_stage_kernel<128, 6, PREC, ROLE_WRITER><<<ctas, 128, 0, s>>>(a);
-        break;
     case ROLE_READER:
-        batched_fill_kernel<PREC><<<dim3(8, a.num_disks), 128, 0, s>>>(a);
+        batched_fill_kernel<128, PREC><<<a.total_units, 128, 0, s>>>(a);
         batched_stage_kernel<128, 6, PREC, ROLE_READER><<<ctas, 128, 0, s>>>(a);
         break;
     default:

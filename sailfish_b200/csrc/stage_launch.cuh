@@ -11,16 +11,11 @@ cudaError_t launch_one(const LaunchShape &s, const Consts &k, const StageDev &st
                        cudaStream_t stream)
 {
     switch (role) {
-    case ROLE_WRITER:
-        stage_kernel<BJ, MINB, PREC, ROLE_WRITER><<<s.grid, BJ, 0, stream>>>(k, st, a);
-        break;
-    case ROLE_READER: {
-        // at most four CTAs per SM, each over rows i, i + grid, ...
-        const int rows = k.ni + 1 < 148 * 4 ? k.ni + 1 : 148 * 4;
-        face_cache_fill_kernel<PREC><<<rows, 128, 0, stream>>>(k, st, a.stage_dev, a.fcache);
+    case ROLE_READER:
+        // the fill over the stage's own tiles, then the stage
+        face_cache_fill_kernel<BJ, PREC><<<s.grid, BJ, 0, stream>>>(k, st, a.stage_dev, a.fcache);
         stage_kernel<BJ, MINB, PREC, ROLE_READER><<<s.grid, BJ, 0, stream>>>(k, st, a);
         break;
-    }
     default:
         stage_kernel<BJ, MINB, PREC, ROLE_NONE><<<s.grid, BJ, 0, stream>>>(k, st, a);
         break;

@@ -73,4 +73,4 @@ def test_batched_face_cache_is_bit_identical():
     for i in range(len(disks)):
         assert np.array_equal(on.solution(i), off.solution(i))
     torch.cuda.synchronize()
-    assert float(on._fcache[0]) == 20260101.5  # the first disk's key was written
+    assert float(on._fcache[0]) == 20261204.5  # the first disk's key was written
