@@ -213,18 +213,17 @@ int cbdiso_b200_stage_record(const cbd_grid_t *grid, const cbd_stage_t *stage, c
  * reference, which recomputes these values in every stage,
  * cbdiso_2d.c:555-558 and :97-175).
  *
- * The face sound speeds, the zones' gravity factors and the zone centres'
- * sound speeds depend only on the mesh, the EOS constants and the point
- * masses' positions, masses and softenings. `role`:
+ * The face sound speeds and the zones' gravity factors depend only on the mesh,
+ * the EOS constants and the point masses' positions, masses and softenings, so
+ * a step's first stage can reuse what the previous step's last stage computed
+ * for the same masses. `role`:
  *   0  no cache use (as cbdiso_b200_advance_stage);
- *   2  reader: a fill pass (an elementwise kernel) computes the values into
- *      `face_cache` when the cache's key does not match the stage's masses;
- *      the stage loads them, its epilogue too when the end-of-step masses
- *      are the stage's, and then records the key. A step's last stage
- *      usually runs with the next step's first-stage masses, so with every
- *      stage a reader the values are computed once per step.
- *   (1, a stage that stored its own stencil's values, is no longer
- *   accepted: CBD_ERR_ARGUMENT.)
+ *   1  writer (RK2's second stage, RK3's second): when the stage's masses equal
+ *      its record's end-of-step masses, also stores the values in `face_cache`
+ *      with a key of everything they depend on;
+ *   2  reader (a step's first stage): a fill pass before the stage computes
+ *      the values when the key does not match the stage's masses; the stage
+ *      loads them and records the key.
  * In EXACT precision the results are bit-identical to
  * cbdiso_b200_advance_stage (in FMA and FAST the compiler may contract the code
  * paths differently: equal to rounding). `face_cache` is a caller-owned,
@@ -339,8 +338,8 @@ int cbdiso_b200_batched_stage(const void *disks, int num_disks, int total_units,
                               void *stream);
 
 /* cbdiso_b200_batched_stage with face caches and a role (as in
- * cbdiso_b200_advance_stage_cached: 0 none, 2 reader, the reader preceded by
- * a fill pass over every disk's tiles; 1 is rejected). Disk d's cache lies at face_cache + its
+ * cbdiso_b200_advance_stage_cached: 0 none, 1 writer, 2 reader, the reader
+ * preceded by a fill pass over every disk's tiles). Disk d's cache lies at face_cache + its
  * record's cache offset, set by cbdiso_b200_batch_disk_set_face_cache (an even
  * number of doubles); it holds cbdiso_b200_face_cache_bytes(its grid) bytes
  * with its first 256 bytes zeroed before the first use, and `face_cache` is

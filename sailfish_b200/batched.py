@@ -202,7 +202,8 @@ class BatchedSolver:
                       self._ptr(pn) if pn is not None else None, self._ptr(wr), self._ptr(self._records),
                       self.rk_order, stage, int(last), self._ptr(self._partials), self._ptr(self._counters), prec)
             # face-cache role: the stage at t0 + dt writes, the next step's first reads
-            role = 0 if self._fcache is None else 2  # every stage reads, behind a fill pass
+            # the stage at t0 + dt writes the cache, the next step's first stage reads
+            role = 0 if self._fcache is None else (2 if stage == 0 else (1 if stage == 1 else 0))
             if role:
                 status = lib.cbdiso_b200_batched_stage_cached(*common, self._ptr(self._fcache), role, stream)
             else:

@@ -674,13 +674,17 @@ class Solver(SolverBase):
             self._stage_hook(s, wr)
 
     def _cache_role(self, s, nstages):
-        """Face-cache role of stage s of a step (0 none, 2 reader): with the
-        cache, every stage reads it behind a fill pass that recomputes the
-        values only when the cached masses are not the stage's. A step's
-        last stage (at t0 + dt) usually has the next step's first-stage
-        masses, so RK2 fills once per step, RK3 twice (its third stage is at
-        t0 + dt / 2) and RK1 once."""
-        return 0 if self._fcache is None else 2
+        """Face-cache role of stage s of a step (0 none, 1 writer, 2 reader):
+        the stage at t0 + dt (RK2's and RK3's second) computes the values in
+        its stencil and stores them, the next step's first stage reads them
+        (behind a fill pass that recomputes them only when the cached masses
+        are not its own); RK1 has no stage at t0 + dt. On one grid this
+        costs less than a separate fill pass every step (measured)."""
+        if self._fcache is None or nstages == 1:
+            return 0
+        if s == 0:
+            return 2
+        return 1 if s == 1 else 0
 
     def _finish_stages(self, nstages, rk2_buffers):
         if nstages == 1 and rk2_buffers is None:

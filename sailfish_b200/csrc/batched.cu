@@ -169,8 +169,8 @@ int cbdiso_b200_batched_stage_cached(const void *disks, int num_disks, int total
                                      unsigned int *counters, int precision, double *face_cache, int role,
                                      void *stream)
 {
-    if (!face_cache || (reinterpret_cast<uintptr_t>(face_cache) & 15) != 0 ||
-        (role != ROLE_NONE && role != ROLE_READER))
+    if (!face_cache || (reinterpret_cast<uintptr_t>(face_cache) & 15) != 0 || role < ROLE_NONE ||
+        role > ROLE_READER)
         return CBD_ERR_ARGUMENT;
     return batched_stage(disks, num_disks, total_units, primitive_rd, primitive_n, primitive_wr, records,
                          num_stages, stage, epilogue, partials, counters, precision, face_cache, role, stream);

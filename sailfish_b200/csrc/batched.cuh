@@ -38,10 +38,11 @@ struct BatchArgs {
     double *fcache;      // face-cache arena (disk d's cache at disks[d].cache_offset), or null
 };
 
-// ROLE (ROLE_*) is what the launch does with each disk's face cache: a reader
-// requires one for every disk (the batch's fill kernel ran before it), skips
-// the tiles of a disk without one, and the disk's first tile records the key.
-template <int BJ, int MINB, int PREC, int ROLE = ROLE_NONE>
+// ROLE (ROLE_*) is what the launch does with each disk's face cache: a writer
+// stores into the caches of the disks that have one; a reader requires one
+// for every disk (the batch's fill kernel ran before it), skips the tiles of
+// a disk without one, and the disk's first tile records the key.
+template <int BJ, int MINB, int PREC, int ROLE = ROLE_NONE, bool EPI = true>
 __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs a)
 {
     constexpr bool FAST = PREC == CBD_PRECISION_FAST;
@@ -111,17 +112,21 @@ __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs
         const int c0 = strip * D.strip_width, r0 = seg * k.rows_per_cta;
         if (st.halt) {
             // the disk's stepper stopped: no march, zero partials
+        } else if (ROLE == ROLE_WRITER) {
+            // the same answer in every thread; the disk's first tile writes the key
+            const bool store = cached && cache_write_check<PREC>(k, st, sa.fcache, t == 0 && u == D.unit_begin);
+            march_tile<BJ, FAST, CACHE_WRITE, EPI>(k, st, sa, c0, D.strip_width, r0, acc, store);
         } else if (ROLE == ROLE_READER) {
             if (cached) {
-                march_tile<BJ, FAST, CACHE_READ>(k, st, sa, c0, D.strip_width, r0, acc);
+                march_tile<BJ, FAST, CACHE_READ, EPI>(k, st, sa, c0, D.strip_width, r0, acc);
                 // the fill kernel ran before this launch; no tile reads the key
                 if (t == 0 && u == D.unit_begin)
                     cache_write_key<PREC>(k, st, sa.fcache);
             }
         } else {
-            march_tile<BJ, FAST, CACHE_NONE>(k, st, sa, c0, D.strip_width, r0, acc);
+            march_tile<BJ, FAST, CACHE_NONE, EPI>(k, st, sa, c0, D.strip_width, r0, acc);
         }
-        if (a.epilogue) {
+        if (EPI) {
             double red[PARTIAL_STRIDE];
             block_reduce<BJ>(acc, sred, red);
             if (t == 0) {
@@ -144,39 +149,43 @@ __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs
 }
 
 // The face caches of every disk valid for a reader stage (see
-// face_cache_fill_kernel): CTA u fills tile u of the batch's tile list (the
-// same tiles as the stage) when its disk has a cache whose key does not match
-// the disk's stage masses. Grid: total_units CTAs of BJ threads.
+// face_cache_fill_kernel): CTA b takes tiles u = b, b + gridDim.x, ... of the
+// batch's tile list (the same tiles as the stage) and fills tile u when its
+// disk has a cache whose key does not match the disk's stage masses.
 template <int BJ, int PREC>
-__global__ void __launch_bounds__(BJ) batched_fill_kernel(const BatchArgs a)
+__global__ void __launch_bounds__(BJ, FILL_WARPS_PER_SM * 32 / BJ) batched_fill_kernel(const BatchArgs a)
 {
     constexpr bool FAST = PREC == CBD_PRECISION_FAST;
     __shared__ StageDev st;
     __shared__ int s_disk, fill;
-    const int u = blockIdx.x;
-    if (threadIdx.x == 0) {
-        int lo = 0, hi = a.num_disks - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) / 2;
-            if (a.disks[mid].unit_begin <= u)
-                lo = mid;
-            else
-                hi = mid - 1;
+    for (int u = blockIdx.x; u < a.total_units; u += gridDim.x) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = a.num_disks - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) / 2;
+                if (a.disks[mid].unit_begin <= u)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            s_disk = lo;
+            const DiskDev &D = a.disks[lo];
+            st = a.records[(size_t)lo * a.num_stages + a.stage];
+            fill = D.cache_offset >= 0 && !st.halt &&
+                   !cache_key_matches<PREC>(D.k, st, a.fcache + D.cache_offset);
         }
-        s_disk = lo;
-        const DiskDev &D = a.disks[lo];
-        st = a.records[(size_t)lo * a.num_stages + a.stage];
-        fill = D.cache_offset >= 0 && !st.halt && !cache_key_matches<PREC>(D.k, st, a.fcache + D.cache_offset);
+        __syncthreads();
+        if (fill) {
+            const DiskDev &D = a.disks[s_disk];
+            const int local = u - D.unit_begin;
+            const int strip = local % D.strips;
+            const int seg = local / D.strips;
+            face_cache_fill_tile<BJ, FAST>(D.k, st.m, a.fcache + D.cache_offset, strip * D.strip_width,
+                                           D.strip_width, seg * D.k.rows_per_cta, D.k.rows_per_cta);
+        }
+        // the shared record is rewritten for the next tile
+        __syncthreads();
     }
-    __syncthreads();
-    if (!fill)
-        return;
-    const DiskDev &D = a.disks[s_disk];
-    const int local = u - D.unit_begin;
-    const int strip = local % D.strips;
-    const int seg = local / D.strips;
-    face_cache_fill_tile<BJ, FAST>(D.k, st.m, a.fcache + D.cache_offset, strip * D.strip_width, D.strip_width,
-                                   seg * D.k.rows_per_cta, D.k.rows_per_cta);
 }
 
 cudaError_t launch_batched_exact(const BatchArgs &a, int ctas, int role, cudaStream_t s);
@@ -189,12 +198,24 @@ template <int PREC>
 cudaError_t launch_batched(const BatchArgs &a, int ctas, int role, cudaStream_t s)
 {
     switch (role) {
+    case ROLE_WRITER:
+        if (a.epilogue)
+            batched_stage_kernel<128, 6, PREC, ROLE_WRITER, true><<<ctas, 128, 0, s>>>(a);
+        else
+            batched_stage_kernel<128, 6, PREC, ROLE_WRITER, false><<<ctas, 128, 0, s>>>(a);
+        break;
     case ROLE_READER:
-        batched_fill_kernel<128, PREC><<<a.total_units, 128, 0, s>>>(a);
-        batched_stage_kernel<128, 6, PREC, ROLE_READER><<<ctas, 128, 0, s>>>(a);
+        batched_fill_kernel<128, PREC><<<a.total_units < 148 * 8 ? a.total_units : 148 * 8, 128, 0, s>>>(a);
+        if (a.epilogue)
+            batched_stage_kernel<128, 6, PREC, ROLE_READER, true><<<ctas, 128, 0, s>>>(a);
+        else
+            batched_stage_kernel<128, 6, PREC, ROLE_READER, false><<<ctas, 128, 0, s>>>(a);
         break;
     default:
-        batched_stage_kernel<128, 6, PREC, ROLE_NONE><<<ctas, 128, 0, s>>>(a);
+        if (a.epilogue)
+            batched_stage_kernel<128, 6, PREC, ROLE_NONE, true><<<ctas, 128, 0, s>>>(a);
+        else
+            batched_stage_kernel<128, 6, PREC, ROLE_NONE, false><<<ctas, 128, 0, s>>>(a);
         break;
     }
     return cudaGetLastError();

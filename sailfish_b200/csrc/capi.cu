@@ -451,8 +451,8 @@ int cbdiso_b200_advance_stage_cached(
     const cbd_epilogue_t *epilogue, double *scratch, double *result, double *face_cache, int role, void *stream)
 {
     // the cache's pairs are loaded and stored as 16-byte vectors
-    if (!face_cache || (reinterpret_cast<uintptr_t>(face_cache) & 15) != 0 ||
-        (role != ROLE_NONE && role != ROLE_READER))
+    if (!face_cache || (reinterpret_cast<uintptr_t>(face_cache) & 15) != 0 || role < ROLE_NONE ||
+        role > ROLE_READER)
         return CBD_ERR_ARGUMENT;
     return advance_stage(grid, stage, stage_dev, primitive_rd, primitive_n, primitive_wr, epilogue, scratch,
                          result, face_cache, role, stream);

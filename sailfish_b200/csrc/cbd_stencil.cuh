@@ -258,10 +258,11 @@ __device__ __forceinline__ double fourth_power(double q)
 // Gravity and sink terms of one mass, added into du (cbdiso_2d.c:97-175).
 // Terms that are exactly zero (no mass, or a zone outside 4 sink radii) are
 // skipped: adding them changes no value. The gravity factor
-// (r^2 + s^2)^-1.5 is taken from *g_in when given (a face-cache value).
+// (r^2 + s^2)^-1.5 is taken from *g_in when given (a face-cache value), and
+// stored to *g_out when given.
 template <bool FAST>
 __device__ __forceinline__ void mass_source(const MassDev &m, double x, double y, double dt, const double *p,
-                                            double *du, const double *g_in = nullptr)
+                                            double *du, const double *g_in = nullptr, double *g_out = nullptr)
 {
     const double sigma = p[0];
     const double dx = x - m.x;
@@ -269,6 +270,8 @@ __device__ __forceinline__ void mass_source(const MassDev &m, double x, double y
     const double r2 = dx * dx + dy * dy;
     if (m.mass != 0.0) {
         const double g = g_in ? *g_in : inv_pow15<FAST>(r2 + m.soft2);
+        if (g_out)
+            *g_out = g;
         const double fnum = sigma * m.mass * g;
         const double fx = -fnum * dx;
         const double fy = -fnum * dy;
@@ -349,37 +352,34 @@ __device__ __forceinline__ void cons_to_prim(const double *u, double *p, const C
     p[2] = copysign(lesser(fabs(div_by<FAST>(u[2], rho, y)), k.vmax), u[2]);
 }
 
-// max |v +- cs| over both directions, cbdiso_2d.c:340-350, given cs = sqrt(cs^2)
-__device__ __forceinline__ double max_wavespeed_cs(const double *p, double cs)
+// max |v +- cs| over both directions, cbdiso_2d.c:340-350
+__device__ __forceinline__ double max_wavespeed(const double *p, double cs2)
 {
+    const double cs = sqrt(cs2);
     const double ax = greater(fabs(p[1] - cs), fabs(p[1] + cs));
     const double ay = greater(fabs(p[2] - cs), fabs(p[2] + cs));
     return greater(ax, ay);
-}
-
-__device__ __forceinline__ double max_wavespeed(const double *p, double cs2)
-{
-    return max_wavespeed_cs(p, sqrt(cs2));
 }
 
 // Source rates of both masses at the end-of-step time with dt = 1 and the
 // reference's on/off switches (cbdiso_2d.py:105-137, cbdiso_2d.c:626-664):
 // rg[p] with gravity only, ra[p] with accretion only, each (mdot, fx, fy).
 // `need` selects which are evaluated (bit p: rg[p], bit 2 + p: ra[p]).
-// `grav` (optional): the zone's gravity factors for these masses, from the
-// face cache; computed here otherwise (the same bits).
 template <bool FAST>
 __device__ __forceinline__ void end_rates(const MassDev *e, int need, double x, double y, const double *p,
-                                          double (&rg)[2][3], double (&ra)[2][3], const double *grav = nullptr)
+                                          double (&rg)[2][3], double (&ra)[2][3])
 {
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         rg[q][0] = rg[q][1] = rg[q][2] = 0.0;
         ra[q][0] = ra[q][1] = ra[q][2] = 0.0;
         if (need & (1 << q)) {
+            // the gravity rates only enter sums whose own rounding (their
+            // summation order) is far above an ulp per zone: rsqrt-based
+            // arithmetic, not the correctly rounded power
             MassDev m = e[q];
             m.sink_rate = 0.0;
-            mass_source<FAST>(m, x, y, 1.0, p, rg[q], grav ? grav + q : nullptr);
+            mass_source<true>(m, x, y, 1.0, p, rg[q]);
         }
         if (need & (4 << q)) {
             MassDev m = e[q];
@@ -463,20 +463,15 @@ __device__ __forceinline__ void diag_value(const cbd_diag_t &d, const MassDev *e
 
 // The end-of-step quantities of one zone, accumulated into acc: slot 0 the
 // CFL wavespeed maximum, slots 1 + 2d, 2 + 2d the diagnostics.
-// With `cached` (the face cache's values for the end-of-step masses): the
-// zone centre's cs^2 and cs = sqrt(cs^2) in cached[0..1], its gravity
-// factors in cached[2..3].
 template <bool FAST>
 __device__ __forceinline__ void accumulate_zone(const Consts &k, const MassDev *e, double x, double y,
-                                                const double *p, double (&acc)[PARTIAL_STRIDE],
-                                                const double *cached = nullptr)
+                                                const double *p, double (&acc)[PARTIAL_STRIDE])
 {
     if (k.want_ws)
-        acc[0] = max_nan(acc[0], cached ? max_wavespeed_cs(p, cached[1])
-                                        : max_wavespeed(p, sound_speed2<FAST>(k, e, x, y)));
+        acc[0] = max_nan(acc[0], max_wavespeed(p, sound_speed2<FAST>(k, e, x, y)));
     if (k.num_diag > 0) {
         double rg[2][3], ra[2][3];
-        end_rates<FAST>(e, k.need_rates, x, y, p, rg, ra, cached ? cached + 2 : nullptr);
+        end_rates<FAST>(e, k.need_rates, x, y, p, rg, ra);
 #pragma unroll
         for (int d = 0; d < MAX_FUSED; ++d) {
             if (d < k.num_diag) {
@@ -609,24 +604,26 @@ struct StageArgs {
 // ---------------------------------------------------------------------------
 // face cache
 //
-// The face sound speeds (cs^2, cs) at every x- and y-face centre, the gravity
-// factors (r^2 + s^2)^-1.5 of both masses at every zone centre and the zone
-// centres' (cs^2, cs) depend only on the mesh, the EOS constants and the
-// point masses' positions, masses and softenings, not on the fluid state.
-// They are evaluated by a fill kernel, an elementwise pass with far more
-// independent arithmetic per thread than the stencil, and loaded by the
-// stage kernels. The host gives each stage launch a role:
-//  * ROLE_READER (every stage on the product path): a fill kernel runs
-//    first; when the cache's key does not match the stage's masses it
-//    computes every value for them. The stage loads them, and its first
-//    thread then writes the key. A step's last stage usually runs with the
-//    masses of the step's end time, which are the next step's first-stage
-//    masses (RK2's second stage at t0 + dt, the next step at
-//    t0 / 2 + (t0 + 2 dt) / 2, equal in all but about 1 step in 5000), so
-//    the next step's first fill finds its key and returns at once: one fill
-//    per step. The epilogue takes the zone-centre values and gravity
-//    factors from the cache when the end-of-step masses are the stage's.
-//  * ROLE_NONE: computes every value in the stencil, no cache.
+// The face sound speeds (cs^2, cs) at every x- and y-face centre and the
+// gravity factors (r^2 + s^2)^-1.5 of both masses at every zone centre depend
+// only on the mesh, the EOS constants and the point masses' positions, masses
+// and softenings, not on the fluid state. A step's last stage usually runs
+// with the masses of the step's end time, which are the next step's
+// first-stage masses (RK2's second stage at t0 + dt, the next step at
+// t0 / 2 + (t0 + 2 dt) / 2, equal in all but about 1 step in 5000). The host
+// gives each stage launch a role:
+//  * ROLE_WRITER (RK2's second stage, RK3's second): computes the values in
+//    its stencil as usual and, when its masses equal its record's
+//    end-of-step masses, also stores them with a key of everything they
+//    depend on (written by one thread).
+//  * ROLE_READER (a step's first stage): a fill kernel runs first; when the
+//    key does not match the stage's masses (a solver's first step, a reset,
+//    the rare time mismatch) it computes every value for them. The stage
+//    loads them and then records the key.
+//  * ROLE_NONE: neither.
+// Evaluating the values inline in the writer costs less than a separate
+// fill pass every step (measured on both the single-grid and the batched
+// path); the fill kernel serves the mismatches.
 // The values are the same bits as recomputing them. Each role is its own
 // kernel, so that each keeps its own register allocation. Launches on one
 // cache must be stream-ordered.
@@ -636,26 +633,23 @@ struct StageArgs {
 //     rows i - 1 and i in column j;
 //   y-faces ni x (nj + 1) pairs: [i][j] is the face between columns j - 1 and
 //     j in row i;
-//   zones ni x nj pairs (g_1, g_2);
-//   zone centres ni x nj pairs (cs^2, cs).
+//   zones ni x nj pairs (g_1, g_2).
 // ---------------------------------------------------------------------------
 
-// role 1 (a stage that stored its own stencil's values) is retired: a fill
-// pass per step costs less than the stencil's inline evaluation
-enum { ROLE_NONE = 0, ROLE_READER = 2 };
-// what one march (march_tile's COP) does with the cache
-enum { CACHE_NONE = 0, CACHE_READ = 2 };
+enum { ROLE_NONE = 0, ROLE_WRITER = 1, ROLE_READER = 2 };
+// what one march (march_tile's COP) does with the cache, by role
+enum { CACHE_NONE = 0, CACHE_WRITE = 1, CACHE_READ = 2 };
 constexpr int CACHE_HEADER = 32;  // doubles
-constexpr int CACHE_KEY = 20;     // doubles of the header in use
+constexpr int CACHE_KEY = 20;     // doubles of the header holding the key
 
 __host__ __device__ inline size_t face_cache_doubles(int ni, int nj)
 {
-    return CACHE_HEADER + 2 * ((size_t)(ni + 1) * nj + (size_t)ni * (nj + 1) + 2 * (size_t)ni * nj);
+    return CACHE_HEADER + 2 * ((size_t)(ni + 1) * nj + (size_t)ni * (nj + 1) + (size_t)ni * nj);
 }
 
-// the four arrays of a cache
+// the three arrays of a cache
 struct CacheArrays {
-    double *xf, *yf, *grav, *centre;
+    double *xf, *yf, *grav;
 };
 
 __host__ __device__ inline CacheArrays cache_arrays(double *fc, int ni, int nj)
@@ -664,7 +658,6 @@ __host__ __device__ inline CacheArrays cache_arrays(double *fc, int ni, int nj)
     c.xf = fc + CACHE_HEADER;
     c.yf = c.xf + 2 * (size_t)(ni + 1) * nj;
     c.grav = c.yf + 2 * (size_t)ni * (nj + 1);
-    c.centre = c.grav + 2 * (size_t)ni * nj;
     return c;
 }
 
@@ -718,9 +711,8 @@ __device__ void cache_write_key(const Consts &k, const StageDev &st, double *fc)
         fc[v] = cache_key_value<PREC>(k, st.m, v);
 }
 
-// The cached values depend on these fields of the masses only: when the
-// end-of-step masses agree with the stage's in them, the epilogue may use
-// the stage's cache (the same answer in every thread).
+// The cached values depend on these fields of the masses only (the same
+// answer in every thread).
 __device__ __forceinline__ bool same_cached_inputs(const StageDev &st)
 {
     bool same = true;
@@ -729,6 +721,17 @@ __device__ __forceinline__ bool same_cached_inputs(const StageDev &st)
         same = same && same_bits(st.m[p].x, st.e[p].x) && same_bits(st.m[p].y, st.e[p].y) &&
                same_bits(st.m[p].mass, st.e[p].mass) && same_bits(st.m[p].soft2, st.e[p].soft2);
     return same;
+}
+
+// A writer stores the values when its masses are the end-of-step masses (the
+// same answer in every thread); `key_writer` (one thread) then writes the key.
+template <int PREC>
+__device__ bool cache_write_check(const Consts &k, const StageDev &st, double *fc, bool key_writer)
+{
+    const bool end_masses = same_cached_inputs(st);
+    if (end_masses && key_writer)
+        cache_write_key<PREC>(k, st, fc);
+    return end_masses;
 }
 
 __device__ __forceinline__ double2 cache_load(const double *p)
@@ -762,12 +765,13 @@ __device__ __forceinline__ StageSmem<BJ> &stage_smem()
 // One tile of the march: columns c0 .. c0 + width - 1 (width <= BJ) and rows
 // r0 .. r0 + k.rows_per_cta - 1 of one grid. `st` must live in shared memory
 // and be visible after the first barrier; epilogue values of the updated
-// zones are accumulated into `acc`. `COP` (CACHE_*) says whether the tile
-// loads the face-cache values from args.fcache. All threads of the block must
-// call it.
-template <int BJ, bool FAST, int COP = CACHE_NONE>
+// zones are accumulated into `acc` when EPI (the launch has an epilogue;
+// without, its code is left out). `COP` (CACHE_*) says what the tile does
+// with args.fcache: CACHE_WRITE stores the face and gravity values if
+// `store`, CACHE_READ loads them. All threads of the block must call it.
+template <int BJ, bool FAST, int COP = CACHE_NONE, bool EPI = true>
 __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, const StageArgs &args, int c0,
-                                           int width, int r0, double (&acc)[PARTIAL_STRIDE])
+                                           int width, int r0, double (&acc)[PARTIAL_STRIDE], bool store = false)
 {
     constexpr int cop = COP;
     StageSmem<BJ> &sm = stage_smem<BJ>();
@@ -791,22 +795,21 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
     double *const cfx = cop != CACHE_NONE ? cache.xf : nullptr;
     double *const cfy = cop != CACHE_NONE ? cache.yf : nullptr;
     double *const cfz = cop != CACHE_NONE ? cache.grav : nullptr;
-    // a reader's epilogue takes the zone-centre values and gravity factors
-    // from the cache when the end-of-step masses are the stage's
-    const bool epi_cached = cop == CACHE_READ && (k.want_ws || k.num_diag > 0) && same_cached_inputs(st);
 
     auto zone = [&](const double *base, int i, int jj) -> const double * {
         return base + (size_t)(i + NG) * row_stride + (size_t)(jj + NG) * NQ;
     };
     // Row i (zones c0-2 .. c0+W+1) into ring slot `slot`, as asynchronous
-    // copies: coalesced over the row's contiguous AoS bytes, scattered into
-    // the field-major shared layout.
+    // copies into the field-major shared layout: thread t copies the three
+    // fields of column t (a warp's copies of one field together cover its
+    // columns' contiguous AoS bytes), and threads 0..3 also the last four
+    // columns when the strip is full.
     auto fetch_row = [&](int slot, int i) {
         const double *src = args.prd + (size_t)(i + NG) * row_stride + (size_t)c0 * NQ;
-        const int n = NQ * (W + 4);
-        for (int d = t; d < n; d += BJ) {
-            const int kk = d / 3;
-            async_copy8(&sp[slot][d - 3 * kk][kk], src + d);
+        for (int kk = t; kk < W + 4; kk += BJ) {
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+                async_copy8(&sp[slot][q][kk], src + NQ * kk + q);
         }
     };
     // The zone (i, j) of the u_n source array, for this thread's own update.
@@ -849,7 +852,7 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
 
         // cached face sound speeds and gravity factors of this row, loaded
         // ahead of the slopes so that their latency overlaps them
-        double2 c_xf = make_double2(0.0, 0.0), c_yf = c_xf, c_ye = c_xf, c_z = c_xf, c_c = c_xf;
+        double2 c_xf = make_double2(0.0, 0.0), c_yf = c_xf, c_ye = c_xf, c_z = c_xf;
         if (cop == CACHE_READ) {
             if (r >= r0 - 1 && active)
                 c_xf = cache_load(cfx + 2 * ((size_t)(r + 1) * nj + j));
@@ -857,8 +860,6 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 if (active) {
                     c_yf = cache_load(cfy + 2 * ((size_t)r * (nj + 1) + j));
                     c_z = cache_load(cfz + 2 * ((size_t)r * nj + j));
-                    if (epi_cached)
-                        c_c = cache_load(cache.centre + 2 * ((size_t)r * nj + j));
                 }
                 if (t == FACE_LANE)
                     c_ye = cache_load(cfy + 2 * ((size_t)r * (nj + 1) + c0 + W));
@@ -924,6 +925,9 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 const double cs2 = sound_speed2<FAST>(k, st.m, xf, yc);
                 double cs;
                 hlle<FAST, 0>(pl, pr, cs2, cs, f1);
+                // face r + 1/2 is stored by the tile below it, except the first
+                if (cop == CACHE_WRITE && store && (r >= r0 || r0 == 0))
+                    cache_store(cfx + 2 * ((size_t)(r + 1) * nj + j), cs2, cs);
             }
             if (viscous) {
                 f1[1] -= k.half_nu * (rs0[0] + rs1[0]);
@@ -959,6 +963,9 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                     const double cs2 = sound_speed2<FAST>(k, st.m, xc, yf);
                     double cs;
                     hlle<FAST, 1>(pl, pr, cs2, cs, g);
+                    // the strip's last face is stored by the next strip, except the last
+                    if (cop == CACHE_WRITE && store && (pass == 0 || c0 + W == nj))
+                        cache_store(cfy + 2 * ((size_t)r * (nj + 1) + c0 + fidx), cs2, cs);
                 }
                 if (viscous) {
                     g[1] -= k.half_nu * (srs[g0][1][fidx] + srs[g0][1][fidx + 1]);
@@ -1004,6 +1011,12 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
             if (cop == CACHE_READ) {
                 mass_source<FAST>(st.m[0], xc, yc, dt, pc, du, &c_z.x);
                 mass_source<FAST>(st.m[1], xc, yc, dt, pc, du, &c_z.y);
+            } else if (cop == CACHE_WRITE) {
+                double grav1 = 0.0, grav2 = 0.0;
+                mass_source<FAST>(st.m[0], xc, yc, dt, pc, du, nullptr, &grav1);
+                mass_source<FAST>(st.m[1], xc, yc, dt, pc, du, nullptr, &grav2);
+                if (store)
+                    cache_store(cfz + 2 * ((size_t)r * nj + j), grav1, grav2);
             } else {
                 mass_source<FAST>(st.m[0], xc, yc, dt, pc, du);
                 mass_source<FAST>(st.m[1], xc, yc, dt, pc, du);
@@ -1022,25 +1035,29 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
             cons_to_prim<FAST>(u, pn, k);
 
             // store the zone and, on the edges, its zero-gradient guard images
-            const int ilo = (r == 0 && k.write_guards) ? -2 : r;
-            const int ihi = (r == ni - 1 && k.write_guards) ? ni + 1 : r;
-            const int jlo = (j == 0 && k.write_guards) ? -2 : j;
-            const int jhi = (j == nj - 1 && k.write_guards) ? nj + 1 : j;
-            for (int ii = ilo; ii <= ihi; ++ii) {
-                for (int jj = jlo; jj <= jhi; ++jj) {
-                    double *z = args.pwr + (size_t)(ii + NG) * row_stride + (size_t)(jj + NG) * NQ;
-                    z[0] = pn[0];
-                    z[1] = pn[1];
-                    z[2] = pn[2];
+            const bool edge = k.write_guards && (r == 0 || r == ni - 1 || j == 0 || j == nj - 1);
+            if (!edge) {
+                double *z = args.pwr + (size_t)(r + NG) * row_stride + (size_t)(j + NG) * NQ;
+                z[0] = pn[0];
+                z[1] = pn[1];
+                z[2] = pn[2];
+            } else {
+                const int ilo = r == 0 ? -2 : r;
+                const int ihi = r == ni - 1 ? ni + 1 : r;
+                const int jlo = j == 0 ? -2 : j;
+                const int jhi = j == nj - 1 ? nj + 1 : j;
+                for (int ii = ilo; ii <= ihi; ++ii) {
+                    for (int jj = jlo; jj <= jhi; ++jj) {
+                        double *z = args.pwr + (size_t)(ii + NG) * row_stride + (size_t)(jj + NG) * NQ;
+                        z[0] = pn[0];
+                        z[1] = pn[1];
+                        z[2] = pn[2];
+                    }
                 }
             }
 
-            if (epi_cached) {
-                const double cached[4] = {c_c.x, c_c.y, c_z.x, c_z.y};
-                accumulate_zone<FAST>(k, st.e, xc, yc, pn, acc, cached);
-            } else {
+            if (EPI)
                 accumulate_zone<FAST>(k, st.e, xc, yc, pn, acc);
-            }
         }
 
 #pragma unroll
@@ -1056,8 +1073,9 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
 }
 
 // One RK stage on one grid: CTA (x, y) marches strip x, segment y. ROLE
-// (ROLE_*) is what the launch does with args.fcache.
-template <int BJ, int MINB, int PREC, int ROLE = ROLE_NONE>
+// (ROLE_*) is what the launch does with args.fcache; EPI whether it has an
+// epilogue (k.want_ws or k.num_diag).
+template <int BJ, int MINB, int PREC, int ROLE = ROLE_NONE, bool EPI = true>
 __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const StageDev st_param, StageArgs args)
 {
     constexpr bool FAST = PREC == CBD_PRECISION_FAST;
@@ -1073,16 +1091,20 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
     __syncthreads();
     if (st.halt)
         return;
-    if (ROLE == ROLE_READER) {
-        march_tile<BJ, FAST, CACHE_READ>(k, st, args, c0, BJ, r0, acc);
+    if (ROLE == ROLE_WRITER) {
+        const bool store = cache_write_check<PREC>(k, st, args.fcache,
+                                                   threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0);
+        march_tile<BJ, FAST, CACHE_WRITE, EPI>(k, st, args, c0, BJ, r0, acc, store);
+    } else if (ROLE == ROLE_READER) {
+        march_tile<BJ, FAST, CACHE_READ, EPI>(k, st, args, c0, BJ, r0, acc);
         // the fill kernel before this launch made the values valid for these
         // masses; say so for the next fill (no one reads the key meanwhile)
         if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0)
             cache_write_key<PREC>(k, st, args.fcache);
     } else {
-        march_tile<BJ, FAST, CACHE_NONE>(k, st, args, c0, BJ, r0, acc);
+        march_tile<BJ, FAST, CACHE_NONE, EPI>(k, st, args, c0, BJ, r0, acc);
     }
-    if (k.want_ws || k.num_diag > 0) {
+    if (EPI) {
         double red[PARTIAL_STRIDE];
         block_reduce<BJ>(acc, sred, red);
         grid_finish<BJ>(red, 1 + 2 * k.num_diag, args.scratch, k.want_ws ? args.result : nullptr, args.result + 1,
@@ -1092,8 +1114,8 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
 
 // Every cached value at mesh point (i, j), 0 <= i <= ni, 0 <= j <= nj, for
 // the masses m, with the stage kernel's own expressions: the x-face pair
-// (i, j) when j < nj, the y-face pair when i < ni, and when both are inside
-// the zone's gravity factors and its centre's (cs^2, cs) (the epilogue's).
+// (i, j) when j < nj, the y-face pair when i < ni, and the zone's gravity
+// factors when both are inside.
 template <bool FAST>
 __device__ __forceinline__ void face_cache_fill_point(const Consts &k, const MassDev *m, const CacheArrays &c,
                                                       int i, int j)
@@ -1122,8 +1144,6 @@ __device__ __forceinline__ void face_cache_fill_point(const Consts &k, const Mas
             }
         }
         cache_store(c.grav + 2 * ((size_t)i * nj + j), g[0], g[1]);
-        const double cs2 = sound_speed2<FAST>(k, m, xc, yc);
-        cache_store(c.centre + 2 * ((size_t)i * nj + j), cs2, sqrt(cs2));
     }
 }
 
@@ -1145,13 +1165,19 @@ __device__ __forceinline__ void face_cache_fill_tile(const Consts &k, const Mass
 }
 
 // Makes the face cache valid for a reader stage: when its key does not match
-// the stage's masses, every CTA fills its tile of the values for those
-// masses (the reader stage then writes the key). Grid: the stage kernel's
-// (strips, segments) of BJ columns x k.rows_per_cta rows. A halted record
-// (a stopped device stepper) fills nothing.
+// the stage's masses, the CTAs fill the stage's tiles (`strips` x `tiles /
+// strips` of BJ columns x k.rows_per_cta rows), CTA b taking tiles b,
+// b + gridDim.x, ..., with the values for those masses (the reader stage then
+// writes the key). A grid of a few CTAs per SM keeps the common case, a
+// matching key, to one check per CTA. A halted record (a stopped device
+// stepper) fills nothing. The evaluation is long chains of dependent
+// operations: many warps per SM, registers capped to allow them.
+constexpr int FILL_WARPS_PER_SM = 24;
+
 template <int BJ, int PREC>
-__global__ void __launch_bounds__(BJ) face_cache_fill_kernel(const Consts k, const StageDev st_param,
-                                                             const StageDev *stage_dev, double *fc)
+__global__ void __launch_bounds__(BJ, FILL_WARPS_PER_SM * 32 / BJ)
+    face_cache_fill_kernel(const Consts k, const StageDev st_param, const StageDev *stage_dev, double *fc, int strips,
+                           int tiles)
 {
     __shared__ StageDev st;
     __shared__ int fill;
@@ -1162,8 +1188,9 @@ __global__ void __launch_bounds__(BJ) face_cache_fill_kernel(const Consts k, con
     __syncthreads();
     if (!fill)
         return;
-    face_cache_fill_tile<BJ, PREC == CBD_PRECISION_FAST>(k, st.m, fc, blockIdx.x * BJ, BJ,
-                                                         blockIdx.y * k.rows_per_cta, k.rows_per_cta);
+    for (int u = blockIdx.x; u < tiles; u += gridDim.x)
+        face_cache_fill_tile<BJ, PREC == CBD_PRECISION_FAST>(k, st.m, fc, (u % strips) * BJ, BJ,
+                                                             (u / strips) * k.rows_per_cta, k.rows_per_cta);
 }
 
 }  // namespace cbd

@@ -54,9 +54,8 @@ def test_face_cache_and_adjoint_settings_host_checks():
     (nothing is launched)."""
     lib = _capi.lib()
     g = _capi.Grid(ni=8, nj=6, xl=-1.0, xr=1.0, yl=-1.0, yr=1.0, eos_type=2, mach2=100.0, plm_theta=1.5)
-    # header, (cs^2, cs) pairs of every x- and y-face, (g_1, g_2) of every zone
-    # and (cs^2, cs) of every zone centre
-    assert lib.cbdiso_b200_face_cache_bytes(ctypes.byref(g)) == 8 * (32 + 2 * (9 * 6 + 8 * 7 + 2 * 8 * 6))
+    # header, (cs^2, cs) pairs of every x- and y-face and (g_1, g_2) of every zone
+    assert lib.cbdiso_b200_face_cache_bytes(ctypes.byref(g)) == 8 * (32 + 2 * (9 * 6 + 8 * 7 + 8 * 6))
     assert lib.cbdiso_b200_face_cache_bytes(ctypes.byref(_capi.Grid(ni=0, nj=6))) == 0
     st = _capi.Stage()
     a, b = ctypes.c_void_p(0x1000), ctypes.c_void_p(0x2000)
@@ -64,7 +63,6 @@ def test_face_cache_and_adjoint_settings_host_checks():
     assert lib.cbdiso_b200_advance_stage_cached(*args, None, 2, None) == 1            # no cache
     assert lib.cbdiso_b200_advance_stage_cached(*args, ctypes.c_void_p(0x1008), 2, None) == 1  # not 16-byte aligned
     assert lib.cbdiso_b200_advance_stage_cached(*args, ctypes.c_void_p(0x3000), 3, None) == 1  # unknown role
-    assert lib.cbdiso_b200_advance_stage_cached(*args, ctypes.c_void_p(0x3000), 1, None) == 1  # retired role
     # disk records take an even, non-negative cache offset
     rec = (ctypes.c_char * int(lib.cbdiso_b200_batch_disk_bytes()))()
     assert lib.cbdiso_b200_batch_disk_set_face_cache(rec, -2) == 1

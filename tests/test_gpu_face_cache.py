@@ -1,11 +1,9 @@
 """
-The face cache (cbdiso_b200_advance_stage_cached): a fill pass computes the
-face sound speeds, zone gravity factors and zone-centre sound speeds for a
-stage's point masses when the cache's key does not match them, and every
-stage loads them (the epilogue too, when the end-of-step masses are the
-stage's). A step's last stage has the next step's first-stage masses, so the
-values are computed once per step. In EXACT precision states, dts and
-reductions must be bit-identical to recomputing them in every stage.
+The face cache (cbdiso_b200_advance_stage_cached): the stage at t0 + dt stores
+the face sound speeds and zone gravity factors for its point masses, and the
+next step's first stage loads them (after a fill pass when the key does not
+match its masses). In EXACT precision states, dts and reductions must be
+bit-identical to recomputing them in every stage.
 """
 
 import ctypes
@@ -93,22 +91,6 @@ def _face_values(s, time):
     return -phi / g.mach2
 
 
-def _centre_values(s, time):
-    """cs^2 at the zone centres, as _face_values."""
-    g = s._grid
-    ni, nj = g.ni, g.nj
-    dx, dy = (g.xr - g.xl) / ni, (g.yr - g.yl) / nj
-    x = g.xl + (np.arange(ni, dtype=np.float64)[:, None] + 0.5) * dx
-    y = g.yl + (np.arange(nj, dtype=np.float64)[None, :] + 0.5) * dy
-    phi = np.zeros((ni, nj))
-    for m in s._point_masses(time):
-        if m.mass > 0.0:
-            dxm, dym = x - m.position_x, y - m.position_y
-            r2 = dxm * dxm + dym * dym
-            phi -= m.mass / np.sqrt(r2 + m.softening_length * m.softening_length)
-    return -phi / g.mach2
-
-
 def test_cache_holds_the_end_of_step_face_sound_speeds():
     d = load("cbd_t15_n64")
     s = product_solver(d, "exact", face_cache=True)
@@ -122,11 +104,35 @@ def test_cache_holds_the_end_of_step_face_sound_speeds():
     want = _face_values(s, s.time)
     assert np.array_equal(pairs[..., 0], want)
     assert np.array_equal(pairs[..., 1], np.sqrt(want))
-    off = 32 + 2 * ((ni + 1) * nj + ni * (nj + 1) + ni * nj)
-    centre = c[off:off + 2 * ni * nj].reshape(ni, nj, 2)
-    want = _centre_values(s, s.time)
-    assert np.array_equal(centre[..., 0], want)
-    assert np.array_equal(centre[..., 1], np.sqrt(want))
+
+
+def test_fill_pass_holds_the_stage_values():
+    """A reader's fill pass computes the face sound speeds for the stage's
+    masses when the key does not match them (here: a new cache)."""
+    from sailfish_b200 import _capi
+
+    d = load("cbd_t15_n64")
+    s = product_solver(d, "exact", face_cache=True)
+    lib, g = s._lib, s._grid
+    st = _capi.Stage()
+    m1, m2 = s._point_masses(0.25)
+    from sailfish_b200.cbdiso_2d import _mass_struct
+
+    _mass_struct(m1, st.mass[0])
+    _mass_struct(m2, st.mass[1])
+    st.a, st.dt, st.buffer_central_mass = 0.0, 1e-4, m1.mass + m2.mass
+    out = torch.empty_like(s._buf[1])
+    assert lib.cbdiso_b200_advance_stage_cached(ctypes.byref(g), ctypes.byref(st), None, s._ptr(s._buf[0]), None,
+                                                s._ptr(out), None, None, None, s._ptr(s._fcache), 2,
+                                                s._stream()) == 0
+    torch.cuda.synchronize()
+    c = s._fcache.cpu().numpy()
+    ni, nj = g.ni, g.nj
+    assert c[0] == 20261204.5  # the reader recorded the key
+    pairs = c[32:32 + 2 * (ni + 1) * nj].reshape(ni + 1, nj, 2)
+    want = _face_values(s, 0.25)
+    assert np.array_equal(pairs[..., 0], want)
+    assert np.array_equal(pairs[..., 1], np.sqrt(want))
 
 
 def test_cache_after_reset():
@@ -159,10 +165,8 @@ def test_cached_entry_rejects_a_misaligned_cache():
     assert lib.cbdiso_b200_advance_stage_cached(*args, ctypes.c_void_p(s._fcache.data_ptr() + 8), 2,
                                                 s._stream()) == 1  # invalid argument
     assert lib.cbdiso_b200_advance_stage_cached(*args, s._ptr(s._fcache), 3, s._stream()) == 1
-    # role 1 (a stage storing its own stencil's values) is retired
-    assert lib.cbdiso_b200_advance_stage_cached(*args, s._ptr(s._fcache), 1, s._stream()) == 1
     assert int(s._lib.cbdiso_b200_face_cache_bytes(ctypes.byref(s._grid))) == \
-        8 * (32 + 2 * (65 * 64 + 64 * 65 + 2 * 64 * 64))
+        8 * (32 + 2 * (65 * 64 + 64 * 65 + 64 * 64))
 
 
 @pytest.mark.parametrize("name", ["gam_n64", "gam_n40_soft_inviscid", "gam_n48_cool_p2", "gam_n256"])
