@@ -304,9 +304,12 @@ class AdjointRun:
         """
         dJ/dprim0 (ni, nj, 3) and dJ/d(q, e, nu, sink_rate) for
         J = weights[0] * mean accretion + weights[1] * mean torque, at the
-        last forward(keep=True) run. With `graph`, the reverse sweep of a full
-        segment is captured once in a CUDA graph and replayed for every full
-        segment (its stage records and Jacobians staged into fixed buffers).
+        last forward(keep=True) run. With `graph`, the sweep runs from CUDA
+        graphs: over a stored trajectory one graph for the whole run;
+        otherwise one graph per full segment that reverses it while the
+        segment before it in time is recomputed from its checkpoint on a
+        second stream (two buffer sets, the stage records and Jacobians staged
+        into them). The results are the same bits either way.
         """
         import torch
 
@@ -333,15 +336,32 @@ class AdjointRun:
             else:
                 sweep.run(history, jac, steps, states=trajectory)
             return sweep.finish()
-        for start in reversed(range(0, steps, K)):
-            stop = min(start + K, steps)
-            sweep.p[0].copy_(f["checkpoints"][start])
-            if graph and stop - start == sweep.k:
-                sweep.hist.copy_(history[start * 2 * nb:stop * 2 * nb])
-                sweep.jac.copy_(jac[start:stop])
-                sweep.replay()
-            else:
+        segments = [(start, min(start + K, steps)) for start in reversed(range(0, steps, K))]
+        cps = f["checkpoints"]
+        if graph and segments and segments[0][1] - segments[0][0] != sweep.k:
+            # a short last segment (reversed first): eagerly
+            start, stop = segments.pop(0)
+            sweep.p[0].copy_(cps[start])
+            sweep.run(history[start * 2 * nb:stop * 2 * nb], jac[start:stop], stop - start)
+        if not graph:
+            for start, stop in segments:
+                sweep.p[0].copy_(cps[start])
                 sweep.run(history[start * 2 * nb:stop * 2 * nb], jac[start:stop], stop - start)
+            return sweep.finish()
+        # full segments, pipelined: segment i is reversed while segment i + 1
+        # (earlier in time) is recomputed into the other buffer set
+        if segments:
+            start, stop = segments[0]
+            sweep.stage(0, cps[start], history[start * 2 * nb:stop * 2 * nb], jac[start:stop])
+            sweep.replay_recompute(0)
+        b = 0
+        for i in range(len(segments)):
+            more = i + 1 < len(segments)
+            if more:
+                start, stop = segments[i + 1]
+                sweep.stage(1 - b, cps[start], history[start * 2 * nb:stop * 2 * nb], jac[start:stop])
+            sweep.replay_pipeline(b, more)
+            b = 1 - b
         return sweep.finish()
 
     def _sweep(self, s, k, w):
@@ -407,11 +427,14 @@ class AdjointRun:
 
 class _ReverseSweep:
     """
-    Buffers of the reverse sweep over one segment of k steps: the recomputed
-    states p[0..k] and stage-1 outputs (none for k = 0: the states come
-    from a recorded trajectory), the adjoint states, the adjoint workspace
-    and the chained parameter accumulator; and the CUDA graph of a full
-    segment, reading its stage records and Jacobians from `hist` and `jac`.
+    Buffers of the reverse sweep over segments of k steps: two sets (0, 1) of
+    the recomputed states p[0..k] and stage-1 outputs with their staged stage
+    records and Jacobians (none for k = 0: the states come from a recorded
+    trajectory), the adjoint states, the adjoint workspace and the chained
+    parameter accumulator; and CUDA graphs of a full segment. The recompute of
+    a segment needs only its checkpoint and stage records, not the adjoint, so
+    in the graphed sweep one set's segment is reversed while the other set's
+    (the next segment back in time) is recomputed on a second stream.
     """
 
     def __init__(self, lib, s, k, w, key):
@@ -423,8 +446,10 @@ class _ReverseSweep:
         shape = s._buf[0].shape
         f64 = dict(dtype=torch.float64, device=s.device)
         self.nb = int(lib.cbdiso_b200_stage_record_bytes())
-        self.p = [torch.empty(shape, **f64) for _ in range(k + 1)]
-        self.stars = [torch.empty(shape, **f64) for _ in range(k)]
+        nsets = 2 if k > 0 else 1
+        self.pset = [[torch.empty(shape, **f64) for _ in range(k + 1)] for _ in range(nsets)]
+        self.sset = [[torch.empty(shape, **f64) for _ in range(k)] for _ in range(nsets)]
+        self.p, self.stars = self.pset[0], self.sset[0]
         self.lam = torch.zeros(shape, **f64)
         self.lam_n = torch.zeros(shape, **f64)
         self.lam_star = torch.empty(shape, **f64)
@@ -433,16 +458,34 @@ class _ReverseSweep:
         self.chain = torch.zeros(self.rows * 4, **f64)
         self.scratch = torch.zeros(int(lib.cbdiso_b200_scratch_bytes(g)) // 8 + 8, **f64)
         self.result = torch.zeros(64, **f64)
-        self.hist = torch.empty(max(k, 1) * 2 * self.nb, dtype=torch.uint8, device=s.device)
-        self.jac = torch.empty((max(k, 1), 60), **f64)
-        self.graph = None
+        self.hset = [torch.empty(max(k, 1) * 2 * self.nb, dtype=torch.uint8, device=s.device) for _ in range(nsets)]
+        self.jset = [torch.empty((max(k, 1), 60), **f64) for _ in range(nsets)]
+        self.hist, self.jac = self.hset[0], self.jset[0]
+        self.graphs = {}
 
-    def run(self, hist, jac, count, states=None):
-        """The recompute and reverse sweep of one segment of `count` steps,
-        with stage records `hist` (2 per step) and Jacobians `jac`
-        (count x 60: stage 1, stage 2, end of step, 10 x 2 each). With
-        `states` (a recorded trajectory: u_n at 2n, the first stage's output
-        at 2n + 1) nothing is recomputed."""
+    def recompute(self, p, stars, hist, count):
+        """The segment's states from p[0] with the recorded stage records,
+        keeping every state (the in-place final stage is replayed out of
+        place: inputs star, p[n] -> p[n + 1]), on the current stream."""
+        import torch
+
+        lib, g, nb = self.lib, ctypes.byref(self.grid), self.nb
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        P = lambda t: ctypes.c_void_p(t.data_ptr())
+        rec = lambda n, k: ctypes.c_void_p(hist.data_ptr() + (2 * n + k) * nb)
+        s1, s2 = _capi.Stage(), _capi.Stage()
+        s2.a = 0.5
+        for n in range(count):
+            _capi.check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s1), rec(n, 0), P(p[n]), None, P(stars[n]),
+                                                      None, None, None, stream), "advance_stage")
+            _capi.check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s2), rec(n, 1), P(stars[n]), P(p[n]),
+                                                      P(p[n + 1]), None, None, None, stream), "advance_stage")
+
+    def reverse(self, p, stars, hist, jac, count):
+        """The reverse sweep over one segment of `count` steps whose states
+        are p[0..count] and stars, with stage records `hist` (2 per step) and
+        Jacobians `jac` (count x 60: stage 1, stage 2, end of step, 10 x 2
+        each), on the current stream."""
         import torch
 
         lib, g, nb = self.lib, ctypes.byref(self.grid), self.nb
@@ -450,22 +493,8 @@ class _ReverseSweep:
         P = lambda t: ctypes.c_void_p(t.data_ptr())
         rec = lambda n, k: ctypes.c_void_p(hist.data_ptr() + (2 * n + k) * nb)
         jp = lambda n, k: ctypes.c_void_p(jac.data_ptr() + (60 * n + 20 * k) * 8)
-        s1, s2 = _capi.Stage(), _capi.Stage()
-        s2.a = 0.5
-        if states is not None:
-            p, stars = states[0::2], states[1::2]
-        else:
-            p, stars = self.p, self.stars
-        scratch, result, ws, chain = P(self.scratch), P(self.result), P(self.ws), P(self.chain)
+        ws, chain = P(self.ws), P(self.chain)
         check = _capi.check
-        # recompute the segment from p[0] with the recorded stage records,
-        # keeping every state (the in-place final stage is replayed out of
-        # place: inputs star, p[n] -> p[n + 1])
-        for n in range(count if states is None else 0):
-            check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s1), rec(n, 0), P(p[n]), None, P(stars[n]), None,
-                                                scratch, result, stream), "advance_stage")
-            check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s2), rec(n, 1), P(stars[n]), P(p[n]), P(p[n + 1]),
-                                                None, scratch, result, stream), "advance_stage")
         lam, lam_n, lam_star = self.lam, self.lam_n, self.lam_star
         for n in reversed(range(count)):
             pn, star, out = p[n], stars[n], p[n + 1]
@@ -487,19 +516,62 @@ class _ReverseSweep:
             self.lam.copy_(lam)
             self.lam_n.zero_()
 
-    def replay(self):
+    def run(self, hist, jac, count, states=None):
+        """Recompute (into set 0) and reverse one segment of `count` steps.
+        With `states` (a recorded trajectory: u_n at 2n, the first stage's
+        output at 2n + 1) nothing is recomputed."""
+        if states is not None:
+            p, stars = states[0::2], states[1::2]
+        else:
+            p, stars = self.p, self.stars
+            self.recompute(p, stars, hist, count)
+        self.reverse(p, stars, hist, jac, count)
+
+    def stage(self, b, checkpoint, hist, jac):
+        """Stage a full segment's inputs into set b."""
+        self.pset[b][0].copy_(checkpoint)
+        self.hset[b].copy_(hist)
+        self.jset[b].copy_(jac)
+
+    def _graph(self, key, body):
         import torch
 
-        if self.graph is None:
+        graph = self.graphs.get(key)
+        if graph is None:
             side = torch.cuda.Stream()
             side.wait_stream(torch.cuda.current_stream())
             graph = torch.cuda.CUDAGraph()
             # capture records the launches without running them
             with capture(graph, side):
-                self.run(self.hist, self.jac, self.k)
+                body(side)
             torch.cuda.current_stream().wait_stream(side)
-            self.graph = graph
-        self.graph.replay()
+            self.graphs[key] = graph
+        graph.replay()
+
+    def replay_recompute(self, b):
+        """Recompute the segment staged in set b (one CUDA graph)."""
+        self._graph(("recompute", b),
+                    lambda side: self.recompute(self.pset[b], self.sset[b], self.hset[b], self.k))
+
+    def replay_pipeline(self, b, recompute_other):
+        """Reverse the segment of set b and, when `recompute_other`, recompute
+        the segment staged in the other set on a second stream at the same
+        time (one CUDA graph)."""
+        import torch
+
+        o = 1 - b
+
+        def body(side):
+            if recompute_other:
+                other = torch.cuda.Stream()
+                other.wait_stream(side)
+                with torch.cuda.stream(other):
+                    self.recompute(self.pset[o], self.sset[o], self.hset[o], self.k)
+            self.reverse(self.pset[b], self.sset[b], self.hset[b], self.jset[b], self.k)
+            if recompute_other:
+                side.wait_stream(other)
+
+        self._graph(("pipeline", b, bool(recompute_other)), body)
 
     def replay_stored(self, hist, jac, count, states):
         """The whole sweep over a stored trajectory from one CUDA graph,
