@@ -593,30 +593,31 @@ def adjoint_extra(cases=((512, 400), (2048, 100))):
     return out
 
 
-def batched_adjoint_extra():
-    """32 disks (half 256^2, half 512^2; own q, e, nu), 200 steps: forward
-    with stored states plus gradient over 8 streams, against the batched
-    forward of the same disks."""
+def batched_adjoint_extra(plain_value):
+    """32 disks (half 256^2, half 512^2; own q, e, nu), 200 steps, stored
+    states: the whole batch's forward and adjoint captured as one CUDA graph
+    (one branch per disk) and replayed, against the batched forward of the
+    same disks (the persistent tile-queue kernel) and the plain single-grid
+    throughput; CUDA events. The eager forward and gradient (disks over 8
+    streams and host threads) are timed beside it for the breakdown."""
     import torch
 
     from sailfish_b200.adjoint import BatchedAdjoint, config4_disks
     from sailfish_b200.batched import BatchedSolver, Disk
 
     disks = config4_disks(32)
-    batch = BatchedAdjoint(disks, steps=200, streams=8)
+    steps = 200
+    batch = BatchedAdjoint(disks, steps=steps, streams=8, store_states=True)
     batch.forward(freeze=True, keep=True)
     batch.gradient((1.0, 0.0))
-    # warm-up with the frozen dt sequences (records this form's CUDA graphs)
-    batch.forward(keep=True)
-    batch.gradient((1.0, 0.0))
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    batch.forward(keep=True)
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    batch.gradient((1.0, 0.0))
-    torch.cuda.synchronize()
-    t2 = time.perf_counter()
+    fwd_eager = _event_ms(lambda: batch.forward(keep=True))
+    grad_eager = _event_ms(lambda: batch.gradient((1.0, 0.0)))
+    batch.capture((1.0, 0.0))
+    batch.replay()
+    graph_ms = min(_event_ms(batch.replay) for _ in range(3))
+    batch.results()
+    batch.replay(gradient=False)
+    graph_fwd_ms = min(_event_ms(lambda: batch.replay(gradient=False)) for _ in range(3))
     members = []
     for d, r, p in zip(disks, batch.runs, batch.prims):
         setup = r.setup(d.params)
@@ -625,18 +626,20 @@ def batched_adjoint_extra():
                                             dict(quantity="mdot", which_mass=2, accretion=True),
                                             dict(quantity="torque", which_mass="both", gravity=True)])
     b.run(16)
-    torch.cuda.synchronize()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record()
-    b.run(200)
-    stop.record()
-    torch.cuda.synchronize()
-    fwd = start.elapsed_time(stop) * 1e-3
+    fwd_batched = _event_ms(lambda: b.run(steps))
+    zones = sum(d.resolution ** 2 for d in disks)
+    value = zones * steps / (graph_ms * 1e-3)
+    del batch, b
+    torch.cuda.empty_cache()
     return {"workload": "32 disks (16 x 256^2, 16 x 512^2), own q / e / nu, 200 RK2 steps, gradients of the "
-                        "mean accretion rate", "forward_stored_s": t1 - t0, "gradient_s": t2 - t1,
-            "batched_forward_s": fwd, "gradient_vs_batched_forward": (t2 - t1) / fwd,
-            "forward_plus_gradient_vs_batched_forward": (t2 - t0) / fwd,
-            "timing": "host wall clock (forward + gradient), CUDA events (batched forward)"}
+                        "mean accretion rate, stored states",
+            "forward_plus_gradient_graph_ms": graph_ms, "forward_graph_ms": graph_fwd_ms,
+            "batched_forward_ms": fwd_batched,
+            "forward_plus_gradient_vs_batched_forward": graph_ms / fwd_batched,
+            "gradient_vs_batched_forward": (graph_ms - graph_fwd_ms) / fwd_batched,
+            "eager_forward_ms": fwd_eager, "eager_gradient_ms": grad_eager,
+            "zone_updates_per_s": value, "vs_plain_single_grid": value / plain_value,
+            "timing": "CUDA events; forward + gradient as one captured graph with a branch per disk"}
 
 
 GAM_SIZE = 2048
@@ -840,7 +843,7 @@ def main():
             line["precision_modes"] = precision_extra(args)
             line["batched"] = batched_extra(line["value"])
             line["adjoint"] = adjoint_extra()
-            line["adjoint_batched"] = batched_adjoint_extra()
+            line["adjoint_batched"] = batched_adjoint_extra(line["value"])
             line["gamma_law"] = gamma_law_extra()
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             n = args.size

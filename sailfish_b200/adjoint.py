@@ -313,17 +313,11 @@ class AdjointRun:
         """
         import torch
 
-        lib = self._lib
         f = self._fwd
         s: Solver = f["solver"]
-        params: Params = f["params"]
         steps, K = self.steps, self.checkpoint_every
         history, nb = f["history"], f["record_bytes"]
-        c = s.mesh.dx * s.mesh.dy / self.dts.sum()
-        w = (weights[0] * c, weights[1] * c)
-        times = self.stage_times(f["t_start"])
-        jac = torch.from_numpy(mass_jacobians(times.reshape(-1), params.mass_ratio,
-                                              params.eccentricity).reshape(steps, 60)).to(s.device)
+        w, jac = self._sweep_inputs(weights)
         trajectory = f["trajectory"]
         sweep = self._sweep(s, 0 if trajectory is not None else min(K, steps), w)
         sweep.chain.zero_()
@@ -363,6 +357,22 @@ class AdjointRun:
             sweep.replay_pipeline(b, more)
             b = 1 - b
         return sweep.finish()
+
+    def _sweep_inputs(self, weights):
+        """The chained objective weights (per unit time, times the zone area)
+        and the device array of every stage's Kepler Jacobians (steps x 60)
+        of the last forward(keep=True) run."""
+        import torch
+
+        f = self._fwd
+        s: Solver = f["solver"]
+        params: Params = f["params"]
+        c = s.mesh.dx * s.mesh.dy / self.dts.sum()
+        w = (weights[0] * c, weights[1] * c)
+        times = self.stage_times(f["t_start"])
+        jac = torch.from_numpy(mass_jacobians(times.reshape(-1), params.mass_ratio,
+                                              params.eccentricity).reshape(self.steps, 60)).to(s.device)
+        return w, jac
 
     def _sweep(self, s, k, w):
         """The reverse-sweep buffers and graph for segments of k steps, cached
@@ -703,6 +713,103 @@ class BatchedAdjoint:
             return self._each(lambda i: self.runs[i].gradient(weights))
         finally:
             lib.cbdiso_b200_set_adjoint_segment_rows(0)
+
+    # ------------------------------------------------------------------
+    # the whole batch's forward and adjoint as one CUDA graph
+
+    def capture(self, weights=(1.0, 0.0)):
+        """
+        Capture the forward run and the reverse sweep of every disk into one
+        CUDA graph: disk d's launches form branch d, on its own stream forked
+        from the capturing one, so that all disks' kernels overlap on the
+        device with no host work between them. Each replay starts every disk
+        from its initial state and initial stepper record (device copies) with
+        the frozen dt sequences; the results are read with results().
+        Requires a forward(keep=True) with stored states and gradient(weights)
+        before (they freeze the dt sequences and set up every buffer); this
+        runs one more forward of every disk with its frozen dt sequence.
+        """
+        import torch
+
+        lib = _capi.lib()
+        # one more forward of every disk with its frozen dt sequence attached
+        # to the stepper record that the graph starts from
+        self.forward(keep=True)
+        for r in self.runs:
+            if r._fwd.get("trajectory") is None:
+                raise ValueError("the captured batch needs stored states (store_states)")
+        self._graph_inputs = []
+        for r in self.runs:
+            f = r._fwd
+            s = f["solver"]
+            w, jac = r._sweep_inputs(weights)
+            sweep = r._sweep(s, 0, w)
+            out4 = torch.zeros(4, dtype=torch.float64, device=s.device)
+            self._graph_inputs.append(dict(run=r, solver=s, trajectory=f["trajectory"], history=f["history"],
+                                           state0=f["trajectory"][0].clone(), record=s.last_stepper_record(),
+                                           jac=jac, sweep=sweep, out4=out4))
+        _capi.check(lib.cbdiso_b200_set_adjoint_segment_rows(SHARED_SWEEP_ROWS), "set_adjoint_segment_rows")
+        try:
+            self._graph = self._capture_branches(gradient=True)
+            self._graph_forward = self._capture_branches(gradient=False)
+        finally:
+            lib.cbdiso_b200_set_adjoint_segment_rows(0)
+
+    def _capture_branches(self, gradient):
+        import torch
+
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        graph = torch.cuda.CUDAGraph()
+        branches = [torch.cuda.Stream() for _ in self.runs]
+        with capture(graph, side):
+            for g_in, st in zip(self._graph_inputs, branches):
+                st.wait_stream(side)
+                with torch.cuda.stream(st):
+                    self._branch_launches(g_in, gradient)
+            for st in branches:
+                side.wait_stream(st)
+        torch.cuda.current_stream().wait_stream(side)
+        return graph
+
+    def _branch_launches(self, g_in, gradient=True):
+        """One disk's forward and (with `gradient`) reverse sweep, launches only."""
+        import torch
+
+        r, s, traj, sweep = g_in["run"], g_in["solver"], g_in["trajectory"], g_in["sweep"]
+        traj[0].copy_(g_in["state0"])
+        s.trajectory_launches(r.steps, traj, g_in["record"])
+        if not gradient:
+            return
+        sweep.chain.zero_()
+        sweep.lam.zero_()
+        sweep.lam_n.zero_()
+        sweep.run(g_in["history"], g_in["jac"], r.steps, states=traj)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _capi.check(sweep.lib.cbdiso_b200_adjoint_chain_finish(ctypes.c_void_p(sweep.chain.data_ptr()), sweep.rows,
+                                                               ctypes.c_void_p(g_in["out4"].data_ptr()), stream),
+                    "chain_finish")
+
+    def replay(self, gradient=True):
+        """Run the captured batch (see capture) on the current stream: forward
+        and adjoint, or (gradient=False) the forward runs alone."""
+        (self._graph if gradient else self._graph_forward).replay()
+
+    def results(self):
+        """Per disk, after replay(): (J, dJ/dprim0, dJ/d(q, e, nu, sink_rate))
+        with J = (mean accretion, mean torque), as forward() and gradient()
+        return them."""
+        out = []
+        for g_in in self._graph_inputs:
+            r, s = g_in["run"], g_in["solver"]
+            rows = s.series_after_launches(r.steps)
+            mdot = np.array([-(row[0] + row[1]) for row in rows])
+            torque = np.array([row[2] for row in rows])
+            wt = r.dts / r.dts.sum()
+            J = np.array([np.dot(wt, mdot), np.dot(wt, torque)])
+            grad_state = g_in["sweep"].lam[NG:-NG, NG:-NG].cpu().numpy()
+            out.append((J, grad_state, g_in["out4"].cpu().numpy()))
+        return out
 
 
 def config4_disks(num=32, seed=4096, sizes=(256, 512)):

@@ -527,6 +527,9 @@ class Solver(SolverBase):
         self.h2d_bytes += nbytes
         epilogue = self._epilogue(self._time, True, self._device_diags if self._fused else [])
         weights = RK_WEIGHTS[self._options.rk_order]
+        # what trajectory_launches() replays: this run's initial stepper record
+        # and epilogue
+        self._last_run = dict(record=host, nvals=nvals, epilogue=epilogue)
 
         def one_step(n=None):
             stream = self._stream()
@@ -598,6 +601,49 @@ class Solver(SolverBase):
         self.d2h_bytes += rows.nbytes + state.numel()
         self.last_series = rows  # raw device rows (time, dt, wavespeed, sums)
         return self._series_rows(rows)
+
+    def trajectory_launches(self, steps, trajectory, record):
+        """
+        The launches of a device-stepped RK2 run of `steps` steps that writes
+        the run into `trajectory` (as run(trajectory=...)), starting from the
+        state in trajectory[0] and the stepper record in `record` (a device
+        copy of the record the last run started from; see
+        last_stepper_record), followed by the final series prologue. Nothing
+        synchronises with the host, so that the launches can be captured into
+        a larger CUDA graph; the time series is left in the device series
+        buffer (read it with series_after_launches). Requires a previous
+        run(trajectory=...) of the same length on this solver, which set up
+        the buffers.
+        """
+        lib = self._lib
+        last = self._last_run
+        nvals, epilogue = last["nvals"], last["epilogue"]
+        stepper, series = self._stepper_dev, self._series_dev
+        weights = RK_WEIGHTS[self._options.rk_order]
+        stepper.copy_(record)
+        for n in range(steps):
+            stream = self._stream()
+            self._check(lib.cbdiso_b200_step_prologue(self._ptr(stepper), self._ptr(self._result),
+                                                      self._ptr(self._records), self._ptr(series), nvals, 0,
+                                                      stream), "step_prologue")
+            self._launch_stages(weights, epilogue, stream,
+                                (trajectory[2 * n], trajectory[2 * n + 1], trajectory[2 * n + 2]))
+        self._check(lib.cbdiso_b200_step_prologue(self._ptr(stepper), self._ptr(self._result),
+                                                  self._ptr(self._records), self._ptr(series), nvals, 1,
+                                                  self._stream()), "step_prologue")
+
+    def last_stepper_record(self):
+        """A device copy of the stepper record the last run() started from."""
+        return self._last_run["record"].to(self.device)
+
+    def series_after_launches(self, steps):
+        """The time series rows of trajectory_launches() (as run() returns
+        them), read from the device; also checks the stepper's status."""
+        state = self._stepper_dev.cpu()
+        _, status = self._stepper_fields(state)
+        if status != 0:
+            raise _capi.CbdError(status, "device stepping")
+        return self._series_rows(self._series_dev[:steps].cpu().numpy())
 
     def _stepper_fields(self, state):
         raw = state.numpy().tobytes()
