@@ -295,8 +295,9 @@ def run_slabs(args, rank, world):
                 "d2h_bytes_per_step": int(float(e2e_bytes.item()) / 2 / e2e_steps), "steps": e2e_steps,
                 "includes": "slab upload, public-API driver loop (host dt each step), slab download"},
         # per step: prologue, first stage (behind its face-cache fill pass when
-        # the cache is on), second stage; plus the final series prologue
-        "gpu_launches": (3 if args.no_face_cache else 4) * args.steps + 1,
+        # the cache is on), second stage and its epilogue (wavespeed and sums);
+        # plus the final series prologue
+        "gpu_launches": (4 if args.no_face_cache else 5) * args.steps + 1,
         "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_source": peak_kind,
                      "note": "per-kernel roofline is reported by the N = 1 line"},
         "clocks": clocks.summary(),
@@ -413,8 +414,9 @@ def run_ours(args, rank, world):
         "step_io": {"h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "note": "value loop: stepper record in, time series out, per step"},
         # per step: prologue, first stage (behind its face-cache fill pass when
-        # the cache is on), second stage; plus the final series prologue
-        "gpu_launches": (3 if args.no_face_cache else 4) * args.steps + 1,
+        # the cache is on), second stage and its epilogue (wavespeed and sums);
+        # plus the final series prologue
+        "gpu_launches": (4 if args.no_face_cache else 5) * args.steps + 1,
         "roofline": roofline,
         "roofline_fp64": fp64,
         "clocks": clocks.summary(),

@@ -785,6 +785,8 @@ class BatchedAdjoint:
         sweep.lam.zero_()
         sweep.lam_n.zero_()
         sweep.run(g_in["history"], g_in["jac"], r.steps, states=traj)
+        # the final reduction adds into its output
+        g_in["out4"].zero_()
         stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         _capi.check(sweep.lib.cbdiso_b200_adjoint_chain_finish(ctypes.c_void_p(sweep.chain.data_ptr()), sweep.rows,
                                                                ctypes.c_void_p(g_in["out4"].data_ptr()), stream),

@@ -1112,6 +1112,55 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
     }
 }
 
+// The epilogue of one tile after its stage has written it: thread t adds up
+// the zones of column c0 + t, rows r0 .. r0 + k.rows_per_cta - 1, of the new
+// state `p` in row order, exactly as the fused march accumulates them.
+template <bool FAST>
+__device__ __forceinline__ void epilogue_tile(const Consts &k, const StageDev &st, const double *p, int c0,
+                                              int width, int r0, double (&acc)[PARTIAL_STRIDE])
+{
+    const int t = threadIdx.x;
+    const int W = min(width, k.nj - c0);
+    const int r1 = min(r0 + k.rows_per_cta, k.ni);
+    if (t >= W)
+        return;
+    const int j = c0 + t;
+    const size_t row_stride = (size_t)(k.nj + 2 * NG) * NQ;
+    const double yc = k.yl + ((double)j + 0.5) * k.dy;
+    const double *z = p + (size_t)(r0 + NG) * row_stride + (size_t)(j + NG) * NQ;
+    for (int r = r0; r < r1; ++r, z += row_stride) {
+        const double pn[NQ] = {z[0], z[1], z[2]};
+        const double xc = k.xl + ((double)r + 0.5) * k.dx;
+        accumulate_zone<FAST>(k, st.e, xc, yc, pn, acc);
+    }
+}
+
+// A stage's epilogue as its own launch, after a stage kernel launched
+// without it (EPI = false) on the same grid: the same CTA tiles, per-thread
+// order, block tree and CTA order, so the same bits as the fused epilogue.
+// Reading the new state back (24 B per zone) costs less than carrying the
+// epilogue's registers and code through the stencil's march.
+template <int BJ, int PREC>
+__global__ void __launch_bounds__(BJ, 4 * 128 / BJ) stage_epilogue_kernel(const Consts k, const StageDev st_param, StageArgs args)
+{
+    constexpr bool FAST = PREC == CBD_PRECISION_FAST;
+    __shared__ StageDev st;
+    __shared__ double sred[PARTIAL_STRIDE * (BJ / 32)];
+    if (threadIdx.x == 0)
+        st = args.stage_dev ? *args.stage_dev : st_param;
+    __syncthreads();
+    if (st.halt)
+        return;
+    double acc[PARTIAL_STRIDE];
+#pragma unroll
+    for (int v = 0; v < PARTIAL_STRIDE; ++v)
+        acc[v] = 0.0;
+    epilogue_tile<FAST>(k, st, args.pwr, blockIdx.x * BJ, BJ, blockIdx.y * k.rows_per_cta, acc);
+    double red[PARTIAL_STRIDE];
+    block_reduce<BJ>(acc, sred, red);
+    grid_finish<BJ>(red, 1 + 2 * k.num_diag, args.scratch, k.want_ws ? args.result : nullptr, args.result + 1, sred);
+}
+
 // Every cached value at mesh point (i, j), 0 <= i <= ni, 0 <= j <= nj, for
 // the masses m, with the stage kernel's own expressions: the x-face pair
 // (i, j) when j < nj, the y-face pair when i < ni, and the zone's gravity

@@ -10,13 +10,12 @@ template <int BJ, int MINB, int PREC>
 cudaError_t launch_one(const LaunchShape &s, const Consts &k, const StageDev &st, const StageArgs &a, int role,
                        cudaStream_t stream)
 {
+    // a stage with an epilogue runs as the stage without it, then the
+    // epilogue kernel over the same tiles (the same bits as fusing them)
     const bool epi = k.want_ws || k.num_diag > 0;
     switch (role) {
     case ROLE_WRITER:
-        if (epi)
-            stage_kernel<BJ, MINB, PREC, ROLE_WRITER, true><<<s.grid, BJ, 0, stream>>>(k, st, a);
-        else
-            stage_kernel<BJ, MINB, PREC, ROLE_WRITER, false><<<s.grid, BJ, 0, stream>>>(k, st, a);
+        stage_kernel<BJ, MINB, PREC, ROLE_WRITER, false><<<s.grid, BJ, 0, stream>>>(k, st, a);
         break;
     case ROLE_READER: {
         // the fill over the stage's own tiles, then the stage
@@ -24,19 +23,15 @@ cudaError_t launch_one(const LaunchShape &s, const Consts &k, const StageDev &st
         const int per_sm = FILL_WARPS_PER_SM * 32 / BJ;
         const int fill_ctas = tiles < 148 * per_sm ? tiles : 148 * per_sm;
         face_cache_fill_kernel<BJ, PREC><<<fill_ctas, BJ, 0, stream>>>(k, st, a.stage_dev, a.fcache, s.grid.x, tiles);
-        if (epi)
-            stage_kernel<BJ, MINB, PREC, ROLE_READER, true><<<s.grid, BJ, 0, stream>>>(k, st, a);
-        else
-            stage_kernel<BJ, MINB, PREC, ROLE_READER, false><<<s.grid, BJ, 0, stream>>>(k, st, a);
+        stage_kernel<BJ, MINB, PREC, ROLE_READER, false><<<s.grid, BJ, 0, stream>>>(k, st, a);
         break;
     }
     default:
-        if (epi)
-            stage_kernel<BJ, MINB, PREC, ROLE_NONE, true><<<s.grid, BJ, 0, stream>>>(k, st, a);
-        else
-            stage_kernel<BJ, MINB, PREC, ROLE_NONE, false><<<s.grid, BJ, 0, stream>>>(k, st, a);
+        stage_kernel<BJ, MINB, PREC, ROLE_NONE, false><<<s.grid, BJ, 0, stream>>>(k, st, a);
         break;
     }
+    if (epi)
+        stage_epilogue_kernel<BJ, PREC><<<s.grid, BJ, 0, stream>>>(k, st, a);
     return cudaGetLastError();
 }
 
