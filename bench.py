@@ -359,32 +359,41 @@ def run_ours(args, rank, world):
     # boundaries), so that the fixed cost and the per-step cost are known
     # whatever the step count.
     e2e_steps = max(1, args.steps)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    s2 = fresh()
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    for _ in range(e2e_steps):
-        dt = mesh.min_spacing() / s2.maximum_wavespeed() * CFL
-        s2.advance(dt)
-        s2.reductions()
-    torch.cuda.synchronize()
-    t2 = time.perf_counter()
-    final = s2.solution
-    t3 = time.perf_counter()
+
+    def e2e_once():
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2 = fresh()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(e2e_steps):
+            dt = mesh.min_spacing() / s2.maximum_wavespeed() * CFL
+            s2.advance(dt)
+            s2.reductions()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        final = s2.solution
+        t3 = time.perf_counter()
+        io = ((s2.h2d_bytes + prim.nbytes) / e2e_steps, (s2.d2h_bytes + final.nbytes) / e2e_steps)
+        del s2, final
+        return (t0, t1, t2, t3), io
+
+    # three repetitions (the host's load moves the set-up and copies): the
+    # median by total time is reported, all three are listed
+    reps = [e2e_once() for _ in range(3)]
+    reps.sort(key=lambda r: r[0][3] - r[0][0])
+    (t0, t1, t2, t3), (e2e_h2d, e2e_d2h) = reps[1]
     e2e_elapsed = t3 - t0
     if dist:
         t = torch.tensor([e2e_elapsed], device="cuda", dtype=torch.float64)
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
         e2e_elapsed = float(t.item())
     e2e_value = zones * e2e_steps * world / e2e_elapsed  # host-driven loop: one dt round trip per step
-    e2e_h2d = (s2.h2d_bytes + prim.nbytes) / e2e_steps
-    e2e_d2h = (s2.d2h_bytes + final.nbytes) / e2e_steps
     e2e_phases = {"setup_and_upload_ms": (t1 - t0) * 1e3, "steps_ms": (t2 - t1) * 1e3,
                   "download_ms": (t3 - t2) * 1e3, "fixed_ms": (t1 - t0 + t3 - t2) * 1e3,
-                  "per_step_ms": (t2 - t1) * 1e3 / e2e_steps}
+                  "per_step_ms": (t2 - t1) * 1e3 / e2e_steps,
+                  "repetitions_ms": [round((r[0][3] - r[0][0]) * 1e3, 2) for r in reps]}
     e2e_phases.update(transfer_floor(prim.nbytes))
-    del s2
 
     kernel_s = stage_kernel_time(solver)
     peak, peak_kind = measured_peaks()
