@@ -113,10 +113,12 @@ def _kepler_complex_many(t, a, m, q, e):
     return np.stack([x1, y1, vx1, vy1, m1 * ones, -x1 / q, -y1 / q, -vx1 / q, -vy1 / q, m2 * ones])
 
 
-# segment rows of the stage adjoints when many sweeps share the GPU (32
-# disks of 256^2 and 512^2 over 8 streams: 8 rows 0.69 s, 32 rows 0.70 s,
-# the lone-sweep choice of 4 / 6 rows 0.72 s for the whole gradient)
-SHARED_SWEEP_ROWS = 8
+# segment rows of the stage adjoints when many sweeps share the GPU: longer
+# segments do less lead-row work per CTA, and the concurrent sweeps supply the
+# CTAs (32 disks of 256^2 and 512^2, forward and adjoint as one captured
+# graph: 4 rows 978 ms, 8 rows 853, 16 rows 791, 32 rows 762; over 8 eager
+# streams 8 and 32 rows ran within 1.5 % of each other)
+SHARED_SWEEP_ROWS = 32
 
 
 def mass_jacobians(times, q, e, a=1.0, m=1.0, h=1e-30):
