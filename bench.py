@@ -138,45 +138,100 @@ def initial_state(n, seed):
 
 
 class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples (every PERIOD_MS) around
+    the timed region. A timed region of a few dozen steps lasts tens of
+    milliseconds, less than nvidia-smi needs to start, so the sampler is
+    started first and waited for (its first sample), the caller keeps the GPU
+    under the timed workload for LOAD_S before the timed region (`load`), and
+    the summary keeps the samples from the start of that load to the end of
+    the timed region: the clocks under exactly the timed steps."""
+
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 50
+    LOAD_S = 0.6
+    START_TIMEOUT_S = 20.0
 
     def __init__(self, device_index):
         self.device_index = device_index
         self.proc = None
+        self.thread = None
         self.error = None
-        self.lines = []
+        self.samples = []  # (host time of arrival, line)
+        self.t_load = self.t_stop = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            if line.strip():
+                self.samples.append((time.perf_counter(), line))
 
     def __enter__(self):
+        import shutil
+        import threading
+
+        cmd = ["nvidia-smi", "-i", str(self.device_index), f"--query-gpu={self.FIELDS}",
+               "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)]
+        if shutil.which("stdbuf"):
+            cmd = ["stdbuf", "-oL"] + cmd  # one line per sample as it is taken
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device_index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, bufsize=1)
         except (OSError, FileNotFoundError) as e:
             self.proc = None
             self.error = f"nvidia-smi could not be started: {e}"
+            return self
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        deadline = time.perf_counter() + self.START_TIMEOUT_S
+        while not self.samples and self.proc.poll() is None and time.perf_counter() < deadline:
+            time.sleep(0.01)
         return self
 
+    def load(self, step_fn, group_max=None):
+        """Runs `step_fn` (some of the timed steps, synchronised) for about
+        LOAD_S, so that samples fall under that load. The call count comes
+        from the first call's duration; `group_max` makes it the same on all
+        ranks where the steps hold collectives."""
+        self.t_load = time.perf_counter()
+        step_fn()
+        once = time.perf_counter() - self.t_load
+        n = max(0, math.ceil(self.LOAD_S / max(once, 1e-6)) - 1)
+        if group_max is not None:
+            n = group_max(n)
+        for _ in range(n):
+            step_fn()
+
+    def stop(self):
+        """Marks the end of the timed region (after its synchronize)."""
+        self.t_stop = time.perf_counter()
+
     def __exit__(self, *exc):
-        self.lines = []
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                out, err = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                out, err = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
-            if not self.lines:
-                self.error = ("nvidia-smi returned no samples (exit code "
-                              f"{self.proc.returncode}): {err.strip()[:200] or 'no message'}")
+        if self.proc is None:
+            return
+        if self.t_stop is None:
+            self.stop()
+        # the sample taken across the end of the timed region
+        deadline = time.perf_counter() + 2.0 * self.PERIOD_MS * 1e-3
+        while time.perf_counter() < deadline and not any(t > self.t_stop for t, _ in self.samples):
+            time.sleep(0.005)
+        self.proc.terminate()
+        try:
+            _, err = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            _, err = self.proc.communicate()
+        self.thread.join(timeout=5)
+        if not self.samples:
+            self.error = ("nvidia-smi returned no samples (exit code "
+                          f"{self.proc.returncode}): {(err or '').strip()[:200] or 'no message'}")
 
     def summary(self):
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in getattr(self, "lines", []):
+        t0 = self.t_load if self.t_load is not None else -math.inf
+        t1 = (self.t_stop if self.t_stop is not None else math.inf) + self.PERIOD_MS * 1e-3
+        window = [line for t, line in self.samples if t0 <= t <= t1]
+        for line in window:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -190,10 +245,19 @@ class ClockSampler:
                     reasons.add(name)
         if not sm:
             # never a silent null: say why there is no clock record
-            why = self.error or f"no parsable samples among {len(self.lines)} lines"
+            why = self.error or f"no parsable samples among {len(window)} lines in the window"
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "unavailable": why}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "period_ms": self.PERIOD_MS,
+                "window": f"{self.LOAD_S} s of the timed steps just before the timed region, and the timed region"}
+
+
+def _max_over_ranks(n, tdist):
+    import torch
+
+    t = torch.tensor([int(n)], device="cuda", dtype=torch.int64)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return int(t.item())
 
 
 # ---------------------------------------------------------------------------
@@ -251,10 +315,16 @@ def run_slabs(args, rank, world):
     torch.cuda.synchronize()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(torch.cuda.current_device()) as clocks:
+        # the same step count on every rank: the halo exchange is collective
+        clocks.load(lambda: (solver.run(max(args.warmup, 3), cfl=CFL), torch.cuda.synchronize()),
+                    group_max=lambda n: _max_over_ranks(n, tdist))
+        tdist.barrier()
+        torch.cuda.synchronize()
         start.record()
         rows = solver.run(args.steps, cfl=CFL)
         stop.record()
         torch.cuda.synchronize()
+        clocks.stop()
     assert len(rows) == args.steps and all(np.isfinite(r[-1]) for r in rows)
     t = torch.tensor([start.elapsed_time(stop) * 1e-3], device="cuda", dtype=torch.float64)
     tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
@@ -337,10 +407,16 @@ def run_ours(args, rank, world):
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     h2d0, d2h0 = solver.h2d_bytes, solver.d2h_bytes
     with ClockSampler(torch.cuda.current_device()) as clocks:
+        clocks.load(lambda: (solver.run(16, cfl=CFL), torch.cuda.synchronize()),
+                    group_max=(lambda n: _max_over_ranks(n, tdist)) if dist else None)
+        if dist:
+            tdist.barrier()
+        torch.cuda.synchronize()
         start.record()
         rows = solver.run(args.steps, cfl=CFL)
         stop.record()
         torch.cuda.synchronize()
+        clocks.stop()
     assert len(rows) == args.steps and all(np.isfinite(r[-1]) for r in rows)
     elapsed = start.elapsed_time(stop) * 1e-3
     if dist:
@@ -481,21 +557,26 @@ def sizes_extra(args, sizes=(1024, 2048), steps=100):
         s = make_solver("cbdiso_2d", physics, dict(rk_order=2, plm_theta=THETA, precision=args.precision),
                         setup=setup, mesh=mesh, solution=prim)
         s.run(16, cfl=CFL)
-        torch.cuda.synchronize()
-        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        start.record()
-        s.run(steps, cfl=CFL)
-        stop.record()
-        torch.cuda.synchronize()
-        ms = start.elapsed_time(stop) / steps
+        reps = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            s.run(steps, cfl=CFL)
+            stop.record()
+            torch.cuda.synchronize()
+            reps.append(start.elapsed_time(stop) / steps)
+        ms = float(np.median(reps))
         kernel_s = stage_kernel_time(s)
         achieved = BYTES_PER_ZONE_UPDATE / 2 * n * n / kernel_s / 1e9
         out[str(n)] = {"value": n * n / (ms * 1e-3), "unit": "zone-updates/s", "ms_per_step": ms,
+                       "repetitions_ms_per_step": [round(v, 4) for v in reps],
                        "steps": steps, "kernel_ms": round(kernel_s * 1e3, 4),
                        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                                     "frac": round(achieved / peak, 4), "peak_source": peak_kind}}
         del s
-    out["note"] = "same workload and loop as `value` at the configuration's other grid sizes"
+    out["note"] = ("same workload and loop as `value` at the configuration's other grid sizes; "
+                   "the median of three repetitions")
     return out
 
 

@@ -49,6 +49,9 @@ NG = 2
 NQ = 3
 RK_WEIGHTS = {1: (0.0,), 2: (0.0, 0.5), 3: (0.0, 0.75, 1.0 / 3.0)}
 COMPLEX_QUANTITIES = ("sigma_m1", "eccentricity_vector")
+# rows of the device time series a run allocates at least: a longer run
+# reallocates it, which drops the captured step graphs (they hold its address)
+SERIES_ROWS = 1024
 
 
 class Options(NamedTuple):
@@ -505,7 +508,7 @@ class Solver(SolverBase):
             self._graphs = {}
         if getattr(self, "_series_dev", None) is None or self._series_dev.shape[0] < steps or \
                 self._series_dev.shape[1] != 3 + nvals:
-            self._series_dev = torch.zeros((max(steps, 64), 3 + nvals), dtype=torch.float64, device=self.device)
+            self._series_dev = torch.zeros((max(steps, SERIES_ROWS), 3 + nvals), dtype=torch.float64, device=self.device)
             self._graphs = {}
         stepper, series = self._stepper_dev, self._series_dev
         host = torch.zeros(nbytes, dtype=torch.uint8).pin_memory()
