@@ -2,9 +2,10 @@
 //
 // Design (one kernel per RK stage):
 //  * A CTA owns a strip of BJ columns (j, the contiguous axis) and marches down
-//    a segment of rows (i). Each iteration stages one new row of primitives in
-//    a four-row shared-memory ring with coalesced loads, so every zone is read
-//    from HBM once per stage (plus a two-row and two-column halo per CTA).
+//    a segment of rows (i) with one barrier per row. Each iteration stages one
+//    new row of primitives in a five-row shared-memory ring with coalesced
+//    loads, so every zone is read from HBM once per stage (plus a two-row and
+//    two-column halo per CTA).
 //  * Every quantity that the reference recomputes per zone (cbdiso_2d.c:447-603)
 //    is computed once and shared: each PLM slope, each x- and y-face HLLE flux
 //    with its viscous term, each zone's rho * strain. The shared values are
@@ -748,11 +749,10 @@ __device__ __forceinline__ void cache_store(double *p, double a, double b)
 // march_tile it holds.
 template <int BJ>
 struct StageSmem {
-    double sp[4][NQ][BJ + 4];   // primitive rows ring, columns c0-2 .. c0+BJ+1
+    double sp[5][NQ][BJ + 4];   // primitive rows ring, columns c0-2 .. c0+BJ+1
     double sgy[2][NQ][BJ + 2];  // y-slopes ring, columns c0-1 .. c0+BJ
     double srs[2][NQ][BJ + 2];  // rho * strain ring, same columns
-    double sg[NQ][BJ + 1];      // y-face fluxes of the current row
-    double sun[2][NQ][BJ];      // u_n source zones, fetched one row ahead
+    double sg[2][NQ][BJ + 1];   // y-face fluxes, by row parity
 };
 
 template <int BJ>
@@ -779,7 +779,6 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
     auto &sgy = sm.sgy;
     auto &srs = sm.srs;
     auto &sg = sm.sg;
-    auto &sun = sm.sun;
 
     const int t = threadIdx.x;
     const int ni = k.ni, nj = k.nj;
@@ -812,15 +811,16 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 async_copy8(&sp[slot][q][kk], src + NQ * kk + q);
         }
     };
-    // The zone (i, j) of the u_n source array, for this thread's own update.
-    // In the in-place final stage this array is also written, by the same
-    // thread and only after the zone has been consumed.
-    auto fetch_un = [&](int i) {
-        if (k.un_kind != 0 && active) {
+    // The zone (i, j) of the u_n source array, for this thread's own update,
+    // loaded into registers a row ahead. In the in-place final stage this
+    // array is also written, by the same thread and only after the zone has
+    // been consumed (so a plain load, not the read-only path).
+    auto load_un = [&](int i, double *z3) {
+        if (k.un_kind != 0 && active && i >= r0 && i < r1) {
             const double *z = zone(args.un, i, j);
-#pragma unroll
-            for (int q = 0; q < NQ; ++q)
-                async_copy8(&sun[i & 1][q][t], z + q);
+            z3[0] = z[0];
+            z3[1] = z[1];
+            z3[2] = z[2];
         }
     };
     // Lanes that do the strip's extra work, spread over different warps: the
@@ -831,24 +831,30 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
     // own-column carried state: x-slope and rho*strain of row r, x-face flux F(r - 1/2)
     double gx0[NQ] = {0.0, 0.0, 0.0}, rs0[NQ] = {0.0, 0.0, 0.0}, f0[NQ] = {0.0, 0.0, 0.0};
 
-    fetch_row((r0 - 2) & 3, r0 - 2);
-    fetch_row((r0 - 1) & 3, r0 - 1);
-    fetch_row(r0 & 3, r0);
+    // One barrier per row. Rows sit in a five-slot ring (slot of row i:
+    // (i - r0 + 2) mod 5). Row r + 4 is fetched right after iteration r's
+    // barrier into the slot of row r - 1 (last read before that barrier),
+    // and each thread waits for its copies of row r + 3 before the barrier,
+    // so the rows r + 1 .. r + 3 that iteration r + 1 reads are resident and
+    // visible. The y-face fluxes alternate between two buffers by row
+    // parity, so iteration r + 1 may write its own while a slower warp still
+    // reads iteration r's.
+    fetch_row(0, r0 - 2);
+    fetch_row(1, r0 - 1);
+    fetch_row(2, r0);
     async_commit();
+    async_wait_all();
+    __syncthreads();
+    if (r0 + 1 <= r1 + 1)
+        fetch_row(3, r0 + 1);
+    async_commit();
+    int s0 = 0;  // ring slot of row r
 
     for (int r = r0 - 2; r < r1; ++r) {
-        // rows r .. r + 2 (and the u_n zone of row r) were fetched one
-        // iteration ago; after the barrier the slot of row r - 1 is free
-        async_wait_all();
-        __syncthreads();
-        if (r + 3 <= r1 + 1)
-            fetch_row((r + 3) & 3, r + 3);
-        if (r + 1 >= r0 && r + 1 < r1)
-            fetch_un(r + 1);
-        async_commit();
-
-        const int s0 = r & 3, s1 = (r + 1) & 3, s2 = (r + 2) & 3;
+        const int s1 = s0 == 4 ? 0 : s0 + 1, s2 = s1 == 4 ? 0 : s1 + 1;
         const int g1 = (r + 1) & 1, g0 = r & 1;
+        double un_cur[NQ] = {0.0, 0.0, 0.0};
+        load_un(r, un_cur);
 
         // cached face sound speeds and gravity factors of this row, loaded
         // ahead of the slopes so that their latency overlaps them
@@ -973,10 +979,18 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 }
 #pragma unroll
                 for (int q = 0; q < NQ; ++q)
-                    sg[q][fidx] = g[q];
+                    sg[g0][q][fidx] = g[q];
             }
         }
+        // row r + 3 has landed for this thread; after the barrier for all,
+        // and the slot of row r - 1 is free for row r + 4
+        async_wait_all();
         __syncthreads();
+        if (r + 4 <= r1 + 1) {
+            const int s4 = s2 >= 3 ? s2 - 3 : s2 + 2;  // (s0 + 4) mod 5
+            fetch_row(s4, r + 4);
+        }
+        async_commit();
 
         // (4) update zone (r, j)
         if (r >= r0 && active) {
@@ -995,7 +1009,7 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 un[1] = u[1];
                 un[2] = u[2];
             } else {
-                const double z0 = sun[r & 1][0][t], z1 = sun[r & 1][1][t], z2 = sun[r & 1][2][t];
+                const double z0 = un_cur[0], z1 = un_cur[1], z2 = un_cur[2];
                 if (k.un_kind == 1) {
                     un[0] = z0;
                     un[1] = z1 * z0;
@@ -1023,7 +1037,7 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
             }
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
-                const double gn = sg[q][t + 1], gs = sg[q][t];
+                const double gn = sg[g0][q][t + 1], gs = sg[g0][q][t];
                 du[q] -= (div_by<FAST>(f1[q] - f0[q], k.dx, k.inv_dx) + div_by<FAST>(gn - gs, k.dy, k.inv_dy)) * dt;
             }
 #pragma unroll
@@ -1066,6 +1080,7 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
             rs0[q] = rs1[q];
             f0[q] = f1[q];
         }
+        s0 = s1;
     }
 
     // leave the shared buffers free for the block's next tile
