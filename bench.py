@@ -35,7 +35,7 @@ BYTES_PER_ZONE_UPDATE = 120.0  # RK2 x FP64 x 3 fields: 48 B stage 1 + 72 B stag
 # kernel, halved per stage); scaled by the zone count. It is above the
 # algorithmic 60 B because of the cache's 48 B per zone and step and the
 # epilogue's 24 B read-back.
-NCU_TRAFFIC_PER_ZONE_LAUNCH = (311.58e6 + 61.30e6 + 219.62e6 + 253.70e6 + 100.91e6 + 3.81e6) / 2 / 2048 ** 2
+NCU_TRAFFIC_PER_ZONE_LAUNCH = (312.26e6 + 61.19e6 + 217.50e6 + 250.14e6 + 100.91e6 + 4.20e6) / 2 / 2048 ** 2
 # FP64 thread-instructions (DADD + DMUL + DFMA) per zone and stage, from the
 # same three launches (ncu, the sum of
 # smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum over zones)
@@ -471,6 +471,7 @@ def run_ours(args, rank, world):
                   "per_step_ms": (t2 - t1) * 1e3 / e2e_steps,
                   "repetitions_ms": [round((r[0][3] - r[0][0]) * 1e3, 2) for r in reps]}
     e2e_phases.update(transfer_floor(prim.nbytes))
+    e2e_phases.update(host_copy_times(prim.nbytes))
 
     kernel_s = stage_kernel_time(solver)
     peak, peak_kind = measured_peaks()
@@ -538,6 +539,48 @@ def transfer_floor(nbytes, repeats=3):
     return {"pinned_h2d_ms": best["h2d"], "pinned_d2h_ms": best["d2h"],
             "pinned_h2d_gbs": nbytes / best["h2d"] / 1e6, "pinned_d2h_gbs": nbytes / best["d2h"] / 1e6,
             "transfer_floor_ms": best["h2d"] + best["d2h"]}
+
+
+def host_copy_times(nbytes, repeats=3):
+    """The host side of the state copies on this box, with the solver's pool
+    threads and row blocks (sailfish_b200/_hostio.py): one state's bytes
+    from a numpy array into pinned memory (the upload's copy), and from
+    pinned memory into a new numpy array, its first touch included (the
+    download's); best of `repeats`. Both are bound by host memory bandwidth,
+    which the device copies share: the upload moves 3 state-sizes through
+    host memory (copy read and write, device-copy read), the download 4
+    (device-copy write, the new array's zero-fill on first touch, copy read
+    and write). `host_traffic_floor_ms` is those 7 state-sizes at the
+    bandwidth the upload's copy reaches."""
+    import torch
+
+    from sailfish_b200 import _hostio
+
+    n = nbytes // 8
+    src = np.ones(n)
+    pinned = torch.empty(n, dtype=torch.float64).pin_memory()
+    staged = pinned.numpy()
+    blocks = _hostio._blocks(n, 2 * _hostio._threads())
+    pool = _hostio._get_pool()
+
+    def parallel_copy(dst, frm):
+        for job in [pool.submit(np.copyto, dst[a:b], frm[a:b]) for a, b in blocks]:
+            job.result()
+
+    copy_in = copy_out = float("inf")
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        parallel_copy(staged, src)
+        t1 = time.perf_counter()
+        out = np.empty(n)
+        parallel_copy(out, staged)
+        t2 = time.perf_counter()
+        del out
+        copy_in, copy_out = min(copy_in, (t1 - t0) * 1e3), min(copy_out, (t2 - t1) * 1e3)
+    del pinned, staged, src
+    host_gbs = 2 * nbytes / copy_in / 1e6
+    return {"host_copy_in_ms": copy_in, "host_copy_out_ms": copy_out, "host_copy_gbs": host_gbs,
+            "host_traffic_floor_ms": 7 * nbytes / host_gbs / 1e6}
 
 
 def sizes_extra(args, sizes=(1024, 2048), steps=100):

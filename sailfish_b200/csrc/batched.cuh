@@ -115,16 +115,16 @@ __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs
         } else if (ROLE == ROLE_WRITER) {
             // the same answer in every thread; the disk's first tile writes the key
             const bool store = cached && cache_write_check<PREC>(k, st, sa.fcache, t == 0 && u == D.unit_begin);
-            march_tile<BJ, FAST, CACHE_WRITE, EPI>(k, st, sa, c0, D.strip_width, r0, acc, store);
+            march_tile<BJ, FAST, CACHE_WRITE, EPI, false>(k, st, sa, c0, D.strip_width, r0, acc, store);
         } else if (ROLE == ROLE_READER) {
             if (cached) {
-                march_tile<BJ, FAST, CACHE_READ, EPI>(k, st, sa, c0, D.strip_width, r0, acc);
+                march_tile<BJ, FAST, CACHE_READ, EPI, false>(k, st, sa, c0, D.strip_width, r0, acc);
                 // the fill kernel ran before this launch; no tile reads the key
                 if (t == 0 && u == D.unit_begin)
                     cache_write_key<PREC>(k, st, sa.fcache);
             }
         } else {
-            march_tile<BJ, FAST, CACHE_NONE, EPI>(k, st, sa, c0, D.strip_width, r0, acc);
+            march_tile<BJ, FAST, CACHE_NONE, EPI, false>(k, st, sa, c0, D.strip_width, r0, acc);
         }
         if (EPI) {
             double red[PARTIAL_STRIDE];

@@ -746,19 +746,22 @@ __device__ __forceinline__ void cache_store(double *p, double a, double b)
 }
 
 // Shared memory of the march, one instance per kernel whichever copies of
-// march_tile it holds.
-template <int BJ>
+// march_tile it holds. ONE_SYNC selects the march with one barrier per row
+// (march_tile).
+template <int BJ, bool ONE_SYNC>
 struct StageSmem {
-    double sp[5][NQ][BJ + 4];   // primitive rows ring, columns c0-2 .. c0+BJ+1
-    double sgy[2][NQ][BJ + 2];  // y-slopes ring, columns c0-1 .. c0+BJ
-    double srs[2][NQ][BJ + 2];  // rho * strain ring, same columns
-    double sg[2][NQ][BJ + 1];   // y-face fluxes, by row parity
+    static constexpr int RING = ONE_SYNC ? 5 : 4;
+    double sp[RING][NQ][BJ + 4];             // primitive rows ring, columns c0-2 .. c0+BJ+1
+    double sgy[2][NQ][BJ + 2];               // y-slopes ring, columns c0-1 .. c0+BJ
+    double srs[2][NQ][BJ + 2];               // rho * strain ring, same columns
+    double sg[ONE_SYNC ? 2 : 1][NQ][BJ + 1];  // y-face fluxes (by row parity with ONE_SYNC)
+    double sun[ONE_SYNC ? 1 : 2][NQ][ONE_SYNC ? 1 : BJ];  // u_n zones a row ahead (two-barrier march)
 };
 
-template <int BJ>
-__device__ __forceinline__ StageSmem<BJ> &stage_smem()
+template <int BJ, bool ONE_SYNC>
+__device__ __forceinline__ StageSmem<BJ, ONE_SYNC> &stage_smem()
 {
-    __shared__ StageSmem<BJ> m;
+    __shared__ StageSmem<BJ, ONE_SYNC> m;
     return m;
 }
 
@@ -768,17 +771,21 @@ __device__ __forceinline__ StageSmem<BJ> &stage_smem()
 // zones are accumulated into `acc` when EPI (the launch has an epilogue;
 // without, its code is left out). `COP` (CACHE_*) says what the tile does
 // with args.fcache: CACHE_WRITE stores the face and gravity values if
-// `store`, CACHE_READ loads them. All threads of the block must call it.
-template <int BJ, bool FAST, int COP = CACHE_NONE, bool EPI = true>
+// `store`, CACHE_READ loads them. ONE_SYNC marches with one barrier per row
+// (five-row ring, u_n in registers), otherwise with two (four-row ring, u_n
+// through shared memory), which needs fewer registers: the persistent
+// batched kernel keeps it. All threads of the block must call it.
+template <int BJ, bool FAST, int COP = CACHE_NONE, bool EPI = true, bool ONE_SYNC = true>
 __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, const StageArgs &args, int c0,
                                            int width, int r0, double (&acc)[PARTIAL_STRIDE], bool store = false)
 {
     constexpr int cop = COP;
-    StageSmem<BJ> &sm = stage_smem<BJ>();
+    StageSmem<BJ, ONE_SYNC> &sm = stage_smem<BJ, ONE_SYNC>();
     auto &sp = sm.sp;
     auto &sgy = sm.sgy;
     auto &srs = sm.srs;
     auto &sg = sm.sg;
+    auto &sun = sm.sun;
 
     const int t = threadIdx.x;
     const int ni = k.ni, nj = k.nj;
@@ -811,16 +818,25 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 async_copy8(&sp[slot][q][kk], src + NQ * kk + q);
         }
     };
-    // The zone (i, j) of the u_n source array, for this thread's own update,
-    // loaded into registers a row ahead. In the in-place final stage this
-    // array is also written, by the same thread and only after the zone has
-    // been consumed (so a plain load, not the read-only path).
+    // The zone (i, j) of the u_n source array, for this thread's own update:
+    // into registers at the top of row i's iteration (ONE_SYNC), or into
+    // shared memory a row ahead. In the in-place final stage this array is
+    // also written, by the same thread and only after the zone has been
+    // consumed (so a plain load, not the read-only path).
     auto load_un = [&](int i, double *z3) {
         if (k.un_kind != 0 && active && i >= r0 && i < r1) {
             const double *z = zone(args.un, i, j);
             z3[0] = z[0];
             z3[1] = z[1];
             z3[2] = z[2];
+        }
+    };
+    auto fetch_un = [&](int i) {
+        if (k.un_kind != 0 && active) {
+            const double *z = zone(args.un, i, j);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+                async_copy8(&sun[ONE_SYNC ? 0 : i & 1][q][ONE_SYNC ? 0 : t], z + q);
         }
     };
     // Lanes that do the strip's extra work, spread over different warps: the
@@ -831,30 +847,55 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
     // own-column carried state: x-slope and rho*strain of row r, x-face flux F(r - 1/2)
     double gx0[NQ] = {0.0, 0.0, 0.0}, rs0[NQ] = {0.0, 0.0, 0.0}, f0[NQ] = {0.0, 0.0, 0.0};
 
-    // One barrier per row. Rows sit in a five-slot ring (slot of row i:
-    // (i - r0 + 2) mod 5). Row r + 4 is fetched right after iteration r's
-    // barrier into the slot of row r - 1 (last read before that barrier),
-    // and each thread waits for its copies of row r + 3 before the barrier,
-    // so the rows r + 1 .. r + 3 that iteration r + 1 reads are resident and
-    // visible. The y-face fluxes alternate between two buffers by row
-    // parity, so iteration r + 1 may write its own while a slower warp still
-    // reads iteration r's.
-    fetch_row(0, r0 - 2);
-    fetch_row(1, r0 - 1);
-    fetch_row(2, r0);
-    async_commit();
-    async_wait_all();
-    __syncthreads();
-    if (r0 + 1 <= r1 + 1)
-        fetch_row(3, r0 + 1);
-    async_commit();
-    int s0 = 0;  // ring slot of row r
+    // ONE_SYNC: one barrier per row. Rows sit in a five-slot ring (slot of
+    // row i: (i - r0 + 2) mod 5). Row r + 4 is fetched right after iteration
+    // r's barrier into the slot of row r - 1 (last read before that
+    // barrier), and each thread waits for its copies of row r + 3 before the
+    // barrier, so the rows r + 1 .. r + 3 that iteration r + 1 reads are
+    // resident and visible. The y-face fluxes alternate between two buffers
+    // by row parity, so iteration r + 1 may write its own while a slower warp
+    // still reads iteration r's.
+    // Otherwise two barriers per row: at the top of iteration r (rows r ..
+    // r + 2 and the u_n zone of row r fetched one iteration ago have landed;
+    // the slot of row r - 1 is free for row r + 3), and between the y-faces
+    // and the zone update. Ring slot of row i: i mod 4.
+    int s0;  // ring slot of row r
+    if constexpr (ONE_SYNC) {
+        fetch_row(0, r0 - 2);
+        fetch_row(1, r0 - 1);
+        fetch_row(2, r0);
+        async_commit();
+        async_wait_all();
+        __syncthreads();
+        if (r0 + 1 <= r1 + 1)
+            fetch_row(3, r0 + 1);
+        async_commit();
+        s0 = 0;
+    } else {
+        fetch_row((r0 - 2) & 3, r0 - 2);
+        fetch_row((r0 - 1) & 3, r0 - 1);
+        fetch_row(r0 & 3, r0);
+        async_commit();
+        s0 = (r0 - 2) & 3;
+    }
 
     for (int r = r0 - 2; r < r1; ++r) {
-        const int s1 = s0 == 4 ? 0 : s0 + 1, s2 = s1 == 4 ? 0 : s1 + 1;
+        if constexpr (!ONE_SYNC) {
+            async_wait_all();
+            __syncthreads();
+            if (r + 3 <= r1 + 1)
+                fetch_row((r + 3) & 3, r + 3);
+            if (r + 1 >= r0 && r + 1 < r1)
+                fetch_un(r + 1);
+            async_commit();
+        }
+        constexpr int RING = StageSmem<BJ, ONE_SYNC>::RING;
+        const int s1 = s0 == RING - 1 ? 0 : s0 + 1, s2 = s1 == RING - 1 ? 0 : s1 + 1;
         const int g1 = (r + 1) & 1, g0 = r & 1;
+        const int gf = ONE_SYNC ? g0 : 0;  // y-face flux buffer of row r
         double un_cur[NQ] = {0.0, 0.0, 0.0};
-        load_un(r, un_cur);
+        if (ONE_SYNC)
+            load_un(r, un_cur);
 
         // cached face sound speeds and gravity factors of this row, loaded
         // ahead of the slopes so that their latency overlaps them
@@ -979,18 +1020,22 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 }
 #pragma unroll
                 for (int q = 0; q < NQ; ++q)
-                    sg[g0][q][fidx] = g[q];
+                    sg[gf][q][fidx] = g[q];
             }
         }
-        // row r + 3 has landed for this thread; after the barrier for all,
-        // and the slot of row r - 1 is free for row r + 4
-        async_wait_all();
-        __syncthreads();
-        if (r + 4 <= r1 + 1) {
-            const int s4 = s2 >= 3 ? s2 - 3 : s2 + 2;  // (s0 + 4) mod 5
-            fetch_row(s4, r + 4);
+        if constexpr (ONE_SYNC) {
+            // row r + 3 has landed for this thread; after the barrier for
+            // all, and the slot of row r - 1 is free for row r + 4
+            async_wait_all();
+            __syncthreads();
+            if (r + 4 <= r1 + 1) {
+                const int s4 = s2 >= 3 ? s2 - 3 : s2 + 2;  // (s0 + 4) mod 5
+                fetch_row(s4, r + 4);
+            }
+            async_commit();
+        } else {
+            __syncthreads();
         }
-        async_commit();
 
         // (4) update zone (r, j)
         if (r >= r0 && active) {
@@ -1009,7 +1054,10 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                 un[1] = u[1];
                 un[2] = u[2];
             } else {
-                const double z0 = un_cur[0], z1 = un_cur[1], z2 = un_cur[2];
+                const int ub = ONE_SYNC ? 0 : r & 1, uc = ONE_SYNC ? 0 : t;
+                const double z0 = ONE_SYNC ? un_cur[0] : sun[ub][0][uc];
+                const double z1 = ONE_SYNC ? un_cur[1] : sun[ub][1][uc];
+                const double z2 = ONE_SYNC ? un_cur[2] : sun[ub][2][uc];
                 if (k.un_kind == 1) {
                     un[0] = z0;
                     un[1] = z1 * z0;
@@ -1037,7 +1085,7 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
             }
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
-                const double gn = sg[g0][q][t + 1], gs = sg[g0][q][t];
+                const double gn = sg[gf][q][t + 1], gs = sg[gf][q][t];
                 du[q] -= (div_by<FAST>(f1[q] - f0[q], k.dx, k.inv_dx) + div_by<FAST>(gn - gs, k.dy, k.inv_dy)) * dt;
             }
 #pragma unroll
