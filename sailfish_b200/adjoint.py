@@ -211,15 +211,13 @@ class AdjointRun:
                                     s.device)
             rows = s.run(steps, cfl=self.cfl, dt_sequence=dts_dev, history=history, trajectory=trajectory)
         else:
+            # one run: a checkpoint before every segment of K steps, taken on
+            # the device between the segments' graph replays
             store = self._checkpoint_store(s) if keep else None
-            for start in range(0, steps, K):
-                stop = min(start + K, steps)
-                if keep:
-                    cps[start] = store[start // K]
-                    cps[start].copy_(s._buf[0])
-                rows += s.run(stop - start, cfl=self.cfl, steps_per_graph=K,
-                              dt_sequence=None if fresh else dts_dev[start:stop],
-                              history=history[start * 2 * nb:stop * 2 * nb] if keep else None)
+            rows = s.run(steps, cfl=self.cfl, steps_per_graph=K, dt_sequence=dts_dev, history=history,
+                         checkpoints=store)
+            if keep:
+                cps = {start: store[start // K] for start in range(0, steps, K)}
         dts = np.array([r[-1] for r in rows])
         if fresh:
             self.dts = dts

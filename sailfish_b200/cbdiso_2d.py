@@ -468,7 +468,7 @@ class Solver(SolverBase):
         return o
 
     def run(self, steps, cfl=None, fixed_dt=None, graph=True, steps_per_graph=16, dt_sequence=None,
-            history=None, trajectory=None):
+            history=None, trajectory=None, checkpoints=None):
         """
         Advance `steps` iterations entirely on the device: each step's dt is
         min(dx, dy) / max wavespeed * cfl (driver.py:508-510) from the previous
@@ -482,8 +482,13 @@ class Solver(SolverBase):
         padded states) receives the whole run instead of the two solver
         buffers: [0] the current state, then per step n the first stage's
         output [2n + 1] and the step's result [2n + 2]; the last is copied
-        back into the solver. Returns the time series: one row per step, the
-        `reductions()` row followed by dt.
+        back into the solver. `checkpoints` (RK2 only; a sequence of device
+        tensors shaped like the padded state, at least steps / steps_per_graph
+        of them) receives the state before every group of `steps_per_graph`
+        steps: checkpoints[g] holds the state after g * steps_per_graph steps,
+        copied on the launching stream with no host synchronisation. Returns
+        the time series: one row per step, the `reductions()` row followed by
+        dt.
         """
         import torch
 
@@ -545,6 +550,18 @@ class Solver(SolverBase):
                 self._launch_stages(weights, epilogue, stream,
                                     (trajectory[2 * n], trajectory[2 * n + 1], trajectory[2 * n + 2]))
 
+        if checkpoints is not None:
+            if self._options.rk_order != 2 or trajectory is not None:
+                raise ValueError("checkpoints are taken in RK2 runs without a trajectory")
+            if len(checkpoints) < -(-steps // steps_per_graph):
+                raise ValueError("fewer checkpoints than groups of steps_per_graph steps")
+        launched = 0
+
+        def group_start():
+            # the state before each group of steps_per_graph steps
+            if checkpoints is not None and launched % steps_per_graph == 0:
+                checkpoints[launched // steps_per_graph].copy_(self._buf[0])
+
         remaining = steps
         if trajectory is not None:
             if self._options.rk_order != 2:
@@ -586,10 +603,14 @@ class Solver(SolverBase):
                 torch.cuda.current_stream().wait_stream(side)
                 self._graphs[key] = cuda_graph
             while remaining >= steps_per_graph:
+                group_start()
                 cuda_graph.replay()
                 remaining -= steps_per_graph
+                launched += steps_per_graph
         for _ in range(remaining):
+            group_start()
             one_step()
+            launched += 1
         self._check(lib.cbdiso_b200_step_prologue(self._ptr(stepper), self._ptr(self._result),
                                                   self._ptr(self._records), self._ptr(series), nvals, 1,
                                                   self._stream()), "step_prologue")

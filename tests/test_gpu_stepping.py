@@ -60,3 +60,27 @@ def test_device_run_rejects_arbitrary_point_mass_callbacks():
     s = make_solver("cbdiso_2d", physics, {}, setup=setup, mesh=setup.mesh(32))
     with pytest.raises(ValueError, match="Kepler binary"):
         s.run(3)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_checkpoints_taken_inside_one_run(graph):
+    """run(checkpoints=...) copies the state before every group of
+    steps_per_graph steps on the device; the checkpoints, the time series and
+    the final state equal those of the same steps run group by group with a
+    host copy of the state before each group (the adjoint's former
+    checkpointed forward)."""
+    d = load("cbd_t15_n64")
+    one, groups = product_solver(d, "exact"), product_solver(d, "exact")
+    steps, k = 23, 5
+    slots = [torch.empty_like(one._buf[0]) for _ in range(-(-steps // k))]
+    rows = one.run(steps, cfl=0.3, graph=graph, steps_per_graph=k, checkpoints=slots)
+    want_rows, want_states = [], []
+    for start in range(0, steps, k):
+        want_states.append(groups._buf[0].clone())
+        want_rows += groups.run(min(k, steps - start), cfl=0.3, graph=graph, steps_per_graph=k)
+    for got, want in zip(slots, want_states):
+        assert torch.equal(got, want)
+    assert np.array_equal(np.array(rows), np.array(want_rows))
+    assert np.array_equal(one.solution, groups.solution)
+    with pytest.raises(ValueError):
+        one.run(steps, cfl=0.3, steps_per_graph=k, checkpoints=slots[:-1])
