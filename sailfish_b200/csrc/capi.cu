@@ -64,6 +64,11 @@ Consts cbd::consts_from_grid(const cbd_grid_t *g)
     k.dy = (g->yr - g->yl) / g->nj;
     k.inv_dx = 1.0 / k.dx;
     k.inv_dy = 1.0 / k.dy;
+    // a power of two has an exact reciprocal, and x * RN(1 / d) then rounds
+    // as x / d does (the same real number, rounded once)
+    int ex, ey;
+    k.spacing_pow2 = std::frexp(k.dx, &ex) == 0.5 && std::frexp(k.dy, &ey) == 0.5 && std::isfinite(k.inv_dx) &&
+                     std::isfinite(k.inv_dy) && k.inv_dx * k.dx == 1.0 && k.inv_dy * k.dy == 1.0;
     k.theta = g->plm_theta;
     k.eos = g->eos_type;
     k.cs2 = g->cs2;
@@ -100,12 +105,15 @@ double buffer_k(double driving_rate, double central_mass, double onset)
 LaunchShape stage_shape(int ni, int nj, int bj, int rows, int occupancy = 0)
 {
     LaunchShape s;
-    if (bj != 64 && bj != 128) {
+    if (bj != 64 && bj != 128 && bj != 256) {
         bj = nj > 96 ? 128 : 64;
         if (occupancy == 0)
             occupancy = bj == 128 ? 6 : 12;
     }
     s.minb = 1;
+    // 256-column strips: 3 CTAs per SM (80 registers, 68 KB of shared memory each)
+    if (bj == 256)
+        s.minb = 3;
     if (bj == 128 && (occupancy == 5 || occupancy == 6))
         s.minb = occupancy;
     if (bj == 64 && (occupancy == 10 || occupancy == 12))

@@ -57,7 +57,7 @@ struct Consts {
     int buffer_on;
     int want_ws;
     int num_diag;       // diagnostics fused into this launch (<= MAX_FUSED)
-    int _pad;
+    int spacing_pow2;   // dx and dy are powers of two: inv_dx, inv_dy are exact
     double xl, yl, dx, dy, inv_dx, inv_dy;
     double theta;
     double cs2, mach2, inv_mach2, neg_inv_mach2;
@@ -223,7 +223,7 @@ __device__ __forceinline__ void hlle(const double *pl, const double *pr, double 
 
 // rho times the trace-free strain (sxx, sxy, syy), cbdiso_2d.c:248-263; the
 // viscous face terms of cbdiso_2d.c:579-586 combine two of these.
-template <bool FAST>
+template <bool FAST, bool P2 = false>
 __device__ __forceinline__ void rho_strain(double rho, const double *gx, const double *gy, const Consts &k,
                                            double *rs)
 {
@@ -236,10 +236,12 @@ __device__ __forceinline__ void rho_strain(double rho, const double *gx, const d
     } else {
         // 4.0 / 3.0 * gx[1] / dx - 2.0 / 3.0 * gy[2] / dy, and so on, with
         // each quotient correctly rounded from the hoisted 1 / dx, 1 / dy
+        // (with P2 these are exact powers of two and the product alone is
+        // the correctly rounded quotient)
         const double ix = k.inv_dx, iy = k.inv_dy;
-        sxx = div_by<false>(4.0 / 3.0 * gx[1], k.dx, ix) - div_by<false>(2.0 / 3.0 * gy[2], k.dy, iy);
-        syy = div_by<false>(-2.0 / 3.0 * gx[1], k.dx, ix) + div_by<false>(4.0 / 3.0 * gy[2], k.dy, iy);
-        sxy = div_by<false>(gx[2], k.dx, ix) + div_by<false>(gy[1], k.dy, iy);
+        sxx = div_by<P2>(4.0 / 3.0 * gx[1], k.dx, ix) - div_by<P2>(2.0 / 3.0 * gy[2], k.dy, iy);
+        syy = div_by<P2>(-2.0 / 3.0 * gx[1], k.dx, ix) + div_by<P2>(4.0 / 3.0 * gy[2], k.dy, iy);
+        sxy = div_by<P2>(gx[2], k.dx, ix) + div_by<P2>(gy[1], k.dy, iy);
     }
     rs[0] = rho * sxx;
     rs[1] = rho * sxy;
@@ -260,8 +262,10 @@ __device__ __forceinline__ double fourth_power(double q)
 // Terms that are exactly zero (no mass, or a zone outside 4 sink radii) are
 // skipped: adding them changes no value. The gravity factor
 // (r^2 + s^2)^-1.5 is taken from *g_in when given (a face-cache value), and
-// stored to *g_out when given.
-template <bool FAST>
+// stored to *g_out when given. GRAV and SINK select the two parts (both
+// for the stage; the diagnostics take one at a time, as the reference's
+// switches do, cbdiso_2d.py:105-137).
+template <bool FAST, bool GRAV = true, bool SINK = true>
 __device__ __forceinline__ void mass_source(const MassDev &m, double x, double y, double dt, const double *p,
                                             double *du, const double *g_in = nullptr, double *g_out = nullptr)
 {
@@ -269,7 +273,7 @@ __device__ __forceinline__ void mass_source(const MassDev &m, double x, double y
     const double dx = x - m.x;
     const double dy = y - m.y;
     const double r2 = dx * dx + dy * dy;
-    if (m.mass != 0.0) {
+    if (GRAV && m.mass != 0.0) {
         const double g = g_in ? *g_in : inv_pow15<FAST>(r2 + m.soft2);
         if (g_out)
             *g_out = g;
@@ -279,7 +283,7 @@ __device__ __forceinline__ void mass_source(const MassDev &m, double x, double y
         du[1] += fx * dt;
         du[2] += fy * dt;
     }
-    if (m.sink_rate == 0.0 || m.sink_model < 1 || m.sink_model > 3 || !(r2 < m.sink_hi2))
+    if (!SINK || m.sink_rate == 0.0 || m.sink_model < 1 || m.sink_model > 3 || !(r2 < m.sink_hi2))
         return;
     const double dr = sqrt(r2);
     if (!(dr < m.sink_r4))
@@ -378,15 +382,10 @@ __device__ __forceinline__ void end_rates(const MassDev *e, int need, double x, 
             // the gravity rates only enter sums whose own rounding (their
             // summation order) is far above an ulp per zone: rsqrt-based
             // arithmetic, not the correctly rounded power
-            MassDev m = e[q];
-            m.sink_rate = 0.0;
-            mass_source<true>(m, x, y, 1.0, p, rg[q]);
+            mass_source<true, true, false>(e[q], x, y, 1.0, p, rg[q]);
         }
-        if (need & (4 << q)) {
-            MassDev m = e[q];
-            m.mass = 0.0;
-            mass_source<FAST>(m, x, y, 1.0, p, ra[q]);
-        }
+        if (need & (4 << q))
+            mass_source<FAST, false, true>(e[q], x, y, 1.0, p, ra[q]);
     }
 }
 
@@ -758,11 +757,28 @@ struct StageSmem {
     double sun[ONE_SYNC ? 1 : 2][NQ][ONE_SYNC ? 1 : BJ];  // u_n zones a row ahead (two-barrier march)
 };
 
+// A static allocation may take up to 48 KB; the march of a 256-column strip
+// (68 KB) takes its shared memory from the launch's dynamic allocation,
+// whose size the launch gives (march_dynamic_smem).
+constexpr size_t STATIC_SMEM_LIMIT = 48 * 1024;
+
 template <int BJ, bool ONE_SYNC>
 __device__ __forceinline__ StageSmem<BJ, ONE_SYNC> &stage_smem()
 {
-    __shared__ StageSmem<BJ, ONE_SYNC> m;
-    return m;
+    if constexpr (sizeof(StageSmem<BJ, ONE_SYNC>) > STATIC_SMEM_LIMIT) {
+        extern __shared__ __align__(16) unsigned char stage_dynamic_smem[];
+        return *reinterpret_cast<StageSmem<BJ, ONE_SYNC> *>(stage_dynamic_smem);
+    } else {
+        __shared__ StageSmem<BJ, ONE_SYNC> m;
+        return m;
+    }
+}
+
+// dynamic shared memory bytes a stage kernel of BJ columns is launched with
+template <int BJ>
+constexpr size_t march_dynamic_smem()
+{
+    return sizeof(StageSmem<BJ, true>) > STATIC_SMEM_LIMIT ? sizeof(StageSmem<BJ, true>) : 0;
 }
 
 // One tile of the march: columns c0 .. c0 + width - 1 (width <= BJ) and rows
@@ -775,7 +791,7 @@ __device__ __forceinline__ StageSmem<BJ, ONE_SYNC> &stage_smem()
 // (five-row ring, u_n in registers), otherwise with two (four-row ring, u_n
 // through shared memory), which needs fewer registers: the persistent
 // batched kernel keeps it. All threads of the block must call it.
-template <int BJ, bool FAST, int COP = CACHE_NONE, bool EPI = true, bool ONE_SYNC = true>
+template <int BJ, bool FAST, int COP = CACHE_NONE, bool EPI = true, bool ONE_SYNC = true, bool P2 = false>
 __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, const StageArgs &args, int c0,
                                            int width, int r0, double (&acc)[PARTIAL_STRIDE], bool store = false)
 {
@@ -935,7 +951,7 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
                     gy[q] = limited_slope(sp[s1][q][kk - 1], sp[s1][q][kk], sp[s1][q][kk + 1], k.theta);
                 }
                 if (viscous)
-                    rho_strain<FAST>(sp[s1][0][kk], gx, gy, k, rs);
+                    rho_strain<FAST, P2>(sp[s1][0][kk], gx, gy, k, rs);
 #pragma unroll
                 for (int q = 0; q < NQ; ++q) {
                     sgy[g1][q][kk - 1] = gy[q];
@@ -1086,7 +1102,9 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
                 const double gn = sg[gf][q][t + 1], gs = sg[gf][q][t];
-                du[q] -= (div_by<FAST>(f1[q] - f0[q], k.dx, k.inv_dx) + div_by<FAST>(gn - gs, k.dy, k.inv_dy)) * dt;
+                du[q] -= (div_by<FAST || P2>(f1[q] - f0[q], k.dx, k.inv_dx) +
+                          div_by<FAST || P2>(gn - gs, k.dy, k.inv_dy)) *
+                         dt;
             }
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
@@ -1137,8 +1155,10 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
 
 // One RK stage on one grid: CTA (x, y) marches strip x, segment y. ROLE
 // (ROLE_*) is what the launch does with args.fcache; EPI whether it has an
-// epilogue (k.want_ws or k.num_diag).
-template <int BJ, int MINB, int PREC, int ROLE = ROLE_NONE, bool EPI = true>
+// epilogue (k.want_ws or k.num_diag); P2 that k.spacing_pow2 is set (the
+// divisions by dx and dy are then the products with their exact
+// reciprocals).
+template <int BJ, int MINB, int PREC, int ROLE = ROLE_NONE, bool EPI = true, bool P2 = false>
 __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const StageDev st_param, StageArgs args)
 {
     constexpr bool FAST = PREC == CBD_PRECISION_FAST;
@@ -1157,15 +1177,15 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
     if (ROLE == ROLE_WRITER) {
         const bool store = cache_write_check<PREC>(k, st, args.fcache,
                                                    threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0);
-        march_tile<BJ, FAST, CACHE_WRITE, EPI>(k, st, args, c0, BJ, r0, acc, store);
+        march_tile<BJ, FAST, CACHE_WRITE, EPI, true, P2>(k, st, args, c0, BJ, r0, acc, store);
     } else if (ROLE == ROLE_READER) {
-        march_tile<BJ, FAST, CACHE_READ, EPI>(k, st, args, c0, BJ, r0, acc);
+        march_tile<BJ, FAST, CACHE_READ, EPI, true, P2>(k, st, args, c0, BJ, r0, acc);
         // the fill kernel before this launch made the values valid for these
         // masses; say so for the next fill (no one reads the key meanwhile)
         if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0)
             cache_write_key<PREC>(k, st, args.fcache);
     } else {
-        march_tile<BJ, FAST, CACHE_NONE, EPI>(k, st, args, c0, BJ, r0, acc);
+        march_tile<BJ, FAST, CACHE_NONE, EPI, true, P2>(k, st, args, c0, BJ, r0, acc);
     }
     if (EPI) {
         double red[PARTIAL_STRIDE];
@@ -1202,7 +1222,9 @@ __device__ __forceinline__ void epilogue_tile(const Consts &k, const StageDev &s
 // without it (EPI = false) on the same grid: the same CTA tiles, per-thread
 // order, block tree and CTA order, so the same bits as the fused epilogue.
 // Reading the new state back (24 B per zone) costs less than carrying the
-// epilogue's registers and code through the stencil's march.
+// epilogue's registers and code through the stencil's march. (As two
+// launches, the wavespeed maximum and the diagnostic sums each with its own
+// register budget, it measured slower.)
 template <int BJ, int PREC>
 __global__ void __launch_bounds__(BJ, 4 * 128 / BJ) stage_epilogue_kernel(const Consts k, const StageDev st_param, StageArgs args)
 {

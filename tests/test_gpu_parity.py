@@ -248,17 +248,22 @@ def _cbd_solver(n, precision="exact", seed=11, tile=None, theta=1.5, rk=2):
     return s, prim
 
 
-def test_tile_shape_does_not_change_results():
+@pytest.mark.parametrize("n", [200, 600])
+def test_tile_shape_does_not_change_results(n):
     """Every face is computed once from the same operands whatever the tiling,
-    so different CTA tiles give bit-identical states."""
+    so different CTA tiles (64-, 128- and 256-column strips, full and partial)
+    give bit-identical states and wavespeed maxima."""
     out = []
-    for tile in [None, (64, 4), (128, 7), (64, 33)]:
-        s, _ = _cbd_solver(200, tile=tile)
+    for tile in [None, (64, 4), (128, 7), (64, 33), (256, 16), (256, 5)]:
+        s, _ = _cbd_solver(n, tile=tile)
+        ws = []
         for _ in range(3):
-            s.advance(s.mesh.min_spacing() / s.maximum_wavespeed() * 0.3)
-        out.append(s.solution)
-    for o in out[1:]:
-        assert np.array_equal(o, out[0])
+            ws.append(s.maximum_wavespeed())
+            s.advance(s.mesh.min_spacing() / ws[-1] * 0.3)
+        out.append((s.solution, ws))
+    for o, ws in out[1:]:
+        assert np.array_equal(o, out[0][0])
+        assert ws == out[0][1]
 
 
 def test_deterministic_reductions():
