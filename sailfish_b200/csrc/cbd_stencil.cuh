@@ -155,20 +155,21 @@ __device__ __forceinline__ double limited_slope(double yl, double y0, double yr,
 template <bool FAST>
 __device__ __forceinline__ double potential(const MassDev *m, double x, double y)
 {
-    double phi = 0.0;
+    // both terms evaluated unconditionally (two independent chains), the
+    // massless ones then left out
+    double term[2];
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
-        if (m[p].mass > 0.0) {
-            double dx = x - m[p].x;
-            double dy = y - m[p].y;
-            double r2 = dx * dx + dy * dy;
-            double s2 = r2 + m[p].soft2;
-            if (FAST)
-                phi -= m[p].mass * rsqrt(s2);
-            else
-                phi -= div_rn<false>(m[p].mass, sqrt(s2));
-        }
+        double dx = x - m[p].x;
+        double dy = y - m[p].y;
+        double r2 = dx * dx + dy * dy;
+        double s2 = r2 + m[p].soft2;
+        term[p] = FAST ? m[p].mass * rsqrt(s2) : div_rn<false>(m[p].mass, sqrt(s2));
     }
+    double phi = 0.0;
+#pragma unroll
+    for (int p = 0; p < 2; ++p)
+        phi = m[p].mass > 0.0 ? phi - term[p] : phi;
     return phi;
 }
 
@@ -1089,15 +1090,22 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
             if (cop == CACHE_READ) {
                 mass_source<FAST>(st.m[0], xc, yc, dt, pc, du, &c_z.x);
                 mass_source<FAST>(st.m[1], xc, yc, dt, pc, du, &c_z.y);
-            } else if (cop == CACHE_WRITE) {
-                double grav1 = 0.0, grav2 = 0.0;
-                mass_source<FAST>(st.m[0], xc, yc, dt, pc, du, nullptr, &grav1);
-                mass_source<FAST>(st.m[1], xc, yc, dt, pc, du, nullptr, &grav2);
-                if (store)
-                    cache_store(cfz + 2 * ((size_t)r * nj + j), grav1, grav2);
             } else {
-                mass_source<FAST>(st.m[0], xc, yc, dt, pc, du);
-                mass_source<FAST>(st.m[1], xc, yc, dt, pc, du);
+                // both gravity factors first (two independent chains), the
+                // terms then as with cached values; a massless mass has no
+                // gravity term and caches 0
+                double g[2];
+#pragma unroll
+                for (int p = 0; p < 2; ++p) {
+                    const double dx = xc - st.m[p].x, dy = yc - st.m[p].y;
+                    const double s2 = dx * dx + dy * dy + st.m[p].soft2;
+                    const double gp = inv_pow15<FAST>(s2);
+                    g[p] = st.m[p].mass != 0.0 ? gp : 0.0;
+                }
+                mass_source<FAST>(st.m[0], xc, yc, dt, pc, du, &g[0]);
+                mass_source<FAST>(st.m[1], xc, yc, dt, pc, du, &g[1]);
+                if (cop == CACHE_WRITE && store)
+                    cache_store(cfz + 2 * ((size_t)r * nj + j), g[0], g[1]);
             }
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
@@ -1211,8 +1219,17 @@ __device__ __forceinline__ void epilogue_tile(const Consts &k, const StageDev &s
     const size_t row_stride = (size_t)(k.nj + 2 * NG) * NQ;
     const double yc = k.yl + ((double)j + 0.5) * k.dy;
     const double *z = p + (size_t)(r0 + NG) * row_stride + (size_t)(j + NG) * NQ;
-    for (int r = r0; r < r1; ++r, z += row_stride) {
-        const double pn[NQ] = {z[0], z[1], z[2]};
+    if (r0 >= r1)
+        return;
+    double nx[NQ] = {z[0], z[1], z[2]};
+    for (int r = r0; r < r1; ++r) {
+        const double pn[NQ] = {nx[0], nx[1], nx[2]};
+        z += row_stride;
+        if (r + 1 < r1) {
+            nx[0] = z[0];
+            nx[1] = z[1];
+            nx[2] = z[2];
+        }
         const double xc = k.xl + ((double)r + 0.5) * k.dx;
         accumulate_zone<FAST>(k, st.e, xc, yc, pn, acc);
     }
