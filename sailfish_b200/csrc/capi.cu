@@ -102,9 +102,9 @@ double buffer_k(double driving_rate, double central_mass, double onset)
 // Launch shape of the stage kernel. Defaults: 256-column strips (3 resident
 // CTAs per SM) on grids of at least 2048^2 zones, 128-column strips compiled
 // for 6 resident CTAs per SM below that (64-column strips and 12 CTAs for
-// narrow grids), and the largest row count <= 32 that still gives at least
-// two full waves. (Measured per step: 4096^2 2.188 -> 2.157 ms and 2048^2
-// 0.657 -> 0.637 ms with 256 columns; 1024^2 0.232 -> 0.234 ms.)
+// narrow grids), and rows per CTA chosen for whole waves (below). (Measured
+// per step at 32 and 16 rows: 4096^2 2.188 -> 2.157 ms and 2048^2 0.657 ->
+// 0.637 ms with 256 columns; 1024^2 0.232 -> 0.234 ms.)
 LaunchShape stage_shape(int ni, int nj, int bj, int rows, int occupancy = 0)
 {
     LaunchShape s;
@@ -123,12 +123,27 @@ LaunchShape stage_shape(int ni, int nj, int bj, int rows, int occupancy = 0)
         s.minb = occupancy;
     const int strips = (nj + bj - 1) / bj;
     if (rows <= 0) {
+        // The CTAs should fill whole waves of the resident slots: a last,
+        // partial wave leaves SMs idle at the end of the launch (4096^2 at
+        // 256 columns: 37 rows, 4.0 waves, 2.127 ms per step; 36 rows, 4.11
+        // waves, 2.239 ms; 32 rows, 4.61 waves, 2.150 ms). Each CTA also
+        // recomputes about two rows' worth of slopes and faces at its
+        // segment's top, and a single wave starts every CTA at once
+        // (2048^2: 19 rows in 1.95 waves 0.607 ms, 38 rows in 0.97 waves
+        // 0.628 ms; 1024^2 at 128 columns: 10 rows in 0.93 waves 0.212 ms,
+        // 5 rows in 1.85 waves 0.219 ms). Score of r rows in W waves:
+        // (W / ceil(W)) (r / (r + 2)), times 0.95 below 1.5 waves.
         const int slots = 148 * (s.minb > 1 ? s.minb : 4);
-        // small grids: shorter segments for more CTAs (a CTA's run time is
-        // about its rows + 4 dependent row steps)
-        rows = 32;
-        while (rows > 4 && (long)strips * ((ni + rows - 1) / rows) < 2L * slots)
-            rows /= 2;
+        rows = 4;
+        double best = -1.0;
+        for (int r = 48; r >= 4; --r) {
+            const double waves = (double)strips * ((ni + r - 1) / r) / slots;
+            const double score = waves / std::ceil(waves) * r / (r + 2.0) * (waves < 1.5 ? 0.95 : 1.0);
+            if (score > best * (1.0 + 1e-3)) {
+                best = score;
+                rows = r;
+            }
+        }
     }
     if (rows < 4)
         rows = 4;
