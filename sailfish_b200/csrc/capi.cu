@@ -193,6 +193,7 @@ int cbd::set_diagnostics(Consts &k, const cbd_epilogue_t *ep, int first, int cou
 {
     k.num_diag = count;
     k.need_rates = 0;
+    k.rates_only = 1;
     for (int d = 0; d < count; ++d) {
         const cbd_diag_t &src = ep->diag[first + d];
         if (src.quantity < CBD_Q_MDOT || src.quantity > CBD_Q_POWER || src.which_mass < 1 || src.which_mass > 3)
@@ -202,6 +203,8 @@ int cbd::set_diagnostics(Consts &k, const cbd_epilogue_t *ep, int first, int cou
                           src.quantity == CBD_Q_TORQUE || src.quantity == CBD_Q_POWER;
         if (rate)
             k.need_rates |= (src.which_mass & 3) << (src.accretion ? 2 : 0);
+        if (!rate || src.has_cut)
+            k.rates_only = 0;
     }
     return CBD_OK;
 }

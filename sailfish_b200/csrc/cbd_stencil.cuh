@@ -65,7 +65,7 @@ struct Consts {
     double vmax, rho_min;
     double buf_sigma, buf_onset, buf_lo2, buf_span, inv_buf_span;
     int need_rates;     // epilogue: bit p gravity rates of mass p, bit 2 + p accretion rates
-    int _pad2;
+    int rates_only;     // epilogue: every diagnostic is a source rate of the masses, without a radial cut
     cbd_diag_t diag[CBD_MAX_DIAG];
 };
 
@@ -391,21 +391,24 @@ __device__ __forceinline__ void end_rates(const MassDev *e, int need, double x, 
 }
 
 // Per-zone value of one diagnostic (cbdiso_2d.py:383-471): out = (re, im).
-template <bool FAST>
+// RATES: the caller knows that d is a source rate (mdot, fx, fy, torque,
+// power) without a radial cut, so only that code is compiled (w = 1 then,
+// the same values).
+template <bool FAST, bool RATES = false>
 __device__ __forceinline__ void diag_value(const cbd_diag_t &d, const MassDev *e, double x, double y,
                                            const double *p, const double (&rg)[2][3], const double (&ra)[2][3],
                                            double *out)
 {
     double w = 1.0, r = 0.0;
-    const bool polar = d.quantity == CBD_Q_SIGMA_M1 || d.quantity == CBD_Q_ECCENTRICITY_VECTOR;
-    if (d.has_cut || polar) {
+    const bool polar = !RATES && (d.quantity == CBD_Q_SIGMA_M1 || d.quantity == CBD_Q_ECCENTRICITY_VECTOR);
+    if (!RATES && (d.has_cut || polar)) {
         r = sqrt(x * x + y * y);
         if (d.has_cut)
             w = ((d.r0 < r) & (r < d.r1)) ? 1.0 : 0.0;
     }
     out[0] = 0.0;
     out[1] = 0.0;
-    switch (d.quantity) {
+    switch (RATES ? CBD_Q_MDOT : d.quantity) {
     case CBD_Q_MDOT:
     case CBD_Q_FX:
     case CBD_Q_FY:
@@ -463,8 +466,9 @@ __device__ __forceinline__ void diag_value(const cbd_diag_t &d, const MassDev *e
 }
 
 // The end-of-step quantities of one zone, accumulated into acc: slot 0 the
-// CFL wavespeed maximum, slots 1 + 2d, 2 + 2d the diagnostics.
-template <bool FAST>
+// CFL wavespeed maximum, slots 1 + 2d, 2 + 2d the diagnostics (RATES: all of
+// them source rates without a radial cut, k.rates_only).
+template <bool FAST, bool RATES = false>
 __device__ __forceinline__ void accumulate_zone(const Consts &k, const MassDev *e, double x, double y,
                                                 const double *p, double (&acc)[PARTIAL_STRIDE])
 {
@@ -477,7 +481,7 @@ __device__ __forceinline__ void accumulate_zone(const Consts &k, const MassDev *
         for (int d = 0; d < MAX_FUSED; ++d) {
             if (d < k.num_diag) {
                 double v[2];
-                diag_value<FAST>(k.diag[d], e, x, y, p, rg, ra, v);
+                diag_value<FAST, RATES>(k.diag[d], e, x, y, p, rg, ra, v);
                 acc[1 + 2 * d] += v[0];
                 acc[2 + 2 * d] += v[1];
             }
@@ -1203,10 +1207,13 @@ __global__ void __launch_bounds__(BJ, MINB) stage_kernel(const Consts k, const S
     }
 }
 
+// resident 128-thread CTAs per SM the rates-only epilogue is built for
+constexpr int EPI_RATES_MINB = 4;
+
 // The epilogue of one tile after its stage has written it: thread t adds up
 // the zones of column c0 + t, rows r0 .. r0 + k.rows_per_cta - 1, of the new
 // state `p` in row order, exactly as the fused march accumulates them.
-template <bool FAST>
+template <bool FAST, bool RATES = false>
 __device__ __forceinline__ void epilogue_tile(const Consts &k, const StageDev &st, const double *p, int c0,
                                               int width, int r0, double (&acc)[PARTIAL_STRIDE])
 {
@@ -1231,7 +1238,7 @@ __device__ __forceinline__ void epilogue_tile(const Consts &k, const StageDev &s
             nx[2] = z[2];
         }
         const double xc = k.xl + ((double)r + 0.5) * k.dx;
-        accumulate_zone<FAST>(k, st.e, xc, yc, pn, acc);
+        accumulate_zone<FAST, RATES>(k, st.e, xc, yc, pn, acc);
     }
 }
 
@@ -1241,9 +1248,11 @@ __device__ __forceinline__ void epilogue_tile(const Consts &k, const StageDev &s
 // Reading the new state back (24 B per zone) costs less than carrying the
 // epilogue's registers and code through the stencil's march. (As two
 // launches, the wavespeed maximum and the diagnostic sums each with its own
-// register budget, it measured slower.)
-template <int BJ, int PREC>
-__global__ void __launch_bounds__(BJ, 4 * 128 / BJ) stage_epilogue_kernel(const Consts k, const StageDev st_param, StageArgs args)
+// register budget, it measured slower.) RATES: the form for k.rates_only,
+// with fewer registers.
+template <int BJ, int PREC, bool RATES = false>
+__global__ void __launch_bounds__(BJ, (RATES ? EPI_RATES_MINB : 4) * 128 / BJ)
+    stage_epilogue_kernel(const Consts k, const StageDev st_param, StageArgs args)
 {
     constexpr bool FAST = PREC == CBD_PRECISION_FAST;
     __shared__ StageDev st;
@@ -1257,7 +1266,7 @@ __global__ void __launch_bounds__(BJ, 4 * 128 / BJ) stage_epilogue_kernel(const 
 #pragma unroll
     for (int v = 0; v < PARTIAL_STRIDE; ++v)
         acc[v] = 0.0;
-    epilogue_tile<FAST>(k, st, args.pwr, blockIdx.x * BJ, BJ, blockIdx.y * k.rows_per_cta, acc);
+    epilogue_tile<FAST, RATES>(k, st, args.pwr, blockIdx.x * BJ, BJ, blockIdx.y * k.rows_per_cta, acc);
     double red[PARTIAL_STRIDE];
     block_reduce<BJ>(acc, sred, red);
     grid_finish<BJ>(red, 1 + 2 * k.num_diag, args.scratch, k.want_ws ? args.result : nullptr, args.result + 1, sred);

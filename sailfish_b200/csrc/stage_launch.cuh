@@ -60,8 +60,12 @@ cudaError_t launch_one_p2(const LaunchShape &s, const Consts &k, const StageDev 
         stage_kernel<BJ, MINB, PREC, ROLE_NONE, false, P2><<<s.grid, BJ, smem, stream>>>(k, st, a);
         break;
     }
-    if (k.want_ws || k.num_diag > 0)
-        stage_epilogue_kernel<BJ, PREC><<<s.grid, BJ, 0, stream>>>(k, st, a);
+    if (k.want_ws || k.num_diag > 0) {
+        if (k.rates_only)
+            stage_epilogue_kernel<BJ, PREC, true><<<s.grid, BJ, 0, stream>>>(k, st, a);
+        else
+            stage_epilogue_kernel<BJ, PREC, false><<<s.grid, BJ, 0, stream>>>(k, st, a);
+    }
     return cudaGetLastError();
 }
 
