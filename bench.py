@@ -35,11 +35,13 @@ BYTES_PER_ZONE_UPDATE = 120.0  # RK2 x FP64 x 3 fields: 48 B stage 1 + 72 B stag
 # kernel, halved per stage); scaled by the zone count. It is above the
 # algorithmic 60 B because of the cache's 48 B per zone and step and the
 # epilogue's 24 B read-back.
-NCU_TRAFFIC_PER_ZONE_LAUNCH = (312.26e6 + 61.19e6 + 217.50e6 + 250.14e6 + 100.91e6 + 4.20e6) / 2 / 2048 ** 2
+NCU_TRAFFIC_PER_ZONE_LAUNCH = (316.53e6 + 62.18e6 + 220.12e6 + 249.12e6 + 100.89e6 + 3.63e6) / 2 / 2048 ** 2
 # FP64 thread-instructions (DADD + DMUL + DFMA) per zone and stage, from the
 # same three launches (ncu, the sum of
-# smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum over zones)
-FP64_INST_PER_ZONE_LAUNCH = (346.9 + 533.3 + 123.1) / 2
+# smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum over zones;
+# 2048^2 runs 19-row segments, 4096^2 37-row ones, which recompute fewer
+# rows at segment tops: at 4096^2 this slightly overstates the count)
+FP64_INST_PER_ZONE_LAUNCH = (318.2 + 509.8 + 114.8) / 2
 GAM_FP64_INST_PER_ZONE_LAUNCH = (1224.8 + 1249.8) / 2
 DIAGNOSTICS = [dict(quantity="time"), dict(quantity="mdot", which_mass=1, accretion=True),
                dict(quantity="mdot", which_mass=2, accretion=True),
