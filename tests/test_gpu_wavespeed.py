@@ -5,8 +5,9 @@ cbdiso_2d.py:174) over the new state, tile by tile in its own launch. It must
 be the same double as the maximum the standalone reduction kernel computes
 zone by zone on the same state: compared bit for bit on a noisy disk at
 three sizes, on columns that are mirror images of themselves (exact ties
-between zones), on a uniform isothermal state (every zone tied) and after a
-NaN in the input state (which the stage's velocity ceiling clamps).
+between zones), on a uniform isothermal state (every zone tied), after a
+NaN in the input state (which the stage's velocity ceiling clamps) and on
+explicit tiles of many and few rows.
 """
 
 import numpy as np
@@ -99,3 +100,18 @@ def test_nan_zone():
                     solution=prim)
     fused, per_zone = _epilogue_and_per_zone(s, 1e-4)
     assert _same(fused, per_zone) or (np.isnan(fused) and np.isnan(per_zone))
+
+
+@pytest.mark.parametrize("tile", [(128, 70), (256, 45), (64, 5)])
+def test_explicit_tiles(tile):
+    """Tiles of many rows (a thread's column of 70 zones), 256-column strips
+    and short 64-column tiles: the maximum is the same double either way."""
+    n = 300
+    setup = CircumbinaryDisk(domain_radius=8.0, nu=1e-3)
+    mesh = setup.mesh(n)
+    prim = initial_condition(setup, mesh, 0.0)
+    prim[..., 0] += oh.seeded_noise(n, n, 5)
+    s = make_solver("cbdiso_2d", setup.physics, dict(rk_order=2, plm_theta=1.5, tile=tile), setup=setup,
+                    mesh=mesh, solution=prim)
+    fused, per_zone = _epilogue_and_per_zone(s, 1e-4, steps=2)
+    assert np.isfinite(fused) and _same(fused, per_zone)
