@@ -324,14 +324,24 @@ int cbdiso_b200_step_prologue(void *stepper_dev, const double *result, void *rec
  * the index of its first tile in the batch; *units receives its tile count.
  * Records are copied to a device array ordered by unit_begin. */
 size_t cbdiso_b200_batch_disk_bytes(void);
+/* 1 when every diagnostic of `ep` is a source rate of the masses (mdot,
+ * fx, fy, torque, power) without a radial cut, else 0; -1 for a null or
+ * malformed epilogue or one of more than four diagnostics. The stage epilogue takes a kernel compiled
+ * for such diagnostics by itself; the batched stage takes it on request
+ * (`epilogue` 2). No counterpart in the reference. */
+int cbdiso_b200_epilogue_rates_only(const cbd_epilogue_t *ep);
 int cbdiso_b200_batch_disk_record(const cbd_grid_t *grid, const cbd_epilogue_t *diagnostics, int strip_width,
                                   int rows, long long offset, int unit_begin, int *units, void *record);
 
 /* One RK stage of every disk in one persistent launch: CTAs take tiles from
  * counters[0] until all total_units are done (both counters return to zero).
  * Stage records are read from records[disk * num_stages + stage]; with
- * `epilogue`, each tile's wavespeed / diagnostic partial goes to
- * partials[tile * 9 ...]. primitive_n (null for the a = 0 stage) gives u_n. */
+ * `epilogue` (1), each tile's wavespeed / diagnostic partial goes to
+ * partials[tile * 9 ...]. `epilogue` 2 does the same with the kernel
+ * compiled for diagnostics that are all source rates of the masses without
+ * a radial cut (cbdiso_b200_epilogue_rates_only true for every disk's
+ * diagnostics; fewer registers, the same values); a disk whose diagnostics
+ * are not gets NaN sums. primitive_n (null for the a = 0 stage) gives u_n. */
 int cbdiso_b200_batched_stage(const void *disks, int num_disks, int total_units, const double *primitive_rd,
                               const double *primitive_n, double *primitive_wr, const void *records, int num_stages,
                               int stage, int epilogue, double *partials, unsigned int *counters, int precision,

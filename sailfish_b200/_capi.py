@@ -117,6 +117,7 @@ def _declare(lib):
         "cbdiso_b200_advance_stage_cached": [POINTER(Grid), POINTER(Stage), P, P, P, P, POINTER(Epilogue), P, P, P,
                                              I, V],
         "cbdiso_b200_reduce": [POINTER(Grid), POINTER(Epilogue), P, P, P, V],
+        "cbdiso_b200_epilogue_rates_only": [POINTER(Epilogue)],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -249,7 +250,7 @@ def exported_symbols():
         "cbdiso_b200_stepper_bytes", "cbdiso_b200_stepper_init",
         "cbdiso_b200_step_prologue", "cbdiso_b200_batch_disk_bytes", "cbdiso_b200_batch_disk_record",
         "cbdiso_b200_batched_stage", "cbdiso_b200_batched_finalize", "cbdiso_b200_batched_prologue",
-        "cbdiso_b200_batched_stage_cached", "cbdiso_b200_batch_disk_set_face_cache",
+        "cbdiso_b200_batched_stage_cached", "cbdiso_b200_batch_disk_set_face_cache", "cbdiso_b200_epilogue_rates_only",
         "cbdiso_b200_adjoint_workspace_bytes", "cbdiso_b200_stage_record_branches", "cbdiso_b200_stage_tangent",
         "cbdiso_b200_stage_adjoint", "cbdiso_b200_objective_tangent", "cbdiso_b200_objective_adjoint",
         "cbdiso_b200_stepper_attach", "cbdiso_b200_stage_adjoint_chained", "cbdiso_b200_objective_adjoint_chained",

@@ -116,12 +116,17 @@ class BatchedSolver:
         cache_offset = 0
         cache_offsets = []
         self.offsets = [0] * n
+        # the last stage's epilogue form: 2 (the kernel compiled for source-rate
+        # diagnostics) when every disk's diagnostics allow it
+        self._epilogue_form = 2
         for slot, i in enumerate(self.order):
             s = self.solvers[i]
             ni, nj = s.mesh.shape
             width, rows = tiles.get((ni, nj), default_tile(ni, nj))
             self.tiles[(ni, nj)] = (width, rows)
             ep = s._epilogue(s.time, True, self._device_diags)
+            if lib.cbdiso_b200_epilogue_rates_only(ctypes.byref(ep)) != 1:
+                self._epilogue_form = 1
             units = ctypes.c_int(0)
             buf = (ctypes.c_char * rec_bytes)()
             _capi.check(lib.cbdiso_b200_batch_disk_record(ctypes.byref(s._grid), ctypes.byref(ep), width, rows,
@@ -200,9 +205,9 @@ class BatchedSolver:
             last = stage == len(plan) - 1
             common = (self._ptr(self._disks_dev), n, self.total_units, self._ptr(rd),
                       self._ptr(pn) if pn is not None else None, self._ptr(wr), self._ptr(self._records),
-                      self.rk_order, stage, int(last), self._ptr(self._partials), self._ptr(self._counters), prec)
-            # face-cache role: the stage at t0 + dt writes, the next step's first reads
-            # the stage at t0 + dt writes the cache, the next step's first stage reads
+                      self.rk_order, stage, self._epilogue_form if last else 0, self._ptr(self._partials),
+                      self._ptr(self._counters), prec)
+            # face-cache role: the stage at t0 + dt writes the cache, the next step's first stage reads
             role = 0 if self._fcache is None else (2 if stage == 0 else (1 if stage == 1 else 0))
             if role:
                 status = lib.cbdiso_b200_batched_stage_cached(*common, self._ptr(self._fcache), role, stream)

@@ -127,7 +127,7 @@ int batched_stage(const void *disks, int num_disks, int total_units, const doubl
     a.records = static_cast<const StageDev *>(records);
     a.num_stages = num_stages;
     a.stage = stage;
-    a.epilogue = epilogue ? 1 : 0;
+    a.epilogue = epilogue == 2 ? 2 : (epilogue ? 1 : 0);
     a.partials = partials;
     a.counters = counters;
     a.fcache = face_cache;

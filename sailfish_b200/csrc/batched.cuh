@@ -31,7 +31,9 @@ struct BatchArgs {
     const StageDev *records;  // records[disk * num_stages + stage]
     int num_stages;
     int stage;
-    int epilogue;        // 1 on the step's last stage
+    int epilogue;        // the step's last stage: 1, or 2 when every disk's diagnostics are source
+                         // rates without a radial cut (Consts::rates_only; the launch then takes the
+                         // kernel compiled for those)
     int _pad;
     double *partials;    // [total_units][PARTIAL_STRIDE]
     unsigned int *counters;  // [0] next tile, [1] CTAs finished; both return to zero at the end
@@ -42,7 +44,7 @@ struct BatchArgs {
 // stores into the caches of the disks that have one; a reader requires one
 // for every disk (the batch's fill kernel ran before it), skips the tiles of
 // a disk without one, and the disk's first tile records the key.
-template <int BJ, int MINB, int PREC, int ROLE = ROLE_NONE, bool EPI = true>
+template <int BJ, int MINB, int PREC, int ROLE = ROLE_NONE, bool EPI = true, bool RATES = false>
 __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs a)
 {
     constexpr bool FAST = PREC == CBD_PRECISION_FAST;
@@ -115,20 +117,27 @@ __global__ void __launch_bounds__(BJ, MINB) batched_stage_kernel(const BatchArgs
         } else if (ROLE == ROLE_WRITER) {
             // the same answer in every thread; the disk's first tile writes the key
             const bool store = cached && cache_write_check<PREC>(k, st, sa.fcache, t == 0 && u == D.unit_begin);
-            march_tile<BJ, FAST, CACHE_WRITE, EPI, false>(k, st, sa, c0, D.strip_width, r0, acc, store);
+            march_tile<BJ, FAST, CACHE_WRITE, EPI, false, false, RATES>(k, st, sa, c0, D.strip_width, r0, acc, store);
         } else if (ROLE == ROLE_READER) {
             if (cached) {
-                march_tile<BJ, FAST, CACHE_READ, EPI, false>(k, st, sa, c0, D.strip_width, r0, acc);
+                march_tile<BJ, FAST, CACHE_READ, EPI, false, false, RATES>(k, st, sa, c0, D.strip_width, r0, acc);
                 // the fill kernel ran before this launch; no tile reads the key
                 if (t == 0 && u == D.unit_begin)
                     cache_write_key<PREC>(k, st, sa.fcache);
             }
         } else {
-            march_tile<BJ, FAST, CACHE_NONE, EPI, false>(k, st, sa, c0, D.strip_width, r0, acc);
+            march_tile<BJ, FAST, CACHE_NONE, EPI, false, false, RATES>(k, st, sa, c0, D.strip_width, r0, acc);
         }
         if (EPI) {
             double red[PARTIAL_STRIDE];
             block_reduce<BJ>(acc, sred, red);
+            // a disk whose diagnostics the rates-only kernel cannot evaluate
+            // (a wrong epilogue form from the caller): NaN sums, not wrong ones
+            if (RATES && !k.rates_only) {
+#pragma unroll
+                for (int v = 1; v < PARTIAL_STRIDE; ++v)
+                    red[v] = __longlong_as_double(0x7ff8000000000000LL);
+            }
             if (t == 0) {
 #pragma unroll
                 for (int v = 0; v < PARTIAL_STRIDE; ++v)
@@ -199,20 +208,26 @@ cudaError_t launch_batched(const BatchArgs &a, int ctas, int role, cudaStream_t 
 {
     switch (role) {
     case ROLE_WRITER:
-        if (a.epilogue)
+        if (a.epilogue == 2)
+            batched_stage_kernel<128, 6, PREC, ROLE_WRITER, true, true><<<ctas, 128, 0, s>>>(a);
+        else if (a.epilogue)
             batched_stage_kernel<128, 6, PREC, ROLE_WRITER, true><<<ctas, 128, 0, s>>>(a);
         else
             batched_stage_kernel<128, 6, PREC, ROLE_WRITER, false><<<ctas, 128, 0, s>>>(a);
         break;
     case ROLE_READER:
         batched_fill_kernel<128, PREC><<<a.total_units < 148 * 8 ? a.total_units : 148 * 8, 128, 0, s>>>(a);
-        if (a.epilogue)
+        if (a.epilogue == 2)
+            batched_stage_kernel<128, 6, PREC, ROLE_READER, true, true><<<ctas, 128, 0, s>>>(a);
+        else if (a.epilogue)
             batched_stage_kernel<128, 6, PREC, ROLE_READER, true><<<ctas, 128, 0, s>>>(a);
         else
             batched_stage_kernel<128, 6, PREC, ROLE_READER, false><<<ctas, 128, 0, s>>>(a);
         break;
     default:
-        if (a.epilogue)
+        if (a.epilogue == 2)
+            batched_stage_kernel<128, 6, PREC, ROLE_NONE, true, true><<<ctas, 128, 0, s>>>(a);
+        else if (a.epilogue)
             batched_stage_kernel<128, 6, PREC, ROLE_NONE, true><<<ctas, 128, 0, s>>>(a);
         else
             batched_stage_kernel<128, 6, PREC, ROLE_NONE, false><<<ctas, 128, 0, s>>>(a);

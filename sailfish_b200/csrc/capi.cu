@@ -217,6 +217,15 @@ extern "C" {
 
 int cbdiso_b200_version(void) { return 1; }
 
+int cbdiso_b200_epilogue_rates_only(const cbd_epilogue_t *ep)
+{
+    if (!ep || ep->num_diag < 0 || ep->num_diag > MAX_FUSED)
+        return -1;
+    Consts k;
+    std::memset(&k, 0, sizeof(k));
+    return set_diagnostics(k, ep, 0, ep->num_diag) == CBD_OK ? k.rates_only : -1;
+}
+
 int cbdiso_b200_set_stream(void *stream)
 {
     g_stream = static_cast<cudaStream_t>(stream);

@@ -796,7 +796,8 @@ constexpr size_t march_dynamic_smem()
 // (five-row ring, u_n in registers), otherwise with two (four-row ring, u_n
 // through shared memory), which needs fewer registers: the persistent
 // batched kernel keeps it. All threads of the block must call it.
-template <int BJ, bool FAST, int COP = CACHE_NONE, bool EPI = true, bool ONE_SYNC = true, bool P2 = false>
+template <int BJ, bool FAST, int COP = CACHE_NONE, bool EPI = true, bool ONE_SYNC = true, bool P2 = false,
+          bool RATES = false>
 __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, const StageArgs &args, int c0,
                                            int width, int r0, double (&acc)[PARTIAL_STRIDE], bool store = false)
 {
@@ -1149,7 +1150,7 @@ __device__ __forceinline__ void march_tile(const Consts &k, const StageDev &st, 
             }
 
             if (EPI)
-                accumulate_zone<FAST>(k, st.e, xc, yc, pn, acc);
+                accumulate_zone<FAST, RATES>(k, st.e, xc, yc, pn, acc);
         }
 
 #pragma unroll

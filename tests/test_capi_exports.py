@@ -80,3 +80,26 @@ def test_face_cache_and_adjoint_settings_host_checks():
     gst = _capi.GamStage()
     assert lib.cbdgam_b200_advance_stage_cached(ctypes.byref(gg), ctypes.byref(gst), a, None, b, None,
                                                 ctypes.c_void_p(0x1008), 2, None) == 1
+
+
+def test_epilogue_rates_only_query():
+    """The host query behind the batched stage's epilogue form: source rates
+    of the masses without a radial cut qualify, anything else does not."""
+    lib = _capi.lib()
+    ep = _capi.Epilogue(want_wavespeed=1, num_diag=2)
+    ep.diag[0] = _capi.Diag(quantity=1, which_mass=1, accretion=1)  # mdot of mass 1
+    ep.diag[1] = _capi.Diag(quantity=4, which_mass=3, gravity=1)  # torque of both
+    assert lib.cbdiso_b200_epilogue_rates_only(ctypes.byref(ep)) == 1
+    ep.diag[1].has_cut = 1
+    ep.diag[1].r0, ep.diag[1].r1 = 0.5, 2.0
+    assert lib.cbdiso_b200_epilogue_rates_only(ctypes.byref(ep)) == 0
+    ep.diag[1] = _capi.Diag(quantity=8, which_mass=1)  # total mass: not a rate
+    assert lib.cbdiso_b200_epilogue_rates_only(ctypes.byref(ep)) == 0
+    ep.num_diag = 0
+    assert lib.cbdiso_b200_epilogue_rates_only(ctypes.byref(ep)) == 1
+    ep.num_diag = _capi.MAX_DIAG + 1
+    assert lib.cbdiso_b200_epilogue_rates_only(ctypes.byref(ep)) == -1
+    ep.num_diag = 1
+    ep.diag[0] = _capi.Diag(quantity=99, which_mass=1)
+    assert lib.cbdiso_b200_epilogue_rates_only(ctypes.byref(ep)) == -1
+    assert lib.cbdiso_b200_epilogue_rates_only(None) == -1
