@@ -321,8 +321,7 @@ class AdjointRun:
         trajectory = f["trajectory"]
         sweep = self._sweep(s, 0 if trajectory is not None else min(K, steps), w)
         sweep.chain.zero_()
-        sweep.lam.zero_()
-        sweep.lam_n.zero_()
+        sweep._lam3.zero_()
         if trajectory is not None:
             # every state of the forward run is at hand: no recompute
             if graph:
@@ -460,14 +459,19 @@ class _ReverseSweep:
         self.pset = [[torch.empty(shape, **f64) for _ in range(k + 1)] for _ in range(nsets)]
         self.sset = [[torch.empty(shape, **f64) for _ in range(k)] for _ in range(nsets)]
         self.p, self.stars = self.pset[0], self.sset[0]
-        self.lam = torch.zeros(shape, **f64)
-        self.lam_n = torch.zeros(shape, **f64)
-        self.lam_star = torch.empty(shape, **f64)
+        # lambda, lambda_star, lambda_n side by side: the two buffers cleared
+        # after each reversed step (lambda_star and the next lambda_n) are
+        # always adjacent, one fill for both
+        self._lam3 = torch.zeros((3,) + tuple(shape), **f64)
+        self.lam, self.lam_star, self.lam_n = self._lam3[0], self._lam3[1], self._lam3[2]
         self.ws = torch.empty(int(lib.cbdiso_b200_adjoint_workspace_bytes(g)) // 8 + 8, **f64)
         self.rows = int(lib.cbdiso_b200_adjoint_chain_blocks(g))
         self.chain = torch.zeros(self.rows * 4, **f64)
         self.scratch = torch.zeros(int(lib.cbdiso_b200_scratch_bytes(g)) // 8 + 8, **f64)
         self.result = torch.zeros(64, **f64)
+        # the recompute's face cache (recomputes never overlap one another);
+        # a zeroed header holds no valid key
+        self.fcache = torch.zeros(int(lib.cbdiso_b200_face_cache_bytes(g)) // 8, **f64) if k > 0 else None
         self.hset = [torch.empty(max(k, 1) * 2 * self.nb, dtype=torch.uint8, device=s.device) for _ in range(nsets)]
         self.jset = [torch.empty((max(k, 1), 60), **f64) for _ in range(nsets)]
         self.hist, self.jac = self.hset[0], self.jset[0]
@@ -476,7 +480,11 @@ class _ReverseSweep:
     def recompute(self, p, stars, hist, count):
         """The segment's states from p[0] with the recorded stage records,
         keeping every state (the in-place final stage is replayed out of
-        place: inputs star, p[n] -> p[n + 1]), on the current stream."""
+        place: inputs star, p[n] -> p[n + 1]), on the current stream. The
+        stages use the sweep's face cache as the forward run does (first
+        stage reader, second writer): the same bits as without it, with the
+        first stage's face sound speeds and gravity factors loaded rather
+        than evaluated (a segment's first step fills the cache)."""
         import torch
 
         lib, g, nb = self.lib, ctypes.byref(self.grid), self.nb
@@ -485,11 +493,14 @@ class _ReverseSweep:
         rec = lambda n, k: ctypes.c_void_p(hist.data_ptr() + (2 * n + k) * nb)
         s1, s2 = _capi.Stage(), _capi.Stage()
         s2.a = 0.5
+        fc = P(self.fcache)
         for n in range(count):
-            _capi.check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s1), rec(n, 0), P(p[n]), None, P(stars[n]),
-                                                      None, None, None, stream), "advance_stage")
-            _capi.check(lib.cbdiso_b200_advance_stage(g, ctypes.byref(s2), rec(n, 1), P(stars[n]), P(p[n]),
-                                                      P(p[n + 1]), None, None, None, stream), "advance_stage")
+            _capi.check(lib.cbdiso_b200_advance_stage_cached(g, ctypes.byref(s1), rec(n, 0), P(p[n]), None,
+                                                             P(stars[n]), None, None, None, fc, 2, stream),
+                        "advance_stage_cached")
+            _capi.check(lib.cbdiso_b200_advance_stage_cached(g, ctypes.byref(s2), rec(n, 1), P(stars[n]), P(p[n]),
+                                                             P(p[n + 1]), None, None, None, fc, 1, stream),
+                        "advance_stage_cached")
 
     def reverse(self, p, stars, hist, jac, count):
         """The reverse sweep over one segment of `count` steps whose states
@@ -512,15 +523,16 @@ class _ReverseSweep:
             # the chained weights are per unit time: dt_n / sum(dt) * dA)
             check(lib.cbdiso_b200_objective_adjoint_chained(g, rec(n, 1), P(out), self.w[0], self.w[1], P(lam),
                                                             jp(n, 2), chain, ws, stream), "objective_adjoint")
-            # stage 2: inputs star (read), pn (u_n)
-            lam_star.zero_()
+            # stage 2: inputs star (read), pn (u_n); lam_star starts at zero
             check(lib.cbdiso_b200_stage_adjoint_chained(g, rec(n, 1), P(star), P(pn), P(out), P(lam), P(lam_star),
                                                         P(lam_n), jp(n, 1), chain, ws, stream), "stage_adjoint")
             # stage 1: input pn
             check(lib.cbdiso_b200_stage_adjoint_chained(g, rec(n, 0), P(pn), None, P(star), P(lam_star), P(lam_n),
                                                         None, jp(n, 0), chain, ws, stream), "stage_adjoint")
             lam, lam_n = lam_n, lam
-            lam_n.zero_()
+            # lam_star and the next lam_n back to zero (adjacent in _lam3)
+            lo = 0 if lam_n.data_ptr() == self._lam3[0].data_ptr() else 1
+            self._lam3[lo:lo + 2].zero_()
         if lam is not self.lam:
             # an odd count leaves the adjoint in the other buffer
             self.lam.copy_(lam)
@@ -782,8 +794,7 @@ class BatchedAdjoint:
         if not gradient:
             return
         sweep.chain.zero_()
-        sweep.lam.zero_()
-        sweep.lam_n.zero_()
+        sweep._lam3.zero_()
         sweep.run(g_in["history"], g_in["jac"], r.steps, states=traj)
         # the final reduction adds into its output
         g_in["out4"].zero_()
