@@ -940,7 +940,8 @@ def run_reference(args, rank, world):
     # whole run stays within a few minutes
     per_step = 6.0 * (n / 4096.0) ** 2 * 8 / max(1, os.cpu_count())
     steps = max(1, min(args.steps, int(120.0 / max(per_step, 1e-3))))
-    warmup = min(args.warmup, 1)
+    # the requested warm-up steps, up to three (about 1.2 s each at 4096^2)
+    warmup = min(args.warmup, 3)
     value, kind, el = time_cpu(n, steps, warmup, args.seed)
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
     return {
