@@ -298,6 +298,7 @@ def run_slabs(args, rank, world):
     import torch
     import torch.distributed as tdist
 
+    from sailfish_b200 import pinned_empty
     from sailfish_b200.cbdiso_2d import initial_condition
     from sailfish_b200.distributed import DistributedSolver, subdivide
     from sailfish_b200.setups import CircumbinaryDisk
@@ -310,6 +311,9 @@ def run_slabs(args, rank, world):
     a, b = list(subdivide(n, world))[rank]
     prim = initial_condition(setup, mesh, 0.0, rows=(a, b))
     prim[..., 0] += 1e-3 * np.random.default_rng(args.seed + rank).uniform(-1.0, 1.0, size=(b - a, n))
+    pinned = pinned_empty(prim.shape)  # the slab in pinned host memory, as in the one-GPU line
+    pinned[...] = prim
+    prim = pinned
     opts = dict(rk_order=2, plm_theta=THETA, precision=args.precision)
     solver = DistributedSolver(setup=setup, mesh=mesh, solution=prim, physics=physics, options=opts)
     solver.run(max(args.warmup, 3), cfl=CFL)
@@ -380,11 +384,17 @@ def run_slabs(args, rank, world):
 def run_ours(args, rank, world):
     import torch
 
-    from sailfish_b200 import make_solver
+    from sailfish_b200 import make_solver, pinned_empty
 
     torch.cuda.set_device(rank % max(torch.cuda.device_count(), 1))
     n = args.size
     setup, mesh, prim = initial_state(n, args.seed + rank)
+    # the initial state in pinned host memory, as a caller that feeds the
+    # device keeps it (filled here, before any timing): the e2e upload is then
+    # one direct host-to-device copy
+    pinned = pinned_empty(prim.shape)
+    pinned[...] = prim
+    prim = pinned
     physics = setup.physics
     physics["diagnostics"] = DIAGNOSTICS
     zones = n * n
@@ -457,8 +467,11 @@ def run_ours(args, rank, world):
         del s2, final
         return (t0, t1, t2, t3), io
 
-    # three repetitions (the host's load moves the set-up and copies): the
-    # median by total time is reported, all three are listed
+    # one untimed repetition (the process's first download pins host memory
+    # for its result, about 0.2 s at 4096^2, which later downloads reuse),
+    # then three (the host's load moves the set-up and copies): the median by
+    # total time is reported, all three are listed
+    e2e_once()
     reps = [e2e_once() for _ in range(3)]
     reps.sort(key=lambda r: r[0][3] - r[0][0])
     (t0, t1, t2, t3), (e2e_h2d, e2e_d2h) = reps[1]
@@ -503,8 +516,9 @@ def run_ours(args, rank, world):
                    "parallelism": "replicas" if world > 1 else "single"},
         "e2e": dict({"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": int(e2e_h2d),
                      "d2h_bytes_per_step": int(e2e_d2h), "steps": e2e_steps,
-                     "includes": "solver set-up and initial-state upload, public-API driver loop, final-state "
-                                 "download"}, **e2e_phases),
+                     "includes": "solver set-up and initial-state upload from pinned host memory, public-API "
+                                 "driver loop, final-state download (into pinned memory the caller owns); one "
+                                 "untimed repetition first"}, **e2e_phases),
         "step_io": {"h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "note": "value loop: stepper record in, time series out, per step"},
         # per step: prologue, first stage (behind its face-cache fill pass when

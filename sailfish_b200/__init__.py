@@ -11,10 +11,14 @@ rebuilt for one NVIDIA B200, behind sailfish's own solver plugin API.
     dt = mesh.min_spacing() / solver.maximum_wavespeed() * 0.3
     solver.advance(dt)
 
+Host states go to the device fastest from pinned memory: `pinned_empty(shape)`
+gives such an array, and `solution` returns one.
+
 The compute path is libcbdiso_b200.so (sources in csrc/, C-ABI in
 include/cbdiso_b200.h), built in-tree by `python -m sailfish_b200._build`.
 """
 
+from ._hostio import pinned_empty  # noqa: F401
 from .solvers import SolverInitializationError, make_solver, register_solver_extension  # noqa: F401
 
-__all__ = ["make_solver", "register_solver_extension", "SolverInitializationError"]
+__all__ = ["make_solver", "register_solver_extension", "SolverInitializationError", "pinned_empty"]

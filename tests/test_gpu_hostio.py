@@ -1,11 +1,14 @@
 """
-Whole-state host <-> device copies through the pinned staging buffer
-(sailfish_b200/_hostio.py): bit-exact round trips for strided device views
-above and below the staging threshold, and concurrent callers. Also the
-FP64 issue-rate probe the benchmark's FP64 roofline divides by.
+Whole-state host <-> device copies (sailfish_b200/_hostio.py): bit-exact
+round trips for strided device views above and below the staging threshold,
+from pageable and from pinned host arrays, downloads into pinned arrays of
+their own and past the pinned hand-out limit, and concurrent callers. Also
+the FP64 issue-rate probe the benchmark's FP64 roofline divides by.
 """
 
+import gc
 import threading
+import warnings
 
 import numpy as np
 import pytest
@@ -34,6 +37,57 @@ def test_round_trip_through_strided_views(n):
     _hostio.upload(host * 2.0, view)
     np.testing.assert_array_equal(back, host)
     np.testing.assert_array_equal(_hostio.download(view), host * 2.0)
+
+
+def _strided_view(n):
+    buf = torch.full((n + 4, n + 7, 3), float("nan"), dtype=torch.float64, device="cuda")
+    return buf, buf[2:-2, 2:-2]
+
+
+def test_downloads_are_pinned_and_pinned_arrays_upload_directly():
+    n = 1100
+    host = np.random.default_rng(1).standard_normal((n, n + 3, 3))
+    buf, view = _strided_view(n)
+    assert not _hostio.is_pinned(host)
+    _hostio.upload(host, view)  # staged: pageable source
+    back = _hostio.download(view)
+    assert _hostio.is_pinned(back) and back.flags.c_contiguous and back.flags.writeable
+    np.testing.assert_array_equal(back, host)
+    # a pinned array goes straight to the device, read-only ones included
+    p = _hostio.pinned_empty(host.shape)
+    assert _hostio.is_pinned(p)
+    p[...] = host * 3.0
+    p.flags.writeable = False
+    with warnings.catch_warnings():
+        warnings.simplefilter("error")
+        _hostio.upload(p, view)
+    assert torch.isnan(buf[:2]).all() and torch.isnan(buf[:, -2:]).all()  # guards untouched
+    np.testing.assert_array_equal(_hostio.download(view), host * 3.0)
+    # the first download is the caller's own: the later copies did not touch it
+    np.testing.assert_array_equal(back, host)
+    # and uploads directly as well
+    _hostio.upload(back, view)
+    np.testing.assert_array_equal(_hostio.download(view), host)
+
+
+def test_pinned_handout_limit(monkeypatch):
+    n = 1100
+    host = np.random.default_rng(2).standard_normal((n, n + 3, 3))
+    _, view = _strided_view(n)
+    _hostio.upload(host, view)
+    gc.collect()
+    before = _hostio._handout_bytes
+    arrays = [_hostio.download(view) for _ in range(2)]
+    assert _hostio._handout_bytes == before + 2 * host.nbytes
+    del arrays
+    gc.collect()
+    assert _hostio._handout_bytes == before
+    # past the limit: a pageable array, the same values
+    monkeypatch.setattr(_hostio, "PINNED_HANDOUT_LIMIT", 0)
+    back = _hostio.download(view)
+    assert not _hostio.is_pinned(back)
+    np.testing.assert_array_equal(back, host)
+    assert _hostio._handout_bytes == before
 
 
 def test_shape_mismatch_raises():
