@@ -7,7 +7,9 @@ sink radius 0.05, sink rate 10, torque-free sinks), Mach 10 locally
 isothermal, nu = 1e-3, PLM theta 1.5, RK2, CFL 0.3, Keplerian buffer beyond
 r = 7, with the accretion-rate and torque reductions every step. One "step"
 is one driver iteration: dt from the CFL wavespeed, advance(dt), reductions().
-Synthetic data: the setup's initial disk plus seeded 1e-3 noise on Sigma.
+Synthetic data: the setup's initial disk plus seeded 1e-3 noise on Sigma,
+held in pinned host memory for the end-to-end (e2e) measurement, which
+uploads it, runs the public driver loop and downloads the final state.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size N]
 
