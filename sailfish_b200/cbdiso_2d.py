@@ -355,10 +355,13 @@ class Solver(SolverBase):
         return value
 
     def advance(self, dt):
-        """One step of the configured RK order. The first stage is launched
-        as soon as its record (point masses at the step's start, whose orbit
-        is usually known from the previous step's end) is staged; the later
-        stages' orbits and records are built on the host while it runs."""
+        """One step of the configured RK order. The first stage goes out as
+        soon as its point masses (at the step's start, usually known from the
+        previous step's end) are set, its record carried by the launch's own
+        parameters, so that the device idles as little as possible between
+        the caller's wavespeed read and this step; the later stages' orbits
+        and records are built on the host while it runs and reach the device
+        as one copy ahead of their launches."""
         import torch
 
         dt = float(dt)
@@ -377,16 +380,10 @@ class Solver(SolverBase):
             t = time0 * a + (t + dt) * (1.0 - a)
         time_end = t
 
-        slot = self._ring_next
-        self._ring_next = (slot + 1) % len(self._ring)
-        if self._ring_events[slot] is not None:
-            self._ring_events[slot].synchronize()
-        host = self._ring[slot]
-        rb = self._rec_bytes
         plan = self._stage_plan(len(weights))
         diags = self._device_diags if self._fused else []
 
-        def record(s, epilogue):
+        def stage(s):
             st = _capi.Stage()
             m1, m2 = self._point_masses(times[s])
             _mass_struct(m1, st.mass[0])
@@ -394,27 +391,34 @@ class Solver(SolverBase):
             st.a = weights[s]
             st.dt = dt
             st.buffer_central_mass = m1.mass + m2.mass
-            self._check(lib.cbdiso_b200_stage_record(ctypes.byref(g), ctypes.byref(st), ctypes.byref(epilogue),
-                                                     ctypes.c_void_p(host.data_ptr() + s * rb)), "stage_record")
+            return st
 
-        first = 0
-        if len(weights) > 1:
-            # the first stage has no epilogue: its record's end-of-step masses
-            # are never read, so any epilogue serves to build it
-            record(0, self._epilogue(times[0], False, []))
-            self._records[:rb].copy_(host[:rb], non_blocking=True)
-            self._launch_stage(0, plan, weights, None, stream)
-            first = 1
-        epilogue = self._epilogue(time_end, True, diags)
-        for s in range(first, len(weights)):
-            record(s, epilogue)
-        self._records[first * rb:].copy_(host[first * rb:], non_blocking=True)
-        ev = torch.cuda.Event()
-        ev.record()
-        self._ring_events[slot] = ev
-        self.h2d_bytes += host.numel()
-        for s in range(first, len(weights)):
-            self._launch_stage(s, plan, weights, epilogue if s == len(weights) - 1 else None, stream)
+        last = len(weights) - 1
+        # the first stage, its record as launch parameters; without an
+        # epilogue (RK2, RK3) its record's end-of-step masses are never read
+        epilogue = self._epilogue(time_end, True, diags) if last == 0 else None
+        self._launch_stage(0, plan, weights, epilogue, stream, stage=stage(0))
+        # the later stages' records: a slot of the pinned ring whose previous
+        # copy has completed, then one copy to the device
+        slot = self._ring_next
+        self._ring_next = (slot + 1) % len(self._ring)
+        if self._ring_events[slot] is not None:
+            self._ring_events[slot].synchronize()
+        host = self._ring[slot]
+        rb = self._rec_bytes
+        if last > 0:
+            epilogue = self._epilogue(time_end, True, diags)
+            for s in range(1, last + 1):
+                self._check(lib.cbdiso_b200_stage_record(ctypes.byref(g), ctypes.byref(stage(s)),
+                                                         ctypes.byref(epilogue),
+                                                         ctypes.c_void_p(host.data_ptr() + s * rb)), "stage_record")
+            self._records[rb:].copy_(host[rb:], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record()
+            self._ring_events[slot] = ev
+            for s in range(1, last + 1):
+                self._launch_stage(s, plan, weights, epilogue if s == last else None, stream)
+        self.h2d_bytes += host.numel()  # every stage's record: launch parameters or the copy
         self._finish_stages(len(weights), None)
         self._time = time_end
         self._cached = None
@@ -723,14 +727,18 @@ class Solver(SolverBase):
         C = self._buf[2]
         return [(A, None, B), (B, A, C), (C, A, A)]
 
-    def _launch_stage(self, s, plan, weights, epilogue, stream):
-        """Stage s of one step, reading its record in self._records; the last
-        stage carries the epilogue."""
+    def _launch_stage(self, s, plan, weights, epilogue, stream, stage=None):
+        """Stage s of one step, reading its record in self._records, or, when
+        `stage` (a host cbd_stage_t) is given, taking the record from it as a
+        launch parameter; the last stage carries the epilogue."""
         rd, pn, wr = plan[s]
-        dummy = _capi.Stage()
-        dummy.a = weights[s]
-        rec = ctypes.c_void_p(self._records.data_ptr() + s * self._rec_bytes)
-        common = (ctypes.byref(self._grid), ctypes.byref(dummy), rec, self._ptr(rd),
+        if stage is None:
+            stage = _capi.Stage()
+            stage.a = weights[s]
+            rec = ctypes.c_void_p(self._records.data_ptr() + s * self._rec_bytes)
+        else:
+            rec = None
+        common = (ctypes.byref(self._grid), ctypes.byref(stage), rec, self._ptr(rd),
                   self._ptr(pn) if pn is not None else None, self._ptr(wr),
                   ctypes.byref(epilogue) if epilogue is not None else None, self._ptr(self._scratch),
                   self._ptr(self._result))
