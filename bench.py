@@ -124,6 +124,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def bench_config(n, precision):
+    """The workload description both arms print for an n^2 run on one GPU."""
+    state_mb = n * n * 3 * 8 / 1e6
+    l2 = (f"state arrays ({state_mb:.0f} MB each at {n}^2) exceed the 126 MB L2; no flush" if state_mb > 126
+          else f"state arrays ({state_mb:.0f} MB each at {n}^2) fit in L2; no flush")
+    return {"workload": f"cbdiso_2d circumbinary disk {n}x{n} FP64 RK2 theta {THETA} CFL {CFL}, "
+                        "per-step mdot/torque reductions", "zones": n * n, "precision": precision, "l2": l2,
+            "parallelism": "single"}
+
+
 def initial_state(n, seed):
     from sailfish_b200.cbdiso_2d import initial_condition
     from sailfish_b200.setups import CircumbinaryDisk
@@ -510,12 +520,9 @@ def run_ours(args, rank, world):
         "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"cbdiso_2d circumbinary disk {n}x{n} FP64 RK2 theta {THETA} CFL {CFL}, "
-                               "per-step mdot/torque reductions", "zones": zones, "precision": args.precision,
-                   "timed": "Solver.run: device-side dt / Kepler, CUDA graph of 16-step groups",
-                   "l2": "state arrays (403 MB each at 4096^2) exceed L2; no flush",
-                   "face_cache": not args.no_face_cache,
-                   "parallelism": "replicas" if world > 1 else "single"},
+        "config": dict(bench_config(n, args.precision), **({"parallelism": "replicas"} if world > 1 else {})),
+        "timed": {"loop": "Solver.run: device-side dt / Kepler, CUDA graph of 16-step groups",
+                  "face_cache": not args.no_face_cache},
         "e2e": dict({"value": e2e_value, "unit": "zone-updates/s", "h2d_bytes_per_step": int(e2e_h2d),
                      "d2h_bytes_per_step": int(e2e_d2h), "steps": e2e_steps,
                      "includes": "solver set-up and initial-state upload from pinned host memory, public-API "
@@ -964,8 +971,7 @@ def run_reference(args, rank, world):
         "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world, "steps": steps,
         "warmup": warmup, "ms_per_step": el / steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": f"cbdiso_2d circumbinary disk {n}x{n} FP64 RK2 theta {THETA} CFL {CFL}, "
-                               "per-step mdot/torque reductions", "zones": n * n},
+        "config": bench_config(n, "exact"),
         "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": cores, "kind": kind,
                          "sample": f"{steps} full driver steps at {n}^2 (advance + wavespeed + reductions)"},
         "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
