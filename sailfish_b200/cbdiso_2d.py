@@ -398,15 +398,15 @@ class Solver(SolverBase):
         # epilogue (RK2, RK3) its record's end-of-step masses are never read
         epilogue = self._epilogue(time_end, True, diags) if last == 0 else None
         self._launch_stage(0, plan, weights, epilogue, stream, stage=stage(0))
-        # the later stages' records: a slot of the pinned ring whose previous
-        # copy has completed, then one copy to the device
-        slot = self._ring_next
-        self._ring_next = (slot + 1) % len(self._ring)
-        if self._ring_events[slot] is not None:
-            self._ring_events[slot].synchronize()
-        host = self._ring[slot]
         rb = self._rec_bytes
         if last > 0:
+            # the later stages' records: a slot of the pinned ring whose
+            # previous copy has completed, then one copy to the device
+            slot = self._ring_next
+            self._ring_next = (slot + 1) % len(self._ring)
+            if self._ring_events[slot] is not None:
+                self._ring_events[slot].synchronize()
+            host = self._ring[slot]
             epilogue = self._epilogue(time_end, True, diags)
             for s in range(1, last + 1):
                 self._check(lib.cbdiso_b200_stage_record(ctypes.byref(g), ctypes.byref(stage(s)),
@@ -418,7 +418,7 @@ class Solver(SolverBase):
             self._ring_events[slot] = ev
             for s in range(1, last + 1):
                 self._launch_stage(s, plan, weights, epilogue if s == last else None, stream)
-        self.h2d_bytes += host.numel()  # every stage's record: launch parameters or the copy
+        self.h2d_bytes += len(weights) * rb  # every stage's record: launch parameters or the copy
         self._finish_stages(len(weights), None)
         self._time = time_end
         self._cached = None
