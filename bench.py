@@ -567,16 +567,19 @@ def transfer_floor(nbytes, repeats=3):
 
 
 def host_copy_times(nbytes, repeats=3):
-    """The host side of the state copies on this box, with the solver's pool
-    threads and row blocks (sailfish_b200/_hostio.py): one state's bytes
-    from a numpy array into pinned memory (the upload's copy), and from
-    pinned memory into a new numpy array, its first touch included (the
-    download's); best of `repeats`. Both are bound by host memory bandwidth,
-    which the device copies share: the upload moves 3 state-sizes through
-    host memory (copy read and write, device-copy read), the download 4
-    (device-copy write, the new array's zero-fill on first touch, copy read
-    and write). `host_traffic_floor_ms` is those 7 state-sizes at the
-    bandwidth the upload's copy reaches."""
+    """The host side of the state copies for a caller whose arrays are
+    ordinary (pageable) numpy memory, with the solver's pool threads and row
+    blocks (sailfish_b200/_hostio.py): one state's bytes from a numpy array
+    into pinned memory (a staged upload's copy), and from pinned memory into
+    a new numpy array, its first touch included (a download past the pinned
+    hand-out limit); best of `repeats`. Both are bound by host memory
+    bandwidth, which the device copies share: a staged upload moves 3
+    state-sizes through host memory (copy read and write, device-copy read),
+    a pageable download 4 (device-copy write, the new array's zero-fill on
+    first touch, copy read and write). `pageable_traffic_floor_ms` is those
+    7 state-sizes at the bandwidth the upload's copy reaches. The e2e figure
+    itself starts from pinned memory and downloads into pinned memory: one
+    state-size each way, the device copies alone (`transfer_floor_ms`)."""
     import torch
 
     from sailfish_b200 import _hostio
@@ -605,7 +608,7 @@ def host_copy_times(nbytes, repeats=3):
     del pinned, staged, src
     host_gbs = 2 * nbytes / copy_in / 1e6
     return {"host_copy_in_ms": copy_in, "host_copy_out_ms": copy_out, "host_copy_gbs": host_gbs,
-            "host_traffic_floor_ms": 7 * nbytes / host_gbs / 1e6}
+            "pageable_traffic_floor_ms": 7 * nbytes / host_gbs / 1e6}
 
 
 def sizes_extra(args, sizes=(1024, 2048), steps=100):
