@@ -29,6 +29,7 @@ a lock, so threads may share this module.
 
 from __future__ import annotations
 
+import collections
 import os
 import threading
 import warnings
@@ -42,6 +43,7 @@ PINNED_HANDOUT_LIMIT = 16 << 30  # bytes of live pinned arrays returned by `down
 _lock = threading.Lock()
 _handout_lock = threading.Lock()
 _handout_bytes = 0
+_released = collections.deque()  # byte counts of freed hand-outs, not yet subtracted
 _staging = None
 _pool = None
 
@@ -117,9 +119,28 @@ def _blocks(n, k):
 
 
 def _release_handout(nbytes):
+    # Runs in whichever thread frees the array, possibly in the middle of this
+    # module's own critical section (a garbage collection there): so no lock,
+    # only a thread-safe append that the next count takes off.
+    _released.append(nbytes)
+
+
+def _drain_released():
+    """Subtract the freed hand-outs from the count; the caller holds
+    _handout_lock."""
     global _handout_bytes
-    with _handout_lock:
+    while True:
+        try:
+            nbytes = _released.popleft()
+        except IndexError:
+            return _handout_bytes
         _handout_bytes -= nbytes
+
+
+def handout_bytes():
+    """Bytes of pinned arrays returned by `download` and still alive."""
+    with _handout_lock:
+        return _drain_released()
 
 
 def _pinned_handout(shape, nbytes):
@@ -130,7 +151,7 @@ def _pinned_handout(shape, nbytes):
 
     global _handout_bytes
     with _handout_lock:
-        if _handout_bytes + nbytes > PINNED_HANDOUT_LIMIT:
+        if _drain_released() + nbytes > PINNED_HANDOUT_LIMIT:
             return None
         _handout_bytes += nbytes
     try:

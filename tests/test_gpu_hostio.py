@@ -76,18 +76,18 @@ def test_pinned_handout_limit(monkeypatch):
     _, view = _strided_view(n)
     _hostio.upload(host, view)
     gc.collect()
-    before = _hostio._handout_bytes
+    before = _hostio.handout_bytes()
     arrays = [_hostio.download(view) for _ in range(2)]
-    assert _hostio._handout_bytes == before + 2 * host.nbytes
+    assert _hostio.handout_bytes() == before + 2 * host.nbytes
     del arrays
     gc.collect()
-    assert _hostio._handout_bytes == before
+    assert _hostio.handout_bytes() == before
     # past the limit: a pageable array, the same values
     monkeypatch.setattr(_hostio, "PINNED_HANDOUT_LIMIT", 0)
     back = _hostio.download(view)
     assert not _hostio.is_pinned(back)
     np.testing.assert_array_equal(back, host)
-    assert _hostio._handout_bytes == before
+    assert _hostio.handout_bytes() == before
 
 
 def test_shape_mismatch_raises():

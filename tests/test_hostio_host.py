@@ -83,19 +83,19 @@ def test_handout_count_follows_the_arrays(monkeypatch):
 
     monkeypatch.setattr(torch, "empty", unpinned_empty)
     gc.collect()
-    before = _hostio._handout_bytes
+    before = _hostio.handout_bytes()
     out = _hostio._pinned_handout((100, 3), 2400)
     arr = _hostio._counted_numpy(out, 2400)
     del out
     gc.collect()
-    assert _hostio._handout_bytes == before + 2400
+    assert _hostio.handout_bytes() == before + 2400
     view = arr[10:20]
     del arr
     gc.collect()
-    assert _hostio._handout_bytes == before + 2400  # a view keeps the memory
+    assert _hostio.handout_bytes() == before + 2400  # a view keeps the memory
     del view
     gc.collect()
-    assert _hostio._handout_bytes == before
+    assert _hostio.handout_bytes() == before
     monkeypatch.setattr(_hostio, "PINNED_HANDOUT_LIMIT", before + 1000)
     assert _hostio._pinned_handout((100, 3), 2400) is None
-    assert _hostio._handout_bytes == before
+    assert _hostio.handout_bytes() == before
