@@ -1,8 +1,8 @@
 """
-The solver-extension route through the
-reference's own code: the one-line shims and the `.sailfish` file are taken
-from INTEGRATION.md as written, the reference's `load_user_config` reads the
-file (sailfish/driver.py:582-620) and registers the shims
+The solver-extension route of the repository's integration guide (its first
+section) through the reference's own code: the one-line shims and the
+`.sailfish` file are taken from the guide as written, the reference's
+`load_user_config` reads the file (sailfish/driver.py:582-620) and registers the shims
 (sailfish/solvers/__init__.py:13-15), and the reference's `make_solver`
 (sailfish/solvers/__init__.py:18-46) is called the way its driver calls it
 (sailfish/driver.py:439-449), with a reference setup's own physics dict and
@@ -29,14 +29,15 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+GUIDE = "INTEGRATION.md"  # the integration guide at the repository root
 
 pytestmark = pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "sailfish")),
                                 reason="the reference tree is not present")
 
 
 def _recipe_blocks():
-    """The fenced python and ini blocks of INTEGRATION.md's section 1."""
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    """The fenced python and ini blocks of the integration guide's first section."""
+    text = open(os.path.join(ROOT, GUIDE)).read()
     section = text.split("## 1.")[1].split("## 2.")[0]
     py = re.findall(r"```python\n(.*?)```", section, re.S)
     ini = re.findall(r"```ini\n(.*?)```", section, re.S)
